@@ -1,0 +1,483 @@
+"""Benchmark of the NNGP fit step (log-likelihood + gradient) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (the reference's FP32 GPU configuration, synthetic data of its shape; seed 0):
+n = 434,874 training points, d = 3, x ~ U[-1, 1]^3 scaled per axis by (1, 0.7, 0.4),
+y = sum_k sin(3 x_k) + N(0, 0.05^2), m = 32 neighbours, ConstantKernel(1) * RBF(0.2) +
+WhiteKernel(1e-3), alpha = 1e-10.  One step = one full fit step over all n points: the
+prefix neighbour search (point i among points [0, i)), the fused local systems with the
+adjoint gradient and the FP64 reduction (FP32 systems, FP64 re-solve below pivot 1e-6).
+Predict throughput at 100,000 test points is reported beside it.
+
+Our arm prints one JSON line (rank 0) with value = fit steps per second with the inputs
+resident in HBM, e2e = the same through the public estimator API uploading X, y from pinned
+host memory on every call, the roofline of the dominant kernel (the neighbour search),
+a cpu_baseline (the reference's NumpyNngpr on the host cores, on a bounded sample of the
+same fit step, extrapolated by row count) and the SM clocks sampled during the timed steps.
+
+--impl reference runs the reference's own CPU implementation (NumpyNngpr from
+baseline/_ref, its _log_likelihood_worker on a bounded sample of rows spread over the same
+fit step, all host cores) and prints the same metric.
+
+With N > 1 GPUs (torchrun) the fit step is split into N row ranges with equal neighbour-search
+pair counts; each rank searches and solves its rows and the (1 + n_theta) partial sums are
+all-reduced over NCCL (strong scaling: the total work is fixed).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+N_TRAIN = 434_874
+D = 3
+M = 32
+LS = 0.2
+NOISE = 1e-3
+ALPHA = 1e-10
+N_PRED = 100_000
+METRIC = 'fit-step loglik+grad/s'
+UNIT = 'fit-steps/s'
+WORKLOAD = 'nngp fit step, n=434874 d=3 m=32, isotropic RBF l=0.2, noise 1e-3, fp32'
+
+
+def make_data(n=N_TRAIN, nq=N_PRED, seed=0):
+    rng = np.random.default_rng(seed)
+    scale = np.array([1.0, 0.7, 0.4])
+    x = rng.uniform(-1, 1, (n, D)) * scale
+    y = np.sin(3 * x).sum(1) + rng.normal(0, 0.05, n)
+    xq = rng.uniform(-1, 1, (nq, D)) * scale
+    return x, y, xq
+
+
+def make_kernel():
+    from sklearn.gaussian_process import kernels as skk
+    return skk.ConstantKernel(1.0) * skk.RBF(LS) + skk.WhiteKernel(NOISE)
+
+
+def row_partition(n, world, pairs_exponent=0.5):
+    """Row boundaries with equal prefix-search pair counts: rank r gets rows
+    [n sqrt(r / R), n sqrt((r + 1) / R))."""
+    b = [int(round(n * (r / world) ** pairs_exponent)) for r in range(world + 1)]
+    b[0], b[-1] = 0, n
+    return b
+
+
+# ------------------------------------------------------------------------------------------
+# CPU baseline: the reference's NumpyNngpr on a bounded sample of rows
+# ------------------------------------------------------------------------------------------
+_CPU = {}
+
+
+def _ref_worker(tasks):
+    from nngpr.base_nngpr import DummyQueue
+    g = _CPU['gpr']
+    t0 = time.perf_counter()
+    lml, grad = g._log_likelihood_worker(0, DummyQueue(tasks), _CPU['n_theta'], _CPU['kernel'], _CPU['x'],
+                                         _CPU['y'], True)
+    return time.perf_counter() - t0, float(lml), np.asarray(grad)
+
+
+def _import_reference():
+    ref_dir = os.path.join(ROOT, 'baseline', '_ref')
+    if os.path.isdir(os.path.join(ref_dir, 'nngpr')):
+        sys.path.insert(0, ref_dir)
+        try:
+            from nngpr.numpy_nngpr import NumpyNngpr
+            from nngpr import batched_kernels
+            return NumpyNngpr, batched_kernels, 'reference'
+        except Exception:
+            sys.path.remove(ref_dir)
+    return None, None, 'port'
+
+
+class CpuBaseline:
+    """Times the reference's FP64 worker (``_log_likelihood_worker``, default ``only-nn``
+    search) on ``cores`` processes, each processing one batch of ``rows`` points placed at
+    stratified positions of the full fit step, and extrapolates to all n points."""
+
+    def __init__(self, x, y, rows_per_task=200, cores=None, seed=1):
+        NumpyNngpr, bk, kind = _import_reference()
+        self.kind = kind
+        self.cores = int(cores or os.cpu_count() or 1)
+        self.rows = rows_per_task
+        self.n = x.shape[0]
+        self.rng = np.random.default_rng(seed)
+        if kind == 'reference':
+            kernel = bk.ConstantKernel(1.0) * bk.RBF(LS) + bk.WhiteKernel(NOISE)
+            gpr = NumpyNngpr(kernel=kernel, num_nn=M, alpha=ALPHA, optimizer=None, batch_size=rows_per_task,
+                             num_workers=1, distribute_method='sequential')
+            # fitted state set directly, as the reference's own tests do (nngpr_base_tester.py:182):
+            # fit() would evaluate the whole n-point log-likelihood on the host first
+            gpr.X_train_, gpr.y_train_, gpr.kernel_ = np.asarray(x, np.float64), np.asarray(y, np.float64), kernel
+            self.kernel = gpr.kernel_
+            _CPU.update(gpr=gpr, kernel=gpr.kernel_, n_theta=len(gpr.kernel_.theta), x=gpr.X_train_,
+                        y=gpr.y_train_[:, None])
+        self.n_tasks = (self.n + rows_per_task - 1) // rows_per_task
+
+    def sample(self):
+        """One bounded sample: ``cores`` tasks at stratified positions, run in parallel on the
+        host cores.  Returns the summed per-task seconds (each task timed inside its worker
+        process) and the rows processed."""
+        edges = np.linspace(0, self.n_tasks, self.cores + 1)
+        tasks = [int(self.rng.integers(int(a), max(int(a) + 1, int(b)))) for a, b in zip(edges[:-1], edges[1:])]
+        tasks = sorted(set(min(t, self.n_tasks - 1) for t in tasks))
+        rows = sum(min(self.n, (t + 1) * self.rows) - t * self.rows for t in tasks)
+        env_keys = ('OPENBLAS_NUM_THREADS', 'MKL_NUM_THREADS', 'OMP_NUM_THREADS')
+        bak = {k: os.environ.get(k) for k in env_keys}
+        for k in env_keys:
+            os.environ[k] = '1'  # the reference's distribute_environ default (base_nngpr.py:173-178)
+        t0 = time.perf_counter()
+        task_s = None
+        if self.kind == 'reference':
+            import multiprocessing as mp
+            with mp.get_context('fork').Pool(len(tasks)) as pool:
+                res = pool.map(_ref_worker, [[t] for t in tasks])
+            task_s = float(sum(r[0] for r in res))
+        else:
+            from oracle import nngp_oracle as O
+            rows_idx = np.concatenate([np.arange(t * self.rows, min(self.n, (t + 1) * self.rows)) for t in tasks])
+            x, y = _CPU_PORT['x'], _CPU_PORT['y']
+            nbr = O.knn(x, x[rows_idx], M, 0, LS, query_index=rows_idx)
+            full = np.full((self.n, M), -1, np.int32)
+            full[rows_idx] = nbr
+            O.loglik_terms(x, y, full, _CPU_PORT['params'], ALPHA, True, rows_idx)
+        dt = time.perf_counter() - t0 if task_s is None else task_s
+        for k, v in bak.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+        return dt, rows
+
+
+_CPU_PORT = {}
+
+
+def cpu_steps_per_s(cb: CpuBaseline, steps: int):
+    """Fit steps per second of the CPU implementation: core-seconds per row measured on the
+    samples, times n rows, divided by the cores (perfect scaling over the cores assumed, which
+    favours the CPU: the reference's pool adds fork and pickling costs on top)."""
+    tot_t, tot_rows = 0.0, 0
+    for _ in range(steps):
+        dt, rows = cb.sample()
+        tot_t += dt
+        tot_rows += rows
+    full_step_s = tot_t * cb.n / tot_rows / cb.cores
+    return 1.0 / full_step_s, full_step_s, tot_rows, tot_t
+
+
+def prepare_cpu_baseline(x, y):
+    cb = CpuBaseline(x, y)
+    if cb.kind != 'reference':
+        from nngpr_b200.kernel_params import extract
+        from oracle import nngp_oracle as O
+        p = extract(make_kernel())
+        _CPU_PORT.update(x=x, y=y[:, None], params=O.KernelParams(p.rbf_level, p.const_value, p.noise_level,
+                                                                  p.length_scale, p.idx_rbf_level, p.idx_const,
+                                                                  p.idx_noise, p.idx_ls, p.n_theta))
+        cb.cores = 1
+    return cb
+
+
+# ------------------------------------------------------------------------------------------
+# Clocks during the timed region
+# ------------------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+              'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+              'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(['nvidia-smi', f'--id={self.gpu}', f'--query-gpu={self.FIELDS}',
+                                          '--format=csv,noheader,nounits', '-lms', '100'],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(',')]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == 'active':
+                    reasons.add(nm)
+        if not sm:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['unsampled'], 'samples': 0}
+        return {'sm_mhz': float(np.median(sm)), 'sm_max_mhz': float(max(mx)), 'reasons': sorted(reasons),
+                'samples': len(sm)}
+
+
+# ------------------------------------------------------------------------------------------
+# Our arm
+# ------------------------------------------------------------------------------------------
+def read_profile_traffic():
+    """DRAM bytes per launch of the neighbour-search kernel from the committed ncu summary
+    (line 'traffic_bytes_per_launch: <int>'), or None."""
+    path = os.path.join(ROOT, 'profiles', 'knn_fit_n434874_d3_m32.md')
+    try:
+        for ln in open(path):
+            if ln.startswith('traffic_bytes_per_launch:'):
+                return int(ln.split(':', 1)[1].strip())
+    except OSError:
+        pass
+    return None
+
+
+def fp32_peak_tflops(torch, L, stream_ptr):
+    """FP32 FMA rate of this GPU measured with the library's probe kernel (TFLOP/s)."""
+    import ctypes
+    blocks = 148 * 8
+    out = torch.empty(blocks * 256, dtype=torch.float32, device='cuda')
+    iters = 4096
+    best = 0.0
+    for _ in range(4):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        st = L.nngp_fma_probe(ctypes.c_void_p(out.data_ptr()), iters, blocks, stream_ptr)
+        e.record()
+        torch.cuda.synchronize()
+        assert st == 0
+        flops = blocks * 256 * iters * 128
+        best = max(best, flops / (s.elapsed_time(e) * 1e-3) / 1e12)
+    return best
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local_rank = int(os.environ.get('LOCAL_RANK', '0'))
+    x, y, xq = make_data()
+    n = x.shape[0]
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # before any CUDA call: the reference's worker pool forks
+        cb = prepare_cpu_baseline(x, y)
+        sps, full_s, rows, t = cpu_steps_per_s(cb, args.cpu_samples)
+        cpu = {'value': sps, 'unit': UNIT, 'cores': cb.cores, 'kind': cb.kind,
+               'sample': f'{rows} rows in batches of {cb.rows} at stratified positions of the n={n} fit step '
+                         f'({t:.1f} core-s; full step extrapolated by row count over {cb.cores} cores: '
+                         f'{full_s:.0f} s)'}
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device('cuda', local_rank)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group('nccl', timeout=timedelta(seconds=120), device_id=dev)
+
+    from nngpr_b200 import B200Nngpr, _lib, ops
+    from nngpr_b200.kernel_params import extract
+
+    L = _lib.lib()
+    _lib.check(L.nngp_check_device(), 'nngp_check_device')
+    kernel = make_kernel()
+    p = extract(kernel)
+    x32 = torch.from_numpy(x).to(dev, torch.float32)
+    y32 = torch.from_numpy(y[:, None]).to(dev, torch.float32)
+    bounds = row_partition(n, world)
+    r0, r1 = bounds[rank], bounds[rank + 1]
+    q_rows = x32[r0:r1]
+    flags = ops.new_flags(dev)
+    out = torch.empty(1 + p.n_theta, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)  # > 126 MB L2
+    stream = torch.cuda.current_stream()
+
+    def step(ev=None):
+        nbr = ops.knn(x32, q_rows, M, r0, LS, flags=flags)  # rows [r0, r1) among points [0, i)
+        if ev is not None:
+            ev.record()
+        ops.loglik(x32, y32, nbr, p, ALPHA, True, flags=flags, out=out, row_begin=r0)
+        if world > 1:
+            dist.all_reduce(out)
+        return out
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if int(flags.item()) & ~_lib.NNGP_FLAG_FP64_FALLBACK:
+        raise RuntimeError(f'kernel status flags {int(flags.item())}')
+
+    # ---- timed steps (device-resident inputs, L2 flushed before every step) -------------
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(torch.cuda.current_device() if world == 1 else local_rank) as clocks:
+        time.sleep(0.3)
+        for i in range(args.steps):
+            flush.zero_()
+            ev[i][0].record()
+            step(ev[i][1])
+            ev[i][2].record()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        time.sleep(0.2)
+    step_ms = [a.elapsed_time(c) for a, b, c in ev]
+    knn_ms = [a.elapsed_time(b) for a, b, c in ev]
+    tot_ms = float(sum(step_ms))
+    if world > 1:
+        t = torch.tensor([tot_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tot_ms = float(t.item())
+    lml_val = float(out[0].item())
+
+    # ---- predict throughput at 100,000 points ---------------------------------------------
+    xq32 = torch.from_numpy(xq).to(dev, torch.float32)
+    pred_ms = None
+    if world == 1:
+        for it in range(2):
+            s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            flush.zero_()
+            s0.record()
+            nq = ops.knn(x32, xq32, M, None, LS, flags=flags)
+            mean, var = ops.predict(x32, y32, xq32, nq, p, ALPHA, flags=flags)
+            s1.record()
+            torch.cuda.synchronize()
+            pred_ms = s0.elapsed_time(s1)
+
+    # ---- e2e through the public API, X and y uploaded from pinned host memory per call ----
+    e2e = None
+    if world == 1:
+        gpr = B200Nngpr(kernel=kernel, num_nn=M, alpha=ALPHA, optimizer=None, allow_downcast_f32='yes',
+                        keep_resident=False, device=dev).fit(x, y)
+        theta = gpr.kernel_.theta.copy()
+        for _ in range(max(1, args.warmup)):
+            gpr.log_marginal_likelihood(theta, eval_gradient=True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            lml_api, grad_api = gpr.log_marginal_likelihood(theta, eval_gradient=True)
+        e2e_s = (time.perf_counter() - t0) / args.steps
+        h2d = int(x.shape[0] * (D + 1) * 4)  # float32 X and y
+        d2h = int((1 + p.n_theta + 1) * 8)  # [lml, grad..., status] in one float64 read
+        e2e = {'value': 1.0 / e2e_s, 'unit': UNIT, 'h2d_bytes_per_step': h2d, 'd2h_bytes_per_step': d2h,
+               'ms_per_step': e2e_s * 1e3}
+
+    if rank == 0:
+        import ctypes
+        peak = fp32_peak_tflops(torch, L, ctypes.c_void_p(stream.cuda_stream))
+        pairs = (r1 * (r1 - 1) - r0 * (r0 - 1)) / 2.0  # prefix pairs of this rank's rows
+        knn_avg_ms = float(np.mean(knn_ms))
+        achieved = 2.0 * D * pairs / (knn_avg_ms * 1e-3) / 1e12
+        ms_per_step = tot_ms / args.steps
+        line = {
+            'metric': METRIC, 'value': 1e3 / ms_per_step, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
+            'warmup': args.warmup, 'ms_per_step': ms_per_step, 'higher_is_better': True,
+            'scaling': 'strong' if world > 1 else 'weak', 'vs_baseline': None, 'dtype': 'f32',
+            'data': 'synthetic (seeded stand-in for 3droad: shape 434874 x 3)',
+            'config': {'workload': WORKLOAD, 'n': n, 'd': D, 'm': M, 'parallelism': f'rows{world}',
+                       'l2': 'flushed (256 MB write) before every timed step', 'lml': lml_val},
+            'e2e': e2e,
+            'roofline': {'bound': 'fp32', 'achieved': achieved, 'peak': peak, 'unit': 'TFLOP/s',
+                         'frac': achieved / peak, 'traffic': read_profile_traffic(),
+                         'kernel': 'knn_topm_kernel<3,32> (prefix search)',
+                         'work': '2*d flops per (query, ref) pair, n(n-1)/2 pairs',
+                         'peak_source': 'FP32 FMA probe measured in this run (MEASURED_PEAKS.json has no FP32 figure)',
+                         'knn_ms': knn_avg_ms},
+            'cpu_baseline': cpu,
+            'predict': None if pred_ms is None else {'value': N_PRED / (pred_ms * 1e-3), 'unit': 'points/s',
+                                                     'ms': pred_ms, 'n_query': N_PRED},
+            'gpu_launches': args.steps * 4,
+            'clocks': clocks.summary(),
+        }
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# ------------------------------------------------------------------------------------------
+# Reference arm
+# ------------------------------------------------------------------------------------------
+def run_reference(args):
+    rank = int(os.environ.get('RANK', '0'))
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    if rank != 0:
+        return
+    x, y, _ = make_data()
+    cb = prepare_cpu_baseline(x, y)
+    for _ in range(args.warmup):
+        cb.sample()
+    sps, full_s, rows, t = cpu_steps_per_s(cb, args.steps)
+    line = {
+        'metric': METRIC, 'value': sps, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
+        'ms_per_step': full_s * 1e3, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+        'dtype': 'f64', 'data': 'synthetic (seeded stand-in for 3droad: shape 434874 x 3)',
+        'config': {'workload': WORKLOAD, 'n': N_TRAIN, 'd': D, 'm': M, 'parallelism': 'host processes'},
+        'impl': 'reference',
+        'cpu_baseline': {'value': sps, 'unit': UNIT, 'cores': cb.cores, 'kind': cb.kind,
+                         'sample': f'{rows} rows in batches of {cb.rows} at stratified positions of the fit step '
+                                   f'({t:.1f} core-s over {args.steps} steps; full step extrapolated by row '
+                                   f'count over {cb.cores} cores)'},
+        'e2e': {'value': sps, 'unit': UNIT, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=10)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', choices=['ours', 'reference'], default='ours')
+    ap.add_argument('--cpu-samples', type=int, default=2)
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == 'reference':
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == '__main__':
+    main()

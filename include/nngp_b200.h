@@ -1,0 +1,208 @@
+/*
+ * nngp_b200.h — C ABI of the B200 (sm_100a) NNGP fit/predict hot path.
+ *
+ * One shared library, libnngp_b200.so, replaces the numerical layers that the
+ * reference nngpr (stavoltafunzia/nngpr 0.1.1) runs per batch:
+ *
+ *   - the kernel-space nearest-neighbour search
+ *       NngprWorker.find_nearest_neighbors        nngpr/base_nngpr.py:1613-1686
+ *       RbfAccelerator.find_nearest_neighbors     nngpr/cuda_kernel_accelerators.py:196-381
+ *       calc_nn (CUDA)                            nngpr/cuda_kernel_accelerators.py:663-743
+ *   - the local covariance fill, batched Cholesky, solves and the log-likelihood
+ *     reduction with its gradient
+ *       Nngpr._log_likelihood_worker              nngpr/base_nngpr.py:453-614
+ *       RbfAccelerator.fill_nn_kernel             nngpr/cuda_kernel_accelerators.py:383-518, 748-863
+ *       TorchWorker.batched_chofactor/chosolve    nngpr/torch_nngpr.py:294-300
+ *   - the predictive mean / standard deviation conditioned on the training set
+ *       Nngpr._predict_worker                     nngpr/base_nngpr.py:1032-1135
+ *
+ * Conventions
+ *   - Every array argument is a DEVICE pointer owned by the caller, except the
+ *     length_scale arrays and the nngp_kernel struct, which are read on the host
+ *     during the call.  Row-major, contiguous.
+ *   - Every call is stream ordered on `stream` (a cudaStream_t passed as void*;
+ *     NULL = legacy default stream) and returns before the GPU work finishes.
+ *     Results and the device status word are valid after the stream reaches them.
+ *   - Calls return an nngp_status; nothing traps or aborts.  The text of the last
+ *     error of the calling thread is returned by nngp_last_error().
+ *   - Scratch memory is caller provided (`workspace`, `workspace_bytes`); the
+ *     *_workspace_size functions return the bytes a call needs.  The library
+ *     allocates no device memory.
+ *   - Conditions that only the GPU can see (a neighbour index out of range, a
+ *     non-positive pivot, a wait that ran out of time) are OR-ed into the optional
+ *     device int32 `status_flags` (NNGP_FLAG_*), never trapped.
+ *   - Calls on different streams may run concurrently if their workspaces differ.
+ */
+#ifndef NNGP_B200_H
+#define NNGP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NNGP_ABI_VERSION 1
+
+typedef enum nngp_status {
+    NNGP_OK = 0,
+    NNGP_ERR_INVALID_ARGUMENT = 1, /* bad size, null pointer, misaligned buffer */
+    NNGP_ERR_UNSUPPORTED = 2,      /* a size this build does not handle (message says which) */
+    NNGP_ERR_WORKSPACE = 3,        /* workspace missing or smaller than *_workspace_size */
+    NNGP_ERR_CUDA = 4,             /* a CUDA runtime call failed (message carries its text) */
+    NNGP_ERR_NO_DEVICE = 5         /* no usable sm_100 device is current */
+} nngp_status;
+
+/* Bits OR-ed into the device status word by the kernels. */
+#define NNGP_FLAG_BAD_INDEX 1      /* a neighbour index outside [0, n) was treated as missing (-1) */
+#define NNGP_FLAG_NOT_PD 2         /* a local system had a non-positive pivot: its terms are NaN */
+#define NNGP_FLAG_TIMEOUT 4        /* a bounded wait inside a kernel gave up; results are invalid */
+#define NNGP_FLAG_FP64_FALLBACK 8  /* some FP32 systems were re-solved in FP64 (informational) */
+
+/*
+ * Kernel  k(a, b) = rbf_level * exp(-sum_f (a_f - b_f)^2 / (2 l_f^2)) + const_value
+ *                   + noise_level * [a is b]
+ * i.e. the WhiteKernel + ConstantKernel + ConstantKernel*RBF family that the reference
+ * accelerates (nngpr/cuda_kernel_accelerators.py:169-194, parameters from
+ * get_kernel_params :520-581).  `alpha` is the GaussianProcessRegressor jitter added to
+ * every valid diagonal slot (base_nngpr.py:555-556; training slots only in predict,
+ * :1106-1107).  The idx_* fields give the position of each free hyperparameter in
+ * kernel.theta (get_kernel_theta_mapping, :583-649), -1 when fixed or absent; the
+ * n_ls length-scale positions are idx_ls, idx_ls+1, ...  Gradients are with respect
+ * to these log-hyperparameters.
+ */
+typedef struct nngp_kernel {
+    double rbf_level;
+    double const_value;
+    double noise_level;
+    double alpha;
+    const double *length_scale; /* HOST pointer: n_ls values, 1 (isotropic) or d (ARD) */
+    int32_t n_ls;               /* 0 = no RBF term (rbf_level must then be 0) */
+    int32_t idx_rbf_level;
+    int32_t idx_const;
+    int32_t idx_noise;
+    int32_t idx_ls;
+    int32_t n_theta;
+} nngp_kernel;
+
+/* ---------------------------------------------------------------------------------------
+ * Library information
+ * ------------------------------------------------------------------------------------- */
+int32_t nngp_abi_version(void);
+/* Text of the last failed call on this thread ("" if none). */
+const char *nngp_last_error(void);
+const char *nngp_status_string(nngp_status status);
+/* NNGP_OK if the current device is an sm_100 part this build runs on. */
+nngp_status nngp_check_device(void);
+
+/* ---------------------------------------------------------------------------------------
+ * Nearest-neighbour search
+ *
+ * Replaces NngprWorker.find_nearest_neighbors (base_nngpr.py:1613-1686) and the CUDA
+ * calc_nn search (cuda_kernel_accelerators.py:196-381, 663-743).
+ *
+ * out_idx[q, k] (n_query x num_nn, int32) = index in `ref` of the k-th nearest ref of
+ * query q, ascending by squared distance of the scaled points x / length_scale
+ * (length_scale == NULL: input-space search, plain Euclidean), equal distances ordered
+ * by lower index, -1 for missing slots.  With has_ref_cut != 0 query q only considers
+ * refs [0, q + ref_cut_index) (the reference's ref_cut_index; the fit step uses
+ * ref = query = X and ref_cut_index = 0, i.e. strictly earlier points in input order);
+ * otherwise every ref.  Distances are evaluated in the input precision with one rounding
+ * per operation, so the lists equal those of an exact search in that precision.
+ * ------------------------------------------------------------------------------------- */
+size_t nngp_knn_workspace_size_f32(int64_t n_ref, int64_t n_query, int32_t d, int32_t num_nn);
+nngp_status nngp_knn_f32(const float *ref, int64_t n_ref, const float *query, int64_t n_query,
+                         int32_t d, const double *length_scale, int32_t n_ls, int32_t num_nn,
+                         int32_t has_ref_cut, int64_t ref_cut_index, int32_t *out_idx,
+                         int32_t *status_flags, void *workspace, size_t workspace_bytes,
+                         void *stream);
+size_t nngp_knn_workspace_size_f64(int64_t n_ref, int64_t n_query, int32_t d, int32_t num_nn);
+nngp_status nngp_knn_f64(const double *ref, int64_t n_ref, const double *query, int64_t n_query,
+                         int32_t d, const double *length_scale, int32_t n_ls, int32_t num_nn,
+                         int32_t has_ref_cut, int64_t ref_cut_index, int32_t *out_idx,
+                         int32_t *status_flags, void *workspace, size_t workspace_bytes,
+                         void *stream);
+
+/* ---------------------------------------------------------------------------------------
+ * Log-likelihood (+ gradient) of the fit step
+ *
+ * Replaces the per-batch arithmetic of Nngpr._log_likelihood_worker (base_nngpr.py:538-614)
+ * together with fill_nn_kernel (cuda_kernel_accelerators.py:383-518) and the batched
+ * Cholesky / solves (torch_nngpr.py:294-300, numpy_nngpr.py:140-170).
+ *
+ * x (n x d), y (n x ydim), nbr (n x m, int32, -1 = missing; the point itself is implicit,
+ * it is NOT a column of nbr).  out[0] = sum over points and outputs of
+ *   -0.5 (y - mu)^2 / sigma^2 - 0.5 log(2 pi) - log(sigma)       (base_nngpr.py:581)
+ * and, if eval_gradient, out[1 + t] = d out[0] / d theta_t for t < kernel->n_theta
+ * (base_nngpr.py:586-614).  out is a device double array, written (not accumulated).
+ * The f32 entry point computes each local system in FP32 and re-solves it in FP64 when a
+ * pivot falls below pivot_tol * (rbf_level + const_value + noise_level + alpha); the
+ * per-point terms are summed in FP64.  The f64 entry point computes in FP64 throughout
+ * (pivot_tol is ignored).
+ * ------------------------------------------------------------------------------------- */
+size_t nngp_loglik_workspace_size(int64_t n, int32_t d, int32_t ydim, int32_t m, int32_t n_theta);
+nngp_status nngp_loglik_f32(const float *x, const float *y, int64_t n, int32_t d, int32_t ydim,
+                            const int32_t *nbr, int32_t m, const nngp_kernel *kernel,
+                            int32_t eval_gradient, double pivot_tol, double *out,
+                            int32_t *status_flags, void *workspace, size_t workspace_bytes,
+                            void *stream);
+nngp_status nngp_loglik_f64(const double *x, const double *y, int64_t n, int32_t d, int32_t ydim,
+                            const int32_t *nbr, int32_t m, const nngp_kernel *kernel,
+                            int32_t eval_gradient, double pivot_tol, double *out,
+                            int32_t *status_flags, void *workspace, size_t workspace_bytes,
+                            void *stream);
+
+/*
+ * Same as nngp_loglik_f32/_f64 restricted to the points [row_begin, row_begin + row_count)
+ * (nbr then has row_count rows; neighbour indices still refer to all n rows of x, y).
+ * Replaces one task of the reference's row-batched worker loop (base_nngpr.py:440-449,
+ * :503-538); summing the outputs of a partition of [0, n) gives the full result.
+ */
+nngp_status nngp_loglik_rows_f32(const float *x, const float *y, int64_t n, int32_t d, int32_t ydim,
+                                 int64_t row_begin, int64_t row_count, const int32_t *nbr, int32_t m,
+                                 const nngp_kernel *kernel, int32_t eval_gradient, double pivot_tol,
+                                 double *out, int32_t *status_flags, void *workspace,
+                                 size_t workspace_bytes, void *stream);
+nngp_status nngp_loglik_rows_f64(const double *x, const double *y, int64_t n, int32_t d, int32_t ydim,
+                                 int64_t row_begin, int64_t row_count, const int32_t *nbr, int32_t m,
+                                 const nngp_kernel *kernel, int32_t eval_gradient, double pivot_tol,
+                                 double *out, int32_t *status_flags, void *workspace,
+                                 size_t workspace_bytes, void *stream);
+
+/* ---------------------------------------------------------------------------------------
+ * Predictive mean / variance conditioned on the training set only
+ *
+ * Replaces Nngpr._predict_worker (base_nngpr.py:1032-1135) for
+ * conditioning_method='only-train'.  Query q's local system is itself plus nbr[q, :]
+ * (training indices, -1 = missing); alpha is added to the training slots only.
+ * mean (nq x ydim) = K_xn K_nn^-1 y_nn, var (nq) = K_00 - K_xn K_nn^-1 K_xn^T (the
+ * reference returns sqrt(var)).  Outputs in the input precision; FP32 systems whose
+ * pivots fall below pivot_tol * (kernel diagonal) are re-solved in FP64.
+ * ------------------------------------------------------------------------------------- */
+nngp_status nngp_predict_f32(const float *x_train, const float *y_train, int64_t n_train,
+                             const float *x_query, int64_t n_query, int32_t d, int32_t ydim,
+                             const int32_t *nbr, int32_t m, const nngp_kernel *kernel,
+                             double pivot_tol, float *mean, float *var, int32_t *status_flags,
+                             void *stream);
+nngp_status nngp_predict_f64(const double *x_train, const double *y_train, int64_t n_train,
+                             const double *x_query, int64_t n_query, int32_t d, int32_t ydim,
+                             const int32_t *nbr, int32_t m, const nngp_kernel *kernel,
+                             double pivot_tol, double *mean, double *var, int32_t *status_flags,
+                             void *stream);
+
+/* ---------------------------------------------------------------------------------------
+ * Measurement utility (no counterpart in the reference)
+ *
+ * Launches `blocks` x 256 threads, each running 8 independent FP32 FMA chains of 8 * iters
+ * steps (128 * iters flops per thread), and writes one float per thread to `out`
+ * (blocks * 256 floats).  Timing the launch gives the FP32 FMA rate that bounds the SIMT
+ * kernels above.
+ * ------------------------------------------------------------------------------------- */
+nngp_status nngp_fma_probe(float *out, int64_t iters, int32_t blocks, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NNGP_B200_H */

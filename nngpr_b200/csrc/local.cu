@@ -1,0 +1,810 @@
+// Fused local systems of the NNGP fit step and predict on B200 (sm_100a).
+//
+// For every point p with neighbours nbr[p, 0..m-1] (reference: Nngpr._log_likelihood_worker,
+// base_nngpr.py:538-614, and Nngpr._predict_worker, :1032-1135) one kernel does, without
+// writing any m x m matrix to HBM:
+//   fill     K of the augmented system [neighbours..., p] for
+//            rbf_level * exp(-|dx / l|^2 / 2) + const (+ noise + alpha on the diagonal), a -1
+//            neighbour giving an identity row/column (fill_nn_kernel semantics,
+//            cuda_kernel_accelerators.py:748-863);
+//   factor   the Cholesky factor of the augmented matrix with p LAST: its last row is
+//            l = L_nn^-1 k and its last pivot is sigma^2 = K_pp - k^T K_nn^-1 k;
+//   solve    z_c = L_nn^-1 y_nn,c, mu_c = l . z_c, r_c = y_c - mu_c;
+//   reduce   log-likelihood -r^2 / (2 sigma^2) - log sigma - log(2 pi) / 2 summed in FP64
+//            (base_nngpr.py:578-584), or mean/variance for predict (:1117-1127);
+//   adjoint  (gradient) b = K_nn^-1 k and v = sum_c (r_c / sigma^2) K_nn^-1 y_nn,c by two
+//            backward solves, then d loglik / d theta_t = sum_ij G_ij dK_ij/dtheta_t with
+//            G_pp = w, G_pj = v_j / 2 - w b_j, G_jk = w b_j b_k - (b_j v_k + v_j b_k) / 2,
+//            w = sum_c (r_c^2 / sigma^2 - 1) / (2 sigma^2): algebraically the reference's
+//            gradient (base_nngpr.py:586-614), evaluated by recomputing the fill instead of
+//            storing dK (n m^2 n_theta values in the reference).
+//
+// Two kernels:
+//   * warp kernel (m <= 32): one warp per point, lane i owns row i of the factor in registers;
+//     FP32 with an FP64 re-solve of the system when a pivot is below the threshold (or FP64
+//     throughout for double inputs);
+//   * block kernel (32 < m <= ~150): one CTA per point, the augmented matrix in shared memory,
+//     FP64.
+// Per-point terms are summed in FP64: per warp, per CTA, then in fixed order by a finalize
+// kernel (deterministic for a given launch shape).
+#include <algorithm>
+#include <cmath>
+#include <string>
+#include <type_traits>
+
+#include "common.cuh"
+
+namespace nngp {
+
+constexpr int kMaxDimLocal = 256;
+constexpr int kMaxTheta = kMaxDimLocal + 3;
+constexpr int kWarpM = 32;
+constexpr int kLocWarps = 4;
+constexpr double kHalfLog2Pi = 0.91893853320467274178;
+
+struct LocalArgs {
+    double rbf, cst, noise, alpha;
+    double pivot_abs;  // FP32 systems with a pivot below this are re-solved in FP64
+    int64_t n_rows;    // rows of x_ref / y_ref (neighbour index bound)
+    int64_t n_points;
+    int d, ydim, m;
+    int ard;  // 1: per-feature length scales
+    int idx_rbf, idx_const, idx_noise, idx_ls, n_theta;
+    double inv_ls[kMaxDimLocal];
+};
+
+template <typename T> __device__ __forceinline__ T dsqrt(T v) { return sqrt(v); }
+template <typename T> __device__ __forceinline__ T dexp(T v) { return exp(v); }
+template <> __device__ __forceinline__ float dexp<float>(float v) { return expf(v); }
+
+// ---------------------------------------------------------------------------------------
+// Warp kernel
+// ---------------------------------------------------------------------------------------
+// Shared memory per warp (bytes): xs (kWarpM + 1) x ds doubles | L kWarpM x (kWarpM + 1) doubles |
+// inverse diagonal kWarpM doubles | gradient accumulator n_theta doubles.
+struct WarpSmem {
+    int ds;  // row stride of xs (d + 1)
+    size_t xs_bytes, l_bytes, idg_bytes, g_bytes, total;
+    __host__ __device__ static WarpSmem make(int d, int n_theta) {
+        WarpSmem s;
+        s.ds = d + 1;
+        s.xs_bytes = (size_t)(kWarpM + 1) * s.ds * 8;
+        s.l_bytes = (size_t)kWarpM * (kWarpM + 1) * 8;
+        s.idg_bytes = (size_t)kWarpM * 8;
+        s.g_bytes = (size_t)(n_theta > 0 ? n_theta : 1) * 8;
+        s.total = (s.xs_bytes + s.l_bytes + s.idg_bytes + s.g_bytes + 15) / 16 * 16;
+        return s;
+    }
+};
+
+// Solves point p's system in precision TC.  Returns false (and commits nothing) when TC is
+// float and a pivot fell below the FP64 threshold.
+template <typename TC, typename TIn, bool GRAD, bool PRED>
+__device__ __forceinline__ bool warp_system(const LocalArgs &a, int64_t p, int lane, const TIn *__restrict__ x_ref,
+                                            const TIn *__restrict__ y_ref, const TIn *__restrict__ x_pt,
+                                            const TIn *__restrict__ y_pt, const int32_t *__restrict__ nbr,
+                                            unsigned char *wsm, double &ll_acc, TIn *__restrict__ mean,
+                                            TIn *__restrict__ var, int32_t *__restrict__ flags) {
+    constexpr int M = kWarpM;
+    const unsigned FULL = 0xffffffffu;
+    const WarpSmem lay = WarpSmem::make(a.d, a.n_theta);
+    TC *xs = reinterpret_cast<TC *>(wsm);
+    TC *Ls = reinterpret_cast<TC *>(wsm + lay.xs_bytes);
+    TC *idg = reinterpret_cast<TC *>(wsm + lay.xs_bytes + lay.l_bytes);
+    double *gacc = reinterpret_cast<double *>(wsm + lay.xs_bytes + lay.l_bytes + lay.idg_bytes);
+    const int d = a.d, ds = lay.ds;
+
+    // ---- neighbour of this lane --------------------------------------------------------
+    int32_t j = -1;
+    if (lane < a.m) {
+        j = __ldg(nbr + p * a.m + lane);
+        if (j < -1 || (int64_t)j >= a.n_rows) {
+            flag_or(flags, NNGP_FLAG_BAD_INDEX);
+            j = -1;
+        }
+    }
+    const bool valid = j >= 0;
+    const unsigned vmask = __ballot_sync(FULL, valid);
+
+    // ---- gather scaled coordinates: rows 0..M-1 neighbours, row M the point ------------
+    __syncwarp();
+    for (int f = 0; f < d; ++f) {
+        const TC s = (TC)a.inv_ls[a.ard ? f : 0];
+        xs[lane * ds + f] = valid ? (TC)x_ref[(int64_t)j * d + f] * s : TC(0);
+    }
+    for (int f = lane; f < d; f += 32) xs[M * ds + f] = (TC)x_pt[p * d + f] * (TC)a.inv_ls[a.ard ? f : 0];
+    __syncwarp();
+
+    // ---- fill: squared scaled distances, then kernel values ------------------------------
+    TC r[M];
+    TC rp = TC(0);
+#pragma unroll
+    for (int k = 0; k < M; ++k) r[k] = TC(0);
+    for (int f = 0; f < d; ++f) {
+        const TC xi = xs[lane * ds + f];
+#pragma unroll
+        for (int k = 0; k < M; ++k) {
+            const TC t = xi - xs[k * ds + f];
+            r[k] = fma(t, t, r[k]);
+        }
+        const TC t = xi - xs[M * ds + f];
+        rp = fma(t, t, rp);
+    }
+    const TC rbf = (TC)a.rbf, cst = (TC)a.cst;
+    const TC diag_add = (TC)a.noise + (TC)a.alpha;
+#pragma unroll
+    for (int k = 0; k < M; ++k) {
+        const bool vk = (vmask >> k) & 1u;
+        const TC e = rbf * dexp<TC>(TC(-0.5) * r[k]);
+        TC kv = (valid && vk) ? e + cst : TC(0);
+        if (k == lane) kv = valid ? kv + diag_add : TC(1);
+        r[k] = kv;
+    }
+    TC kvec = valid ? rbf * dexp<TC>(TC(-0.5) * rp) + cst : TC(0);  // K[p][lane]
+    const TC kpp = rbf + cst + (TC)a.noise + (PRED ? TC(0) : (TC)a.alpha);
+
+    // ---- Cholesky of the neighbour block fused with l = L^-1 k ----------------------------
+    TC minpiv = TC(3.0e38);
+    TC ss = TC(0);
+    TC l_own = TC(0);
+    TC dg_own = TC(1);
+#pragma unroll
+    for (int k = 0; k < M; ++k) {
+        const TC piv = __shfl_sync(FULL, r[k], k);
+        minpiv = piv < minpiv ? piv : minpiv;
+        const TC sq = dsqrt<TC>(piv);
+        const TC inv = TC(1) / sq;
+        r[k] = (lane == k) ? sq : r[k] * inv;
+        if (lane == k) dg_own = sq;
+        const TC lk = __shfl_sync(FULL, kvec, k) * inv;
+        if (lane == k) l_own = lk;
+        if (lane > k) kvec = fma(-r[k], lk, kvec);
+        ss = fma(lk, lk, ss);
+#pragma unroll
+        for (int jj = k + 1; jj < M; ++jj) {
+            const TC ljk = __shfl_sync(FULL, r[k], jj);
+            r[jj] = fma(-r[k], ljk, r[jj]);
+        }
+    }
+    const TC s2 = kpp - ss;
+    if constexpr (std::is_same<TC, float>::value) {
+        if (!(minpiv >= (TC)a.pivot_abs) || !(s2 >= (TC)a.pivot_abs)) return false;  // NaN-safe
+    }
+    if (!(minpiv > TC(0)) || !(s2 > TC(0))) flag_or(flags, NNGP_FLAG_NOT_PD);
+
+    // L (strictly lower part) and inverse diagonal to shared memory for the backward solves
+#pragma unroll
+    for (int k = 0; k < M; ++k) Ls[lane * (M + 1) + k] = r[k];
+    idg[lane] = TC(1) / dg_own;
+    __syncwarp();
+
+    // ---- outputs ------------------------------------------------------------------------
+    TC zw = TC(0);
+    TC wsum = TC(0);
+    double ll = 0.0;
+    for (int c = 0; c < a.ydim; ++c) {
+        TC yv = valid ? (TC)y_ref[(int64_t)j * a.ydim + c] : TC(0);
+        TC z_own = TC(0);
+#pragma unroll
+        for (int k = 0; k < M; ++k) {
+            const TC zk = __shfl_sync(FULL, yv, k) * idg[k];
+            if (lane == k) z_own = zk;
+            if (lane > k) yv = fma(-r[k], zk, yv);
+        }
+        const TC mu = warp_sum(l_own * z_own);
+        if (PRED) {
+            if (lane == 0) mean[p * a.ydim + c] = (TIn)mu;
+        } else {
+            const TC res = (TC)y_pt[p * a.ydim + c] - mu;
+            const double rd = (double)res, sd = (double)s2;
+            ll += -0.5 * rd * rd / sd - 0.5 * log(sd) - kHalfLog2Pi;
+            if (GRAD) {
+                const TC rs = res / s2;
+                zw = fma(rs, z_own, zw);
+                wsum += (res * rs - TC(1)) / (TC(2) * s2);
+            }
+        }
+    }
+    if (PRED) {
+        if (lane == 0) var[p] = (TIn)s2;
+        return true;
+    }
+    if (!GRAD) {
+        if (lane == 0) ll_acc += ll;
+        return true;
+    }
+
+    // ---- adjoint: b = L^-T l, v = L^-T zw ------------------------------------------------
+    TC bv = l_own, vv = zw, b_own = TC(0), v_own = TC(0);
+#pragma unroll
+    for (int k = M - 1; k >= 0; --k) {
+        const TC ik = idg[k];
+        const TC bk = __shfl_sync(FULL, bv, k) * ik;
+        const TC vk = __shfl_sync(FULL, vv, k) * ik;
+        if (lane == k) { b_own = bk; v_own = vk; }
+        const TC lkj = Ls[k * (M + 1) + lane];
+        if (lane < k) {
+            bv = fma(-lkj, bk, bv);
+            vv = fma(-lkj, vk, vv);
+        }
+    }
+
+    // recompute squared distances (xs is intact)
+#pragma unroll
+    for (int k = 0; k < M; ++k) r[k] = TC(0);
+    rp = TC(0);
+    for (int f = 0; f < d; ++f) {
+        const TC xi = xs[lane * ds + f];
+#pragma unroll
+        for (int k = 0; k < M; ++k) {
+            const TC t = xi - xs[k * ds + f];
+            r[k] = fma(t, t, r[k]);
+        }
+        const TC t = xi - xs[M * ds + f];
+        rp = fma(t, t, rp);
+    }
+    TC g_amp = TC(0), g_cst = TC(0), g_noise = TC(0), g_iso = TC(0);
+#pragma unroll
+    for (int k = 0; k < M; ++k) {
+        const TC bk = __shfl_sync(FULL, b_own, k);
+        const TC vk = __shfl_sync(FULL, v_own, k);
+        const bool vk_ok = (vmask >> k) & 1u;
+        const TC G = wsum * b_own * bk - TC(0.5) * (b_own * vk + v_own * bk);
+        const TC wgt = (valid && vk_ok) ? (k < lane ? TC(2) : (k == lane ? TC(1) : TC(0))) : TC(0);
+        const TC e = rbf * dexp<TC>(TC(-0.5) * r[k]);
+        const TC gw = wgt * G;
+        const TC ge = gw * e;
+        g_amp += ge;
+        g_cst += gw;
+        g_iso = fma(ge, r[k], g_iso);
+        if (k == lane && valid) g_noise += G;
+        r[k] = ge;  // kept for the per-feature length-scale terms
+    }
+    // pair (p, lane), weight 2, and (p, p)
+    const TC Gp = valid ? TC(0.5) * v_own - wsum * b_own : TC(0);
+    const TC ep = rbf * dexp<TC>(TC(-0.5) * rp);
+    const TC gpe = TC(2) * Gp * ep;
+    g_amp += gpe;
+    g_cst += TC(2) * Gp;
+    g_iso = fma(gpe, rp, g_iso);
+    const double amp_t = (double)warp_sum(g_amp) + (double)wsum * a.rbf;
+    const double cst_t = (double)warp_sum(g_cst) + (double)wsum;
+    const double noi_t = (double)warp_sum(g_noise) + (double)wsum;
+    const double iso_t = (double)warp_sum(g_iso);
+    if (lane == 0) {
+        ll_acc += ll;
+        if (a.idx_rbf >= 0) gacc[a.idx_rbf] += amp_t;
+        if (a.idx_const >= 0) gacc[a.idx_const] += a.cst * cst_t;
+        if (a.idx_noise >= 0) gacc[a.idx_noise] += a.noise * noi_t;
+        if (a.idx_ls >= 0 && !a.ard) gacc[a.idx_ls] += iso_t;
+    }
+    if (a.idx_ls >= 0 && a.ard) {
+        for (int f = 0; f < d; ++f) {
+            const TC xi = xs[lane * ds + f];
+            TC acc = TC(0);
+#pragma unroll
+            for (int k = 0; k < M; ++k) {
+                const TC t = xi - xs[k * ds + f];
+                acc = fma(r[k] * t, t, acc);
+            }
+            const TC t = xi - xs[M * ds + f];
+            acc = fma(gpe * t, t, acc);
+            const double s = (double)warp_sum(acc);
+            if (lane == 0) gacc[a.idx_ls + f] += s;
+        }
+    }
+    __syncwarp();
+    return true;
+}
+
+template <typename TIn, bool GRAD, bool PRED>
+__global__ void __launch_bounds__(kLocWarps * 32) local_warp_kernel(
+    const __grid_constant__ LocalArgs a, const TIn *__restrict__ x_ref, const TIn *__restrict__ y_ref,
+    const TIn *__restrict__ x_pt, const TIn *__restrict__ y_pt, const int32_t *__restrict__ nbr,
+    double *__restrict__ block_out, TIn *__restrict__ mean, TIn *__restrict__ var, int32_t *__restrict__ flags) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const WarpSmem lay = WarpSmem::make(a.d, a.n_theta);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned char *wsm = smem_raw + warp * lay.total;
+    double *gacc = reinterpret_cast<double *>(wsm + lay.xs_bytes + lay.l_bytes + lay.idg_bytes);
+    for (int t = lane; t < a.n_theta; t += 32) gacc[t] = 0.0;
+    __syncwarp();
+    double ll_acc = 0.0;
+    bool used_fp64 = false;
+    const int64_t nwarps = (int64_t)gridDim.x * kLocWarps;
+    for (int64_t p = (int64_t)blockIdx.x * kLocWarps + warp; p < a.n_points; p += nwarps) {
+        bool done = false;
+        if constexpr (std::is_same<TIn, float>::value) {
+            done = warp_system<float, TIn, GRAD, PRED>(a, p, lane, x_ref, y_ref, x_pt, y_pt, nbr, wsm, ll_acc, mean,
+                                                       var, flags);
+        }
+        if (!done) {
+            if constexpr (std::is_same<TIn, float>::value) used_fp64 = true;
+            warp_system<double, TIn, GRAD, PRED>(a, p, lane, x_ref, y_ref, x_pt, y_pt, nbr, wsm, ll_acc, mean, var,
+                                                 flags);
+        }
+    }
+    if (used_fp64 && lane == 0) flag_or(flags, NNGP_FLAG_FP64_FALLBACK);
+    if (PRED) return;
+    // CTA reduction in fixed order: warp w's totals -> slot w, then warp 0 sums
+    __shared__ double red[kLocWarps];
+    if (lane == 0) red[warp] = ll_acc;
+    __syncthreads();
+    const int nt = 1 + (GRAD ? a.n_theta : 0);
+    double *o = block_out + (int64_t)blockIdx.x * nt;
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < kLocWarps; ++w) s += red[w];
+        o[0] = s;
+    }
+    if (GRAD) {
+        for (int t = threadIdx.x; t < a.n_theta; t += blockDim.x) {
+            double s = 0.0;
+            for (int w = 0; w < kLocWarps; ++w)
+                s += reinterpret_cast<const double *>(smem_raw + w * lay.total + lay.xs_bytes + lay.l_bytes +
+                                                      lay.idg_bytes)[t];
+            o[1 + t] = s;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Block kernel (32 < m): one CTA per point, FP64, augmented matrix in shared memory
+// ---------------------------------------------------------------------------------------
+constexpr int kBlkThreads = 256;
+
+struct BlockSmem {
+    int n1, lda, ds;
+    size_t a_off, xs_off, vec_off, idx_off, total;
+    __host__ __device__ static BlockSmem make(int m, int d) {
+        BlockSmem s;
+        s.n1 = m + 1;
+        s.lda = m + 2;
+        s.ds = d;
+        size_t off = 0;
+        s.a_off = off;
+        off += (size_t)s.n1 * s.lda * 8;
+        s.xs_off = off;
+        off += (size_t)s.n1 * d * 8;
+        s.vec_off = off;
+        off += (size_t)6 * s.n1 * 8 + 64 * 8;  // yv, z, zw, b, v, tmp + reduction scratch
+        s.idx_off = off;
+        off += (size_t)s.n1 * 4;
+        s.total = (off + 15) / 16 * 16;
+        return s;
+    }
+};
+
+__device__ __forceinline__ double block_sum(double v, double *scratch) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    v = warp_sum(v);
+    __syncthreads();
+    if (lane == 0) scratch[warp] = v;
+    __syncthreads();
+    double s = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += scratch[w];
+    return s;
+}
+
+template <typename TIn, bool GRAD, bool PRED>
+__global__ void __launch_bounds__(kBlkThreads) local_block_kernel(
+    const __grid_constant__ LocalArgs a, const TIn *__restrict__ x_ref, const TIn *__restrict__ y_ref,
+    const TIn *__restrict__ x_pt, const TIn *__restrict__ y_pt, const int32_t *__restrict__ nbr,
+    double *__restrict__ block_out, TIn *__restrict__ mean, TIn *__restrict__ var, int32_t *__restrict__ flags) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const BlockSmem L = BlockSmem::make(a.m, a.d);
+    double *A = reinterpret_cast<double *>(smem_raw + L.a_off);
+    double *xs = reinterpret_cast<double *>(smem_raw + L.xs_off);
+    double *yv = reinterpret_cast<double *>(smem_raw + L.vec_off);
+    double *z = yv + L.n1, *zw = z + L.n1, *bb = zw + L.n1, *vv = bb + L.n1, *tmp = vv + L.n1;
+    double *scratch = tmp + L.n1;
+    int32_t *ids = reinterpret_cast<int32_t *>(smem_raw + L.idx_off);
+    const int m = a.m, n1 = L.n1, lda = L.lda, d = a.d, tid = threadIdx.x;
+    const int nth = 1 + a.n_theta;
+    double ll_acc = 0.0;
+    double g_loc[4] = {0, 0, 0, 0};  // amp, const, noise, iso (thread partials)
+
+    // per-feature length-scale terms are added to this CTA's output slots system by system
+    double *o = block_out + (int64_t)blockIdx.x * nth;
+    if (!PRED && tid < nth) o[tid] = 0.0;
+
+    for (int64_t p = blockIdx.x; p < a.n_points; p += gridDim.x) {
+        __syncthreads();
+        for (int i = tid; i < n1; i += blockDim.x) {
+            int32_t jj = -2;  // -2: the point itself (row m)
+            if (i < m) {
+                jj = nbr[p * m + i];
+                if (jj < -1 || (int64_t)jj >= a.n_rows) {
+                    flag_or(flags, NNGP_FLAG_BAD_INDEX);
+                    jj = -1;
+                }
+            }
+            ids[i] = jj;
+        }
+        __syncthreads();
+        for (int e = tid; e < n1 * d; e += blockDim.x) {
+            const int i = e / d, f = e - i * d;
+            const int32_t jj = ids[i];
+            const double s = a.inv_ls[a.ard ? f : 0];
+            double v = 0.0;
+            if (jj >= 0) v = (double)x_ref[(int64_t)jj * d + f] * s;
+            else if (jj == -2) v = (double)x_pt[p * d + f] * s;
+            xs[i * d + f] = v;
+        }
+        __syncthreads();
+        // fill the lower triangle (i >= j) of the augmented matrix, point = row m
+        for (int e = tid; e < n1 * n1; e += blockDim.x) {
+            const int i = e / n1, jx = e - i * n1;
+            if (jx > i) continue;
+            const bool vi = ids[i] != -1, vj = ids[jx] != -1;
+            double kv;
+            if (vi && vj) {
+                double r = 0.0;
+                for (int f = 0; f < d; ++f) {
+                    const double t = xs[i * d + f] - xs[jx * d + f];
+                    r = fma(t, t, r);
+                }
+                kv = a.rbf * exp(-0.5 * r) + a.cst;
+                if (i == jx) kv += a.noise + ((i == m && PRED) ? 0.0 : a.alpha);
+            } else {
+                kv = (i == jx) ? 1.0 : 0.0;
+            }
+            A[i * lda + jx] = kv;
+        }
+        __syncthreads();
+        // right-looking Cholesky
+        bool notpd = false;
+        for (int k = 0; k < n1; ++k) {
+            __syncthreads();  // the previous trailing update is complete
+            const double piv = A[k * lda + k];
+            if (!(piv > 0.0)) notpd = true;
+            const double sq = sqrt(piv);
+            const double inv = 1.0 / sq;
+            __syncthreads();  // every thread has read the pivot before it is overwritten
+            for (int i = k + 1 + tid; i < n1; i += blockDim.x) A[i * lda + k] *= inv;
+            if (tid == 0) A[k * lda + k] = sq;
+            __syncthreads();
+            const int rem = n1 - k - 1;
+            for (int e = tid; e < rem * rem; e += blockDim.x) {
+                const int i = k + 1 + e / rem, jx = k + 1 + e % rem;
+                if (jx <= i) A[i * lda + jx] = fma(-A[i * lda + k], A[jx * lda + k], A[i * lda + jx]);
+            }
+        }
+        __syncthreads();
+        if (notpd && tid == 0) flag_or(flags, NNGP_FLAG_NOT_PD);
+        const double sigma = A[m * lda + m];
+        const double s2 = sigma * sigma;
+        double wsum = 0.0, ll = 0.0;
+        for (int i = tid; i < n1; i += blockDim.x) zw[i] = 0.0;
+        for (int c = 0; c < a.ydim; ++c) {
+            __syncthreads();
+            for (int i = tid; i < m; i += blockDim.x) yv[i] = ids[i] >= 0 ? (double)y_ref[(int64_t)ids[i] * a.ydim + c] : 0.0;
+            __syncthreads();
+            // forward solve with warp 0: z = L_nn^-1 yv
+            if (tid < 32) {
+                for (int k = 0; k < m; ++k) {
+                    double part = 0.0;
+                    for (int jx = tid; jx < k; jx += 32) part = fma(A[k * lda + jx], z[jx], part);
+                    part = warp_sum(part);
+                    if (tid == 0) z[k] = (yv[k] - part) / A[k * lda + k];
+                    __syncwarp();
+                }
+                double part = 0.0;
+                for (int jx = tid; jx < m; jx += 32) part = fma(A[m * lda + jx], z[jx], part);
+                part = warp_sum(part);
+                if (tid == 0) tmp[0] = part;  // mu
+            }
+            __syncthreads();
+            const double mu = tmp[0];
+            if (PRED) {
+                if (tid == 0) mean[p * a.ydim + c] = (TIn)mu;
+            } else {
+                const double res = (double)y_pt[p * a.ydim + c] - mu;
+                ll += -0.5 * res * res / s2 - log(sigma) - kHalfLog2Pi;
+                if (GRAD) {
+                    const double rs = res / s2;
+                    for (int i = tid; i < m; i += blockDim.x) zw[i] = fma(rs, z[i], zw[i]);
+                    wsum += (res * rs - 1.0) / (2.0 * s2);
+                }
+            }
+        }
+        if (PRED) {
+            if (tid == 0) var[p] = (TIn)s2;
+            continue;
+        }
+        if (tid == 0) ll_acc += ll;
+        if (!GRAD) continue;
+        __syncthreads();
+        // backward solves with warp 0: b = L^-T l, v = L^-T zw (l = row m of the factor)
+        if (tid < 32) {
+            for (int k = m - 1; k >= 0; --k) {
+                double pb = 0.0, pv = 0.0;
+                for (int jx = k + 1 + tid; jx < m; jx += 32) {
+                    pb = fma(A[jx * lda + k], bb[jx], pb);
+                    pv = fma(A[jx * lda + k], vv[jx], pv);
+                }
+                pb = warp_sum(pb);
+                pv = warp_sum(pv);
+                if (tid == 0) {
+                    bb[k] = (A[m * lda + k] - pb) / A[k * lda + k];
+                    vv[k] = (zw[k] - pv) / A[k * lda + k];
+                }
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        // G-weighted recomputed fill over pairs i >= j of the augmented matrix
+        double t_amp = 0.0, t_cst = 0.0, t_noise = 0.0, t_iso = 0.0;
+        for (int e = tid; e < n1 * n1; e += blockDim.x) {
+            const int i = e / n1, jx = e - i * n1;
+            if (jx > i) continue;
+            if (ids[i] == -1 || ids[jx] == -1) continue;
+            double G;
+            if (i == m && jx == m) G = wsum;
+            else if (i == m) G = 0.5 * vv[jx] - wsum * bb[jx];
+            else G = wsum * bb[i] * bb[jx] - 0.5 * (bb[i] * vv[jx] + vv[i] * bb[jx]);
+            const double wgt = (i == jx) ? 1.0 : 2.0;
+            double r = 0.0;
+            for (int f = 0; f < d; ++f) {
+                const double t = xs[i * d + f] - xs[jx * d + f];
+                r = fma(t, t, r);
+            }
+            const double e0 = a.rbf * exp(-0.5 * r);
+            t_amp += wgt * G * e0;
+            t_cst += wgt * G;
+            if (i == jx) t_noise += G;
+            t_iso += wgt * G * e0 * r;
+        }
+        g_loc[0] += t_amp;
+        g_loc[1] += t_cst;
+        g_loc[2] += t_noise;
+        g_loc[3] += t_iso;
+        if (a.idx_ls >= 0 && a.ard) {
+            for (int f = 0; f < d; ++f) {
+                double acc = 0.0;
+                for (int e = tid; e < n1 * n1; e += blockDim.x) {
+                    const int i = e / n1, jx = e - i * n1;
+                    if (jx >= i) continue;  // diagonal terms vanish (dx = 0)
+                    if (ids[i] == -1 || ids[jx] == -1) continue;
+                    double G;
+                    if (i == m) G = 0.5 * vv[jx] - wsum * bb[jx];
+                    else G = wsum * bb[i] * bb[jx] - 0.5 * (bb[i] * vv[jx] + vv[i] * bb[jx]);
+                    double r = 0.0;
+                    for (int ff = 0; ff < d; ++ff) {
+                        const double t = xs[i * d + ff] - xs[jx * d + ff];
+                        r = fma(t, t, r);
+                    }
+                    const double t = xs[i * d + f] - xs[jx * d + f];
+                    acc += 2.0 * G * a.rbf * exp(-0.5 * r) * t * t;
+                }
+                const double s = block_sum(acc, scratch);
+                if (tid == 0) o[1 + a.idx_ls + f] += s;
+            }
+        }
+    }
+    if (PRED) return;
+    __syncthreads();
+    const double s_ll = block_sum(ll_acc, scratch);
+    if (tid == 0) o[0] = s_ll;
+    if (GRAD) {
+        const double s0 = block_sum(g_loc[0], scratch);
+        const double s1 = block_sum(g_loc[1], scratch);
+        const double s2v = block_sum(g_loc[2], scratch);
+        const double s3 = block_sum(g_loc[3], scratch);
+        if (tid == 0) {
+            if (a.idx_rbf >= 0) o[1 + a.idx_rbf] += s0;
+            if (a.idx_const >= 0) o[1 + a.idx_const] += a.cst * s1;
+            if (a.idx_noise >= 0) o[1 + a.idx_noise] += a.noise * s2v;
+            if (a.idx_ls >= 0 && !a.ard) o[1 + a.idx_ls] += s3;
+        }
+    }
+}
+
+// Fixed-order sum of the per-CTA partials: out[t] = sum_b block_out[b * nt + t].
+__global__ void finalize_kernel(const double *__restrict__ block_out, int nblocks, int nt, double *__restrict__ out) {
+    __shared__ double scratch[32];
+    for (int t = 0; t < nt; ++t) {
+        double s = 0.0;
+        for (int b = threadIdx.x; b < nblocks; b += blockDim.x) s += block_out[(int64_t)b * nt + t];
+        s = block_sum(s, scratch);
+        if (threadIdx.x == 0) out[t] = s;
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------------------
+namespace {
+
+int num_sms() {
+    static int cached = 0;
+    if (!cached) {
+        int dev = 0, v = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && v > 0)
+            cached = v;
+        else
+            cached = kNumSMsB200;
+    }
+    return cached;
+}
+
+size_t block_smem_limit() { return 227 * 1024; }
+
+struct LocalPlan {
+    bool warp = true;
+    int grid = 0;
+    size_t smem = 0;
+    int nt = 1;
+    size_t ws_bytes = 0;
+};
+
+LocalPlan plan_local(int64_t n_points, int d, int m, int n_theta, bool grad) {
+    LocalPlan p;
+    p.warp = m <= kWarpM;
+    p.nt = 1 + (grad ? n_theta : 0);
+    const int sms = num_sms();
+    if (p.warp) {
+        p.smem = WarpSmem::make(d, n_theta).total * kLocWarps;
+        const int64_t need = (n_points + kLocWarps - 1) / kLocWarps;
+        p.grid = (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)sms * 8));
+    } else {
+        p.smem = BlockSmem::make(m, d).total;
+        p.grid = (int)std::max<int64_t>(1, std::min<int64_t>(n_points, (int64_t)sms * 2));
+    }
+    p.ws_bytes = align_up((size_t)p.grid * p.nt * sizeof(double), 256) + 256;
+    return p;
+}
+
+nngp_status fill_args(LocalArgs &a, const nngp_kernel *k, int d, int ydim, int m, int64_t n_rows, int64_t n_points,
+                      double pivot_tol, bool grad) {
+    if (!k) return fail(NNGP_ERR_INVALID_ARGUMENT, "kernel parameters are null");
+    if (d <= 0 || d > kMaxDimLocal) return fail(NNGP_ERR_UNSUPPORTED, "d must be in [1, 256]");
+    if (ydim <= 0) return fail(NNGP_ERR_INVALID_ARGUMENT, "ydim must be >= 1");
+    if (m < 0) return fail(NNGP_ERR_INVALID_ARGUMENT, "m must be >= 0");
+    if (k->n_ls != 0 && k->n_ls != 1 && k->n_ls != d) return fail(NNGP_ERR_INVALID_ARGUMENT, "n_ls must be 0, 1 or d");
+    if (k->n_ls > 0 && !k->length_scale) return fail(NNGP_ERR_INVALID_ARGUMENT, "length_scale is null");
+    if (grad && (k->n_theta < 0 || k->n_theta > kMaxTheta)) return fail(NNGP_ERR_UNSUPPORTED, "n_theta out of range");
+    if (m > kWarpM) {
+        const size_t need = BlockSmem::make(m, d).total;
+        if (need > block_smem_limit())
+            return fail(NNGP_ERR_UNSUPPORTED, "m = " + std::to_string(m) + " with d = " + std::to_string(d) +
+                                                  " needs more shared memory than one CTA has");
+    }
+    a.rbf = k->rbf_level;
+    a.cst = k->const_value;
+    a.noise = k->noise_level;
+    a.alpha = k->alpha;
+    a.pivot_abs = pivot_tol * std::fabs(k->rbf_level + k->const_value + k->noise_level + k->alpha);
+    a.n_rows = n_rows;
+    a.n_points = n_points;
+    a.d = d;
+    a.ydim = ydim;
+    a.m = m;
+    a.ard = k->n_ls == d && d > 1;
+    a.idx_rbf = grad ? k->idx_rbf_level : -1;
+    a.idx_const = grad ? k->idx_const : -1;
+    a.idx_noise = grad ? k->idx_noise : -1;
+    a.idx_ls = grad ? k->idx_ls : -1;
+    a.n_theta = grad ? k->n_theta : 0;
+    auto chk = [&](int idx, int span) { return idx < 0 || idx + span <= a.n_theta; };
+    if (grad && !(chk(a.idx_rbf, 1) && chk(a.idx_const, 1) && chk(a.idx_noise, 1) && chk(a.idx_ls, a.ard ? d : 1)))
+        return fail(NNGP_ERR_INVALID_ARGUMENT, "a theta index is outside [0, n_theta)");
+    for (int f = 0; f < kMaxDimLocal; ++f) a.inv_ls[f] = 1.0;
+    if (k->n_ls > 0) {
+        for (int f = 0; f < (a.ard ? d : 1); ++f) {
+            const double l = k->length_scale[a.ard ? f : 0];
+            if (!(l > 0.0)) return fail(NNGP_ERR_INVALID_ARGUMENT, "length scales must be > 0");
+            a.inv_ls[f] = 1.0 / l;
+        }
+    }
+    return NNGP_OK;
+}
+
+template <typename TIn, bool GRAD, bool PRED>
+nngp_status launch_local(const LocalPlan &pl, const LocalArgs &a, const TIn *x_ref, const TIn *y_ref, const TIn *x_pt,
+                         const TIn *y_pt, const int32_t *nbr, double *block_out, TIn *mean, TIn *var, int32_t *flags,
+                         cudaStream_t stream) {
+    if (pl.warp) {
+        auto fn = local_warp_kernel<TIn, GRAD, PRED>;
+        NNGP_CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void *>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)pl.smem));
+        fn<<<pl.grid, kLocWarps * 32, pl.smem, stream>>>(a, x_ref, y_ref, x_pt, y_pt, nbr, block_out, mean, var, flags);
+    } else {
+        auto fn = local_block_kernel<TIn, GRAD, PRED>;
+        NNGP_CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void *>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)pl.smem));
+        fn<<<pl.grid, kBlkThreads, pl.smem, stream>>>(a, x_ref, y_ref, x_pt, y_pt, nbr, block_out, mean, var, flags);
+    }
+    NNGP_CUDA_TRY(cudaGetLastError());
+    return NNGP_OK;
+}
+
+template <typename TIn>
+nngp_status loglik_impl(const TIn *x, const TIn *y, int64_t n, int d, int ydim, int64_t row_begin, int64_t rows,
+                        const int32_t *nbr, int m, const nngp_kernel *k, int eval_gradient, double pivot_tol,
+                        double *out, int32_t *flags, void *ws, size_t ws_bytes, cudaStream_t stream) {
+    if (n < 0 || rows < 0 || row_begin < 0 || row_begin + rows > n)
+        return fail(NNGP_ERR_INVALID_ARGUMENT, "loglik: rows outside [0, n)");
+    if (!out) return fail(NNGP_ERR_INVALID_ARGUMENT, "loglik: out is null");
+    const bool grad = eval_gradient != 0;
+    LocalArgs a;
+    nngp_status st = fill_args(a, k, d, ydim, m, n, rows, pivot_tol, grad);
+    if (st != NNGP_OK) return st;
+    const int nt = 1 + (grad ? a.n_theta : 0);
+    if (rows == 0) {
+        NNGP_CUDA_TRY(cudaMemsetAsync(out, 0, nt * sizeof(double), stream));
+        return NNGP_OK;
+    }
+    if (!x || !y || (m > 0 && !nbr)) return fail(NNGP_ERR_INVALID_ARGUMENT, "loglik: null input pointer");
+    const LocalPlan pl = plan_local(rows, d, m, a.n_theta, grad);
+    if (!ws || ws_bytes < pl.ws_bytes) return fail(NNGP_ERR_WORKSPACE, "loglik: workspace missing or too small");
+    double *block_out = reinterpret_cast<double *>(align_up(reinterpret_cast<uintptr_t>(ws), 256));
+    const TIn *x_pt = x + row_begin * d;
+    const TIn *y_pt = y + row_begin * ydim;
+    if (grad)
+        st = launch_local<TIn, true, false>(pl, a, x, y, x_pt, y_pt, nbr, block_out, nullptr, nullptr, flags, stream);
+    else
+        st = launch_local<TIn, false, false>(pl, a, x, y, x_pt, y_pt, nbr, block_out, nullptr, nullptr, flags, stream);
+    if (st != NNGP_OK) return st;
+    finalize_kernel<<<1, 256, 0, stream>>>(block_out, pl.grid, pl.nt, out);
+    NNGP_CUDA_TRY(cudaGetLastError());
+    return NNGP_OK;
+}
+
+template <typename TIn>
+nngp_status predict_impl(const TIn *xt, const TIn *yt, int64_t nt, const TIn *xq, int64_t nq, int d, int ydim,
+                         const int32_t *nbr, int m, const nngp_kernel *k, double pivot_tol, TIn *mean, TIn *var,
+                         int32_t *flags, cudaStream_t stream) {
+    if (nt < 0 || nq < 0) return fail(NNGP_ERR_INVALID_ARGUMENT, "predict: negative size");
+    LocalArgs a;
+    nngp_status st = fill_args(a, k, d, ydim, m, nt, nq, pivot_tol, false);
+    if (st != NNGP_OK) return st;
+    if (nq == 0) return NNGP_OK;
+    if (!xq || !mean || !var || (m > 0 && (!nbr || !xt || !yt))) return fail(NNGP_ERR_INVALID_ARGUMENT, "predict: null pointer");
+    const LocalPlan pl = plan_local(nq, d, m, 0, false);
+    return launch_local<TIn, false, true>(pl, a, xt, yt, xq, nullptr, nbr, nullptr, mean, var, flags, stream);
+}
+
+}  // namespace
+
+size_t loglik_workspace(int64_t n, int d, int ydim, int m, int n_theta) {
+    (void)ydim;
+    return plan_local(std::max<int64_t>(n, 1), std::max(d, 1), m, std::max(n_theta, 0), true).ws_bytes;
+}
+
+nngp_status loglik_f32(const float *x, const float *y, int64_t n, int d, int ydim, const int32_t *nbr, int m,
+                       const nngp_kernel *k, int eval_gradient, double pivot_tol, double *out, int32_t *flags, void *ws,
+                       size_t ws_bytes, cudaStream_t stream) {
+    return loglik_impl<float>(x, y, n, d, ydim, 0, n, nbr, m, k, eval_gradient, pivot_tol, out, flags, ws, ws_bytes,
+                              stream);
+}
+nngp_status loglik_f64(const double *x, const double *y, int64_t n, int d, int ydim, const int32_t *nbr, int m,
+                       const nngp_kernel *k, int eval_gradient, double pivot_tol, double *out, int32_t *flags, void *ws,
+                       size_t ws_bytes, cudaStream_t stream) {
+    return loglik_impl<double>(x, y, n, d, ydim, 0, n, nbr, m, k, eval_gradient, pivot_tol, out, flags, ws, ws_bytes,
+                               stream);
+}
+nngp_status loglik_rows_f32(const float *x, const float *y, int64_t n, int d, int ydim, int64_t r0, int64_t rc,
+                            const int32_t *nbr, int m, const nngp_kernel *k, int eval_gradient, double pivot_tol,
+                            double *out, int32_t *flags, void *ws, size_t ws_bytes, cudaStream_t stream) {
+    return loglik_impl<float>(x, y, n, d, ydim, r0, rc, nbr, m, k, eval_gradient, pivot_tol, out, flags, ws, ws_bytes,
+                              stream);
+}
+nngp_status loglik_rows_f64(const double *x, const double *y, int64_t n, int d, int ydim, int64_t r0, int64_t rc,
+                            const int32_t *nbr, int m, const nngp_kernel *k, int eval_gradient, double pivot_tol,
+                            double *out, int32_t *flags, void *ws, size_t ws_bytes, cudaStream_t stream) {
+    return loglik_impl<double>(x, y, n, d, ydim, r0, rc, nbr, m, k, eval_gradient, pivot_tol, out, flags, ws, ws_bytes,
+                               stream);
+}
+nngp_status predict_f32(const float *xt, const float *yt, int64_t nt, const float *xq, int64_t nq, int d, int ydim,
+                        const int32_t *nbr, int m, const nngp_kernel *k, double pivot_tol, float *mean, float *var,
+                        int32_t *flags, cudaStream_t stream) {
+    return predict_impl<float>(xt, yt, nt, xq, nq, d, ydim, nbr, m, k, pivot_tol, mean, var, flags, stream);
+}
+nngp_status predict_f64(const double *xt, const double *yt, int64_t nt, const double *xq, int64_t nq, int d, int ydim,
+                        const int32_t *nbr, int m, const nngp_kernel *k, double pivot_tol, double *mean, double *var,
+                        int32_t *flags, cudaStream_t stream) {
+    return predict_impl<double>(xt, yt, nt, xq, nq, d, ydim, nbr, m, k, pivot_tol, mean, var, flags, stream);
+}
+
+}  // namespace nngp

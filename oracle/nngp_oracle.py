@@ -1,0 +1,331 @@
+"""CPU oracle for the NNGP fit/predict hot path.
+
+TEST INFRASTRUCTURE ONLY.  Only ``tests/``, ``__graft_entry__.smoke()`` and the
+``cpu_baseline`` leg of ``bench.py`` may import this module, and only as the
+checker.  The product path (``nngpr_b200``) never calls it and has no CPU
+fallback.
+
+This is a numpy restatement of the reference nngpr (stavoltafunzia/nngpr 0.1.1)
+algorithm for the accelerated ``WhiteKernel + ConstantKernel * RBF`` path.
+Every function names the reference lines it restates.  The restatement is
+pinned by the golden vectors in ``tests/golden/`` that ``tests/golden/make_golden.py``
+produced by running the reference ``NumpyNngpr`` itself (FP64, sequential), and
+by the reference's own known-answer test (NNGP with ``num_nn = n`` equals the exact
+GP of scikit-learn, ``nngpr/test/nngpr_base_tester.py:174-192``).
+
+Kernel parameters are passed explicitly (``KernelParams``); turning a kernel
+object into them is product code (``nngpr_b200.kernel_params``) and is tested
+against the reference separately.
+"""
+
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+LOG_2PI = math.log(2.0 * math.pi)
+
+
+@dataclasses.dataclass
+class KernelParams:
+    """Parameters of ``White(noise) + const + rbf_level * RBF(length_scale)``.
+
+    Mirrors the dictionary returned by ``RbfAccelerator.get_kernel_params``
+    (``nngpr/cuda_kernel_accelerators.py:520-581``) and the theta index map of
+    ``get_kernel_theta_mapping`` (``:583-649``).  ``idx_*`` are positions in
+    ``kernel.theta`` (``-1`` when the hyperparameter is fixed or absent);
+    ``idx_ls`` is the first of ``len(length_scale)`` consecutive positions.
+    """
+
+    rbf_level: float = 1.0
+    const_value: float = 0.0
+    noise_level: float = 0.0
+    length_scale: object = 1.0  # float (isotropic) or 1-D array (ARD)
+    idx_rbf_level: int = -1
+    idx_const: int = -1
+    idx_noise: int = -1
+    idx_ls: int = -1
+    n_theta: int = 0
+
+    @property
+    def ard(self) -> bool:
+        return np.ndim(self.length_scale) > 0
+
+    def ls_vector(self, d: int) -> np.ndarray:
+        ls = np.asarray(self.length_scale, dtype=np.float64).reshape(-1)
+        if ls.size == 1:
+            return np.full(d, ls[0])
+        assert ls.size == d
+        return ls
+
+
+# ----------------------------------------------------------------------------------------------
+# Nearest neighbours
+# ----------------------------------------------------------------------------------------------
+
+def scale_for_search(x: np.ndarray, length_scale, dtype=np.float32) -> np.ndarray:
+    """Inputs divided by the length scale in the search dtype.
+
+    Restates ``cuda_kernel_accelerators.py:235-239``: the search arrays are cast
+    to the search dtype first (``base_nngpr.py:1170-1173`` downcasts to float32
+    unless ``allow_downcast_f32 == 'no'``), then ``x / ls`` is evaluated in that
+    dtype (numpy promotion rules: a Python float length scale is cast to the
+    array dtype; an ARD vector is cast with ``cp.array(ls, dtype=data_type)``).
+    ``length_scale=None`` means input-space search (plain Euclidean, no scaling).
+    """
+    xs = np.asarray(x).astype(dtype, copy=False)
+    if length_scale is None:
+        return np.array(xs, dtype=dtype, copy=True)
+    ls = np.asarray(length_scale, dtype=np.float64).reshape(-1).astype(dtype)
+    return (xs / ls).astype(dtype, copy=False)
+
+
+def pairwise_sqdist(query: np.ndarray, ref: np.ndarray) -> np.ndarray:
+    """Squared distances ``sum_f (ref_f - query_f)^2`` accumulated feature by feature.
+
+    Same operation order as the ``calc_nn`` kernel (``cuda_kernel_accelerators.py:718-723``):
+    ``tmp = ref_f - query_f; distance += tmp * tmp`` for ``f = 0 .. d-1``.  numpy
+    evaluates each step with one IEEE rounding (no fused multiply-add), which is the
+    arithmetic the GPU kernels use for their exact distances, so the results agree
+    bit for bit in float32 and float64.
+    """
+    dt = query.dtype
+    out = np.zeros((query.shape[0], ref.shape[0]), dtype=dt)
+    for f in range(query.shape[1]):
+        t = ref[None, :, f] - query[:, None, f]
+        out += t * t
+    return out
+
+
+def knn(ref: np.ndarray, query: np.ndarray, num_nn: int, ref_cut_index=None, length_scale=1.0,
+        dtype=np.float32, chunk: int = 512, query_index=None) -> np.ndarray:
+    """Exact top-``num_nn`` search, ascending distance, ties broken by the lower index.
+
+    Semantics of ``NngprWorker.find_nearest_neighbors`` (``base_nngpr.py:1613-1686``) with
+    the accelerated ``calc_nn`` ranking (``cuda_kernel_accelerators.py:663-743``):
+
+    * kernel space = squared Euclidean distance of the length-scale-scaled inputs
+      (``length_scale=None``: input space, unscaled);
+    * with ``ref_cut_index = c`` query ``j`` may only use refs ``[0, j + c)``
+      (``base_nngpr.py:1660-1671``, ``cuda_kernel_accelerators.py:357-362``);
+      ``None`` means every ref;
+    * equal distances keep the lower index first (the ``<=`` break of the insertion
+      sort, ``cuda_kernel_accelerators.py:728``);
+    * missing slots are ``-1`` (``base_nngpr.py:1648``, ``:1675-1681``).
+
+    ``query_index`` (optional) gives each query row's position in the full query set, so
+    that a sample of rows can be checked with the cut of its original position.
+
+    Returns int32 of shape ``(n_query, num_nn)``.
+    """
+    refs = scale_for_search(ref, length_scale, dtype)
+    qs = scale_for_search(query, length_scale, dtype)
+    nr, nq = refs.shape[0], qs.shape[0]
+    out = np.full((nq, num_nn), -1, dtype=np.int32)
+    if nr == 0 or num_nn == 0:
+        return out
+    ar = np.arange(nr, dtype=np.int64)
+    qidx = np.arange(nq, dtype=np.int64) if query_index is None else np.asarray(query_index, dtype=np.int64)
+    for q0 in range(0, nq, chunk):
+        q1 = min(nq, q0 + chunk)
+        d2 = pairwise_sqdist(qs[q0:q1], refs)
+        # (distance, index) packed into one int64: the bit pattern of a non-negative
+        # IEEE float is monotone, so integer order == lexicographic (distance, index).
+        if dtype == np.float32:
+            bits = d2.view(np.int32).astype(np.int64)
+            key = (bits << 32) | ar[None, :]
+            big = np.int64(np.iinfo(np.int64).max)
+        else:
+            # float64 distances: sort with a stable argsort (ties -> lower index).
+            key = None
+        if ref_cut_index is not None:
+            allowed = (qidx[q0:q1, None] + ref_cut_index) > ar[None, :]
+        else:
+            allowed = np.ones((q1 - q0, nr), dtype=bool)
+        k = min(num_nn, nr)
+        if key is not None:
+            key = np.where(allowed, key, big)
+            part = np.argpartition(key, k - 1, axis=1)[:, :k] if k < nr else np.tile(ar, (q1 - q0, 1))
+            pk = np.take_along_axis(key, part, axis=1)
+            order = np.argsort(pk, axis=1, kind='stable')
+            sel = np.take_along_axis(part, order, axis=1)
+        else:
+            d2 = np.where(allowed, d2, np.inf)
+            sel = np.argsort(d2, axis=1, kind='stable')[:, :k]
+        ok = np.take_along_axis(allowed, sel, axis=1)
+        sel = np.where(ok, sel, -1).astype(np.int32)
+        out[q0:q1, :k] = sel
+    return out
+
+
+def fit_neighbours(x: np.ndarray, num_nn: int, length_scale=1.0, dtype=np.float32) -> np.ndarray:
+    """Neighbour lists of the fit step: point ``i`` uses the ``num_nn`` nearest of the points
+    ``[0, i)`` in input order (``base_nngpr.py:530-535`` with ``ref_cut_index = i0`` over the
+    whole training set).  Returns ``(n, num_nn)`` without the self column."""
+    return knn(x, x, num_nn, ref_cut_index=0, length_scale=length_scale, dtype=dtype)
+
+
+# ----------------------------------------------------------------------------------------------
+# Local covariance fill
+# ----------------------------------------------------------------------------------------------
+
+def fill_nn_kernel(x_full: np.ndarray, nn_indices: np.ndarray, p: KernelParams, eval_gradient: bool):
+    """Local covariance ``K (b, k, k)`` and gradient ``dK (b, k, k, n_theta)`` of a neighbour list.
+
+    Restates the ``fill_nn_kernel`` CUDA kernel (``cuda_kernel_accelerators.py:748-863``) and
+    the generic fill (``base_nngpr.py:1781-1805``): for valid pairs
+    ``K = rbf_level * exp(-sum_f d_f^2 / (2 l_f^2)) + const (+ noise on the index diagonal)``;
+    a ``-1`` slot gives an identity row/column and a zero gradient.  Gradients are with
+    respect to the log hyperparameters: noise -> ``noise`` on the diagonal, const -> ``const``,
+    rbf_level -> the RBF part, isotropic l -> ``RBF * sum_f d_f^2 / l^2``, ARD l_f ->
+    ``RBF * d_f^2 / l_f^2``.
+    """
+    x_full = np.asarray(x_full, dtype=np.float64)
+    idx = np.asarray(nn_indices)
+    b, k = idx.shape
+    d = x_full.shape[1]
+    valid = idx >= 0
+    xn = x_full[np.where(valid, idx, 0)]  # (b, k, d)
+    ls = p.ls_vector(d)
+    diff = (xn[:, :, None, :] - xn[:, None, :, :]) / ls  # (b, k, k, d)
+    sq = diff * diff
+    dist = 0.5 * sq.sum(-1)
+    E = p.rbf_level * np.exp(-dist)
+    eye = np.eye(k, dtype=bool)[None]
+    pair = valid[:, :, None] & valid[:, None, :]
+    K = np.where(pair, E + p.const_value + np.where(eye, p.noise_level, 0.0), 0.0)
+    K = np.where(~pair & eye, 1.0, K)
+    if not eval_gradient:
+        return K, None
+    G = np.zeros((b, k, k, p.n_theta))
+    if p.idx_noise >= 0:
+        G[..., p.idx_noise] = np.where(pair & eye, p.noise_level, 0.0)
+    if p.idx_const >= 0:
+        G[..., p.idx_const] = np.where(pair, p.const_value, 0.0)
+    if p.idx_rbf_level >= 0:
+        G[..., p.idx_rbf_level] = np.where(pair, E, 0.0)
+    if p.idx_ls >= 0:
+        if p.ard:
+            for f in range(d):
+                G[..., p.idx_ls + f] = np.where(pair, E * sq[..., f], 0.0)
+        else:
+            G[..., p.idx_ls] = np.where(pair, E * sq.sum(-1), 0.0)
+    return K, G
+
+
+# ----------------------------------------------------------------------------------------------
+# Log-likelihood and gradient
+# ----------------------------------------------------------------------------------------------
+
+def _gather_y(y: np.ndarray, idx: np.ndarray) -> np.ndarray:
+    """``_build_ytrain_given_nn_indices`` (``base_nngpr.py:1336-1368``): y of each neighbour,
+    zero for ``-1`` slots."""
+    valid = idx >= 0
+    out = y[np.where(valid, idx, 0)]
+    out[~valid] = 0.0
+    return out
+
+
+def _chol_solve(L: np.ndarray, rhs: np.ndarray) -> np.ndarray:
+    """``K^-1 rhs`` from the lower Cholesky factor, batched (``numpy_nngpr.py:140-170`` does the
+    same with LAPACK ``cho_solve`` one matrix at a time)."""
+    z = np.linalg.solve(L, rhs)
+    return np.linalg.solve(np.swapaxes(L, -1, -2), z)
+
+
+def loglik_terms(x: np.ndarray, y: np.ndarray, nbr: np.ndarray, p: KernelParams, alpha: float,
+                 eval_gradient: bool, rows=None):
+    """Per-point log-likelihood (summed over outputs) and its per-point gradient.
+
+    Restates ``Nngpr._log_likelihood_worker`` (``base_nngpr.py:453-614``) in FP64 for the
+    points ``rows`` (default: all).  ``nbr`` is ``(n, m)`` without the self column; the
+    self column is prepended as in ``base_nngpr.py:533-535``.
+    """
+    x = np.asarray(x, dtype=np.float64)
+    y = np.asarray(y, dtype=np.float64)
+    if y.ndim == 1:
+        y = y[:, None]
+    rows = np.arange(x.shape[0]) if rows is None else np.asarray(rows)
+    idx = np.concatenate([rows[:, None], np.asarray(nbr)[rows]], axis=1)
+    K, dK = fill_nn_kernel(x, idx, p, eval_gradient)
+    valid = idx >= 0
+    # K[ind[0], ind[1], ind[1]] += alpha on every valid slot (base_nngpr.py:555-556)
+    ii = np.arange(idx.shape[1])
+    K[:, ii, ii] += np.where(valid, alpha, 0.0)
+    n = K.shape[0]
+    L = np.linalg.cholesky(K[:, 1:, 1:])  # base_nngpr.py:564
+    y_nn = _gather_y(y, idx)  # (n, k, ydim)
+    yt = y[rows]
+    K_xn = K[:, 0, 1:][:, None, :]  # (n, 1, m)
+    a = _chol_solve(L, y_nn[:, 1:])  # K_nn^-1 y_nn
+    b = _chol_solve(L, np.swapaxes(K_xn, 1, 2))  # K_nn^-1 K_xn^T
+    mu = (K_xn @ a)[:, 0, :]  # base_nngpr.py:578
+    sigma = np.sqrt(K[:, 0, 0][:, None] - (K_xn @ b)[:, 0, :])  # :579-580
+    ll = -0.5 * (yt - mu) ** 2 / sigma ** 2 - 0.5 * LOG_2PI - np.log(sigma)  # :581
+    ll = ll.sum(-1)
+    if not eval_gradient:
+        return ll, None
+    dK = np.moveaxis(dK, -1, 0)  # (t, n, k, k)
+    dKnn = dK[:, :, 1:, 1:]
+    dkx = dK[:, :, 0, 1:][:, :, None, :]  # (t, n, 1, m)
+    # dK_nn^-1 r = -K_nn^-1 dK_nn K_nn^-1 r (base_nngpr.py:591-592)
+    dinv_y = -_chol_solve(L[None], dKnn @ a[None])
+    dinv_k = -_chol_solve(L[None], dKnn @ b[None])
+    dmu = (dkx @ a[None])[:, :, 0, :] + (K_xn[None] @ dinv_y)[:, :, 0, :]  # :596-598
+    dsig = 0.5 / sigma[None] * (dK[:, :, 0, 0][..., None] - 2 * (dkx @ b[None])[:, :, 0, :]
+                                - (K_xn[None] @ dinv_k)[:, :, 0, :])  # :602-606
+    r = (yt - mu)[None]
+    g = (-1 / sigma[None] + r ** 2 / sigma[None] ** 3) * dsig + r / sigma[None] ** 2 * dmu  # :609-610
+    return ll, g.sum(-1).T  # (n, t)
+
+
+def log_marginal_likelihood(x, y, nbr, p: KernelParams, alpha: float, eval_gradient: bool = False,
+                            chunk: int = 4096):
+    """``Nngpr.log_marginal_likelihood`` (``base_nngpr.py:385-451``): sum of the per-point terms
+    over all points and outputs (FP64)."""
+    n = np.asarray(x).shape[0]
+    total = 0.0
+    grad = np.zeros(p.n_theta)
+    for i0 in range(0, n, chunk):
+        rows = np.arange(i0, min(n, i0 + chunk))
+        ll, g = loglik_terms(x, y, nbr, p, alpha, eval_gradient, rows)
+        total += float(ll.sum())
+        if eval_gradient:
+            grad += g.sum(0)
+    return (total, grad) if eval_gradient else total
+
+
+# ----------------------------------------------------------------------------------------------
+# Predict (conditioning on the training set only)
+# ----------------------------------------------------------------------------------------------
+
+def predict(x_train, y_train, x_query, nbr, p: KernelParams, alpha: float):
+    """Predictive mean ``(nq, ydim)`` and standard deviation ``(nq,)``.
+
+    Restates ``Nngpr._predict_worker`` (``base_nngpr.py:1032-1135``) for
+    ``conditioning_method='only-train'``: the query is column 0 of the local system
+    (index ``nt + i`` in ``x_full = [x_train; x_query]``, ``base_nngpr.py:1461-1462``);
+    alpha is added only to training slots (``:1106-1107``), so ``K_00`` carries the
+    white noise but no alpha; ``mean = K_xn K_nn^-1 y_nn``, ``std = sqrt(K_00 - K_xn K_nn^-1 K_xn^T)``.
+    ``nbr`` is ``(nq, m)`` of training indices (``-1`` padded).
+    """
+    x_train = np.asarray(x_train, dtype=np.float64)
+    x_query = np.asarray(x_query, dtype=np.float64)
+    y_train = np.asarray(y_train, dtype=np.float64)
+    if y_train.ndim == 1:
+        y_train = y_train[:, None]
+    nt, nq = x_train.shape[0], x_query.shape[0]
+    x_full = np.concatenate([x_train, x_query])
+    idx = np.concatenate([np.arange(nt, nt + nq)[:, None], np.asarray(nbr)], axis=1)
+    K, _ = fill_nn_kernel(x_full, idx, p, False)
+    train = (idx >= 0) & (idx < nt)
+    ii = np.arange(idx.shape[1])
+    K[:, ii, ii] += np.where(train, alpha, 0.0)
+    L = np.linalg.cholesky(K[:, 1:, 1:])
+    y_nn = _gather_y(y_train, np.asarray(nbr))
+    K_xn = K[:, :1, 1:]
+    mean = (K_xn @ _chol_solve(L, y_nn))[:, 0, :]
+    var = K[:, 0, 0] - (K_xn @ _chol_solve(L, np.swapaxes(K_xn, 1, 2)))[:, 0, 0]
+    return mean, np.sqrt(var)

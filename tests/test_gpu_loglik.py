@@ -1,0 +1,116 @@
+"""Fit-step log-likelihood and gradient through the C ABI vs the oracle / golden vectors.
+
+Tolerances: FP64 entry point 1e-10 relative (lml) and 1e-9 (gradient, max-norm relative);
+FP32 entry point 1e-5 relative for the lml and the gradient (max-norm relative).
+"""
+import numpy as np
+import pytest
+import torch
+
+from nngpr_b200 import _lib, ops
+from nngpr_b200.kernel_params import extract
+from oracle import nngp_oracle as O
+from sklearn.gaussian_process import kernels as skk
+
+from _common import CASES, KERNELS, load, normalized_y, oracle_params, rel
+
+pytestmark = pytest.mark.gpu
+
+F64_LML, F64_GRAD = 1e-10, 1e-9
+F32_LML, F32_GRAD = 1e-5, 1e-5
+
+
+def gpu_loglik(x, y, nbr, p, alpha, grad, dtype, pivot_tol=1e-6):
+    tdt = torch.float32 if dtype == np.float32 else torch.float64
+    xt = torch.from_numpy(np.ascontiguousarray(x)).to('cuda', tdt)
+    yt = torch.from_numpy(np.ascontiguousarray(y.reshape(len(y), -1))).to('cuda', tdt)
+    nt = torch.from_numpy(np.ascontiguousarray(nbr, dtype=np.int32)).cuda()
+    flags = ops.new_flags(xt.device)
+    out = ops.loglik(xt, yt, nt, p, alpha, grad, pivot_tol, flags=flags).cpu().numpy()
+    return out, int(flags.item())
+
+
+@pytest.mark.parametrize('name', CASES)
+@pytest.mark.parametrize('dtype', [np.float64, np.float32])
+def test_loglik_golden(name, dtype):
+    g = load(name)
+    p = extract(KERNELS[name]().clone_with_theta(g['theta']))
+    y, _, _ = normalized_y(g)
+    nbr = g['nbr_fit_f32']
+    out, flags = gpu_loglik(g['x'], y, nbr, p, float(g['alpha']), True, dtype)
+    assert flags & ~_lib.NNGP_FLAG_FP64_FALLBACK == 0
+    tol_l, tol_g = (F64_LML, F64_GRAD) if dtype == np.float64 else (F32_LML, F32_GRAD)
+    assert abs(out[0] / g['lml'] - 1) < tol_l, (out[0], g['lml'])
+    assert rel(out[1:], g['grad']) < tol_g, (out[1:], g['grad'])
+
+
+@pytest.mark.parametrize('dtype', [np.float64, np.float32])
+def test_loglik_without_gradient(dtype):
+    g = load('cpu_n2000_d3_m16')
+    p = extract(KERNELS['cpu_n2000_d3_m16']().clone_with_theta(g['theta']))
+    out, _ = gpu_loglik(g['x'], g['y'], g['nbr_fit_f32'], p, float(g['alpha']), False, dtype)
+    assert out.shape == (1,)
+    assert abs(out[0] / g['lml'] - 1) < (F64_LML if dtype == np.float64 else F32_LML)
+
+
+@pytest.mark.parametrize('m', [40, 64])
+def test_loglik_block_kernel_matches_oracle(m):
+    """m > 32 runs the one-CTA-per-point FP64 kernel."""
+    rng = np.random.default_rng(m)
+    n, d = 500, 4
+    x = rng.uniform(0, 1, (n, d))
+    y = np.stack([np.sin(4 * x[:, 0]) + x[:, 1], np.cos(3 * x[:, 2])], 1) + rng.normal(0, 0.05, (n, 2))
+    k = skk.ConstantKernel(0.8) * skk.RBF(np.array([0.3, 0.4, 0.5, 0.6])) + skk.WhiteKernel(0.02) + skk.ConstantKernel(0.1)
+    p = extract(k)
+    nbr = O.fit_neighbours(x, m, p.length_scale, np.float32)
+    want_l, want_g = O.log_marginal_likelihood(x, y, nbr, oracle_params(p), 1e-8, True)
+    for dtype in (np.float64, np.float32):
+        out, flags = gpu_loglik(x, y, nbr, p, 1e-8, True, dtype)
+        assert flags == 0
+        assert abs(out[0] / want_l - 1) < 1e-10
+        assert rel(out[1:], want_g) < 1e-9
+
+
+def test_loglik_subset_of_config2_fp32_vs_fp64_oracle():
+    """20,000 points of the n=434,874, d=3, m=32 workload: FP32 kernel vs FP64 oracle."""
+    rng = np.random.default_rng(0)
+    n = 20000
+    x = rng.uniform(-1, 1, (n, 3)) * np.array([1.0, 0.7, 0.4])
+    y = np.sin(3 * x).sum(1) + rng.normal(0, 0.05, n)
+    k = skk.ConstantKernel(1.0) * skk.RBF(0.2) + skk.WhiteKernel(1e-3)
+    p = extract(k)
+    nbr = O.fit_neighbours(x, 32, 0.2, np.float32)
+    want_l, want_g = O.log_marginal_likelihood(x, y, nbr, oracle_params(p), 1e-10, True)
+    out, flags = gpu_loglik(x, y, nbr, p, 1e-10, True, np.float32)
+    assert flags & ~_lib.NNGP_FLAG_FP64_FALLBACK == 0
+    assert abs(out[0] / want_l - 1) < F32_LML
+    assert rel(out[1:], want_g) < F32_GRAD
+    out64, _ = gpu_loglik(x, y, nbr, p, 1e-10, True, np.float64)
+    assert abs(out64[0] / want_l - 1) < F64_LML
+    assert rel(out64[1:], want_g) < F64_GRAD
+
+
+def test_fp64_fallback_on_near_singular_systems():
+    """Duplicated points and a tiny nugget: FP32 pivots collapse, the FP64 re-solve keeps the
+    result at the FP64 oracle's value and the status word says so."""
+    rng = np.random.default_rng(4)
+    base = rng.uniform(0, 1, (300, 2))
+    x = np.concatenate([base, base + 1e-7])
+    y = np.sin(5 * x[:, 0]) + rng.normal(0, 0.01, len(x))
+    p = extract(skk.ConstantKernel(1.0) * skk.RBF(0.5) + skk.WhiteKernel(1e-6))
+    nbr = O.fit_neighbours(x, 16, 0.5, np.float32)
+    want_l, want_g = O.log_marginal_likelihood(x, y, nbr, oracle_params(p), 1e-10, True)
+    out, flags = gpu_loglik(x, y, nbr, p, 1e-10, True, np.float32, pivot_tol=1e-4)
+    assert flags & _lib.NNGP_FLAG_FP64_FALLBACK
+    assert abs(out[0] / want_l - 1) < F32_LML
+
+
+def test_bad_neighbour_index_is_flagged_not_read():
+    g = load('const_n300_d2_m10')
+    p = extract(KERNELS['const_n300_d2_m10']().clone_with_theta(g['theta']))
+    nbr = g['nbr_fit_f32'].copy()
+    nbr[50, 3] = 10 ** 6
+    _, flags = gpu_loglik(g['x'], g['y'], nbr, p, 1e-6, True, np.float32)
+    assert flags & _lib.NNGP_FLAG_BAD_INDEX
+    with pytest.raises(IndexError):
+        ops.raise_on_flags(flags, 'loglik')
