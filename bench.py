@@ -51,7 +51,8 @@ ALPHA = 1e-10
 N_PRED = 100_000
 METRIC = 'fit-step loglik+grad/s'
 UNIT = 'fit-steps/s'
-WORKLOAD = 'nngp fit step, n=434874 d=3 m=32, isotropic RBF l=0.2, noise 1e-3, fp32'
+WORKLOAD = ('nngp fit step, n=434874 d=3 m=32, isotropic RBF l=0.2, noise 1e-3; '
+            'fp32 exact neighbour search, fp64 local systems (allow_downcast_f32=only-nn)')
 
 
 def make_data(n=N_TRAIN, nq=N_PRED, seed=0):
@@ -104,6 +105,18 @@ def _import_reference():
     return None, None, 'port'
 
 
+def default_cpu_workers(gb_per_worker=4.0, cap=32):
+    """Host processes for the CPU implementation: every core, but no more than the free RAM
+    allows (one reference task at this n peaks at ~2-3 GB) and at most ``cap``."""
+    cores = os.cpu_count() or 1
+    try:
+        import psutil
+        avail_gb = psutil.virtual_memory().available / 2 ** 30
+    except Exception:
+        avail_gb = 16.0
+    return max(1, min(cores, cap, int(avail_gb / gb_per_worker)))
+
+
 class CpuBaseline:
     """Times the reference's FP64 worker (``_log_likelihood_worker``, default ``only-nn``
     search) on ``cores`` processes, each processing one batch of ``rows`` points placed at
@@ -112,7 +125,7 @@ class CpuBaseline:
     def __init__(self, x, y, rows_per_task=200, cores=None, seed=1):
         NumpyNngpr, bk, kind = _import_reference()
         self.kind = kind
-        self.cores = int(cores or os.cpu_count() or 1)
+        self.cores = int(cores or default_cpu_workers())
         self.rows = rows_per_task
         self.n = x.shape[0]
         self.rng = np.random.default_rng(seed)
@@ -318,8 +331,9 @@ def run_ours(args):
     _lib.check(L.nngp_check_device(), 'nngp_check_device')
     kernel = make_kernel()
     p = extract(kernel)
-    x32 = torch.from_numpy(x).to(dev, torch.float32)
-    y32 = torch.from_numpy(y[:, None]).to(dev, torch.float32)
+    x64 = torch.from_numpy(x).to(dev, torch.float64)
+    y64 = torch.from_numpy(y[:, None]).to(dev, torch.float64)
+    x32 = x64.to(torch.float32)
     bounds = row_partition(n, world)
     r0, r1 = bounds[rank], bounds[rank + 1]
     q_rows = x32[r0:r1]
@@ -332,7 +346,7 @@ def run_ours(args):
         nbr = ops.knn(x32, q_rows, M, r0, LS, flags=flags)  # rows [r0, r1) among points [0, i)
         if ev is not None:
             ev.record()
-        ops.loglik(x32, y32, nbr, p, ALPHA, True, flags=flags, out=out, row_begin=r0)
+        ops.loglik(x64, y64, nbr, p, ALPHA, True, flags=flags, out=out, row_begin=r0)
         if world > 1:
             dist.all_reduce(out)
         return out
@@ -370,7 +384,8 @@ def run_ours(args):
     lml_val = float(out[0].item())
 
     # ---- predict throughput at 100,000 points ---------------------------------------------
-    xq32 = torch.from_numpy(xq).to(dev, torch.float32)
+    xq64 = torch.from_numpy(xq).to(dev, torch.float64)
+    xq32 = xq64.to(torch.float32)
     pred_ms = None
     if world == 1:
         for it in range(2):
@@ -378,7 +393,7 @@ def run_ours(args):
             flush.zero_()
             s0.record()
             nq = ops.knn(x32, xq32, M, None, LS, flags=flags)
-            mean, var = ops.predict(x32, y32, xq32, nq, p, ALPHA, flags=flags)
+            mean, var = ops.predict(x64, y64, xq64, nq, p, ALPHA, flags=flags)
             s1.record()
             torch.cuda.synchronize()
             pred_ms = s0.elapsed_time(s1)
@@ -386,8 +401,8 @@ def run_ours(args):
     # ---- e2e through the public API, X and y uploaded from pinned host memory per call ----
     e2e = None
     if world == 1:
-        gpr = B200Nngpr(kernel=kernel, num_nn=M, alpha=ALPHA, optimizer=None, allow_downcast_f32='yes',
-                        keep_resident=False, device=dev).fit(x, y)
+        gpr = B200Nngpr(kernel=kernel, num_nn=M, alpha=ALPHA, optimizer=None, keep_resident=False,
+                        device=dev).fit(x, y)
         theta = gpr.kernel_.theta.copy()
         for _ in range(max(1, args.warmup)):
             gpr.log_marginal_likelihood(theta, eval_gradient=True)
@@ -396,7 +411,7 @@ def run_ours(args):
         for _ in range(args.steps):
             lml_api, grad_api = gpr.log_marginal_likelihood(theta, eval_gradient=True)
         e2e_s = (time.perf_counter() - t0) / args.steps
-        h2d = int(x.shape[0] * (D + 1) * 4)  # float32 X and y
+        h2d = int(x.shape[0] * (D + 1) * 8)  # float64 X and y (the search copy is cast on the device)
         d2h = int((1 + p.n_theta + 1) * 8)  # [lml, grad..., status] in one float64 read
         e2e = {'value': 1.0 / e2e_s, 'unit': UNIT, 'h2d_bytes_per_step': h2d, 'd2h_bytes_per_step': d2h,
                'ms_per_step': e2e_s * 1e3}
@@ -411,7 +426,7 @@ def run_ours(args):
         line = {
             'metric': METRIC, 'value': 1e3 / ms_per_step, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
             'warmup': args.warmup, 'ms_per_step': ms_per_step, 'higher_is_better': True,
-            'scaling': 'strong' if world > 1 else 'weak', 'vs_baseline': None, 'dtype': 'f32',
+            'scaling': 'strong' if world > 1 else 'weak', 'vs_baseline': None, 'dtype': 'f32 search + f64 local',
             'data': 'synthetic (seeded stand-in for 3droad: shape 434874 x 3)',
             'config': {'workload': WORKLOAD, 'n': n, 'd': D, 'm': M, 'parallelism': f'rows{world}',
                        'l2': 'flushed (256 MB write) before every timed step', 'lml': lml_val},
@@ -425,7 +440,7 @@ def run_ours(args):
             'cpu_baseline': cpu,
             'predict': None if pred_ms is None else {'value': N_PRED / (pred_ms * 1e-3), 'unit': 'points/s',
                                                      'ms': pred_ms, 'n_query': N_PRED},
-            'gpu_launches': args.steps * 4,
+            'gpu_launches': args.steps * 4,  # per step: scale, search, local systems, finalize
             'clocks': clocks.summary(),
         }
         print(json.dumps(line))

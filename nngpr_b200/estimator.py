@@ -47,9 +47,10 @@ class B200Nngpr(GaussianProcessRegressor):
 
     device : str or torch.device, default 'cuda'
         The CUDA device holding the training set and running the kernels.
-    pivot_tol : float, default 1e-6
+    pivot_tol : float, default 1e-2
         With ``allow_downcast_f32='yes'``, an FP32 local system whose Cholesky pivot falls
-        below ``pivot_tol`` times the kernel diagonal is re-solved in FP64.
+        below ``pivot_tol`` times the kernel diagonal is re-solved in FP64 (1e-2 keeps the
+        log-likelihood within 1e-5 of FP64 for nuggets down to 1e-3; ``ops.DEFAULT_PIVOT_TOL``).
     keep_resident : bool, default True
         Keep the training set in HBM between calls.  ``False`` uploads it on every call, the
         reference's behaviour.
@@ -80,7 +81,7 @@ class B200Nngpr(GaussianProcessRegressor):
                  normalize_y=False, copy_X_train=True, n_targets=None, random_state=None, num_nn=None,
                  nn_type=None, batch_size=None, allow_downcast_f32=None, distribute_method=None,
                  mp_start_method=None, random_gen_batch_byte_size=None, distribute_environ=None,
-                 device=None, pivot_tol=1e-6, keep_resident=True):
+                 device=None, pivot_tol=1e-2, keep_resident=True):
         super().__init__(kernel=kernel, alpha=alpha, optimizer=optimizer,
                          n_restarts_optimizer=n_restarts_optimizer, normalize_y=normalize_y,
                          copy_X_train=copy_X_train, n_targets=n_targets, random_state=random_state)
@@ -258,7 +259,12 @@ class B200Nngpr(GaussianProcessRegressor):
         p = self._params(kernel)
         search_dt, local_dt = self._dtypes()
         x, y = self._train_tensors(local_dt)
-        xs = x if search_dt == local_dt else self._train_tensors(search_dt)[0]
+        if search_dt == local_dt:
+            xs = x
+        elif self.keep_resident:
+            xs = self._train_tensors(search_dt)[0]
+        else:
+            xs = x.to(search_dt)  # one upload per call; the search copy is cast on the device
         flags = ops.new_flags(x.device)
         nbr = self.fit_neighbours(kernel, xs, flags)
         out = ops.loglik(x, y, nbr, p, float(self.alpha), eval_gradient, self.pivot_tol, flags=flags)

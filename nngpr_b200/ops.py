@@ -16,7 +16,11 @@ import torch
 from . import _lib
 from .kernel_params import RbfParams
 
-DEFAULT_PIVOT_TOL = 1e-6
+# FP32 local systems with a Cholesky pivot (sigma^2 included) below this fraction of the kernel
+# diagonal are re-solved in FP64.  Measured on 20,000 points of the n=434,874, d=3, l=0.2,
+# noise 1e-3 workload against the FP64 oracle: 1e-3 -> 2.4e-5 relative lml error (FP32 keeps
+# the sigma^2 ~ 1e-3 systems), 3e-3 -> 6e-8, 1e-2 -> 6e-9.
+DEFAULT_PIVOT_TOL = 1e-2
 
 
 def _ptr(t):

@@ -20,7 +20,7 @@ F64_LML, F64_GRAD = 1e-10, 1e-9
 F32_LML, F32_GRAD = 1e-5, 1e-5
 
 
-def gpu_loglik(x, y, nbr, p, alpha, grad, dtype, pivot_tol=1e-6):
+def gpu_loglik(x, y, nbr, p, alpha, grad, dtype, pivot_tol=ops.DEFAULT_PIVOT_TOL):
     tdt = torch.float32 if dtype == np.float32 else torch.float64
     xt = torch.from_numpy(np.ascontiguousarray(x)).to('cuda', tdt)
     yt = torch.from_numpy(np.ascontiguousarray(y.reshape(len(y), -1))).to('cuda', tdt)
@@ -64,15 +64,19 @@ def test_loglik_block_kernel_matches_oracle(m):
     p = extract(k)
     nbr = O.fit_neighbours(x, m, p.length_scale, np.float32)
     want_l, want_g = O.log_marginal_likelihood(x, y, nbr, oracle_params(p), 1e-8, True)
-    for dtype in (np.float64, np.float32):
+    for dtype, tl, tg in ((np.float64, F64_LML, F64_GRAD), (np.float32, F32_LML, F32_GRAD)):
         out, flags = gpu_loglik(x, y, nbr, p, 1e-8, True, dtype)
         assert flags == 0
-        assert abs(out[0] / want_l - 1) < 1e-10
-        assert rel(out[1:], want_g) < 1e-9
+        assert abs(out[0] / want_l - 1) < tl
+        assert rel(out[1:], want_g) < tg
 
 
-def test_loglik_subset_of_config2_fp32_vs_fp64_oracle():
-    """20,000 points of the n=434,874, d=3, m=32 workload: FP32 kernel vs FP64 oracle."""
+def test_loglik_subset_of_config2_vs_fp64_oracle():
+    """20,000 points of the n=434,874, d=3, m=32 workload (noise 1e-3): the FP64 local
+    systems match the FP64 oracle to 1e-10; FP32 systems meet 1e-5 with the default FP64
+    re-solve threshold (1e-2 of the kernel diagonal, which covers the small-nugget pivots);
+    a 1e-6 threshold leaves FP32 systems with sigma^2 ~ 1e-3 and an error of ~2.4e-5,
+    recorded here as a bound."""
     rng = np.random.default_rng(0)
     n = 20000
     x = rng.uniform(-1, 1, (n, 3)) * np.array([1.0, 0.7, 0.4])
@@ -81,18 +85,21 @@ def test_loglik_subset_of_config2_fp32_vs_fp64_oracle():
     p = extract(k)
     nbr = O.fit_neighbours(x, 32, 0.2, np.float32)
     want_l, want_g = O.log_marginal_likelihood(x, y, nbr, oracle_params(p), 1e-10, True)
+    out64, _ = gpu_loglik(x, y, nbr, p, 1e-10, True, np.float64)
+    assert abs(out64[0] / want_l - 1) < F64_LML
+    assert rel(out64[1:], want_g) < F64_GRAD
     out, flags = gpu_loglik(x, y, nbr, p, 1e-10, True, np.float32)
     assert flags & ~_lib.NNGP_FLAG_FP64_FALLBACK == 0
     assert abs(out[0] / want_l - 1) < F32_LML
     assert rel(out[1:], want_g) < F32_GRAD
-    out64, _ = gpu_loglik(x, y, nbr, p, 1e-10, True, np.float64)
-    assert abs(out64[0] / want_l - 1) < F64_LML
-    assert rel(out64[1:], want_g) < F64_GRAD
+    out, _ = gpu_loglik(x, y, nbr, p, 1e-10, True, np.float32, pivot_tol=1e-6)
+    assert abs(out[0] / want_l - 1) < 1e-4
 
 
 def test_fp64_fallback_on_near_singular_systems():
-    """Duplicated points and a tiny nugget: FP32 pivots collapse, the FP64 re-solve keeps the
-    result at the FP64 oracle's value and the status word says so."""
+    """Duplicated points and a 1e-6 nugget: every local system is near singular; with the
+    default FP64 re-solve threshold they are re-solved in FP64, the result stays at the FP64
+    oracle's value and the status word says so."""
     rng = np.random.default_rng(4)
     base = rng.uniform(0, 1, (300, 2))
     x = np.concatenate([base, base + 1e-7])
@@ -100,9 +107,10 @@ def test_fp64_fallback_on_near_singular_systems():
     p = extract(skk.ConstantKernel(1.0) * skk.RBF(0.5) + skk.WhiteKernel(1e-6))
     nbr = O.fit_neighbours(x, 16, 0.5, np.float32)
     want_l, want_g = O.log_marginal_likelihood(x, y, nbr, oracle_params(p), 1e-10, True)
-    out, flags = gpu_loglik(x, y, nbr, p, 1e-10, True, np.float32, pivot_tol=1e-4)
+    out, flags = gpu_loglik(x, y, nbr, p, 1e-10, True, np.float32, pivot_tol=ops.DEFAULT_PIVOT_TOL)
     assert flags & _lib.NNGP_FLAG_FP64_FALLBACK
     assert abs(out[0] / want_l - 1) < F32_LML
+    assert rel(out[1:], want_g) < F32_GRAD
 
 
 def test_bad_neighbour_index_is_flagged_not_read():

@@ -20,7 +20,7 @@ pytestmark = pytest.mark.gpu
 def gpu_predict(xt, yt, xq, nbr, p, alpha, dtype):
     tdt = torch.float32 if dtype == np.float32 else torch.float64
     a = torch.from_numpy(np.ascontiguousarray(xt)).to('cuda', tdt)
-    b = torch.from_numpy(np.ascontiguousarray(yt.reshape(len(yt), -1))).to('cuda', tdt)
+    b = torch.from_numpy(np.ascontiguousarray(yt if yt.ndim == 2 else yt[:, None])).to("cuda", tdt)
     c = torch.from_numpy(np.ascontiguousarray(xq)).to('cuda', tdt)
     nb = torch.from_numpy(np.ascontiguousarray(nbr, dtype=np.int32)).cuda()
     flags = ops.new_flags(a.device)
