@@ -217,12 +217,26 @@ class ClockSampler:
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.proc = None
-        self.lines = []
+        self.lines = []  # (host time, csv line)
+        self.t_start = self.t_end = None
+
+    def mark_start(self):
+        self.t_start = time.time()
+
+    def mark_end(self):
+        self.t_end = time.time()
+
+    def wait_first_sample(self, timeout=5.0):
+        t0 = time.time()
+        while self.proc is not None and not self.lines and time.time() - t0 < timeout:
+            time.sleep(0.05)
 
     def __enter__(self):
+        if self.proc is not None:
+            return self
         try:
             self.proc = subprocess.Popen(['nvidia-smi', f'--id={self.gpu}', f'--query-gpu={self.FIELDS}',
-                                          '--format=csv,noheader,nounits', '-lms', '100'],
+                                          '--format=csv,noheader,nounits', '-lms', '50'],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -232,7 +246,7 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
 
     def __exit__(self, *exc):
         if self.proc is not None:
@@ -243,9 +257,15 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
+        """Median SM clock and the throttle reasons seen in the samples taken between
+        mark_start and mark_end (the timed steps; the sample in flight at either end included)."""
         sm, mx, reasons = [], [], set()
         names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
-        for ln in self.lines:
+        lo = (self.t_start or 0) - 0.06
+        hi = (self.t_end or time.time()) + 0.06
+        for t, ln in self.lines:
+            if not lo <= t <= hi:
+                continue
             parts = [p.strip() for p in ln.split(',')]
             if len(parts) < 9:
                 continue
@@ -305,7 +325,7 @@ def run_ours(args):
     world = int(os.environ.get('WORLD_SIZE', '1'))
     rank = int(os.environ.get('RANK', '0'))
     local_rank = int(os.environ.get('LOCAL_RANK', '0'))
-    x, y, xq = make_data()
+    x, y, xq = make_data(n=args.n)
     n = x.shape[0]
 
     cpu = None
@@ -351,6 +371,8 @@ def run_ours(args):
             dist.all_reduce(out)
         return out
 
+    clocks = ClockSampler(local_rank).__enter__()
+    clocks.wait_first_sample()
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -363,17 +385,17 @@ def run_ours(args):
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    with ClockSampler(torch.cuda.current_device() if world == 1 else local_rank) as clocks:
-        time.sleep(0.3)
+    with clocks:
+        clocks.mark_start()
         for i in range(args.steps):
             flush.zero_()
             ev[i][0].record()
             step(ev[i][1])
             ev[i][2].record()
         torch.cuda.synchronize()
+        clocks.mark_end()
         if world > 1:
             dist.barrier()
-        time.sleep(0.2)
     step_ms = [a.elapsed_time(c) for a, b, c in ev]
     knn_ms = [a.elapsed_time(b) for a, b, c in ev]
     tot_ms = float(sum(step_ms))
@@ -387,7 +409,7 @@ def run_ours(args):
     xq64 = torch.from_numpy(xq).to(dev, torch.float64)
     xq32 = xq64.to(torch.float32)
     pred_ms = None
-    if world == 1:
+    if world == 1 and not args.no_predict:
         for it in range(2):
             s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             flush.zero_()
@@ -400,7 +422,7 @@ def run_ours(args):
 
     # ---- e2e through the public API, X and y uploaded from pinned host memory per call ----
     e2e = None
-    if world == 1:
+    if world == 1 and not args.no_e2e:
         gpr = B200Nngpr(kernel=kernel, num_nn=M, alpha=ALPHA, optimizer=None, keep_resident=False,
                         device=dev).fit(x, y)
         theta = gpr.kernel_.theta.copy()
@@ -485,6 +507,10 @@ def main():
     ap.add_argument('--impl', choices=['ours', 'reference'], default='ours')
     ap.add_argument('--cpu-samples', type=int, default=2)
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--no-e2e', action='store_true', help='skip the end-to-end API timing')
+    ap.add_argument('--no-predict', action='store_true', help='skip the predict timing')
+    ap.add_argument('--n', type=int, default=N_TRAIN,
+                    help='training points (smaller cases are for profiling; the metric is quoted at 434874)')
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

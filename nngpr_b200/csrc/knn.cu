@@ -4,23 +4,31 @@
 // CUDA calc_nn kernel, cuda_kernel_accelerators.py:663-743): for each query, the num_nn refs
 // with the smallest squared distance sum_f (r_f - q_f)^2 of the length-scale-scaled points,
 // ascending, equal distances ordered by lower ref index, -1 for missing slots; with a ref cut
-// query q only sees refs [0, q + cut).
+// query q only sees refs [0, q + cut).  "Exact" means the distance of the CPU restatement:
+// x / l rounded once (correctly rounded division), then per feature one rounding for the
+// difference, the square and the running sum, features in order.
 //
-// Design:
-//   * a prep kernel writes the scaled points (x / l in the search precision, correctly
-//     rounded division) into the workspace, rows padded to DP = round_up(d, 4) floats and the
-//     ref array padded with zero rows to whole tiles, so every tile is one aligned TMA copy;
-//   * the search kernel gives every thread one query (coordinates in registers) and streams
-//     the ref tiles through shared memory with cp.async.bulk (TMA, no multicast) into a
-//     4-stage mbarrier ring; every thread reads each ref once from shared memory (broadcast);
-//   * each thread keeps its top-M list sorted in registers (M = num_nn rounded up to 8, 16,
-//     32 or 64; the unused M - num_nn leading slots hold -inf and never move), inserting with
-//     an unrolled compare/select network;
-//   * distances use one rounding per operation (__fsub_rn/__fmul_rn/__fadd_rn), the arithmetic
-//     of the CPU restatement, so the lists are bit-identical to an exact search;
-//   * prefix (fit) searches are triangular: blocks are issued heaviest first.
-// A generic kernel (lists in the workspace, any d <= 256, any num_nn, float or double) covers
-// the shapes the register kernel does not.
+// Screened kernel (d <= 32, num_nn <= 64, float):
+//   * prep kernels write, per ref, a 16-byte-aligned record [ -2 rc, |rc|^2 | r ] where r is
+//     the scaled point and rc = r - c its copy centred on the ref mean c; the records are padded
+//     to whole tiles so that every tile is one cp.async.bulk (TMA) copy into shared memory,
+//     4-stage mbarrier ring, no multicast;
+//   * one thread = one query.  Each (query, ref) pair is first SCREENED with
+//     s = |rc|^2 - 2 qc.rc (d FMAs; four pairs share one compare through min): with the current
+//     M-th best exact distance tau, the ref can only enter the list if
+//     s < tau - |qc|^2 + eps, where eps = (4d + 16) u (|qc| + max|rc|)^2 bounds the FP32 error
+//     of the screen against the exact distance (u = 2^-24).  Every ref that the exact
+//     algorithm would insert passes the screen, so the lists are bit-identical;
+//   * refs that pass are appended (tile-local index, one byte) to a per-thread candidate buffer
+//     in shared memory and merged into the sorted top-M list in registers (exact distance,
+//     unrolled compare/select insertion, strict <) in index order; merges run once per 32-ref
+//     sub-block only when a lane's buffer could overflow, and once per tile otherwise.  The
+//     threshold only decreases, so a candidate screened with a stale threshold is re-tested
+//     exactly at merge time and the insertion sequence equals the exact scan's;
+//   * top-M list: M = num_nn rounded up to 8/16/32/64; the M - num_nn leading slots hold -inf
+//     and never move; prefix (fit) searches are triangular and issue the heaviest blocks first.
+// Generic kernel (any d <= 256, any num_nn, float or double): exact distances, query
+// coordinates in shared memory, sorted lists in the workspace.
 #include <algorithm>
 #include <cstring>
 #include <string>
@@ -32,7 +40,7 @@ namespace nngp {
 
 constexpr int kKnnThreads = 128;
 constexpr int kKnnStages = 4;
-constexpr int kKnnTileBytes = 4096;
+constexpr int kCandCap = 64;  // candidate-buffer entries per thread (bytes)
 constexpr int kMaxDim = 256;
 
 template <typename T> struct LsParam {
@@ -57,55 +65,188 @@ __global__ void scale_pad_kernel(const T *__restrict__ src, int64_t n, int d, in
 }
 
 // ---------------------------------------------------------------------------------------
-// Register top-M search kernel (float)
+// Screened kernel
 // ---------------------------------------------------------------------------------------
-template <int D, int M>
-struct KnnCfg {
-    static constexpr int DP = (D + 3) / 4 * 4;
-    static constexpr int TJ = kKnnTileBytes / (DP * 4);  // refs per tile
-    static constexpr int SMEM = kKnnStages * kKnnTileBytes + 64;
+template <int D>
+struct ScreenCfg {
+    static constexpr int DP = (D + 3) / 4 * 4;  // row length of the scaled arrays
+    static constexpr int SP = (D + 1 + 3) / 4;  // float4s of the screening part
+    static constexpr int EP = (D + 3) / 4;      // float4s of the exact part
+    static constexpr int REC = SP + EP;         // float4s per ref record
+    static constexpr int TJ_RAW = 16384 / (REC * 16);
+    static constexpr int TJ = TJ_RAW >= 256 ? 256 : (TJ_RAW >= 128 ? 128 : (TJ_RAW >= 64 ? 64 : 32));
+    static constexpr int TILE_BYTES = TJ * REC * 16;
+    static constexpr int SMEM = kKnnStages * TILE_BYTES + kCandCap * kKnnThreads + 64;
 };
 
+// Per-feature sums of the scaled refs (double), for the centre c = sum / n.
+__global__ void center_sum_kernel(const float *__restrict__ xs, int64_t n, int dp, int d, double *__restrict__ acc) {
+    __shared__ double part[32][8];
+    for (int f0 = 0; f0 < d; f0 += 8) {
+        double loc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+            for (int k = 0; k < 8 && f0 + k < d; ++k) loc[k] += xs[i * dp + f0 + k];
+        for (int k = 0; k < 8; ++k) {
+            double v = warp_sum(loc[k]);
+            if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5][k] = v;
+        }
+        __syncthreads();
+        if (threadIdx.x < 8 && f0 + threadIdx.x < d) {
+            double s = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += part[w][threadIdx.x];
+            atomicAdd(acc + f0 + threadIdx.x, s);
+        }
+        __syncthreads();
+    }
+}
+
+// Records [-2 rc, |rc|^2 | r] of every (padded) ref and the max of |rc|^2 (as float bits).
+template <int D>
+__global__ void build_records_kernel(const float *__restrict__ xs, int64_t n, int64_t n_pad,
+                                     const double *__restrict__ acc, float4 *__restrict__ rec,
+                                     unsigned int *__restrict__ r2max_bits) {
+    using C = ScreenCfg<D>;
+    float c[D];
+#pragma unroll
+    for (int f = 0; f < D; ++f) c[f] = n > 0 ? (float)(acc[f] / (double)n) : 0.f;
+    float mx = 0.f;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n_pad; i += (int64_t)gridDim.x * blockDim.x) {
+        float sv[C::SP * 4], ev[C::EP * 4];
+#pragma unroll
+        for (int k = 0; k < C::SP * 4; ++k) sv[k] = 0.f;
+#pragma unroll
+        for (int k = 0; k < C::EP * 4; ++k) ev[k] = 0.f;
+        if (i < n) {
+            float nr = 0.f;
+#pragma unroll
+            for (int f = 0; f < D; ++f) {
+                const float r = xs[i * C::DP + f];
+                const float rc = r - c[f];
+                ev[f] = r;
+                sv[f] = -2.f * rc;
+                nr = fmaf(rc, rc, nr);
+            }
+            sv[D] = nr;
+            mx = fmaxf(mx, nr);
+        }
+        float4 *o = rec + i * C::REC;
+#pragma unroll
+        for (int k = 0; k < C::SP; ++k) o[k] = make_float4(sv[4 * k], sv[4 * k + 1], sv[4 * k + 2], sv[4 * k + 3]);
+#pragma unroll
+        for (int k = 0; k < C::EP; ++k) o[C::SP + k] = make_float4(ev[4 * k], ev[4 * k + 1], ev[4 * k + 2], ev[4 * k + 3]);
+    }
+    mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, 16));
+    mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, 8));
+    mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, 4));
+    mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, 2));
+    mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
+    if ((threadIdx.x & 31) == 0) atomicMax(r2max_bits, __float_as_uint(mx));  // non-negative floats order as uints
+}
+
+template <int M>
+__device__ __forceinline__ void topm_insert(float (&dist)[M], int32_t (&idx)[M], float d2, int32_t j) {
+#pragma unroll
+    for (int k = M - 1; k > 0; --k) {
+        const bool sh = d2 < dist[k - 1];
+        const bool here = d2 < dist[k];
+        const float nd = sh ? dist[k - 1] : (here ? d2 : dist[k]);
+        const int32_t ni = sh ? idx[k - 1] : (here ? j : idx[k]);
+        dist[k] = nd;
+        idx[k] = ni;
+    }
+    if (d2 < dist[0]) {
+        dist[0] = d2;
+        idx[0] = j;
+    }
+}
+
+template <int D>
+__device__ __forceinline__ float screen_score(const float4 *__restrict__ rec, const float (&qc)[D]) {
+    using C = ScreenCfg<D>;
+    float sv[C::SP * 4];
+#pragma unroll
+    for (int k = 0; k < C::SP; ++k) {
+        const float4 v = rec[k];
+        sv[4 * k] = v.x; sv[4 * k + 1] = v.y; sv[4 * k + 2] = v.z; sv[4 * k + 3] = v.w;
+    }
+    float s = sv[D];
+#pragma unroll
+    for (int f = 0; f < D; ++f) s = fmaf(qc[f], sv[f], s);
+    return s;
+}
+
+template <int D>
+__device__ __forceinline__ float exact_d2(const float4 *__restrict__ rec, const float (&qo)[D]) {
+    using C = ScreenCfg<D>;
+    float ev[C::EP * 4];
+#pragma unroll
+    for (int k = 0; k < C::EP; ++k) {
+        const float4 v = rec[C::SP + k];
+        ev[4 * k] = v.x; ev[4 * k + 1] = v.y; ev[4 * k + 2] = v.z; ev[4 * k + 3] = v.w;
+    }
+    const float t0 = sub_rn(ev[0], qo[0]);
+    float d2 = mul_rn(t0, t0);
+#pragma unroll
+    for (int f = 1; f < D; ++f) {
+        const float t = sub_rn(ev[f], qo[f]);
+        d2 = add_rn(d2, mul_rn(t, t));
+    }
+    return d2;
+}
+
 template <int D, int M>
-__global__ void __launch_bounds__(kKnnThreads) knn_topm_kernel(const float *__restrict__ refs, const float *__restrict__ qs,
-                                                               int64_t n_query, int64_t n_ref, int has_cut, int64_t cut,
-                                                               int m, int32_t *__restrict__ out,
-                                                               int32_t *__restrict__ flags) {
-    using Cfg = KnnCfg<D, M>;
-    constexpr int DP = Cfg::DP;
-    constexpr int TJ = Cfg::TJ;
+__global__ void __launch_bounds__(kKnnThreads) knn_screen_kernel(const float4 *__restrict__ recs,
+                                                                 const float *__restrict__ qs,
+                                                                 const double *__restrict__ acc,
+                                                                 const unsigned int *__restrict__ r2max_bits,
+                                                                 int64_t n_query, int64_t n_ref, int has_cut,
+                                                                 int64_t cut, int m, int32_t *__restrict__ out,
+                                                                 int32_t *__restrict__ flags) {
+    using C = ScreenCfg<D>;
+    constexpr int TJ = C::TJ;
+    constexpr int REC = C::REC;
+    constexpr unsigned FULL = 0xffffffffu;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     float4 *tiles = reinterpret_cast<float4 *>(smem_raw);
-    uint64_t *full = reinterpret_cast<uint64_t *>(smem_raw + kKnnStages * kKnnTileBytes);
+    uint8_t *cbuf = smem_raw + kKnnStages * C::TILE_BYTES;  // [kCandCap][kKnnThreads]
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem_raw + kKnnStages * C::TILE_BYTES + kCandCap * kKnnThreads);
 
-    // heaviest (latest) query blocks first for the triangular prefix search
     const int64_t qblock = has_cut ? (int64_t)(gridDim.x - 1 - blockIdx.x) : (int64_t)blockIdx.x;
     const int64_t q0 = qblock * kKnnThreads;
     const int64_t q = q0 + threadIdx.x;
     const bool active = q < n_query;
-
     auto limit_of = [&](int64_t qq) -> int64_t {
         if (!has_cut) return n_ref;
         int64_t l = qq + cut;
         return l < 0 ? 0 : (l > n_ref ? n_ref : l);
     };
     const int64_t limit = active ? limit_of(q) : 0;
-    const int64_t qlast = min(q0 + kKnnThreads, n_query) - 1;
-    const int64_t block_limit = limit_of(qlast);  // non-decreasing in q
+    const int64_t block_limit = limit_of(min(q0 + kKnnThreads, n_query) - 1);
     const int64_t ntiles = (block_limit + TJ - 1) / TJ;
 
-    float qv[D];
+    // query: exact scaled coordinates, centred copy, screening threshold offset
+    float qo[D], qc[D];
+    float nq = 0.f;
     {
-        const float4 *qp = reinterpret_cast<const float4 *>(qs + (active ? q : 0) * DP);
+        const float4 *qp = reinterpret_cast<const float4 *>(qs + (active ? q : 0) * C::DP);
 #pragma unroll
-        for (int c = 0; c < DP / 4; ++c) {
-            const float4 v = qp[c];
-            if (4 * c + 0 < D) qv[4 * c + 0] = v.x;
-            if (4 * c + 1 < D) qv[4 * c + 1] = v.y;
-            if (4 * c + 2 < D) qv[4 * c + 2] = v.z;
-            if (4 * c + 3 < D) qv[4 * c + 3] = v.w;
+        for (int k = 0; k < C::DP / 4; ++k) {
+            const float4 v = qp[k];
+            if (4 * k + 0 < D) qo[4 * k + 0] = v.x;
+            if (4 * k + 1 < D) qo[4 * k + 1] = v.y;
+            if (4 * k + 2 < D) qo[4 * k + 2] = v.z;
+            if (4 * k + 3 < D) qo[4 * k + 3] = v.w;
+        }
+#pragma unroll
+        for (int f = 0; f < D; ++f) {
+            const float cf = n_ref > 0 ? (float)(acc[f] / (double)n_ref) : 0.f;
+            qc[f] = qo[f] - cf;
+            nq = fmaf(qc[f], qc[f], nq);
         }
     }
+    const float rmax = sqrtf(__uint_as_float(*r2max_bits)) * 1.0001f;
+    const float span = sqrtf(nq) * 1.0001f + rmax;
+    const float eps = (float)(4 * D + 16) * 5.9604645e-8f * span * span;
 
     float dist[M];
     int32_t idx[M];
@@ -114,6 +255,8 @@ __global__ void __launch_bounds__(kKnnThreads) knn_topm_kernel(const float *__re
         dist[k] = (k < M - m) ? neg_inf<float>() : pos_inf<float>();
         idx[k] = -1;
     }
+    float tq = pos_inf<float>();  // screening threshold: tau - |qc|^2 + eps
+    int cnt = 0;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < kKnnStages; ++s) mbar_init(&full[s], 1);
@@ -122,10 +265,20 @@ __global__ void __launch_bounds__(kKnnThreads) knn_topm_kernel(const float *__re
     __syncthreads();
     if (threadIdx.x == 0) {
         for (int s = 0; s < kKnnStages && s < ntiles; ++s) {
-            mbar_arrive_expect_tx(&full[s], kKnnTileBytes);
-            tma_bulk_g2s(tiles + s * (kKnnTileBytes / 16), refs + (int64_t)s * TJ * DP, kKnnTileBytes, &full[s]);
+            mbar_arrive_expect_tx(&full[s], C::TILE_BYTES);
+            tma_bulk_g2s(tiles + s * (TJ * REC), recs + (int64_t)s * TJ * REC, C::TILE_BYTES, &full[s]);
         }
     }
+
+    auto merge = [&](const float4 *T, int64_t j0) {
+        for (int k = 0; k < cnt; ++k) {
+            const int jj = cbuf[k * kKnnThreads + threadIdx.x];
+            const float d2 = exact_d2<D>(T + jj * REC, qo);
+            if (d2 < dist[M - 1]) topm_insert<M>(dist, idx, d2, (int32_t)(j0 + jj));
+        }
+        cnt = 0;
+        tq = (dist[M - 1] - nq) + eps;
+    };
 
     for (int64_t t = 0; t < ntiles; ++t) {
         const int s = (int)(t % kKnnStages);
@@ -141,71 +294,45 @@ __global__ void __launch_bounds__(kKnnThreads) knn_topm_kernel(const float *__re
             __syncthreads();
             return;
         }
-        const float4 *tile = tiles + s * (kKnnTileBytes / 16);
+        const float4 *T = tiles + s * (TJ * REC);
         const int64_t j0 = t * TJ;
-        const int64_t jn = limit - j0;  // refs of this tile the thread may use
-        if (jn >= TJ) {
+        const int64_t jn64 = limit - j0;
+        const int jn = jn64 >= TJ ? TJ : (jn64 > 0 ? (int)jn64 : 0);  // refs of this tile the query may use
+        if (__all_sync(FULL, jn == TJ)) {
+            // whole tile allowed for every lane of the warp
+            for (int sb = 0; sb < TJ; sb += 32) {
 #pragma unroll 2
-            for (int jj = 0; jj < TJ; ++jj) {
-                float rv[DP];
-#pragma unroll
-                for (int c = 0; c < DP / 4; ++c) {
-                    const float4 v = tile[jj * (DP / 4) + c];
-                    rv[4 * c + 0] = v.x; rv[4 * c + 1] = v.y; rv[4 * c + 2] = v.z; rv[4 * c + 3] = v.w;
-                }
-                float d2 = mul_rn(sub_rn(rv[0], qv[0]), sub_rn(rv[0], qv[0]));
-#pragma unroll
-                for (int f = 1; f < D; ++f) {
-                    const float tf = sub_rn(rv[f], qv[f]);
-                    d2 = add_rn(d2, mul_rn(tf, tf));
-                }
-                if (d2 < dist[M - 1]) {
-                    const int32_t j = (int32_t)(j0 + jj);
-#pragma unroll
-                    for (int k = M - 1; k > 0; --k) {
-                        const bool sh = d2 < dist[k - 1];
-                        const bool here = d2 < dist[k];
-                        const float nd = sh ? dist[k - 1] : (here ? d2 : dist[k]);
-                        const int32_t ni = sh ? idx[k - 1] : (here ? j : idx[k]);
-                        dist[k] = nd;
-                        idx[k] = ni;
+                for (int g = 0; g < 32; g += 4) {
+                    const int jj = sb + g;
+                    const float s0 = screen_score<D>(T + (jj + 0) * REC, qc);
+                    const float s1 = screen_score<D>(T + (jj + 1) * REC, qc);
+                    const float s2 = screen_score<D>(T + (jj + 2) * REC, qc);
+                    const float s3 = screen_score<D>(T + (jj + 3) * REC, qc);
+                    if (fminf(fminf(s0, s1), fminf(s2, s3)) < tq) {
+                        if (s0 < tq) cbuf[(cnt++) * kKnnThreads + threadIdx.x] = (uint8_t)(jj + 0);
+                        if (s1 < tq) cbuf[(cnt++) * kKnnThreads + threadIdx.x] = (uint8_t)(jj + 1);
+                        if (s2 < tq) cbuf[(cnt++) * kKnnThreads + threadIdx.x] = (uint8_t)(jj + 2);
+                        if (s3 < tq) cbuf[(cnt++) * kKnnThreads + threadIdx.x] = (uint8_t)(jj + 3);
                     }
-                    if (d2 < dist[0]) { dist[0] = d2; idx[0] = j; }
                 }
+                if (__any_sync(FULL, cnt > kCandCap - 32)) merge(T, j0);
             }
-        } else if (jn > 0) {
-            for (int jj = 0; jj < (int)jn; ++jj) {
-                float rv[DP];
-#pragma unroll
-                for (int c = 0; c < DP / 4; ++c) {
-                    const float4 v = tile[jj * (DP / 4) + c];
-                    rv[4 * c + 0] = v.x; rv[4 * c + 1] = v.y; rv[4 * c + 2] = v.z; rv[4 * c + 3] = v.w;
+        } else {
+            // boundary tile of the prefix search: per-lane limit jn
+            for (int sb = 0; sb < TJ; sb += 32) {
+                for (int g = 0; g < 32; ++g) {
+                    const int jj = sb + g;
+                    const float s0 = screen_score<D>(T + jj * REC, qc);
+                    if (s0 < tq && jj < jn) cbuf[(cnt++) * kKnnThreads + threadIdx.x] = (uint8_t)jj;
                 }
-                float d2 = mul_rn(sub_rn(rv[0], qv[0]), sub_rn(rv[0], qv[0]));
-#pragma unroll
-                for (int f = 1; f < D; ++f) {
-                    const float tf = sub_rn(rv[f], qv[f]);
-                    d2 = add_rn(d2, mul_rn(tf, tf));
-                }
-                if (d2 < dist[M - 1]) {
-                    const int32_t j = (int32_t)(j0 + jj);
-#pragma unroll
-                    for (int k = M - 1; k > 0; --k) {
-                        const bool sh = d2 < dist[k - 1];
-                        const bool here = d2 < dist[k];
-                        const float nd = sh ? dist[k - 1] : (here ? d2 : dist[k]);
-                        const int32_t ni = sh ? idx[k - 1] : (here ? j : idx[k]);
-                        dist[k] = nd;
-                        idx[k] = ni;
-                    }
-                    if (d2 < dist[0]) { dist[0] = d2; idx[0] = j; }
-                }
+                if (__any_sync(FULL, cnt > kCandCap - 32)) merge(T, j0);
             }
         }
+        if (__any_sync(FULL, cnt > 0)) merge(T, j0);
         __syncthreads();  // every thread is done with stage s before it is refilled
         if (threadIdx.x == 0 && t + kKnnStages < ntiles) {
-            mbar_arrive_expect_tx(&full[s], kKnnTileBytes);
-            tma_bulk_g2s(tiles + s * (kKnnTileBytes / 16), refs + (t + kKnnStages) * TJ * DP, kKnnTileBytes, &full[s]);
+            mbar_arrive_expect_tx(&full[s], C::TILE_BYTES);
+            tma_bulk_g2s(tiles + s * (TJ * REC), recs + (t + kKnnStages) * TJ * REC, C::TILE_BYTES, &full[s]);
         }
     }
 
@@ -305,29 +432,39 @@ int round_d(int d) {
     return 0;
 }
 
-using TopmFn = void (*)(const float *, const float *, int64_t, int64_t, int, int64_t, int, int32_t *, int32_t *);
+using ScreenFn = void (*)(const float4 *, const float *, const double *, const unsigned int *, int64_t, int64_t, int,
+                          int64_t, int, int32_t *, int32_t *);
+using RecordFn = void (*)(const float *, int64_t, int64_t, const double *, float4 *, unsigned int *);
 
-template <int D, int M> TopmFn topm_entry() { return knn_topm_kernel<D, M>; }
-template <int D, int M> int topm_smem() { return KnnCfg<D, M>::SMEM; }
-template <int D, int M> int topm_tj() { return KnnCfg<D, M>::TJ; }
-
-struct TopmVariant {
-    TopmFn fn;
-    int smem;
-    int tj;
+struct ScreenVariant {
+    ScreenFn fn = nullptr;
+    RecordFn rec = nullptr;
+    int smem = 0, tj = 0, rec_f4 = 0, dp = 0;
 };
 
-template <int D> TopmVariant pick_m(int M) {
-    switch (M) {
-        case 8: return {topm_entry<D, 8>(), topm_smem<D, 8>(), topm_tj<D, 8>()};
-        case 16: return {topm_entry<D, 16>(), topm_smem<D, 16>(), topm_tj<D, 16>()};
-        case 32: return {topm_entry<D, 32>(), topm_smem<D, 32>(), topm_tj<D, 32>()};
-        case 64: return {topm_entry<D, 64>(), topm_smem<D, 64>(), topm_tj<D, 64>()};
-    }
-    return {nullptr, 0, 0};
+template <int D, int M> ScreenVariant make_variant() {
+    using C = ScreenCfg<D>;
+    ScreenVariant v;
+    v.fn = knn_screen_kernel<D, M>;
+    v.rec = build_records_kernel<D>;
+    v.smem = C::SMEM;
+    v.tj = C::TJ;
+    v.rec_f4 = C::REC;
+    v.dp = C::DP;
+    return v;
 }
 
-TopmVariant pick_topm(int D, int M) {
+template <int D> ScreenVariant pick_m(int M) {
+    switch (M) {
+        case 8: return make_variant<D, 8>();
+        case 16: return make_variant<D, 16>();
+        case 32: return make_variant<D, 32>();
+        case 64: return make_variant<D, 64>();
+    }
+    return ScreenVariant{};
+}
+
+ScreenVariant pick_screen(int D, int M) {
     switch (D) {
         case 1: return pick_m<1>(M);
         case 2: return pick_m<2>(M);
@@ -344,15 +481,15 @@ TopmVariant pick_topm(int D, int M) {
         case 28: return pick_m<28>(M);
         case 32: return pick_m<32>(M);
     }
-    return {nullptr, 0, 0};
+    return ScreenVariant{};
 }
 
 struct KnnPlan {
     bool fast = false;
-    int dp = 0;        // padded row length of the scaled arrays
+    int dp = 0;  // padded row length of the scaled arrays
     int64_t n_ref_pad = 0;
-    size_t off_ref = 0, off_q = 0, off_ldist = 0, off_lidx = 0, total = 0;
-    TopmVariant v{};
+    size_t off_ref = 0, off_q = 0, off_rec = 0, off_acc = 0, off_r2 = 0, off_ldist = 0, off_lidx = 0, total = 0;
+    ScreenVariant v{};
 };
 
 template <typename T>
@@ -362,11 +499,11 @@ KnnPlan make_plan(int64_t n_ref, int64_t n_query, int d, int m, bool same) {
     const int D = round_d(d);
     p.fast = std::is_same<T, float>::value && M != 0 && D != 0 && !(M == 64 && D > 16);
     if (p.fast) {
-        p.v = pick_topm(D, M);
+        p.v = pick_screen(D, M);
         p.fast = p.v.fn != nullptr;
     }
     if (p.fast) {
-        p.dp = (D + 3) / 4 * 4;
+        p.dp = p.v.dp;
         p.n_ref_pad = (n_ref + p.v.tj - 1) / p.v.tj * p.v.tj;
     } else {
         p.dp = d;
@@ -377,7 +514,14 @@ KnnPlan make_plan(int64_t n_ref, int64_t n_query, int d, int m, bool same) {
     off = align_up(off + (size_t)p.n_ref_pad * p.dp * sizeof(T), 256);
     p.off_q = same ? p.off_ref : off;
     if (!same) off = align_up(off + (size_t)n_query * p.dp * sizeof(T), 256);
-    if (!p.fast) {
+    if (p.fast) {
+        p.off_rec = off;
+        off = align_up(off + (size_t)p.n_ref_pad * p.v.rec_f4 * 16, 256);
+        p.off_acc = off;
+        off = align_up(off + (size_t)kMaxDim * sizeof(double), 256);
+        p.off_r2 = off;
+        off = align_up(off + 16, 256);
+    } else {
         p.off_ldist = off;
         off = align_up(off + (size_t)n_query * m * sizeof(T), 256);
         p.off_lidx = off;
@@ -385,6 +529,10 @@ KnnPlan make_plan(int64_t n_ref, int64_t n_query, int d, int m, bool same) {
     }
     p.total = off + 256;  // slack for base alignment
     return p;
+}
+
+int grid_for(int64_t work, int per_block = 256) {
+    return (int)std::max<int64_t>(1, std::min<int64_t>((work + per_block - 1) / per_block, (int64_t)kNumSMsB200 * 16));
 }
 
 template <typename T>
@@ -411,26 +559,36 @@ nngp_status knn_impl(const T *ref, int64_t n_ref, const T *query, int64_t n_quer
     LsParam<T> lp;
     for (int f = 0; f < d; ++f) lp.v[f] = ls ? (T)(n_ls == 1 ? ls[0] : ls[f]) : T(1);
     const int use_ls = ls != nullptr;
-    {
-        const int64_t tot = p.n_ref_pad * p.dp;
-        const int grid = (int)std::min<int64_t>((tot + 255) / 256, 148 * 16);
-        scale_pad_kernel<T><<<grid, 256, 0, stream>>>(ref, n_ref, d, p.dp, p.n_ref_pad, lp, use_ls, refs);
+    scale_pad_kernel<T><<<grid_for(p.n_ref_pad * p.dp), 256, 0, stream>>>(ref, n_ref, d, p.dp, p.n_ref_pad, lp, use_ls,
+                                                                          refs);
+    NNGP_CUDA_TRY(cudaGetLastError());
+    if (!same) {
+        scale_pad_kernel<T><<<grid_for(n_query * p.dp), 256, 0, stream>>>(query, n_query, d, p.dp, n_query, lp,
+                                                                          use_ls, qsc);
         NNGP_CUDA_TRY(cudaGetLastError());
-        if (!same) {
-            const int64_t totq = n_query * p.dp;
-            const int gq = (int)std::min<int64_t>((totq + 255) / 256, 148 * 16);
-            scale_pad_kernel<T><<<gq, 256, 0, stream>>>(query, n_query, d, p.dp, n_query, lp, use_ls, qsc);
-            NNGP_CUDA_TRY(cudaGetLastError());
-        }
     }
     if (p.fast) {
-        const int grid = (int)((n_query + kKnnThreads - 1) / kKnnThreads);
-        NNGP_CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void *>(p.v.fn),
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, p.v.smem));
-        void *args[] = {(void *)&refs, (void *)&qsc, (void *)&n_query, (void *)&n_ref, (void *)&has_cut,
-                        (void *)&cut, (void *)&m, (void *)&out, (void *)&flags};
-        NNGP_CUDA_TRY(cudaLaunchKernel(reinterpret_cast<const void *>(p.v.fn), dim3(grid), dim3(kKnnThreads), args,
-                                       (size_t)p.v.smem, stream));
+        if constexpr (std::is_same<T, float>::value) {
+            double *acc = reinterpret_cast<double *>(base + p.off_acc);
+            unsigned int *r2 = reinterpret_cast<unsigned int *>(base + p.off_r2);
+            float4 *recs = reinterpret_cast<float4 *>(base + p.off_rec);
+            NNGP_CUDA_TRY(cudaMemsetAsync(base + p.off_acc, 0, p.off_r2 + 16 - p.off_acc, stream));
+            center_sum_kernel<<<grid_for(n_ref), 256, 0, stream>>>(refs, n_ref, p.dp, d, acc);
+            NNGP_CUDA_TRY(cudaGetLastError());
+            p.v.rec<<<grid_for(p.n_ref_pad), 256, 0, stream>>>(refs, n_ref, p.n_ref_pad, acc, recs, r2);
+            NNGP_CUDA_TRY(cudaGetLastError());
+            const int grid = (int)((n_query + kKnnThreads - 1) / kKnnThreads);
+            NNGP_CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void *>(p.v.fn),
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, p.v.smem));
+            const float4 *recs_c = recs;
+            const float *q_c = qsc;
+            const double *acc_c = acc;
+            const unsigned int *r2_c = r2;
+            void *args[] = {(void *)&recs_c, (void *)&q_c, (void *)&acc_c, (void *)&r2_c, (void *)&n_query,
+                            (void *)&n_ref, (void *)&has_cut, (void *)&cut, (void *)&m, (void *)&out, (void *)&flags};
+            NNGP_CUDA_TRY(cudaLaunchKernel(reinterpret_cast<const void *>(p.v.fn), dim3(grid), dim3(kKnnThreads), args,
+                                           (size_t)p.v.smem, stream));
+        }
     } else {
         T *ldist = reinterpret_cast<T *>(base + p.off_ldist);
         int32_t *lidx = reinterpret_cast<int32_t *>(base + p.off_lidx);
