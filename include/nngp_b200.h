@@ -170,6 +170,26 @@ nngp_status nngp_loglik_rows_f64(const double *x, const double *y, int64_t n, in
                                  double *out, int32_t *status_flags, void *workspace,
                                  size_t workspace_bytes, void *stream);
 
+/*
+ * nngp_loglik_f64 without a workspace: no counterpart in the reference.
+ *
+ * For callers that cannot allocate device memory — for instance a serving process whose
+ * device memory is fixed at start-up, or a foreign-language binding (cgo, JNI, ctypes) that
+ * cannot own CUDA allocations — and so cannot pass the workspace nngp_loglik_f64 needs.
+ * The per-CTA partial sums go to a fixed device array inside the library (333 KiB, held by
+ * every GPU that loads the library until the process exits); the call allocates nothing.
+ * Same inputs, outputs and results as nngp_loglik_f64 (which it matches bit for bit on a
+ * 148-SM B200); it rejects more than 35 hyperparameters (n_theta > 35 with eval_gradient)
+ * with NNGP_ERR_UNSUPPORTED.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.  All calls share
+ * the array: calls that overlap on the GPU (other streams or host threads on the same device)
+ * race on it and must be serialised by the caller.
+ */
+nngp_status nngp_loglik_f64_noalloc(const double *x, const double *y, int64_t n, int32_t d, int32_t ydim,
+                                    const int32_t *nbr, int32_t m, const nngp_kernel *kernel,
+                                    int32_t eval_gradient, double *out, int32_t *status_flags,
+                                    void *stream);
+
 /* ---------------------------------------------------------------------------------------
  * Predictive mean / variance conditioned on the training set only
  *

@@ -24,7 +24,7 @@ EXPORTED = (
     'nngp_abi_version', 'nngp_last_error', 'nngp_status_string', 'nngp_check_device',
     'nngp_knn_workspace_size_f32', 'nngp_knn_f32', 'nngp_knn_workspace_size_f64', 'nngp_knn_f64',
     'nngp_loglik_workspace_size', 'nngp_loglik_f32', 'nngp_loglik_f64',
-    'nngp_loglik_rows_f32', 'nngp_loglik_rows_f64',
+    'nngp_loglik_rows_f32', 'nngp_loglik_rows_f64', 'nngp_loglik_f64_noalloc',
     'nngp_predict_f32', 'nngp_predict_f64', 'nngp_fma_probe',
 )
 
@@ -73,6 +73,7 @@ _SIGS = {
                              ctypes.c_int),
     'nngp_loglik_rows_f64': ([_vp, _vp, _i64, _i32, _i32, _i64, _i64, _vp, _i32, _kp, _i32, _f64, _vp, _vp, _vp, _sz, _vp],
                              ctypes.c_int),
+    'nngp_loglik_f64_noalloc': ([_vp, _vp, _i64, _i32, _i32, _vp, _i32, _kp, _i32, _vp, _vp, _vp], ctypes.c_int),
     'nngp_predict_f32': ([_vp, _vp, _i64, _vp, _i64, _i32, _i32, _vp, _i32, _kp, _f64, _vp, _vp, _vp, _vp], ctypes.c_int),
     'nngp_predict_f64': ([_vp, _vp, _i64, _vp, _i64, _i32, _i32, _vp, _i32, _kp, _f64, _vp, _vp, _vp, _vp], ctypes.c_int),
     'nngp_fma_probe': ([_vp, _i64, _i32, _vp], ctypes.c_int),

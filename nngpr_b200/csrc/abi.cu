@@ -25,6 +25,8 @@ nngp_status loglik_rows_f32(const float *, const float *, int64_t, int, int, int
                             const nngp_kernel *, int, double, double *, int32_t *, void *, size_t, cudaStream_t);
 nngp_status loglik_rows_f64(const double *, const double *, int64_t, int, int, int64_t, int64_t, const int32_t *, int,
                             const nngp_kernel *, int, double, double *, int32_t *, void *, size_t, cudaStream_t);
+nngp_status loglik_f64_noalloc(const double *, const double *, int64_t, int, int, const int32_t *, int,
+                               const nngp_kernel *, int, double *, int32_t *, cudaStream_t);
 nngp_status predict_f32(const float *, const float *, int64_t, const float *, int64_t, int, int, const int32_t *, int,
                         const nngp_kernel *, double, float *, float *, int32_t *, cudaStream_t);
 nngp_status predict_f64(const double *, const double *, int64_t, const double *, int64_t, int, int, const int32_t *,
@@ -171,6 +173,15 @@ nngp_status nngp_loglik_rows_f64(const double *x, const double *y, int64_t n, in
     return guarded([&] {
         return loglik_rows_f64(x, y, n, d, ydim, row_begin, row_count, nbr, m, kernel, eval_gradient, pivot_tol, out,
                                status_flags, workspace, workspace_bytes, as_stream(stream));
+    });
+}
+
+nngp_status nngp_loglik_f64_noalloc(const double *x, const double *y, int64_t n, int32_t d, int32_t ydim,
+                                   const int32_t *nbr, int32_t m, const nngp_kernel *kernel, int32_t eval_gradient,
+                                   double *out, int32_t *status_flags, void *stream) {
+    return guarded([&] {
+        return loglik_f64_noalloc(x, y, n, d, ydim, nbr, m, kernel, eval_gradient, out, status_flags,
+                                  as_stream(stream));
     });
 }
 

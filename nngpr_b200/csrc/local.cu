@@ -29,6 +29,7 @@
 // kernel (deterministic for a given launch shape).
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <string>
 #include <type_traits>
 
@@ -766,6 +767,74 @@ nngp_status predict_impl(const TIn *xt, const TIn *yt, int64_t nt, const TIn *xq
 }
 
 }  // namespace
+
+// ---------------------------------------------------------------------------------------
+// Allocation-free variant of the FP64 log-likelihood (nngp_loglik_f64_noalloc)
+// ---------------------------------------------------------------------------------------
+// For callers that cannot allocate device memory (and so cannot supply the workspace of
+// nngp_loglik_f64), the per-CTA partial sums live in this file-scope device array instead.
+// Every GPU that loads the library holds it (kStaticBlocks * kStaticSlots doubles = 333 KiB)
+// until the process exits.  All calls share it: calls that overlap on the GPU (different
+// streams, or different host threads on one device) race on it.  Each launch writes every slot
+// it later reads, so nothing has to be cleared between calls.
+constexpr int kStaticBlocks = 1184;  // the local kernels' largest grid on a 148-SM B200
+constexpr int kStaticSlots = 36;     // 1 + n_theta: up to 35 hyperparameters
+static __device__ __align__(256) double g_loglik_scratch[kStaticBlocks * kStaticSlots];
+
+namespace {
+std::mutex g_scratch_mu;
+double *g_scratch_addr[64] = {};
+
+// Device address of g_loglik_scratch on the current device (looked up once per device;
+// in host code the symbol itself is only a host-side stand-in, never a device address).
+nngp_status static_scratch(double **out) {
+    int dev = -1;
+    NNGP_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail(NNGP_ERR_UNSUPPORTED, "device ordinal above 63");
+    std::lock_guard<std::mutex> lock(g_scratch_mu);
+    if (!g_scratch_addr[dev]) {
+        void *p = nullptr;
+        NNGP_CUDA_TRY(cudaGetSymbolAddress(&p, g_loglik_scratch));
+        g_scratch_addr[dev] = static_cast<double *>(p);
+    }
+    *out = g_scratch_addr[dev];
+    return NNGP_OK;
+}
+}  // namespace
+
+nngp_status loglik_f64_noalloc(const double *x, const double *y, int64_t n, int d, int ydim, const int32_t *nbr, int m,
+                               const nngp_kernel *k, int eval_gradient, double *out, int32_t *flags,
+                               cudaStream_t stream) {
+    if (n < 0) return fail(NNGP_ERR_INVALID_ARGUMENT, "loglik_noalloc: n < 0");
+    if (!out) return fail(NNGP_ERR_INVALID_ARGUMENT, "loglik_noalloc: out is null");
+    const bool grad = eval_gradient != 0;
+    LocalArgs a;
+    nngp_status st = fill_args(a, k, d, ydim, m, n, n, 0.0, grad);
+    if (st != NNGP_OK) return st;
+    const int nt = 1 + (grad ? a.n_theta : 0);
+    if (nt > kStaticSlots)
+        return fail(NNGP_ERR_UNSUPPORTED, "loglik_noalloc: " + std::to_string(nt - 1) +
+                                              " hyperparameters; the static scratch holds at most " +
+                                              std::to_string(kStaticSlots - 1));
+    if (n == 0) {
+        NNGP_CUDA_TRY(cudaMemsetAsync(out, 0, nt * sizeof(double), stream));
+        return NNGP_OK;
+    }
+    if (!x || !y || (m > 0 && !nbr)) return fail(NNGP_ERR_INVALID_ARGUMENT, "loglik_noalloc: null input pointer");
+    double *block_out = nullptr;
+    st = static_scratch(&block_out);
+    if (st != NNGP_OK) return st;
+    LocalPlan pl = plan_local(n, d, m, a.n_theta, grad);
+    pl.grid = std::min(pl.grid, kStaticBlocks);  // the kernels stride over the points
+    if (grad)
+        st = launch_local<double, true, false>(pl, a, x, y, x, y, nbr, block_out, nullptr, nullptr, flags, stream);
+    else
+        st = launch_local<double, false, false>(pl, a, x, y, x, y, nbr, block_out, nullptr, nullptr, flags, stream);
+    if (st != NNGP_OK) return st;
+    finalize_kernel<<<1, 256, 0, stream>>>(block_out, pl.grid, pl.nt, out);
+    NNGP_CUDA_TRY(cudaGetLastError());
+    return NNGP_OK;
+}
 
 size_t loglik_workspace(int64_t n, int d, int ydim, int m, int n_theta) {
     (void)ydim;
