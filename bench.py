@@ -69,14 +69,6 @@ def make_kernel():
     return skk.ConstantKernel(1.0) * skk.RBF(LS) + skk.WhiteKernel(NOISE)
 
 
-def row_partition(n, world, pairs_exponent=0.5):
-    """Row boundaries with equal prefix-search pair counts: rank r gets rows
-    [n sqrt(r / R), n sqrt((r + 1) / R))."""
-    b = [int(round(n * (r / world) ** pairs_exponent)) for r in range(world + 1)]
-    b[0], b[-1] = 0, n
-    return b
-
-
 # ------------------------------------------------------------------------------------------
 # CPU baseline: the reference's NumpyNngpr on a bounded sample of rows
 # ------------------------------------------------------------------------------------------
@@ -346,6 +338,7 @@ def run_ours(args):
 
     from nngpr_b200 import B200Nngpr, _lib, ops
     from nngpr_b200.kernel_params import extract
+    from nngpr_b200.sharding import fit_step_rows, row_partition
 
     L = _lib.lib()
     _lib.check(L.nngp_check_device(), 'nngp_check_device')
@@ -363,10 +356,12 @@ def run_ours(args):
     stream = torch.cuda.current_stream()
 
     def step(ev=None):
-        nbr = ops.knn(x32, q_rows, M, r0, LS, flags=flags)  # rows [r0, r1) among points [0, i)
-        if ev is not None:
+        if ev is None:
+            fit_step_rows(x32, x64, y64, p, ALPHA, M, r0, r1, LS, flags=flags, out=out)
+        else:  # the same two calls, with an event between them to time the search alone
+            nbr = ops.knn(x32, q_rows, M, r0, LS, flags=flags)  # rows [r0, r1) among points [0, i)
             ev.record()
-        ops.loglik(x64, y64, nbr, p, ALPHA, True, flags=flags, out=out, row_begin=r0)
+            ops.loglik(x64, y64, nbr, p, ALPHA, True, flags=flags, out=out, row_begin=r0)
         if world > 1:
             dist.all_reduce(out)
         return out

@@ -1,0 +1,47 @@
+"""Row sharding of one fit step across ranks (one process per GPU).
+
+The fit-step log-likelihood is a sum over points, and point i's term depends only on X, y
+and its neighbours among points [0, i) (``base_nngpr.py:453-614``).  A rank therefore owns a
+contiguous row range: it searches its rows against the prefix (``ref_cut_index = row_begin``,
+the reference's own batching rule, ``base_nngpr.py:530-535``), solves their local systems
+(``nngp_loglik_rows_*``) and contributes a (1 + n_theta) partial sum; one all-reduce per step
+gives every rank the full value and gradient.  X and y are replicated.
+
+Rows are split so that the prefix-search pair counts (row i scans i refs) are equal:
+rank r owns ``[n sqrt(r / R), n sqrt((r + 1) / R))``.
+"""
+
+from __future__ import annotations
+
+import math
+
+
+def row_partition(n: int, world: int) -> list[int]:
+    """Boundaries ``b[0] = 0 <= b[1] <= ... <= b[world] = n`` with equal pair counts."""
+    if world < 1:
+        raise ValueError('world must be >= 1')
+    b = [int(round(n * math.sqrt(r / world))) for r in range(world + 1)]
+    b[0], b[-1] = 0, n
+    for r in range(1, world + 1):
+        b[r] = max(b[r], b[r - 1])
+    return b
+
+
+def prefix_pairs(r0: int, r1: int) -> int:
+    """Prefix-search pairs of rows [r0, r1): sum of i for i in [r0, r1)."""
+    return (r1 * (r1 - 1) - r0 * (r0 - 1)) // 2
+
+
+def fit_step_rows(x_search, x, y, p, alpha, num_nn, row_begin, row_end, length_scale, eval_gradient=True,
+                  pivot_tol=None, flags=None, out=None):
+    """This rank's partial [lml, grad...] of one fit step on the device (torch tensors).
+
+    ``x_search`` is the search copy of X (float32 for the default precision), ``x``/``y`` the
+    local-system copies; rows ``[row_begin, row_end)``.  The caller all-reduces the result.
+    """
+    from . import ops
+    q = x_search[row_begin:row_end]
+    m = min(num_nn, max(x_search.shape[0] - 1, 0))
+    nbr = ops.knn(x_search, q, m, row_begin, length_scale, flags=flags)
+    kw = {} if pivot_tol is None else {'pivot_tol': pivot_tol}
+    return ops.loglik(x, y, nbr, p, alpha, eval_gradient, flags=flags, out=out, row_begin=row_begin, **kw)
