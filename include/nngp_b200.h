@@ -221,6 +221,13 @@ nngp_status nngp_predict_f64(const double *x_train, const double *y_train, int64
  * ------------------------------------------------------------------------------------- */
 nngp_status nngp_fma_probe(float *out, int64_t iters, int32_t blocks, void *stream);
 
+/* Self-test of the tensor-core operand layout used by the search (no counterpart in the
+ * reference): d (128 x 128) = a (128 x kp) * b (128 x kp)^T in TF32 with FP32 accumulation,
+ * a and b row-major device arrays, kp = 8, 16 or 32, through the same shared-memory layout,
+ * descriptors, tcgen05.mma and TMEM reads as the search kernel.  One CTA. */
+nngp_status nngp_tc_layout_selftest(const float *a, const float *b, int32_t kp, float *d, int32_t *status_flags,
+                                    void *stream);
+
 #ifdef __cplusplus
 }
 #endif

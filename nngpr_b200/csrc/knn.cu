@@ -30,11 +30,14 @@
 // Generic kernel (any d <= 256, any num_nn, float or double): exact distances, query
 // coordinates in shared memory, sorted lists in the workspace.
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <type_traits>
 
 #include "common.cuh"
+#include "knn_tc.cuh"
 
 namespace nngp {
 
@@ -357,7 +360,7 @@ __global__ void __launch_bounds__(kGenThreads) knn_generic_kernel(const T *__res
                                                                   int has_cut, int64_t cut, int m,
                                                                   T *__restrict__ ldist, int32_t *__restrict__ lidx,
                                                                   int32_t *__restrict__ out) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     T *qsm = reinterpret_cast<T *>(smem_raw);           // d x kGenThreads
     T *tile = qsm + (size_t)d * kGenThreads;            // kGenTile x dp
     const int64_t qblock = has_cut ? (int64_t)(gridDim.x - 1 - blockIdx.x) : (int64_t)blockIdx.x;
@@ -484,12 +487,35 @@ ScreenVariant pick_screen(int D, int M) {
     return ScreenVariant{};
 }
 
+enum class KnnPath { Tc, Simt, Generic };
+
+// Search kernel: the tensor-core screen for d >= 12 (or when the SIMT screen has no variant),
+// else the SIMT screen, else the generic kernel.  NNGP_KNN_KERNEL=tc|simt|generic forces a
+// kernel where the shape has one (testing and comparisons); unset or any other value selects
+// automatically.
+KnnPath choose_path(int d, int m, bool is_float) {
+    const char *env = std::getenv("NNGP_KNN_KERNEL");
+    const std::string want = env ? env : "auto";
+    const int M = round_m(m), D = round_d(d);
+    const bool tc_ok = is_float && D != 0 && M != 0 && M <= 32 && tc_variant(D, M).fn != nullptr;
+    const bool simt_ok = is_float && D != 0 && M != 0 && !(M == 64 && D > 16);
+    if (want == "generic") return KnnPath::Generic;
+    if (want == "simt") return simt_ok ? KnnPath::Simt : KnnPath::Generic;
+    if (want == "tc" && tc_ok) return KnnPath::Tc;
+    // measured on B200: the SIMT screen wins at small d (cheap distances), the tensor-core
+    // screen from d >= 12 on
+    if (tc_ok && (D >= 12 || !simt_ok)) return KnnPath::Tc;
+    return simt_ok ? KnnPath::Simt : KnnPath::Generic;
+}
+
 struct KnnPlan {
-    bool fast = false;
+    KnnPath path = KnnPath::Generic;
     int dp = 0;  // padded row length of the scaled arrays
     int64_t n_ref_pad = 0;
-    size_t off_ref = 0, off_q = 0, off_rec = 0, off_acc = 0, off_r2 = 0, off_ldist = 0, off_lidx = 0, total = 0;
+    size_t off_ref = 0, off_q = 0, off_rec = 0, off_acc = 0, off_r2 = 0, off_ctr = 0, off_ldist = 0, off_lidx = 0,
+           total = 0;
     ScreenVariant v{};
+    tc::TcVariant tv{};
 };
 
 template <typename T>
@@ -497,12 +523,13 @@ KnnPlan make_plan(int64_t n_ref, int64_t n_query, int d, int m, bool same) {
     KnnPlan p;
     const int M = round_m(m);
     const int D = round_d(d);
-    p.fast = std::is_same<T, float>::value && M != 0 && D != 0 && !(M == 64 && D > 16);
-    if (p.fast) {
+    p.path = choose_path(d, m, std::is_same<T, float>::value);
+    if (p.path == KnnPath::Tc) {
+        p.tv = tc_variant(D, M);
+        p.dp = p.tv.dp;
+        p.n_ref_pad = (n_ref + tc::kTcRefTile - 1) / tc::kTcRefTile * tc::kTcRefTile;
+    } else if (p.path == KnnPath::Simt) {
         p.v = pick_screen(D, M);
-        p.fast = p.v.fn != nullptr;
-    }
-    if (p.fast) {
         p.dp = p.v.dp;
         p.n_ref_pad = (n_ref + p.v.tj - 1) / p.v.tj * p.v.tj;
     } else {
@@ -514,12 +541,16 @@ KnnPlan make_plan(int64_t n_ref, int64_t n_query, int d, int m, bool same) {
     off = align_up(off + (size_t)p.n_ref_pad * p.dp * sizeof(T), 256);
     p.off_q = same ? p.off_ref : off;
     if (!same) off = align_up(off + (size_t)n_query * p.dp * sizeof(T), 256);
-    if (p.fast) {
+    if (p.path != KnnPath::Generic) {
         p.off_rec = off;
-        off = align_up(off + (size_t)p.n_ref_pad * p.v.rec_f4 * 16, 256);
+        const size_t rec_bytes = p.path == KnnPath::Tc ? (size_t)(p.n_ref_pad / tc::kTcRefTile) * p.tv.stage_bytes
+                                                        : (size_t)p.n_ref_pad * p.v.rec_f4 * 16;
+        off = align_up(off + rec_bytes, 1024);
         p.off_acc = off;
         off = align_up(off + (size_t)kMaxDim * sizeof(double), 256);
         p.off_r2 = off;
+        off = align_up(off + 16, 256);
+        p.off_ctr = off;
         off = align_up(off + 16, 256);
     } else {
         p.off_ldist = off;
@@ -527,8 +558,20 @@ KnnPlan make_plan(int64_t n_ref, int64_t n_query, int d, int m, bool same) {
         p.off_lidx = off;
         off = align_up(off + (size_t)n_query * m * sizeof(int32_t), 256);
     }
-    p.total = off + 256;  // slack for base alignment
+    p.total = off + 1024;  // slack for base alignment
     return p;
+}
+
+int num_sms_knn() {
+    static int cached = 0;
+    if (!cached) {
+        int dev = 0, v = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && v > 0)
+            cached = v;
+        else
+            cached = kNumSMsB200;
+    }
+    return cached;
 }
 
 int grid_for(int64_t work, int per_block = 256) {
@@ -552,7 +595,7 @@ nngp_status knn_impl(const T *ref, int64_t n_ref, const T *query, int64_t n_quer
     const bool same = (ref == query) && (n_ref == n_query);
     KnnPlan p = make_plan<T>(n_ref, n_query, d, m, same);
     if (!ws || ws_bytes < p.total) return fail(NNGP_ERR_WORKSPACE, "knn: workspace missing or too small");
-    char *base = reinterpret_cast<char *>(align_up(reinterpret_cast<uintptr_t>(ws), 256));
+    char *base = reinterpret_cast<char *>(align_up(reinterpret_cast<uintptr_t>(ws), 1024));
     T *refs = reinterpret_cast<T *>(base + p.off_ref);
     T *qsc = reinterpret_cast<T *>(base + p.off_q);
 
@@ -567,7 +610,41 @@ nngp_status knn_impl(const T *ref, int64_t n_ref, const T *query, int64_t n_quer
                                                                           use_ls, qsc);
         NNGP_CUDA_TRY(cudaGetLastError());
     }
-    if (p.fast) {
+    if (p.path == KnnPath::Tc) {
+        if constexpr (std::is_same<T, float>::value) {
+            double *acc = reinterpret_cast<double *>(base + p.off_acc);
+            unsigned int *r2 = reinterpret_cast<unsigned int *>(base + p.off_r2);
+            int *ctr = reinterpret_cast<int *>(base + p.off_ctr);
+            unsigned char *tiles = reinterpret_cast<unsigned char *>(base + p.off_rec);
+            NNGP_CUDA_TRY(cudaMemsetAsync(base + p.off_acc, 0, p.off_ctr + 16 - p.off_acc, stream));
+            center_sum_kernel<<<grid_for(n_ref), 256, 0, stream>>>(refs, n_ref, p.dp, d, acc);
+            NNGP_CUDA_TRY(cudaGetLastError());
+            p.tv.build<<<grid_for(p.n_ref_pad), 256, 0, stream>>>(refs, n_ref, p.n_ref_pad, acc, tiles, r2);
+            NNGP_CUDA_TRY(cudaGetLastError());
+            NNGP_CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void *>(p.tv.fn),
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, p.tv.smem));
+            NNGP_CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void *>(p.tv.fn),
+                                               cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+            const int64_t n_items = (n_query + tc::kTcQueryTile - 1) / tc::kTcQueryTile;
+            int per_sm = 1;
+            NNGP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, p.tv.fn, tc::kTcThreads,
+                                                                        (size_t)p.tv.smem));
+            per_sm = std::max(1, std::min(per_sm, 2));  // two CTAs x 256 TMEM columns fill an SM
+            const int grid = (int)std::min<int64_t>(n_items, (int64_t)num_sms_knn() * per_sm);
+            if (const char *dbg = std::getenv("NNGP_KNN_DEBUG"); dbg && dbg[0] == '1')
+                std::fprintf(stderr, "nngp_knn: tensor-core path d=%d m=%d items=%lld ctas/sm=%d grid=%d smem=%d\n", d,
+                             m, (long long)n_items, per_sm, grid, p.tv.smem);
+            const unsigned char *tiles_c = tiles;
+            const float *q_c = qsc;
+            const double *acc_c = acc;
+            const unsigned int *r2_c = r2;
+            void *args[] = {(void *)&tiles_c, (void *)&q_c, (void *)&acc_c, (void *)&r2_c, (void *)&ctr,
+                            (void *)&n_query, (void *)&n_ref, (void *)&has_cut, (void *)&cut, (void *)&m,
+                            (void *)&out, (void *)&flags};
+            NNGP_CUDA_TRY(cudaLaunchKernel(reinterpret_cast<const void *>(p.tv.fn), dim3(grid),
+                                           dim3(tc::kTcThreads), args, (size_t)p.tv.smem, stream));
+        }
+    } else if (p.path == KnnPath::Simt) {
         if constexpr (std::is_same<T, float>::value) {
             double *acc = reinterpret_cast<double *>(base + p.off_acc);
             unsigned int *r2 = reinterpret_cast<unsigned int *>(base + p.off_r2);

@@ -1,0 +1,630 @@
+// Exact k-nearest-neighbour search with a tensor-core (tcgen05) screen, B200 (sm_100a).
+//
+// Same contract and results as the screened SIMT kernel in knn.cu (exact lists: the FP32
+// distance of the CPU restatement, ascending, lower index first on ties, -1 padding, ref cut).
+// What changes is who computes the screening scores s_qr = |rc|^2 - 2 qc.rc (centred
+// coordinates, the candidate test being s < tau - |qc|^2 + eps) and how candidates are merged:
+//
+//   * the scores of a 128-query x 128-ref tile are one UMMA product D = A B^T in TMEM
+//     (tcgen05.mma kind::tf32, M=128, N=128, FP32 accumulate).  To keep FP32-level accuracy each
+//     operand a = a_hi + a_lo is split (a_hi = a rounded to TF32, a_lo = a - a_hi, exact), and
+//     A' = [a_hi | a_hi | a_lo], B' = [b_hi | b_lo | b_hi] (each block d+1 wide: the d centred
+//     coordinates and the 1 / |rc|^2 column) so that A' B'^T = a_hi b_hi + a_hi b_lo + a_lo b_hi.
+//     The dropped and truncated terms are below 2^-21 |a||b| per product, the FP32 accumulation
+//     adds at most K' ulps; eps = 2^-16 (|qc| + max|rc|)^2 covers both with a margin of 4 or more,
+//     so every ref the exact algorithm inserts still passes the screen;
+//   * persistent CTAs (work items = query tiles handed out heaviest first through a global
+//     counter), 160 threads: warp 4 allocates TMEM (256 columns = two 128-column accumulators) and
+//     one of its lanes issues the TMA bulk copies of ref tiles into a shared-memory ring (operands
+//     and exact coordinates in one copy) and the MMAs; warps 0-3 are the epilogue, warp w owning
+//     query rows 32w..32w+31 (its TMEM lane quadrant).  Two CTAs share an SM when shared memory
+//     allows (small d), so that each scheduler has two epilogue warps;
+//   * epilogue: each 32-column chunk of a row is one tcgen05.ld, screened with three-input min
+//     against the row's threshold (a rolled loop: the code stays small enough for the instruction
+//     cache); when a chunk has candidates each lane walks its own candidate columns, one per warp
+//     iteration, and rescores them exactly (exact coordinates from the same smem stage, the
+//     oracle's arithmetic), the survivors are compacted into a per-warp queue with ballots, and the warp
+//     inserts them cooperatively into the rows' top-32 lists kept in shared memory (one list slot
+//     per lane: ballot of "entry < candidate" in (distance, index) order gives the position,
+//     shfl_up shifts the tail) — converged, order independent, ties by lower index;
+//   * mbarriers: b_full (TMA -> MMA), b_empty (MMA commit + 4 epilogue warps -> producer),
+//     t_full (MMA commit -> epilogue), t_empty (4 epilogue warps -> MMA), a_ready (query operand
+//     written by the epilogue -> MMA).  Every wait is bounded; on a timeout the CTA raises
+//     NNGP_FLAG_TIMEOUT, drains what it issued (bounded), frees TMEM and returns.
+// No TMA multicast and no cluster launch.
+#include <algorithm>
+#include <string>
+#include <type_traits>
+
+#include "common.cuh"
+#include "knn_tc.cuh"
+
+namespace nngp {
+namespace tc {
+
+constexpr int QT = kTcQueryTile;  // queries per tile (UMMA M)
+constexpr int RT = kTcRefTile;    // refs per tile (UMMA N)
+constexpr int EPI_WARPS = 4;      // one per TMEM lane quadrant
+constexpr int THREADS = (EPI_WARPS + 1) * 32;
+static_assert(THREADS == kTcThreads, "thread count");
+constexpr int LIST = 32;       // list slots per query (one per lane); num_nn <= 32
+constexpr int QCAP = 512;      // candidate queue entries per epilogue warp
+constexpr uint32_t TMEM_COLS = 2 * RT;
+constexpr float kEpsTc = 1.52587890625e-05f;       // 2^-16
+constexpr float kPadNorm = 1.7014118346046923e38f;  // 2^127: padded refs never pass a finite screen
+
+template <int D>
+struct Cfg {
+    static constexpr int U = D + 1;                 // coordinates + the norm column
+    static constexpr int KP = (3 * U + 7) / 8 * 8;  // split operand width (tf32), multiple of 8
+    static constexpr int NMMA = KP / 8;             // UMMA K = 8 for tf32
+    static constexpr int DP = (D + 3) / 4 * 4;      // exact-coordinate row length
+    static constexpr int OP_BYTES = RT * KP * 4;    // B operand block of a ref tile
+    static constexpr int EX_BYTES = RT * DP * 4;    // exact coordinates of a ref tile
+    static constexpr int STAGE_BYTES = OP_BYTES + EX_BYTES;
+    static constexpr int A_BYTES = QT * KP * 4;
+    static constexpr int LIST_BYTES = QT * LIST * 8;                 // distances + indices
+    static constexpr int QUEUE_BYTES = EPI_WARPS * QCAP * (4 + 4 + 1);
+    static constexpr int BAR_BYTES = 256;
+    static constexpr int FIXED = 1024 + A_BYTES + LIST_BYTES + QUEUE_BYTES + BAR_BYTES;
+    // two CTAs per SM if at least 3 stages fit in half an SM's shared memory, else one CTA
+    static constexpr int HALF_SM = 112 * 1024;
+    static constexpr int ST2 = (HALF_SM - FIXED) / STAGE_BYTES;
+    static constexpr int ST1 = (220 * 1024 - FIXED) / STAGE_BYTES;
+    static constexpr int STAGES = ST2 >= 3 ? (ST2 > 4 ? 4 : ST2) : (ST1 > 4 ? 4 : ST1);
+    static constexpr int SMEM = FIXED + STAGES * STAGE_BYTES;
+    static constexpr int CTAS_PER_SM = ST2 >= 3 ? 2 : 1;
+    static_assert(STAGES >= 2, "ref tile too large for two stages");
+    // K-major no-swizzle canonical layout: 8-row x 16-byte core matrices, SBO = 128 B between
+    // 8-row groups, LBO between 16-byte K chunks
+    static constexpr uint32_t A_LBO = (QT / 8) * 128;
+    static constexpr uint32_t B_LBO = (RT / 8) * 128;
+};
+
+// byte offset of element (row, k) of a K-major, no-swizzle UMMA operand with `rows` rows
+__host__ __device__ __forceinline__ uint32_t op_offset(int row, int k, int rows) {
+    return (uint32_t)((k >> 2) * (rows / 8) * 128 + (row >> 3) * 128 + (row & 7) * 16 + (k & 3) * 4);
+}
+
+__device__ __forceinline__ float tf32_round(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;  // descriptor version for sm_100
+    return d;                // base offset 0, lbo mode 0, layout SWIZZLE_NONE
+}
+
+// instruction descriptor: F32 accumulate, TF32 A and B, both K-major, N = RT, M = QT
+constexpr uint32_t kIdesc =
+    (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(RT >> 3) << 17) | ((uint32_t)(QT >> 4) << 24);
+
+__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_addr(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// 32 columns of this thread's TMEM lane, no wait (the caller issues tcgen05.wait::ld)
+__device__ __forceinline__ void tmem_ld32_nowait(uint32_t taddr, uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+__device__ __forceinline__ float min3f(float a, float b, float c) {
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
+// Ref tiles in global memory: per tile [B' operand block (UMMA layout) | exact coordinates (RT x DP)].
+// xs: scaled refs (n_pad x DP, zero padded); acc: per-feature sums for the centre.
+template <int D>
+__global__ void build_tc_tiles_kernel(const float *__restrict__ xs, int64_t n, int64_t n_pad,
+                                      const double *__restrict__ acc, unsigned char *__restrict__ tiles,
+                                      unsigned int *__restrict__ r2max_bits) {
+    using C = Cfg<D>;
+    float c[D];
+#pragma unroll
+    for (int f = 0; f < D; ++f) c[f] = n > 0 ? (float)(acc[f] / (double)n) : 0.f;
+    float mx = 0.f;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n_pad; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t t = i / RT;
+        const int row = (int)(i - t * RT);
+        unsigned char *base = tiles + t * C::STAGE_BYTES;
+        float b[C::U];
+        float ex[C::DP];
+#pragma unroll
+        for (int k = 0; k < C::DP; ++k) ex[k] = 0.f;
+        if (i < n) {
+            float nr = 0.f;
+#pragma unroll
+            for (int f = 0; f < D; ++f) {
+                const float r = xs[i * C::DP + f];
+                const float rc = r - c[f];
+                ex[f] = r;
+                b[f] = -2.f * rc;
+                nr = fmaf(rc, rc, nr);
+            }
+            b[D] = nr;
+            mx = fmaxf(mx, nr);
+        } else {
+#pragma unroll
+            for (int f = 0; f < D; ++f) b[f] = 0.f;
+            b[D] = kPadNorm;
+        }
+        float *op = reinterpret_cast<float *>(base);
+        for (int k = 0; k < C::KP; ++k) {
+            float v = 0.f;
+            const int blk = k / C::U, f = k - blk * C::U;
+            if (blk < 3) {
+                const float hi = tf32_round(b[f]);
+                v = (blk == 1) ? (b[f] - hi) : hi;  // [b_hi | b_lo | b_hi]
+            }
+            op[op_offset(row, k, RT) / 4] = v;
+        }
+        float *exo = reinterpret_cast<float *>(base + C::OP_BYTES) + row * C::DP;
+#pragma unroll
+        for (int k = 0; k < C::DP; ++k) exo[k] = ex[k];
+    }
+    mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, 16));
+    mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, 8));
+    mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, 4));
+    mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, 2));
+    mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
+    if ((threadIdx.x & 31) == 0) atomicMax(r2max_bits, __float_as_uint(mx));
+}
+
+template <int D>
+__global__ void __launch_bounds__(THREADS, Cfg<D>::CTAS_PER_SM) knn_tc_kernel(const unsigned char *__restrict__ tiles_g,
+                                                         const float *__restrict__ qs,
+                                                         const double *__restrict__ acc,
+                                                         const unsigned int *__restrict__ r2max_bits,
+                                                         int *__restrict__ work_counter, int64_t n_query,
+                                                         int64_t n_ref, int has_cut, int64_t cut, int m,
+                                                         int32_t *__restrict__ out, int32_t *__restrict__ flags) {
+    using C = Cfg<D>;
+    constexpr int S = C::STAGES;
+    constexpr unsigned FULL = 0xffffffffu;
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char *sm =
+        reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    unsigned char *sA = sm;
+    unsigned char *sB = sA + C::A_BYTES;
+    float *Ld = reinterpret_cast<float *>(sB + S * C::STAGE_BYTES);  // [QT][LIST]
+    int32_t *Li = reinterpret_cast<int32_t *>(Ld + QT * LIST);      // [QT][LIST]
+    unsigned char *qbase = reinterpret_cast<unsigned char *>(Li + QT * LIST);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(qbase + C::QUEUE_BYTES);
+    uint64_t *b_full = bars;        // [S <= 4]
+    uint64_t *b_empty = bars + 4;   // [S <= 4]
+    uint64_t *t_full = bars + 8;    // [2]
+    uint64_t *t_empty = bars + 10;  // [2]
+    uint64_t *a_ready = bars + 12;  // [1]
+    volatile uint32_t *tmem_slot = reinterpret_cast<volatile uint32_t *>(bars + 14);
+    volatile int *s_item = reinterpret_cast<volatile int *>(bars + 15);
+    volatile int *s_abort = reinterpret_cast<volatile int *>(bars + 16);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const bool producer_warp = warp == EPI_WARPS;
+    const int64_t n_items = (n_query + QT - 1) / QT;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; ++s) {
+            mbar_init(&b_full[s], 1);
+            mbar_init(&b_empty[s], 1 + EPI_WARPS);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&t_full[b], 1);
+            mbar_init(&t_empty[b], EPI_WARPS);
+        }
+        mbar_init(a_ready, EPI_WARPS * 32);
+        *s_abort = 0;
+        fence_mbar_init();
+    }
+    if (producer_warp) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_addr(const_cast<uint32_t *>(tmem_slot))),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+    const float rmax = sqrtf(__uint_as_float(*r2max_bits)) * 1.0001f;
+
+    uint32_t g_tile = 0;  // tiles this CTA has streamed (phases of the ring and TMEM buffers)
+    uint32_t it = 0;      // work items this CTA has processed (phase of a_ready)
+    bool aborted = false;
+    uint32_t tma_issued = 0, tma_landed = 0;  // producer lane: copies issued / waited for (drain on abort)
+
+    auto limit_of = [&](int64_t qq) -> int64_t {
+        if (!has_cut) return n_ref;
+        int64_t l = qq + cut;
+        return l < 0 ? 0 : (l > n_ref ? n_ref : l);
+    };
+
+    while (true) {
+        if (threadIdx.x == 0) *s_item = atomicAdd(work_counter, 1);
+        __syncthreads();
+        const int item = *s_item;
+        const bool stop = (item >= n_items) || (*s_abort != 0);
+        __syncthreads();
+        if (stop) break;
+        const int64_t qtile = has_cut ? (n_items - 1 - item) : item;  // heaviest first for the prefix search
+        const int64_t q0 = qtile * QT;
+        const int64_t block_limit = limit_of(min(q0 + QT, n_query) - 1);
+        const uint32_t ntiles = (uint32_t)((block_limit + RT - 1) / RT);
+
+        if (producer_warp) {
+            if (lane == 0) {
+                if (!mbar_wait_bounded(a_ready, it & 1)) aborted = true;  // query operand of this item
+                const uint32_t G = g_tile;
+                auto wait_empty = [&](uint32_t g) -> bool {
+                    const uint32_t k = g / S;
+                    return mbar_wait_bounded(&b_empty[g % S], (k & 1) ^ 1);
+                };
+                auto issue_tma = [&](uint32_t g) {
+                    const uint32_t s = g % S;
+                    const int64_t t = (int64_t)(g - G);
+                    mbar_arrive_expect_tx(&b_full[s], C::STAGE_BYTES);
+                    tma_bulk_g2s(sB + s * C::STAGE_BYTES, tiles_g + t * C::STAGE_BYTES, C::STAGE_BYTES, &b_full[s]);
+                    tma_issued = g + 1;
+                };
+                for (uint32_t k = 0; k < (uint32_t)S && k < ntiles && !aborted; ++k) {
+                    if (!wait_empty(G + k)) {
+                        aborted = true;
+                        break;
+                    }
+                    issue_tma(G + k);
+                }
+                const uint32_t a_addr = smem_addr(sA);
+                for (uint32_t t = 0; t < ntiles && !aborted; ++t) {
+                    const uint32_t g = G + t;
+                    const uint32_t s = g % S, b = g & 1;
+                    if (!mbar_wait_bounded(&b_full[s], (g / S) & 1)) {
+                        aborted = true;
+                        break;
+                    }
+                    tma_landed = g + 1;
+                    if (!mbar_wait_bounded(&t_empty[b], ((g >> 1) & 1) ^ 1)) {
+                        aborted = true;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t b_addr = smem_addr(sB + s * C::STAGE_BYTES);
+                    const uint32_t d_tmem = tmem_base + b * RT;
+#pragma unroll
+                    for (int i = 0; i < C::NMMA; ++i) {
+                        const uint64_t ad = smem_desc(a_addr + i * 2 * C::A_LBO, C::A_LBO, 128);
+                        const uint64_t bd = smem_desc(b_addr + i * 2 * C::B_LBO, C::B_LBO, 128);
+                        mma_tf32(d_tmem, ad, bd, i > 0 ? 1u : 0u);
+                    }
+                    mma_commit(&t_full[b]);
+                    mma_commit(&b_empty[s]);
+                    const uint32_t gr = g - 1 + S;  // refill the stage that MMA g-1 used
+                    if (t > 0 && gr < G + ntiles) {
+                        if (!wait_empty(gr)) {
+                            aborted = true;
+                            break;
+                        }
+                        issue_tma(gr);
+                    }
+                }
+            }
+            __syncwarp();
+        } else {
+            // ---------------- epilogue warps ----------------
+            const int row = warp * 32 + lane;  // query row in the tile = TMEM lane
+            const int64_t q = q0 + row;
+            const bool active = q < n_query;
+            const int64_t limit = active ? limit_of(q) : 0;
+            float qo[D], qc[D];
+            float nq = 0.f;
+#pragma unroll
+            for (int f = 0; f < D; ++f) {
+                qo[f] = active ? qs[q * C::DP + f] : 0.f;
+                const float cf = n_ref > 0 ? (float)(acc[f] / (double)n_ref) : 0.f;
+                qc[f] = qo[f] - cf;
+                nq = fmaf(qc[f], qc[f], nq);
+            }
+            const float span = sqrtf(nq) * 1.0001f + rmax;
+            const float eps = kEpsTc * span * span;
+            {  // query operand row: A' = [a_hi | a_hi | a_lo], a = [qc, 1]
+                float a[C::U];
+#pragma unroll
+                for (int f = 0; f < D; ++f) a[f] = active ? qc[f] : 0.f;
+                a[D] = active ? 1.f : 0.f;
+                for (int k = 0; k < C::KP; ++k) {
+                    float v = 0.f;
+                    const int blk = k / C::U, f = k - blk * C::U;
+                    if (blk < 3) {
+                        const float hi = tf32_round(a[f]);
+                        v = (blk == 2) ? (a[f] - hi) : hi;
+                    }
+                    *reinterpret_cast<float *>(sA + op_offset(row, k, QT)) = v;
+                }
+            }
+            fence_proxy_async_smem();
+            mbar_arrive(a_ready);
+
+            // this warp's 32 lists: slot k of row r at [r * LIST + k]; the LIST - m leading slots
+            // hold -inf (never displaced), the others start at +inf / -1
+            for (int rr = 0; rr < 32; ++rr) {
+                const int r = warp * 32 + rr;
+                Ld[r * LIST + lane] = lane < LIST - m ? neg_inf<float>() : pos_inf<float>();
+                Li[r * LIST + lane] = -1;
+            }
+            float *qd = reinterpret_cast<float *>(qbase) + warp * QCAP;
+            int32_t *qj = reinterpret_cast<int32_t *>(qbase + EPI_WARPS * QCAP * 4) + warp * QCAP;
+            uint8_t *qr = qbase + EPI_WARPS * QCAP * 8 + warp * QCAP;
+            __syncwarp();
+            // rows past the last query never take candidates
+            const float tq_off = active ? pos_inf<float>() : neg_inf<float>();
+            float tq = tq_off;                 // screening threshold of this row
+            float worst = pos_inf<float>();    // exact distance of this row's m-th entry
+            int qcount = 0;
+            auto drain = [&]() {
+                __syncwarp();
+                for (int e = 0; e < qcount; ++e) {
+                    const int r = warp * 32 + qr[e];
+                    const float d2 = qd[e];
+                    const int32_t j = qj[e];
+                    const float dk = Ld[r * LIST + lane];
+                    const int32_t ik = Li[r * LIST + lane];
+                    const bool less = (dk < d2) || (dk == d2 && (uint32_t)ik < (uint32_t)j);
+                    const int p = __popc(__ballot_sync(FULL, less));
+                    const float pd = __shfl_up_sync(FULL, dk, 1);
+                    const int32_t pi = __shfl_up_sync(FULL, ik, 1);
+                    if (p < LIST) {
+                        if (lane == p) {
+                            Ld[r * LIST + lane] = d2;
+                            Li[r * LIST + lane] = j;
+                        } else if (lane > p) {
+                            Ld[r * LIST + lane] = pd;
+                            Li[r * LIST + lane] = pi;
+                        }
+                    }
+                    __syncwarp();
+                }
+                qcount = 0;
+                worst = Ld[row * LIST + LIST - 1];
+                tq = fminf((worst - nq) + eps, tq_off);
+            };
+
+            const uint32_t G = g_tile;
+            for (uint32_t t = 0; t < ntiles; ++t) {
+                const uint32_t g = G + t;
+                const uint32_t s = g % S, b = g & 1;
+                if (!mbar_wait_bounded(&t_full[b], (g >> 1) & 1)) aborted = true;
+                if (__any_sync(FULL, aborted)) {
+                    aborted = true;
+                    break;
+                }
+                tc_fence_after();
+                const float *exs = reinterpret_cast<const float *>(sB + s * C::STAGE_BYTES + C::OP_BYTES);
+                const int64_t j0 = (int64_t)t * RT;
+                const uint32_t taddr = tmem_base + ((uint32_t)(warp * 32) << 16) + b * RT;
+#pragma unroll 1
+                for (int c = 0; c < RT / 32; ++c) {
+                    uint32_t v[32];
+                    tmem_ld32_nowait(taddr + c * 32, v);
+                    tmem_wait_ld();
+                    if (c == RT / 32 - 1) {
+                        // the accumulator buffer is free once every lane holds its last chunk
+                        tc_fence_before();
+                        __syncwarp();
+                        if (lane == 0) mbar_arrive(&t_empty[b]);
+                    }
+                    float mn = min3f(__uint_as_float(v[0]), __uint_as_float(v[1]), __uint_as_float(v[2]));
+#pragma unroll
+                    for (int k = 3; k < 31; k += 2) mn = min3f(mn, __uint_as_float(v[k]), __uint_as_float(v[k + 1]));
+                    mn = fminf(mn, __uint_as_float(v[31]));
+                    if (!__any_sync(FULL, mn < tq)) continue;
+                    // rare path: each lane walks its own candidate columns; one warp iteration
+                    // handles one candidate per lane, so the cost follows the busiest row
+                    uint32_t cm = 0;
+#pragma unroll
+                    for (int k = 0; k < 32; ++k) cm |= (__uint_as_float(v[k]) < tq ? 1u : 0u) << k;
+                    const int64_t jc = j0 + c * 32;
+                    const int64_t room = limit - jc;  // columns with j < limit
+                    if (room < 32) cm &= room <= 0 ? 0u : ((1u << (uint32_t)room) - 1u);
+                    while (__any_sync(FULL, cm != 0)) {
+                        if (qcount > QCAP - 32) drain();
+                        bool keep = false;
+                        float d2 = 0.f;
+                        int k = 0;
+                        if (cm != 0) {
+                            k = __ffs(cm) - 1;
+                            cm &= cm - 1;
+                            const float *rp = exs + (c * 32 + k) * C::DP;
+                            const float t0 = sub_rn(rp[0], qo[0]);
+                            d2 = mul_rn(t0, t0);
+#pragma unroll
+                            for (int f = 1; f < D; ++f) {
+                                const float tf = sub_rn(rp[f], qo[f]);
+                                d2 = add_rn(d2, mul_rn(tf, tf));
+                            }
+                            keep = d2 <= worst;  // NaN never kept
+                        }
+                        const unsigned mk = __ballot_sync(FULL, keep);
+                        if (keep) {
+                            const int pos = qcount + __popc(mk & ((1u << lane) - 1u));
+                            qd[pos] = d2;
+                            qj[pos] = (int32_t)(jc + k);
+                            qr[pos] = (uint8_t)lane;
+                        }
+                        qcount += __popc(mk);
+                    }
+                    __syncwarp();
+                    if (qcount > 0) drain();
+                }
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&b_empty[s]);
+            }
+            // write this warp's rows
+            __syncwarp();
+            if (!aborted) {
+                for (int rr = 0; rr < 32; ++rr) {
+                    const int r = warp * 32 + rr;
+                    const int64_t qq = q0 + r;
+                    if (qq < n_query && lane >= LIST - m) out[qq * m + (lane - (LIST - m))] = Li[r * LIST + lane];
+                }
+            }
+        }
+        g_tile += ntiles;
+        ++it;
+        if (aborted) *s_abort = 1;
+        __syncthreads();
+    }
+
+    // teardown: report a timeout, let copies and MMAs this CTA issued finish (bounded), free TMEM
+    if ((aborted || *s_abort) && threadIdx.x == 0) flag_or(flags, NNGP_FLAG_TIMEOUT);
+    if (producer_warp && lane == 0 && (aborted || *s_abort)) {
+        // copies issued but never waited for: let them land before the CTA's shared memory goes
+        for (uint32_t g = tma_landed; g < tma_issued; ++g) mbar_wait_bounded(&b_full[g % S], (g / S) & 1);
+        // MMAs in flight: the last t_full phase of each accumulator buffer
+        if (g_tile > 0) mbar_wait_bounded(&t_full[(g_tile - 1) & 1], ((g_tile - 1) >> 1) & 1);
+        if (g_tile > 1) mbar_wait_bounded(&t_full[(g_tile - 2) & 1], ((g_tile - 2) >> 1) & 1);
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (producer_warp) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS));
+    }
+}
+
+// Self-test of the UMMA operand layout: D = A B^T for A, B given row-major (128 x KP), through
+// the same shared-memory layout, descriptors, tcgen05.mma and tcgen05.ld path as the search.
+template <int KP>
+__global__ void __launch_bounds__(THREADS) tc_layout_selftest_kernel(const float *__restrict__ a,
+                                                                    const float *__restrict__ b,
+                                                                    float *__restrict__ d,
+                                                                    int32_t *__restrict__ flags) {
+    __shared__ __align__(1024) unsigned char sA[QT * KP * 4];
+    __shared__ __align__(1024) unsigned char sB[RT * KP * 4];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint32_t tmem_slot;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int e = threadIdx.x; e < QT * KP; e += blockDim.x)
+        *reinterpret_cast<float *>(sA + op_offset(e / KP, e % KP, QT)) = a[e];
+    for (int e = threadIdx.x; e < RT * KP; e += blockDim.x)
+        *reinterpret_cast<float *>(sB + op_offset(e / KP, e % KP, RT)) = b[e];
+    fence_proxy_async_smem();
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+    }
+    if (warp == EPI_WARPS) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_slot)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = tmem_slot;
+    if (warp == EPI_WARPS && lane == 0) {
+        constexpr uint32_t A_LBO = (QT / 8) * 128, B_LBO = (RT / 8) * 128;
+#pragma unroll
+        for (int i = 0; i < KP / 8; ++i)
+            mma_tf32(tmem_base, smem_desc(smem_addr(sA) + i * 2 * A_LBO, A_LBO, 128),
+                     smem_desc(smem_addr(sB) + i * 2 * B_LBO, B_LBO, 128), i > 0 ? 1u : 0u);
+        mma_commit(&bar);
+    }
+    const bool ok = mbar_wait_bounded(&bar, 0);
+    if (!ok && threadIdx.x == 0) flag_or(flags, NNGP_FLAG_TIMEOUT);
+    tc_fence_after();
+    if (warp < EPI_WARPS && ok) {
+        uint32_t v[32];
+        for (int c = 0; c < RT / 32; ++c) {
+            tmem_ld32_nowait(tmem_base + ((uint32_t)(warp * 32) << 16) + c * 32, v);
+            tmem_wait_ld();
+            for (int k = 0; k < 32; ++k) d[(warp * 32 + lane) * RT + c * 32 + k] = __uint_as_float(v[k]);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == EPI_WARPS) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS));
+    }
+}
+
+template <int D> TcVariant tc_make() {
+    TcVariant v;
+    v.fn = knn_tc_kernel<D>;
+    v.build = build_tc_tiles_kernel<D>;
+    v.smem = Cfg<D>::SMEM;
+    v.stage_bytes = Cfg<D>::STAGE_BYTES;
+    v.dp = Cfg<D>::DP;
+    return v;
+}
+
+}  // namespace tc
+
+tc::TcVariant tc_variant(int D, int M) {
+    if (M > tc::LIST) return tc::TcVariant{};
+    switch (D) {
+        case 1: return tc::tc_make<1>();
+        case 2: return tc::tc_make<2>();
+        case 3: return tc::tc_make<3>();
+        case 4: return tc::tc_make<4>();
+        case 5: return tc::tc_make<5>();
+        case 6: return tc::tc_make<6>();
+        case 7: return tc::tc_make<7>();
+        case 8: return tc::tc_make<8>();
+        case 12: return tc::tc_make<12>();
+        case 16: return tc::tc_make<16>();
+    }
+    return tc::TcVariant{};
+}
+
+}  // namespace nngp
+
+extern "C" nngp_status nngp_tc_layout_selftest(const float *a, const float *b, int32_t kp, float *d, int32_t *flags,
+                                               void *stream) {
+    using namespace nngp;
+    set_error("");
+    if (!a || !b || !d) return fail(NNGP_ERR_INVALID_ARGUMENT, "tc_layout_selftest: null pointer");
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    switch (kp) {
+        case 8: tc::tc_layout_selftest_kernel<8><<<1, tc::THREADS, 0, st>>>(a, b, d, flags); break;
+        case 16: tc::tc_layout_selftest_kernel<16><<<1, tc::THREADS, 0, st>>>(a, b, d, flags); break;
+        case 32: tc::tc_layout_selftest_kernel<32><<<1, tc::THREADS, 0, st>>>(a, b, d, flags); break;
+        default: return fail(NNGP_ERR_UNSUPPORTED, "tc_layout_selftest: kp must be 8, 16 or 32");
+    }
+    NNGP_CUDA_TRY(cudaGetLastError());
+    return NNGP_OK;
+}

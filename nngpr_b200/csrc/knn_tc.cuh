@@ -1,0 +1,30 @@
+// Host-side handle of the tensor-core search kernels (knn_tc.cu), used by the dispatcher in knn.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace nngp {
+namespace tc {
+
+constexpr int kTcRefTile = 128;    // refs per tile (UMMA N)
+constexpr int kTcQueryTile = 128;  // queries per tile (UMMA M)
+constexpr int kTcThreads = 160;    // 4 epilogue warps + 1 producer/MMA warp
+
+using TcFn = void (*)(const unsigned char *, const float *, const double *, const unsigned int *, int *, int64_t,
+                      int64_t, int, int64_t, int, int32_t *, int32_t *);
+using TcBuildFn = void (*)(const float *, int64_t, int64_t, const double *, unsigned char *, unsigned int *);
+
+struct TcVariant {
+    TcFn fn = nullptr;
+    TcBuildFn build = nullptr;
+    int smem = 0, stage_bytes = 0, dp = 0;
+};
+
+}  // namespace tc
+
+// Kernels for dimension D (exact for d <= 8, else round_up(d, 4)); num_nn <= 32 (M = 8, 16, 32);
+// fn == nullptr when the shape has no tensor-core variant.
+tc::TcVariant tc_variant(int D, int M);
+
+}  // namespace nngp

@@ -9,6 +9,14 @@ from oracle import nngp_oracle as O
 pytestmark = pytest.mark.gpu
 
 
+@pytest.fixture(params=['tc', 'simt', 'generic'], autouse=True)
+def knn_kernel(request, monkeypatch):
+    """Every test runs on each search kernel: the tensor-core screen ('tc', where the shape has
+    one), the SIMT screen and the generic kernel."""
+    monkeypatch.setenv('NNGP_KNN_KERNEL', request.param)
+    return request.param
+
+
 def run_knn(ref, q, m, cut, ls, dtype=np.float32):
     tdt = torch.float32 if dtype == np.float32 else torch.float64
     r = torch.from_numpy(np.ascontiguousarray(ref, dtype=dtype)).cuda()
