@@ -281,7 +281,7 @@ class ClockSampler:
 def read_profile_traffic():
     """DRAM bytes per launch of the neighbour-search kernel from the committed ncu summary
     (line 'traffic_bytes_per_launch: <int>'), or None."""
-    path = os.path.join(ROOT, 'profiles', 'knn_fit_n434874_d3_m32.md')
+    path = os.path.join(ROOT, 'profiles', 'knn_tc_kernel_fit_n434874_d3_m32.md')
     try:
         for ln in open(path):
             if ln.startswith('traffic_bytes_per_launch:'):
@@ -450,14 +450,15 @@ def run_ours(args):
             'e2e': e2e,
             'roofline': {'bound': 'fp32', 'achieved': achieved, 'peak': peak, 'unit': 'TFLOP/s',
                          'frac': achieved / peak, 'traffic': read_profile_traffic(),
-                         'kernel': 'knn_topm_kernel<3,32> (prefix search)',
-                         'work': '2*d flops per (query, ref) pair, n(n-1)/2 pairs',
+                         'kernel': 'knn_tc_kernel<3> (prefix search: tcgen05 TF32-split screen, exact FP32 rescoring)',
+                         'work': '2*d flops per (query, ref) pair, n(n-1)/2 pairs, whichever pipe computes them',
                          'peak_source': 'FP32 FMA probe measured in this run (MEASURED_PEAKS.json has no FP32 figure)',
                          'knn_ms': knn_avg_ms},
             'cpu_baseline': cpu,
             'predict': None if pred_ms is None else {'value': N_PRED / (pred_ms * 1e-3), 'unit': 'points/s',
                                                      'ms': pred_ms, 'n_query': N_PRED},
-            'gpu_launches': args.steps * 4,  # per step: scale, search, local systems, finalize
+            # per step: scale, centre sums, tile build, search, local systems, finalize
+            'gpu_launches': args.steps * 6,
             'clocks': clocks.summary(),
         }
         print(json.dumps(line))

@@ -489,8 +489,8 @@ ScreenVariant pick_screen(int D, int M) {
 
 enum class KnnPath { Tc, Simt, Generic };
 
-// Search kernel: the tensor-core screen for d >= 12 (or when the SIMT screen has no variant),
-// else the SIMT screen, else the generic kernel.  NNGP_KNN_KERNEL=tc|simt|generic forces a
+// Search kernel: the tensor-core screen where the shape has a variant (FP32, d <= 8, 12, 16,
+// num_nn <= 32), else the SIMT screen, else the generic kernel.  NNGP_KNN_KERNEL=tc|simt|generic forces a
 // kernel where the shape has one (testing and comparisons); unset or any other value selects
 // automatically.
 KnnPath choose_path(int d, int m, bool is_float) {
@@ -502,9 +502,7 @@ KnnPath choose_path(int d, int m, bool is_float) {
     if (want == "generic") return KnnPath::Generic;
     if (want == "simt") return simt_ok ? KnnPath::Simt : KnnPath::Generic;
     if (want == "tc" && tc_ok) return KnnPath::Tc;
-    // measured on B200: the SIMT screen wins at small d (cheap distances), the tensor-core
-    // screen from d >= 12 on
-    if (tc_ok && (D >= 12 || !simt_ok)) return KnnPath::Tc;
+    if (tc_ok) return KnnPath::Tc;  // faster than the SIMT screen at every d measured on B200 (3, 8, 16)
     return simt_ok ? KnnPath::Simt : KnnPath::Generic;
 }
 
@@ -626,10 +624,9 @@ nngp_status knn_impl(const T *ref, int64_t n_ref, const T *query, int64_t n_quer
             NNGP_CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void *>(p.tv.fn),
                                                cudaFuncAttributePreferredSharedMemoryCarveout, 100));
             const int64_t n_items = (n_query + tc::kTcQueryTile - 1) / tc::kTcQueryTile;
-            int per_sm = 1;
-            NNGP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, p.tv.fn, tc::kTcThreads,
-                                                                        (size_t)p.tv.smem));
-            per_sm = std::max(1, std::min(per_sm, 2));  // two CTAs x 256 TMEM columns fill an SM
+            // persistent grid: the CTAs one SM holds (shared memory and TMEM sized for them) per SM;
+            // CTAs that find no SM free start late and pick up no items, nothing waits on them
+            const int per_sm = p.tv.ctas_per_sm;
             const int grid = (int)std::min<int64_t>(n_items, (int64_t)num_sms_knn() * per_sm);
             if (const char *dbg = std::getenv("NNGP_KNN_DEBUG"); dbg && dbg[0] == '1')
                 std::fprintf(stderr, "nngp_knn: tensor-core path d=%d m=%d items=%lld ctas/sm=%d grid=%d smem=%d\n", d,

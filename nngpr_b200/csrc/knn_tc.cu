@@ -9,7 +9,7 @@
 //     (tcgen05.mma kind::tf32, M=128, N=128, FP32 accumulate).  To keep FP32-level accuracy each
 //     operand a = a_hi + a_lo is split (a_hi = a rounded to TF32, a_lo = a - a_hi, exact), and
 //     A' = [a_hi | a_hi | a_lo], B' = [b_hi | b_lo | b_hi] (each block d+1 wide: the d centred
-//     coordinates and the 1 / |rc|^2 column) so that A' B'^T = a_hi b_hi + a_hi b_lo + a_lo b_hi.
+//     coordinates, the constant 1 and the |rc|^2 column) so that A' B'^T = a_hi b_hi + a_hi b_lo + a_lo b_hi.
 //     The dropped and truncated terms are below 2^-21 |a||b| per product, the FP32 accumulation
 //     adds at most K' ulps; eps = 2^-16 (|qc| + max|rc|)^2 covers both with a margin of 4 or more,
 //     so every ref the exact algorithm inserts still passes the screen;
@@ -19,14 +19,17 @@
 //     and exact coordinates in one copy) and the MMAs; warps 0-3 are the epilogue, warp w owning
 //     query rows 32w..32w+31 (its TMEM lane quadrant).  Two CTAs share an SM when shared memory
 //     allows (small d), so that each scheduler has two epilogue warps;
-//   * epilogue: each 32-column chunk of a row is one tcgen05.ld, screened with three-input min
-//     against the row's threshold (a rolled loop: the code stays small enough for the instruction
-//     cache); when a chunk has candidates each lane walks its own candidate columns, one per warp
+//   * epilogue: each 32-column chunk of a row is one tcgen05.ld (issued one chunk ahead into a
+//     second register set), screened with three-input min over groups of 8 columns against the
+//     row's threshold (a rolled loop: the code stays small enough for the instruction cache).
+//     When a chunk has candidates each lane walks its own candidate columns, one per warp
 //     iteration, and rescores them exactly (exact coordinates from the same smem stage, the
-//     oracle's arithmetic), the survivors are compacted into a per-warp queue with ballots, and the warp
-//     inserts them cooperatively into the rows' top-32 lists kept in shared memory (one list slot
-//     per lane: ballot of "entry < candidate" in (distance, index) order gives the position,
-//     shfl_up shifts the tail) — converged, order independent, ties by lower index;
+//     oracle's arithmetic); survivors of the row's current bound are compacted with ballots into a
+//     per-warp queue.  Once 32 entries are queued the warp drains them into the rows' lists: each
+//     row keeps its best m as a max-heap of 64-bit keys (distance bits << 32 | index) in shared
+//     memory, 32 entries go in per pass, one per lane, entries of one row serialised by match_any.
+//     The key order is (distance, index), so the final sets do not depend on insertion order; at
+//     the end of a work item each heap is sorted across the warp (bitonic) and written out;
 //   * mbarriers: b_full (TMA -> MMA), b_empty (MMA commit + 4 epilogue warps -> producer),
 //     t_full (MMA commit -> epilogue), t_empty (4 epilogue warps -> MMA), a_ready (query operand
 //     written by the epilogue -> MMA).  Every wait is bounded; on a timeout the CTA raises
@@ -44,14 +47,20 @@ namespace tc {
 
 constexpr int QT = kTcQueryTile;  // queries per tile (UMMA M)
 constexpr int RT = kTcRefTile;    // refs per tile (UMMA N)
+static_assert(RT == 128, "the epilogue screens a ref tile as four 32-column chunks");
 constexpr int EPI_WARPS = 4;      // one per TMEM lane quadrant
 constexpr int THREADS = (EPI_WARPS + 1) * 32;
 static_assert(THREADS == kTcThreads, "thread count");
-constexpr int LIST = 32;       // list slots per query (one per lane); num_nn <= 32
+constexpr int LIST = 32;       // largest num_nn
+constexpr int HS = 33;         // heap row stride in 64-bit keys (odd: rows of a warp hit distinct banks)
+constexpr int DRAIN_AT = 32;   // queued entries that trigger a drain at the end of a chunk
 constexpr int QCAP = 512;      // candidate queue entries per epilogue warp
 constexpr uint32_t TMEM_COLS = 2 * RT;
 constexpr float kEpsTc = 1.52587890625e-05f;       // 2^-16
 constexpr float kPadNorm = 1.7014118346046923e38f;  // 2^127: padded refs never pass a finite screen
+// list key: FP32 distance bits (non-negative, so integer order = float order) << 32 | index;
+// an empty slot is (+inf, 0xffffffff), larger than every real entry, read back as index -1
+constexpr uint64_t kEmptyKey = (uint64_t)0x7F800000u << 32 | 0xFFFFFFFFu;
 
 template <int D>
 struct Cfg {
@@ -63,17 +72,17 @@ struct Cfg {
     static constexpr int EX_BYTES = RT * DP * 4;    // exact coordinates of a ref tile
     static constexpr int STAGE_BYTES = OP_BYTES + EX_BYTES;
     static constexpr int A_BYTES = QT * KP * 4;
-    static constexpr int LIST_BYTES = QT * LIST * 8;                 // distances + indices
+    static constexpr int LIST_BYTES = QT * HS * 8;  // one heap of keys per query
     static constexpr int QUEUE_BYTES = EPI_WARPS * QCAP * (4 + 4 + 1);
     static constexpr int BAR_BYTES = 256;
     static constexpr int FIXED = 1024 + A_BYTES + LIST_BYTES + QUEUE_BYTES + BAR_BYTES;
-    // two CTAs per SM if at least 3 stages fit in half an SM's shared memory, else one CTA
+    // two CTAs per SM if at least 2 stages fit in half an SM's shared memory, else one CTA
     static constexpr int HALF_SM = 112 * 1024;
     static constexpr int ST2 = (HALF_SM - FIXED) / STAGE_BYTES;
     static constexpr int ST1 = (220 * 1024 - FIXED) / STAGE_BYTES;
-    static constexpr int STAGES = ST2 >= 3 ? (ST2 > 4 ? 4 : ST2) : (ST1 > 4 ? 4 : ST1);
+    static constexpr int STAGES = ST2 >= 2 ? (ST2 > 4 ? 4 : ST2) : (ST1 > 4 ? 4 : ST1);
     static constexpr int SMEM = FIXED + STAGES * STAGE_BYTES;
-    static constexpr int CTAS_PER_SM = ST2 >= 3 ? 2 : 1;
+    static constexpr int CTAS_PER_SM = ST2 >= 2 ? 2 : 1;
     static_assert(STAGES >= 2, "ref tile too large for two stages");
     // K-major no-swizzle canonical layout: 8-row x 16-byte core matrices, SBO = 128 B between
     // 8-row groups, LBO between 16-byte K chunks
@@ -139,7 +148,41 @@ __device__ __forceinline__ void tmem_ld32_nowait(uint32_t taddr, uint32_t (&r)[3
         : "r"(taddr));
 }
 
-__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+// Wait for this thread's outstanding tcgen05.ld; the registers of the load are operands, so no
+// use of them can be scheduled before the wait.
+__device__ __forceinline__ void tmem_wait_ld(uint32_t (&r)[32]) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+                   "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]),
+                   "+r"(r[15]), "+r"(r[16]), "+r"(r[17]), "+r"(r[18]), "+r"(r[19]), "+r"(r[20]), "+r"(r[21]),
+                   "+r"(r[22]), "+r"(r[23]), "+r"(r[24]), "+r"(r[25]), "+r"(r[26]), "+r"(r[27]), "+r"(r[28]),
+                   "+r"(r[29]), "+r"(r[30]), "+r"(r[31])
+                 :
+                 : "memory");
+}
+
+// Max-heap of the m best keys (root = current m-th best): replace the root by x when x is
+// smaller and sift it down.
+__device__ __forceinline__ void heap_insert(uint64_t *h, int m, uint64_t x) {
+    if (!(x < h[0])) return;
+    int i = 0;
+    while (true) {
+        int c = 2 * i + 1;
+        if (c >= m) break;
+        uint64_t kc = h[c];
+        if (c + 1 < m) {
+            const uint64_t k2 = h[c + 1];
+            if (k2 > kc) {
+                kc = k2;
+                ++c;
+            }
+        }
+        if (kc <= x) break;
+        h[i] = kc;
+        i = c;
+    }
+    h[i] = x;
+}
 
 __device__ __forceinline__ float min3f(float a, float b, float c) {
     float r;
@@ -221,9 +264,8 @@ __global__ void __launch_bounds__(THREADS, Cfg<D>::CTAS_PER_SM) knn_tc_kernel(co
         reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     unsigned char *sA = sm;
     unsigned char *sB = sA + C::A_BYTES;
-    float *Ld = reinterpret_cast<float *>(sB + S * C::STAGE_BYTES);  // [QT][LIST]
-    int32_t *Li = reinterpret_cast<int32_t *>(Ld + QT * LIST);      // [QT][LIST]
-    unsigned char *qbase = reinterpret_cast<unsigned char *>(Li + QT * LIST);
+    uint64_t *H = reinterpret_cast<uint64_t *>(sB + S * C::STAGE_BYTES);  // [QT][HS] heaps
+    unsigned char *qbase = reinterpret_cast<unsigned char *>(H + QT * HS);
     uint64_t *bars = reinterpret_cast<uint64_t *>(qbase + C::QUEUE_BYTES);
     uint64_t *b_full = bars;        // [S <= 4]
     uint64_t *b_empty = bars + 4;   // [S <= 4]
@@ -241,7 +283,7 @@ __global__ void __launch_bounds__(THREADS, Cfg<D>::CTAS_PER_SM) knn_tc_kernel(co
     if (threadIdx.x == 0) {
         for (int s = 0; s < S; ++s) {
             mbar_init(&b_full[s], 1);
-            mbar_init(&b_empty[s], 1 + EPI_WARPS);
+            mbar_init(&b_empty[s], 1 + EPI_WARPS);  // the MMA commit + the epilogue warps (exact coordinates)
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(&t_full[b], 1);
@@ -378,13 +420,9 @@ __global__ void __launch_bounds__(THREADS, Cfg<D>::CTAS_PER_SM) knn_tc_kernel(co
             fence_proxy_async_smem();
             mbar_arrive(a_ready);
 
-            // this warp's 32 lists: slot k of row r at [r * LIST + k]; the LIST - m leading slots
-            // hold -inf (never displaced), the others start at +inf / -1
-            for (int rr = 0; rr < 32; ++rr) {
-                const int r = warp * 32 + rr;
-                Ld[r * LIST + lane] = lane < LIST - m ? neg_inf<float>() : pos_inf<float>();
-                Li[r * LIST + lane] = -1;
-            }
+            // this warp's rows: row rr's heap at heap[rr * HS .. + m)
+            uint64_t *heap = H + (warp * 32) * HS;
+            for (int rr = 0; rr < 32; ++rr) heap[rr * HS + lane] = kEmptyKey;
             float *qd = reinterpret_cast<float *>(qbase) + warp * QCAP;
             int32_t *qj = reinterpret_cast<int32_t *>(qbase + EPI_WARPS * QCAP * 4) + warp * QCAP;
             uint8_t *qr = qbase + EPI_WARPS * QCAP * 8 + warp * QCAP;
@@ -392,33 +430,31 @@ __global__ void __launch_bounds__(THREADS, Cfg<D>::CTAS_PER_SM) knn_tc_kernel(co
             // rows past the last query never take candidates
             const float tq_off = active ? pos_inf<float>() : neg_inf<float>();
             float tq = tq_off;                 // screening threshold of this row
-            float worst = pos_inf<float>();    // exact distance of this row's m-th entry
+            float worst = pos_inf<float>();    // distance of this row's heap root (m-th best so far)
             int qcount = 0;
+            // insert the queued entries: 32 at a time, each lane into its entry's row heap; entries
+            // of one row go in one after the other (match_any groups), so any order gives the same heap set
             auto drain = [&]() {
                 __syncwarp();
-                for (int e = 0; e < qcount; ++e) {
-                    const int r = warp * 32 + qr[e];
-                    const float d2 = qd[e];
-                    const int32_t j = qj[e];
-                    const float dk = Ld[r * LIST + lane];
-                    const int32_t ik = Li[r * LIST + lane];
-                    const bool less = (dk < d2) || (dk == d2 && (uint32_t)ik < (uint32_t)j);
-                    const int p = __popc(__ballot_sync(FULL, less));
-                    const float pd = __shfl_up_sync(FULL, dk, 1);
-                    const int32_t pi = __shfl_up_sync(FULL, ik, 1);
-                    if (p < LIST) {
-                        if (lane == p) {
-                            Ld[r * LIST + lane] = d2;
-                            Li[r * LIST + lane] = j;
-                        } else if (lane > p) {
-                            Ld[r * LIST + lane] = pd;
-                            Li[r * LIST + lane] = pi;
+                for (int base = 0; base < qcount; base += 32) {
+                    const int e = base + lane;
+                    bool pend = e < qcount;
+                    const int r = pend ? (int)qr[e] : 32 + lane;  // idle lanes: distinct dummy rows
+                    const uint64_t x = pend ? ((uint64_t)__float_as_uint(qd[e]) << 32 | (uint32_t)qj[e]) : 0;
+                    const unsigned grp = __match_any_sync(FULL, r);
+                    unsigned todo = __ballot_sync(FULL, pend);
+                    while (todo) {
+                        const unsigned g = grp & todo;
+                        if (pend && (g & (0u - g)) == (1u << lane)) {
+                            heap_insert(heap + r * HS, m, x);
+                            pend = false;
                         }
+                        __syncwarp();
+                        todo = __ballot_sync(FULL, pend);
                     }
-                    __syncwarp();
                 }
                 qcount = 0;
-                worst = Ld[row * LIST + LIST - 1];
+                worst = __uint_as_float((uint32_t)(heap[lane * HS] >> 32));
                 tq = fminf((worst - nq) + eps, tq_off);
             };
 
@@ -435,30 +471,34 @@ __global__ void __launch_bounds__(THREADS, Cfg<D>::CTAS_PER_SM) knn_tc_kernel(co
                 const float *exs = reinterpret_cast<const float *>(sB + s * C::STAGE_BYTES + C::OP_BYTES);
                 const int64_t j0 = (int64_t)t * RT;
                 const uint32_t taddr = tmem_base + ((uint32_t)(warp * 32) << 16) + b * RT;
-#pragma unroll 1
-                for (int c = 0; c < RT / 32; ++c) {
-                    uint32_t v[32];
-                    tmem_ld32_nowait(taddr + c * 32, v);
-                    tmem_wait_ld();
-                    if (c == RT / 32 - 1) {
-                        // the accumulator buffer is free once every lane holds its last chunk
-                        tc_fence_before();
-                        __syncwarp();
-                        if (lane == 0) mbar_arrive(&t_empty[b]);
-                    }
-                    float mn = min3f(__uint_as_float(v[0]), __uint_as_float(v[1]), __uint_as_float(v[2]));
+                // screen one 32-column chunk (scores in v) and queue its candidates
+                auto chunk = [&](const uint32_t (&v)[32], const int c) {
+                    float gmin[4];  // minimum of each group of 8 columns
 #pragma unroll
-                    for (int k = 3; k < 31; k += 2) mn = min3f(mn, __uint_as_float(v[k]), __uint_as_float(v[k + 1]));
-                    mn = fminf(mn, __uint_as_float(v[31]));
-                    if (!__any_sync(FULL, mn < tq)) continue;
-                    // rare path: each lane walks its own candidate columns; one warp iteration
-                    // handles one candidate per lane, so the cost follows the busiest row
+                    for (int gi = 0; gi < 4; ++gi) {
+#define NNGP_V(k) __uint_as_float(v[gi * 8 + (k)])
+                        gmin[gi] = fminf(min3f(NNGP_V(0), NNGP_V(1), NNGP_V(2)),
+                                         min3f(NNGP_V(3), NNGP_V(4), fminf(NNGP_V(5), fminf(NNGP_V(6), NNGP_V(7)))));
+#undef NNGP_V
+                    }
+                    const float mn = fminf(min3f(gmin[0], gmin[1], gmin[2]), gmin[3]);
+                    if (!__any_sync(FULL, mn < tq)) return;
+                    // rare path: candidate mask of this row (only groups whose minimum passes)
                     uint32_t cm = 0;
 #pragma unroll
-                    for (int k = 0; k < 32; ++k) cm |= (__uint_as_float(v[k]) < tq ? 1u : 0u) << k;
+                    for (int gi = 0; gi < 4; ++gi) {
+                        if (gmin[gi] < tq) {
+#pragma unroll
+                            for (int k = 0; k < 8; ++k)
+                                cm |= (__uint_as_float(v[gi * 8 + k]) < tq ? 1u : 0u) << (gi * 8 + k);
+                        }
+                    }
                     const int64_t jc = j0 + c * 32;
                     const int64_t room = limit - jc;  // columns with j < limit
                     if (room < 32) cm &= room <= 0 ? 0u : ((1u << (uint32_t)room) - 1u);
+                    // each lane walks its own candidates, one per warp iteration (the cost follows the
+                    // busiest row), rescoring them exactly from the stage's coordinates; survivors of the
+                    // row's current bound are queued and drained into the heaps in batches
                     while (__any_sync(FULL, cm != 0)) {
                         if (qcount > QCAP - 32) drain();
                         bool keep = false;
@@ -467,6 +507,7 @@ __global__ void __launch_bounds__(THREADS, Cfg<D>::CTAS_PER_SM) knn_tc_kernel(co
                         if (cm != 0) {
                             k = __ffs(cm) - 1;
                             cm &= cm - 1;
+                            // the oracle's arithmetic: ((x0 - q0)^2 + (x1 - q1)^2) + ..., each step rounded
                             const float *rp = exs + (c * 32 + k) * C::DP;
                             const float t0 = sub_rn(rp[0], qo[0]);
                             d2 = mul_rn(t0, t0);
@@ -486,19 +527,49 @@ __global__ void __launch_bounds__(THREADS, Cfg<D>::CTAS_PER_SM) knn_tc_kernel(co
                         }
                         qcount += __popc(mk);
                     }
-                    __syncwarp();
-                    if (qcount > 0) drain();
+                    if (qcount >= DRAIN_AT) drain();
+                };
+                // chunks in flight one ahead of the one being screened (two register sets)
+                uint32_t va[32], vb[32];
+                tmem_ld32_nowait(taddr, va);
+                tmem_wait_ld(va);
+#pragma unroll 1
+                for (int cp = 0; cp < RT / 64; ++cp) {
+                    tmem_ld32_nowait(taddr + (2 * cp + 1) * 32, vb);
+                    chunk(va, 2 * cp);
+                    tmem_wait_ld(vb);
+                    if (cp + 1 < RT / 64) {
+                        tmem_ld32_nowait(taddr + (2 * cp + 2) * 32, va);
+                    } else {
+                        // every chunk is in registers: the accumulator buffer is free
+                        tc_fence_before();
+                        __syncwarp();
+                        if (lane == 0) mbar_arrive(&t_empty[b]);
+                    }
+                    chunk(vb, 2 * cp + 1);
+                    if (cp + 1 < RT / 64) tmem_wait_ld(va);
                 }
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&b_empty[s]);
             }
-            // write this warp's rows
-            __syncwarp();
+            // write this warp's rows: each heap sorted ascending across the warp (bitonic, keys unique
+            // except empty slots), index -1 for empty slots
             if (!aborted) {
+                if (qcount > 0) drain();
+                __syncwarp();
                 for (int rr = 0; rr < 32; ++rr) {
-                    const int r = warp * 32 + rr;
-                    const int64_t qq = q0 + r;
-                    if (qq < n_query && lane >= LIST - m) out[qq * m + (lane - (LIST - m))] = Li[r * LIST + lane];
+                    uint64_t x = lane < m ? heap[rr * HS + lane] : ~0ull;
+#pragma unroll
+                    for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+                        for (int jj = k >> 1; jj > 0; jj >>= 1) {
+                            const uint64_t o = __shfl_xor_sync(FULL, x, jj);
+                            const bool take_min = ((lane & jj) == 0) == ((lane & k) == 0);
+                            x = take_min ? (o < x ? o : x) : (o > x ? o : x);
+                        }
+                    }
+                    const int64_t qq = q0 + warp * 32 + rr;
+                    if (qq < n_query && lane < m) out[qq * m + lane] = (int32_t)(uint32_t)x;
                 }
             }
         }
@@ -570,7 +641,7 @@ __global__ void __launch_bounds__(THREADS) tc_layout_selftest_kernel(const float
         uint32_t v[32];
         for (int c = 0; c < RT / 32; ++c) {
             tmem_ld32_nowait(tmem_base + ((uint32_t)(warp * 32) << 16) + c * 32, v);
-            tmem_wait_ld();
+            tmem_wait_ld(v);
             for (int k = 0; k < 32; ++k) d[(warp * 32 + lane) * RT + c * 32 + k] = __uint_as_float(v[k]);
         }
     }
@@ -589,6 +660,7 @@ template <int D> TcVariant tc_make() {
     v.smem = Cfg<D>::SMEM;
     v.stage_bytes = Cfg<D>::STAGE_BYTES;
     v.dp = Cfg<D>::DP;
+    v.ctas_per_sm = Cfg<D>::CTAS_PER_SM;
     return v;
 }
 

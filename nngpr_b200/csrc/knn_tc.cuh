@@ -19,6 +19,7 @@ struct TcVariant {
     TcFn fn = nullptr;
     TcBuildFn build = nullptr;
     int smem = 0, stage_bytes = 0, dp = 0;
+    int ctas_per_sm = 1;  // CTAs the shared memory of one SM holds (the kernel's launch bounds)
 };
 
 }  // namespace tc
