@@ -310,6 +310,54 @@ def fp32_peak_tflops(torch, L, stream_ptr):
     return best
 
 
+def run_plain(args, torch, x32, y64, xq32, p, flags, flush, lml_ours):
+    """Time the plain FP32 GPU form of the same fit step and predict (the comparator of the
+    metric): returns the 'plain_gpu' object of the bench line."""
+    from nngpr_b200 import ops
+    from nngpr_b200.plain import plain_knn, plain_loglik, plain_predict
+
+    y32 = y64.to(torch.float32)
+    nbr_ours = ops.knn(x32, x32, M, 0, LS, flags=flags)
+
+    def step(ev=None):
+        nb = plain_knn(x32, x32, M, 0, LS)
+        if ev is not None:
+            ev.record()
+        return nb, plain_loglik(x32, y32, nb, p, ALPHA, True)
+
+    step()  # warm-up
+    ms, knn_ms = [], []
+    for _ in range(args.plain_steps):
+        a, b, c = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        flush.zero_()
+        a.record()
+        nb, (lml, grad) = step(b)
+        c.record()
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(c))
+        knn_ms.append(a.elapsed_time(b))
+    same = bool(torch.equal(nb, nbr_ours))
+    lml = float(lml.item())
+    # predict at the benchmark's query count
+    nq = plain_knn(x32, xq32, M, None, LS)
+    plain_predict(x32, y32, xq32, nq, p, ALPHA)
+    a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    flush.zero_()
+    a.record()
+    nq = plain_knn(x32, xq32, M, None, LS)
+    plain_predict(x32, y32, xq32, nq, p, ALPHA)
+    c.record()
+    torch.cuda.synchronize()
+    pred_ms = a.elapsed_time(c)
+    step_ms = float(np.mean(ms))
+    return {'value': 1e3 / step_ms, 'unit': UNIT, 'ms_per_step': step_ms, 'knn_ms': float(np.mean(knn_ms)),
+            'steps': args.plain_steps, 'lists_identical': same, 'lml': lml,
+            'lml_rel_diff_vs_ours': abs(lml - lml_ours) / abs(lml_ours),
+            'predict': {'value': N_PRED / (pred_ms * 1e-3), 'unit': 'points/s', 'ms': pred_ms},
+            'form': 'one thread per query FP32 search (calc_nn structure) + torch FP32 batched fill, '
+                    'Cholesky and cholesky_solve with materialised dK (the reference worker), one launch per stage'}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -433,6 +481,12 @@ def run_ours(args):
         e2e = {'value': 1.0 / e2e_s, 'unit': UNIT, 'h2d_bytes_per_step': h2d, 'd2h_bytes_per_step': d2h,
                'ms_per_step': e2e_s * 1e3}
 
+    # ---- the plain FP32 GPU form (one thread per query search + batched torch FP32 systems) --
+    plain = None
+    if world == 1 and not args.no_plain:
+        plain = run_plain(args, torch, x32, y64, xq32, p, flags, flush, lml_val)
+        plain['speedup'] = (1e3 / (tot_ms / args.steps)) / plain['value']
+
     if rank == 0:
         import ctypes
         peak = fp32_peak_tflops(torch, L, ctypes.c_void_p(stream.cuda_stream))
@@ -455,6 +509,7 @@ def run_ours(args):
                          'peak_source': 'FP32 FMA probe measured in this run (MEASURED_PEAKS.json has no FP32 figure)',
                          'knn_ms': knn_avg_ms},
             'cpu_baseline': cpu,
+            'plain_gpu': plain,
             'predict': None if pred_ms is None else {'value': N_PRED / (pred_ms * 1e-3), 'unit': 'points/s',
                                                      'ms': pred_ms, 'n_query': N_PRED},
             # per step: scale, centre sums, tile build, search, local systems, finalize
@@ -505,6 +560,8 @@ def main():
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-e2e', action='store_true', help='skip the end-to-end API timing')
     ap.add_argument('--no-predict', action='store_true', help='skip the predict timing')
+    ap.add_argument('--no-plain', action='store_true', help='skip the plain FP32 GPU comparator')
+    ap.add_argument('--plain-steps', type=int, default=2, help='timed steps of the plain comparator')
     ap.add_argument('--n', type=int, default=N_TRAIN,
                     help='training points (smaller cases are for profiling; the metric is quoted at 434874)')
     args = ap.parse_args()

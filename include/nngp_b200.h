@@ -221,6 +221,18 @@ nngp_status nngp_predict_f64(const double *x_train, const double *y_train, int64
  * ------------------------------------------------------------------------------------- */
 nngp_status nngp_fma_probe(float *out, int64_t iters, int32_t blocks, void *stream);
 
+/* Plain FP32 GPU form of the neighbour search: the comparator the optimised search is measured
+ * against (no counterpart in the reference's plugin interface; it restates the structure of the
+ * reference's `calc_nn`, nngpr/cuda_kernel_accelerators.py:663-743: one thread per query, a
+ * serial scan of the eligible refs, a sorted top-m list in shared memory).  Inputs are already
+ * divided by the length scale, row-major (n, d) FP32.  Same results as nngp_knn_f32
+ * (identical FP32 distance arithmetic, lower index first on ties, -1 padding, ref cut as there).
+ * num_nn <= 256.  No workspace, no status flags.
+ * ------------------------------------------------------------------------------------- */
+nngp_status nngp_plain_knn_f32(const float *ref_scaled, int64_t n_ref, const float *query_scaled,
+                               int64_t n_query, int32_t d, int32_t num_nn, int32_t has_ref_cut,
+                               int64_t ref_cut_index, int32_t *out_idx, void *stream);
+
 /* Self-test of the tensor-core operand layout used by the search (no counterpart in the
  * reference): d (128 x 128) = a (128 x kp) * b (128 x kp)^T in TF32 with FP32 accumulation,
  * a and b row-major device arrays, kp = 8, 16 or 32, through the same shared-memory layout,

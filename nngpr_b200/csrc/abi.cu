@@ -27,6 +27,8 @@ nngp_status loglik_rows_f64(const double *, const double *, int64_t, int, int, i
                             const nngp_kernel *, int, double, double *, int32_t *, void *, size_t, cudaStream_t);
 nngp_status loglik_f64_noalloc(const double *, const double *, int64_t, int, int, const int32_t *, int,
                                const nngp_kernel *, int, double *, int32_t *, cudaStream_t);
+nngp_status plain_knn_f32(const float *, int64_t, const float *, int64_t, int, int, bool, int64_t, int32_t *,
+                          cudaStream_t);
 nngp_status predict_f32(const float *, const float *, int64_t, const float *, int64_t, int, int, const int32_t *, int,
                         const nngp_kernel *, double, float *, float *, int32_t *, cudaStream_t);
 nngp_status predict_f64(const double *, const double *, int64_t, const double *, int64_t, int, int, const int32_t *,
@@ -129,6 +131,15 @@ nngp_status nngp_knn_f64(const double *ref, int64_t n_ref, const double *query, 
     return guarded([&] {
         return knn_f64(ref, n_ref, query, n_query, d, length_scale, n_ls, num_nn, has_ref_cut != 0, ref_cut_index,
                        out_idx, status_flags, workspace, workspace_bytes, as_stream(stream));
+    });
+}
+
+nngp_status nngp_plain_knn_f32(const float *ref_scaled, int64_t n_ref, const float *query_scaled, int64_t n_query,
+                               int32_t d, int32_t num_nn, int32_t has_ref_cut, int64_t ref_cut_index,
+                               int32_t *out_idx, void *stream) {
+    return guarded([&] {
+        return plain_knn_f32(ref_scaled, n_ref, query_scaled, n_query, d, num_nn, has_ref_cut != 0, ref_cut_index,
+                             out_idx, as_stream(stream));
     });
 }
 
