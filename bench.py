@@ -7,8 +7,15 @@ n = 434,874 training points, d = 3, x ~ U[-1, 1]^3 scaled per axis by (1, 0.7, 0
 y = sum_k sin(3 x_k) + N(0, 0.05^2), m = 32 neighbours, ConstantKernel(1) * RBF(0.2) +
 WhiteKernel(1e-3), alpha = 1e-10.  One step = one full fit step over all n points: the
 prefix neighbour search (point i among points [0, i)), the fused local systems with the
-adjoint gradient and the FP64 reduction (FP32 systems, FP64 re-solve below pivot 1e-6).
-Predict throughput at 100,000 test points is reported beside it.
+adjoint gradient (FP64 systems, the default allow_downcast_f32='only-nn') and the FP64
+reduction.  Predict throughput at 100,000 test points is reported beside it.
+
+--workload precision: the mixed-precision configuration instead (n = 1,000,000, d = 16, x from
+a 64-component Gaussian mixture with means ~ U[-3, 3]^16 and std 0.5, y = 256 random Fourier
+features (omega ~ N(0, 1/0.8^2), phases ~ U[0, 2 pi], weights N(0, 1) sqrt(2/256)) +
+N(0, 0.01^2), m = 32, ConstantKernel(1) * RBF(0.8) + WhiteKernel(1e-4)): FP32 search on the
+tensor cores, FP32 local systems with an FP64 re-solve of small pivots, FP64 reductions; the
+line adds the log-likelihood error against FP64 local systems on the same neighbour lists.
 
 Our arm prints one JSON line (rank 0) with value = fit steps per second with the inputs
 resident in HBM, e2e = the same through the public estimator API uploading X, y from pinned
@@ -53,10 +60,38 @@ METRIC = 'fit-step loglik+grad/s'
 UNIT = 'fit-steps/s'
 WORKLOAD = ('nngp fit step, n=434874 d=3 m=32, isotropic RBF l=0.2, noise 1e-3; '
             'fp32 exact neighbour search, fp64 local systems (allow_downcast_f32=only-nn)')
+LOCAL = 'f64'  # precision of the local systems
+DATA = 'synthetic (seeded stand-in for 3droad: shape 434874 x 3)'
+DTYPE = 'f32 search + f64 local'
+
+WORKLOADS = {
+    'fit3d': {},
+    'precision': dict(
+        N_TRAIN=1_000_000, D=16, M=32, LS=0.8, NOISE=1e-4, ALPHA=1e-10, LOCAL='f32',
+        WORKLOAD=('nngp fit step, n=1000000 d=16 m=32, 64-component Gaussian mixture, isotropic RBF l=0.8, '
+                  'noise 1e-4; tensor-core fp32 exact neighbour search, fp32 local systems with fp64 re-solve of '
+                  'small pivots, fp64 reductions'),
+        DATA='synthetic (64-component GMM in 16-d, 256 random Fourier features; shape 1000000 x 16)',
+        DTYPE='f32 search (tf32-split tensor screen) + f32 local (f64 re-solve) + f64 sums'),
+}
+_WL = 'fit3d'
 
 
-def make_data(n=N_TRAIN, nq=N_PRED, seed=0):
+def make_data(n=None, nq=N_PRED, seed=0):
+    n = N_TRAIN if n is None else n
     rng = np.random.default_rng(seed)
+    if _WL == 'precision':
+        means = rng.uniform(-3, 3, (64, D))
+        x = means[rng.integers(0, 64, n)] + 0.5 * rng.normal(size=(n, D))
+        xq = means[rng.integers(0, 64, nq)] + 0.5 * rng.normal(size=(nq, D))
+        omega = rng.normal(0, 1 / 0.8, (256, D))
+        phase = rng.uniform(0, 2 * np.pi, 256)
+        w = rng.normal(size=256) * np.sqrt(2.0 / 256)
+        y = np.empty(n)
+        for i0 in range(0, n, 65536):
+            y[i0:i0 + 65536] = np.cos(x[i0:i0 + 65536] @ omega.T + phase) @ w
+        y += rng.normal(0, 0.01, n)
+        return x, y, xq
     scale = np.array([1.0, 0.7, 0.4])
     x = rng.uniform(-1, 1, (n, D)) * scale
     y = np.sin(3 * x).sum(1) + rng.normal(0, 0.05, n)
@@ -278,10 +313,13 @@ class ClockSampler:
 # ------------------------------------------------------------------------------------------
 # Our arm
 # ------------------------------------------------------------------------------------------
+PROFILE = {'fit3d': 'knn_tc_kernel_fit_n434874_d3_m32.md', 'precision': 'knn_tc_kernel_fit_n1000000_d16_m32.md'}
+
+
 def read_profile_traffic():
-    """DRAM bytes per launch of the neighbour-search kernel from the committed ncu summary
-    (line 'traffic_bytes_per_launch: <int>'), or None."""
-    path = os.path.join(ROOT, 'profiles', 'knn_tc_kernel_fit_n434874_d3_m32.md')
+    """DRAM bytes per launch of the neighbour-search kernel of this workload from the committed
+    ncu summary (line 'traffic_bytes_per_launch: <int>'), or None."""
+    path = os.path.join(ROOT, 'profiles', PROFILE[_WL])
     try:
         for ln in open(path):
             if ln.startswith('traffic_bytes_per_launch:'):
@@ -395,6 +433,8 @@ def run_ours(args):
     x64 = torch.from_numpy(x).to(dev, torch.float64)
     y64 = torch.from_numpy(y[:, None]).to(dev, torch.float64)
     x32 = x64.to(torch.float32)
+    # the local systems' copies (FP64, or FP32 with FP64 re-solves for the precision workload)
+    xl, yl = (x64, y64) if LOCAL == 'f64' else (x32, y64.to(torch.float32))
     bounds = row_partition(n, world)
     r0, r1 = bounds[rank], bounds[rank + 1]
     q_rows = x32[r0:r1]
@@ -405,11 +445,11 @@ def run_ours(args):
 
     def step(ev=None):
         if ev is None:
-            fit_step_rows(x32, x64, y64, p, ALPHA, M, r0, r1, LS, flags=flags, out=out)
+            fit_step_rows(x32, xl, yl, p, ALPHA, M, r0, r1, LS, flags=flags, out=out)
         else:  # the same two calls, with an event between them to time the search alone
             nbr = ops.knn(x32, q_rows, M, r0, LS, flags=flags)  # rows [r0, r1) among points [0, i)
             ev.record()
-            ops.loglik(x64, y64, nbr, p, ALPHA, True, flags=flags, out=out, row_begin=r0)
+            ops.loglik(xl, yl, nbr, p, ALPHA, True, flags=flags, out=out, row_begin=r0)
         if world > 1:
             dist.all_reduce(out)
         return out
@@ -447,6 +487,11 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         tot_ms = float(t.item())
     lml_val = float(out[0].item())
+    lml_err = None
+    if LOCAL != 'f64' and world == 1:  # error of the mixed-precision result against FP64 systems
+        nbr_all = ops.knn(x32, x32, M, 0, LS, flags=flags)
+        ref64 = ops.loglik(x64, y64, nbr_all, p, ALPHA, True, flags=flags)
+        lml_err = abs(lml_val - float(ref64[0].item())) / abs(float(ref64[0].item()))
 
     # ---- predict throughput at 100,000 points ---------------------------------------------
     xq64 = torch.from_numpy(xq).to(dev, torch.float64)
@@ -467,7 +512,7 @@ def run_ours(args):
     e2e = None
     if world == 1 and not args.no_e2e:
         gpr = B200Nngpr(kernel=kernel, num_nn=M, alpha=ALPHA, optimizer=None, keep_resident=False,
-                        device=dev).fit(x, y)
+                        allow_downcast_f32='yes' if LOCAL == 'f32' else None, device=dev).fit(x, y)
         theta = gpr.kernel_.theta.copy()
         for _ in range(max(1, args.warmup)):
             gpr.log_marginal_likelihood(theta, eval_gradient=True)
@@ -476,7 +521,8 @@ def run_ours(args):
         for _ in range(args.steps):
             lml_api, grad_api = gpr.log_marginal_likelihood(theta, eval_gradient=True)
         e2e_s = (time.perf_counter() - t0) / args.steps
-        h2d = int(x.shape[0] * (D + 1) * 8)  # float64 X and y (the search copy is cast on the device)
+        # X and y in the local systems' precision (the search copy is cast on the device)
+        h2d = int(x.shape[0] * (D + 1) * (8 if LOCAL == 'f64' else 4))
         d2h = int((1 + p.n_theta + 1) * 8)  # [lml, grad..., status] in one float64 read
         e2e = {'value': 1.0 / e2e_s, 'unit': UNIT, 'h2d_bytes_per_step': h2d, 'd2h_bytes_per_step': d2h,
                'ms_per_step': e2e_s * 1e3}
@@ -485,6 +531,8 @@ def run_ours(args):
     plain = None
     if world == 1 and not args.no_plain:
         plain = run_plain(args, torch, x32, y64, xq32, p, flags, flush, lml_val)
+        plain['lml_rel_err_vs_fp64_local'] = (None if lml_err is None else
+                                              abs(plain['lml'] - lml_val) / abs(lml_val))
         plain['speedup'] = (1e3 / (tot_ms / args.steps)) / plain['value']
 
     if rank == 0:
@@ -497,14 +545,15 @@ def run_ours(args):
         line = {
             'metric': METRIC, 'value': 1e3 / ms_per_step, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
             'warmup': args.warmup, 'ms_per_step': ms_per_step, 'higher_is_better': True,
-            'scaling': 'strong' if world > 1 else 'weak', 'vs_baseline': None, 'dtype': 'f32 search + f64 local',
-            'data': 'synthetic (seeded stand-in for 3droad: shape 434874 x 3)',
+            'scaling': 'strong' if world > 1 else 'weak', 'vs_baseline': None, 'dtype': DTYPE,
+            'data': DATA,
             'config': {'workload': WORKLOAD, 'n': n, 'd': D, 'm': M, 'parallelism': f'rows{world}',
-                       'l2': 'flushed (256 MB write) before every timed step', 'lml': lml_val},
+                       'l2': 'flushed (256 MB write) before every timed step', 'lml': lml_val,
+                       'lml_rel_err_vs_fp64_local': lml_err},
             'e2e': e2e,
             'roofline': {'bound': 'fp32', 'achieved': achieved, 'peak': peak, 'unit': 'TFLOP/s',
                          'frac': achieved / peak, 'traffic': read_profile_traffic(),
-                         'kernel': 'knn_tc_kernel<3> (prefix search: tcgen05 TF32-split screen, exact FP32 rescoring)',
+                         'kernel': f'knn_tc_kernel<{D}> (prefix search: tcgen05 TF32-split screen, exact FP32 rescoring)',
                          'work': '2*d flops per (query, ref) pair, n(n-1)/2 pairs, whichever pipe computes them',
                          'peak_source': 'FP32 FMA probe measured in this run (MEASURED_PEAKS.json has no FP32 figure)',
                          'knn_ms': knn_avg_ms},
@@ -562,11 +611,16 @@ def main():
     ap.add_argument('--no-predict', action='store_true', help='skip the predict timing')
     ap.add_argument('--no-plain', action='store_true', help='skip the plain FP32 GPU comparator')
     ap.add_argument('--plain-steps', type=int, default=2, help='timed steps of the plain comparator')
-    ap.add_argument('--n', type=int, default=N_TRAIN,
+    ap.add_argument('--workload', choices=sorted(WORKLOADS), default='fit3d',
+                    help='fit3d: n=434,874 d=3 (default); precision: n=1,000,000 d=16 mixed precision')
+    ap.add_argument('--n', type=int, default=None,
                     help='training points (smaller cases are for profiling; the metric is quoted at 434874)')
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    global _WL
+    _WL = args.workload
+    globals().update(WORKLOADS[args.workload])
     if args.impl == 'reference':
         run_reference(args)
     else:
