@@ -74,12 +74,32 @@ WORKLOADS = {
         DATA='synthetic (64-component GMM in 16-d, 256 random Fourier features; shape 1000000 x 16)',
         DTYPE='f32 search (tf32-split tensor screen) + f32 local (f64 re-solve) + f64 sums'),
 }
+WORKLOADS['differentiation'] = dict(
+    N_TRAIN=434_874, D=8, M=32, NOISE=4e-4, ALPHA=1e-10, LOCAL='f32',
+    WORKLOAD=('nngp fit step, n=434874 d=8 m=32, x~U[0,1]^8, ARD RBF (8 length scales), noise 4e-4; '
+              'fp32 exact neighbour search, fp32 local systems with fp64 re-solves, gradient w.r.t. 10 log '
+              'hyperparameters; plus 50 device L-BFGS iterations through the autograd function'),
+    DATA='synthetic (U[0,1]^8, 512 random Fourier features with log-uniform ARD length scales; shape 434874 x 8)',
+    DTYPE='f32 search (tf32-split tensor screen) + f32 local (f64 re-solve) + f64 sums')
 _WL = 'fit3d'
 
 
 def make_data(n=None, nq=N_PRED, seed=0):
     n = N_TRAIN if n is None else n
     rng = np.random.default_rng(seed)
+    if _WL == 'differentiation':
+        global LS
+        x = rng.uniform(0, 1, (n, D))
+        xq = rng.uniform(0, 1, (nq, D))
+        LS = np.exp(rng.uniform(np.log(0.1), np.log(1.0), D))
+        omega = rng.normal(size=(512, D)) / LS
+        phase = rng.uniform(0, 2 * np.pi, 512)
+        w = rng.normal(size=512) * np.sqrt(2.0 / 512)
+        y = np.empty(n)
+        for i0 in range(0, n, 65536):
+            y[i0:i0 + 65536] = np.cos(x[i0:i0 + 65536] @ omega.T + phase) @ w
+        y += rng.normal(0, 0.02, n)
+        return x, y, xq
     if _WL == 'precision':
         means = rng.uniform(-3, 3, (64, D))
         x = means[rng.integers(0, 64, n)] + 0.5 * rng.normal(size=(n, D))
@@ -319,6 +339,8 @@ PROFILE = {'fit3d': 'knn_tc_kernel_fit_n434874_d3_m32.md', 'precision': 'knn_tc_
 def read_profile_traffic():
     """DRAM bytes per launch of the neighbour-search kernel of this workload from the committed
     ncu summary (line 'traffic_bytes_per_launch: <int>'), or None."""
+    if _WL not in PROFILE:
+        return None
     path = os.path.join(ROOT, 'profiles', PROFILE[_WL])
     try:
         for ln in open(path):
@@ -493,6 +515,22 @@ def run_ours(args):
         ref64 = ops.loglik(x64, y64, nbr_all, p, ALPHA, True, flags=flags)
         lml_err = abs(lml_val - float(ref64[0].item())) / abs(float(ref64[0].item()))
 
+    # ---- differentiation workload: device L-BFGS through the autograd function ----------------
+    lbfgs = None
+    if _WL == 'differentiation' and world == 1:
+        from nngpr_b200.autograd import LogLikProblem, fit_lbfgs
+        prob = LogLikProblem(x32, xl, yl, p, M, ALPHA)
+        theta0 = kernel.theta.copy()
+        lml0 = float(prob.evaluate(theta0)[0].item())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        th, lml1, evals = fit_lbfgs(prob, theta0, kernel.bounds, max_iter=50)
+        e1.record()
+        torch.cuda.synchronize()
+        lb_ms = e0.elapsed_time(e1)
+        lbfgs = {'max_iter': 50, 'evaluations': evals, 'ms': lb_ms, 'ms_per_evaluation': lb_ms / max(evals, 1),
+                 'lml_start': lml0, 'lml_end': lml1, 'theta_end': [float(v) for v in th]}
+
     # ---- predict throughput at 100,000 points ---------------------------------------------
     xq64 = torch.from_numpy(xq).to(dev, torch.float64)
     xq32 = xq64.to(torch.float32)
@@ -559,6 +597,7 @@ def run_ours(args):
                          'knn_ms': knn_avg_ms},
             'cpu_baseline': cpu,
             'plain_gpu': plain,
+            'lbfgs': lbfgs,
             'predict': None if pred_ms is None else {'value': N_PRED / (pred_ms * 1e-3), 'unit': 'points/s',
                                                      'ms': pred_ms, 'n_query': N_PRED},
             # per step: scale, centre sums, tile build, search, local systems, finalize

@@ -3,6 +3,8 @@
 * ``B200Nngpr``: scikit-learn estimator, drop-in for the reference ``NumpyNngpr``/``TorchNngpr``.
 * ``ops``: torch-facing calls of the C ABI (``include/nngp_b200.h``, ``libnngp_b200.so``).
 * ``kernel_params``: reduction of a kernel tree to ``White + const + rbf_level * RBF``.
+* ``autograd``: the log-likelihood as a ``torch.autograd.Function`` and an L-BFGS fit on it.
+* ``plain``: the plain FP32 GPU form (the benchmark's comparator).
 """
 
 from .kernel_params import RbfParams, extract  # noqa: F401
@@ -15,6 +17,6 @@ def __getattr__(name):
     import importlib
     if name == 'B200Nngpr':
         return importlib.import_module('.estimator', __name__).B200Nngpr
-    if name in ('ops', 'estimator'):
+    if name in ('ops', 'estimator', 'autograd', 'plain'):
         return importlib.import_module('.' + name, __name__)
     raise AttributeError(name)

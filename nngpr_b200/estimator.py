@@ -54,6 +54,9 @@ class B200Nngpr(GaussianProcessRegressor):
     keep_resident : bool, default True
         Keep the training set in HBM between calls.  ``False`` uploads it on every call, the
         reference's behaviour.
+    optimizer : 'fmin_l_bfgs_b', 'device-lbfgs', callable or None
+        As scikit-learn's, plus ``'device-lbfgs'``: ``torch.optim.LBFGS`` on the device through
+        the differentiable log-likelihood (``nngpr_b200.autograd``).
 
     ``distribute_method``, ``mp_start_method``, ``random_gen_batch_byte_size`` and
     ``distribute_environ`` are accepted for signature compatibility; with one device and
@@ -75,6 +78,7 @@ class B200Nngpr(GaussianProcessRegressor):
         "device": [str, torch.device, None],
         "pivot_tol": [Interval(Real, 0, None, closed="left")],
         "keep_resident": ["boolean"],
+        "optimizer": [StrOptions({"fmin_l_bfgs_b", "device-lbfgs"}), callable, None],
     }
 
     def __init__(self, kernel=None, *, alpha=1e-10, optimizer="fmin_l_bfgs_b", n_restarts_optimizer=0,
@@ -225,6 +229,16 @@ class B200Nngpr(GaussianProcessRegressor):
         else:
             self.log_marginal_likelihood_value_ = self.log_marginal_likelihood(self.kernel_.theta, clone_kernel=False)
         return self
+
+    def _constrained_optimization(self, obj_func, initial_theta, bounds):
+        """``optimizer='device-lbfgs'``: ``torch.optim.LBFGS`` on the device through the
+        differentiable log-likelihood (:mod:`nngpr_b200.autograd`), at most 50 iterations;
+        every other optimizer as scikit-learn runs it."""
+        if self.optimizer == 'device-lbfgs':
+            from .autograd import LogLikProblem, fit_lbfgs
+            theta, lml, _ = fit_lbfgs(LogLikProblem.from_estimator(self), initial_theta, bounds)
+            return theta, -lml
+        return super()._constrained_optimization(obj_func, initial_theta, bounds)
 
     # ---- fit step -------------------------------------------------------------------------
     def _dtypes(self):

@@ -201,3 +201,25 @@ def extract(kernel) -> RbfParams:
     p.idx_ls = ls_idx[0] if isinstance(ls_idx, list) else ls_idx
     p.n_theta = len(kernel.theta)
     return p
+
+
+def params_from_theta(template: RbfParams, theta) -> RbfParams:
+    """The parameters of ``template``'s kernel at log-hyperparameters ``theta`` (the values a
+    ``kernel.clone_with_theta(theta)`` would hold): every free hyperparameter is ``exp`` of its
+    theta entry, fixed ones keep the template's value."""
+    th = np.asarray(theta, dtype=np.float64).reshape(-1)
+    if th.size != template.n_theta:
+        raise ValueError(f'theta has {th.size} entries, the kernel {template.n_theta}')
+    p = dataclasses.replace(template)
+    if template.idx_rbf_level >= 0:
+        p.rbf_level = float(np.exp(th[template.idx_rbf_level]))
+    if template.idx_const >= 0:
+        p.const_value = float(np.exp(th[template.idx_const]))
+    if template.idx_noise >= 0:
+        p.noise_level = float(np.exp(th[template.idx_noise]))
+    if template.idx_ls >= 0 and template.length_scale is not None:
+        if template.ard:
+            p.length_scale = np.exp(th[template.idx_ls:template.idx_ls + template.n_ls])
+        else:
+            p.length_scale = float(np.exp(th[template.idx_ls]))
+    return p

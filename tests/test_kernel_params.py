@@ -78,3 +78,25 @@ def test_reference_batched_kernels_are_accepted():
     p = extract(k)
     assert p.rbf_level == pytest.approx(0.7) and p.noise_level == pytest.approx(0.05)
     assert theta_map(k) == {'rbf_level': 0, 'length_scale': [1, 2], 'noise_level': 3}
+
+
+@pytest.mark.parametrize('kernel', [
+    skk.ConstantKernel(2.0) * skk.RBF(0.3) + skk.WhiteKernel(0.01),
+    skk.ConstantKernel(0.5) + skk.ConstantKernel(1.3) * skk.RBF(np.array([0.1, 0.2, 0.3])) + skk.WhiteKernel(0.02),
+    skk.ConstantKernel(1.0, constant_value_bounds='fixed') * skk.RBF(0.4) + skk.WhiteKernel(0.1),
+    skk.RBF(np.array([0.5, 2.0])) + skk.WhiteKernel(0.3, noise_level_bounds='fixed'),
+])
+def test_params_from_theta_equals_clone_with_theta(kernel):
+    from nngpr_b200.kernel_params import params_from_theta
+    rng = np.random.default_rng(3)
+    theta = kernel.theta + rng.normal(0, 0.3, kernel.theta.shape)
+    want = extract(kernel.clone_with_theta(theta))
+    got = params_from_theta(extract(kernel), theta)
+    for f in ('rbf_level', 'const_value', 'noise_level'):
+        assert getattr(got, f) == pytest.approx(getattr(want, f), rel=1e-14)
+    if want.length_scale is None:
+        assert got.length_scale is None
+    else:
+        np.testing.assert_allclose(np.asarray(got.length_scale), np.asarray(want.length_scale), rtol=1e-14)
+    assert (got.idx_rbf_level, got.idx_const, got.idx_noise, got.idx_ls, got.n_theta) == (
+        want.idx_rbf_level, want.idx_const, want.idx_noise, want.idx_ls, want.n_theta)
