@@ -81,14 +81,28 @@ WORKLOADS['differentiation'] = dict(
               'hyperparameters; plus 50 device L-BFGS iterations through the autograd function'),
     DATA='synthetic (U[0,1]^8, 512 random Fourier features with log-uniform ARD length scales; shape 434874 x 8)',
     DTYPE='f32 search (tf32-split tensor screen) + f32 local (f64 re-solve) + f64 sums')
+WORKLOADS['serving'] = dict(
+    N_TRAIN=16_599, D=18, M=32, NOISE=1e-2, ALPHA=1e-10, LOCAL='f32',
+    WORKLOAD=('served predict, fitted model n=16599 d=18 m=32 held in HBM, ARD RBF, noise 1e-2; Poisson stream '
+              'of requests with log-uniform sizes in [1, 65536]; continuous batching, CUDA graphs per size bucket'),
+    DATA='synthetic (N(0,1)^18, ARD length scales log-uniform in [0.5, 5], 256 random Fourier features)',
+    DTYPE='f32 search (tf32-split tensor screen) + f32 local (f64 re-solve)')
 _WL = 'fit3d'
 
 
 def make_data(n=None, nq=N_PRED, seed=0):
     n = N_TRAIN if n is None else n
     rng = np.random.default_rng(seed)
+    global LS
+    if _WL == 'serving':
+        x = rng.normal(size=(n, D))
+        xq = rng.normal(size=(nq, D))
+        LS = np.exp(rng.uniform(np.log(0.5), np.log(5.0), D))
+        omega = rng.normal(size=(256, D)) / LS
+        y = np.cos(x @ omega.T + rng.uniform(0, 2 * np.pi, 256)) @ (rng.normal(size=256) * np.sqrt(2.0 / 256))
+        y += rng.normal(0, 0.1, n)
+        return x, y, xq
     if _WL == 'differentiation':
-        global LS
         x = rng.uniform(0, 1, (n, D))
         xq = rng.uniform(0, 1, (nq, D))
         LS = np.exp(rng.uniform(np.log(0.1), np.log(1.0), D))
@@ -418,6 +432,114 @@ def run_plain(args, torch, x32, y64, xq32, p, flags, flush, lml_ours):
                     'Cholesky and cholesky_solve with materialised dK (the reference worker), one launch per stage'}
 
 
+def _pct(v, q):
+    return float(np.percentile(np.asarray(v) * 1e3, q)) if len(v) else None
+
+
+def run_serving(args):
+    """Served predict: a Poisson stream of requests against PredictServer (continuous batching,
+    CUDA graphs per size bucket), then the same stream one request per launch through the plain
+    FP32 form.  Latency = completion on the host - scheduled arrival (host clock: it is what a
+    client sees, H2D/D2H and queueing included)."""
+    import torch
+    from nngpr_b200 import B200Nngpr
+    from nngpr_b200.plain import plain_knn, plain_predict
+    from nngpr_b200.serving import PredictServer
+
+    dev = torch.device('cuda', int(os.environ.get('LOCAL_RANK', '0')))
+    torch.cuda.set_device(dev)
+    x, y, _ = make_data()
+    kernel = make_kernel()
+    gpr = B200Nngpr(kernel=kernel, num_nn=M, alpha=ALPHA, optimizer=None, allow_downcast_f32='yes',
+                    device=dev).fit(x, y)
+    rng = np.random.default_rng(1)
+    n_req = args.requests
+    sizes = np.minimum(np.exp(rng.uniform(0, np.log(65536), n_req)).astype(int), 65536)
+    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, n_req))
+    reqs = [rng.normal(size=(int(s), D)) for s in sizes]
+    clocks = ClockSampler(dev.index).__enter__()
+    clocks.wait_first_sample()
+    srv = PredictServer(gpr)
+    for r in reqs[:8]:  # warm-up
+        srv.predict(r)
+    # 1k-point requests on an idle server
+    one_k = []
+    for _ in range(args.warmup + 50):
+        q = rng.normal(size=(1000, D))
+        t0 = time.perf_counter()
+        srv.predict(q)
+        one_k.append(time.perf_counter() - t0)
+    one_k = one_k[args.warmup:]
+    # the stream
+    done_at = [0.0] * n_req
+    futs = [None] * n_req
+    with clocks:
+        clocks.mark_start()
+        t0 = time.perf_counter()
+        for k in range(n_req):
+            wait = t0 + arrivals[k] - time.perf_counter()
+            if wait > 0:
+                time.sleep(wait)
+            futs[k] = srv.submit(reqs[k])
+            futs[k].add_done_callback(lambda f, k=k: done_at.__setitem__(k, time.perf_counter()))
+        for f in futs:
+            f.result()
+        t_end = max(done_at)
+        clocks.mark_end()
+    # capacity: the same requests submitted at once
+    ts = time.perf_counter()
+    for f in [srv.submit(r) for r in reqs]:
+        f.result()
+    t_sat = time.perf_counter() - ts
+    srv.close()
+    lat = [done_at[k] - (t0 + arrivals[k]) for k in range(n_req)]
+    small = [lat[k] for k in range(n_req) if sizes[k] <= 1024]
+    points = int(sizes.sum())
+    ours = {'points_per_s': points / (t_end - t0), 'p50_ms': _pct(lat, 50), 'p99_ms': _pct(lat, 99),
+            'p50_ms_le_1k_points': _pct(small, 50), 'p99_ms_le_1k_points': _pct(small, 99)}
+    # plain FP32 form, one request per launch, same arrival times
+    p = gpr._params(gpr.kernel_)
+    xt32 = torch.from_numpy(x).to(dev, torch.float32)
+    yt32 = torch.from_numpy((y - gpr._y_train_mean) / gpr._y_train_std).to(dev, torch.float32)
+    ls = gpr._search_ls(p)
+
+    def plain_one(xq):
+        q = torch.from_numpy(xq).to(dev, torch.float32)
+        nb = plain_knn(xt32, q, M, None, ls)
+        mean, std = plain_predict(xt32, yt32, q, nb, p, ALPHA)
+        return mean.cpu().numpy(), std.cpu().numpy()
+
+    for r in reqs[:4]:
+        plain_one(r)
+    n_plain = min(n_req, args.plain_requests)
+    plain_lat = []
+    t0p = time.perf_counter()
+    for k in range(n_plain):
+        arr = t0p + arrivals[k]
+        now = time.perf_counter()
+        if now < arr:
+            time.sleep(arr - now)
+        plain_one(reqs[k])
+        plain_lat.append(time.perf_counter() - arr)
+    t_plain = time.perf_counter() - t0p
+    p_small = [plain_lat[k] for k in range(n_plain) if sizes[k] <= 1024]
+    plain = {'points_per_s': float(sizes[:n_plain].sum()) / t_plain, 'p50_ms': _pct(plain_lat, 50),
+             'p99_ms': _pct(plain_lat, 99), 'p99_ms_le_1k_points': _pct(p_small, 99), 'requests': n_plain,
+             'form': 'one request per launch: H2D, one-thread-per-query FP32 search, torch FP32 local systems, D2H'}
+    line = {'metric': 'served predict points/s', 'value': ours['points_per_s'], 'unit': 'points/s', 'n_gpus': 1,
+            'steps': n_req, 'warmup': args.warmup, 'higher_is_better': True, 'vs_baseline': None, 'dtype': DTYPE,
+            'data': DATA, 'config': {'workload': WORKLOAD, 'n': N_TRAIN, 'd': D, 'm': M, 'requests': n_req,
+                                     'rate_per_s': args.rate, 'points': points, 'slots': srv.n_slots,
+                                     'buckets': list(srv.buckets)},
+            'latency': ours,
+            'saturated': {'points_per_s': int(sizes.sum()) / t_sat, 'seconds': t_sat,
+                          'note': 'all requests of the stream submitted at once'},
+            'one_k_alone': {'p50_ms': _pct(one_k, 50), 'p99_ms': _pct(one_k, 99), 'n': len(one_k)},
+            'plain_gpu': plain, 'speedup_points_per_s': ours['points_per_s'] / plain['points_per_s'],
+            'clocks': clocks.summary()}
+    print(json.dumps(line))
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -650,6 +772,9 @@ def main():
     ap.add_argument('--no-predict', action='store_true', help='skip the predict timing')
     ap.add_argument('--no-plain', action='store_true', help='skip the plain FP32 GPU comparator')
     ap.add_argument('--plain-steps', type=int, default=2, help='timed steps of the plain comparator')
+    ap.add_argument('--requests', type=int, default=400, help='serving workload: requests in the stream')
+    ap.add_argument('--rate', type=float, default=200.0, help='serving workload: mean arrivals per second')
+    ap.add_argument('--plain-requests', type=int, default=100, help='serving workload: requests the plain form runs')
     ap.add_argument('--workload', choices=sorted(WORKLOADS), default='fit3d',
                     help='fit3d: n=434,874 d=3 (default); precision: n=1,000,000 d=16 mixed precision')
     ap.add_argument('--n', type=int, default=None,
@@ -662,6 +787,8 @@ def main():
     globals().update(WORKLOADS[args.workload])
     if args.impl == 'reference':
         run_reference(args)
+    elif args.workload == 'serving':
+        run_serving(args)
     else:
         run_ours(args)
 

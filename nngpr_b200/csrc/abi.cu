@@ -2,8 +2,12 @@
 // Declarations and the reference interface each entry point replaces: include/nngp_b200.h.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <exception>
+#include <map>
+#include <mutex>
 #include <string>
+#include <utility>
 
 #include "common.cuh"
 
@@ -51,6 +55,26 @@ nngp_status cuda_fail(cudaError_t e, const char *what) {
 }
 
 const char *last_error_cstr() { return g_last_error.c_str(); }
+
+cudaError_t ensure_smem_limit(const void *fn, int bytes, int carveout) {
+    static std::mutex mu;
+    static std::map<std::pair<const void *, int>, std::pair<int, int>> done;  // (fn, device) -> (bytes, carveout)
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = done.find({fn, dev});
+    if (it != done.end() && it->second.first >= bytes && (carveout < 0 || it->second.second == carveout))
+        return cudaSuccess;
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess && carveout >= 0) e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, carveout);
+    if (e == cudaSuccess) {
+        auto &v = done[{fn, dev}];
+        v.first = std::max(v.first, bytes);
+        if (carveout >= 0) v.second = carveout;
+    }
+    return e;
+}
 
 }  // namespace nngp
 

@@ -35,6 +35,11 @@ nngp_status cuda_fail(cudaError_t e, const char *what);
 
 inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
+// Raise a kernel's dynamic shared-memory limit (and, carveout >= 0, its preferred carveout) once
+// per process and device: later calls, including calls made while a stream is being captured
+// into a CUDA graph, find the setting cached and make no CUDA call.  Defined in abi.cu.
+cudaError_t ensure_smem_limit(const void *fn, int bytes, int carveout = -1);
+
 // ---------------------------------------------------------------------------------------
 // Device helpers
 // ---------------------------------------------------------------------------------------

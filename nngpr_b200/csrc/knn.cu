@@ -489,8 +489,8 @@ ScreenVariant pick_screen(int D, int M) {
 
 enum class KnnPath { Tc, Simt, Generic };
 
-// Search kernel: the tensor-core screen where the shape has a variant (FP32, d <= 8, 12, 16,
-// num_nn <= 32), else the SIMT screen, else the generic kernel.  NNGP_KNN_KERNEL=tc|simt|generic forces a
+// Search kernel: the tensor-core screen where the shape has a variant (FP32, d <= 24 apart
+// from 9-11 padded to 12 etc., num_nn <= 32), else the SIMT screen, else the generic kernel.  NNGP_KNN_KERNEL=tc|simt|generic forces a
 // kernel where the shape has one (testing and comparisons); unset or any other value selects
 // automatically.
 KnnPath choose_path(int d, int m, bool is_float) {
@@ -619,10 +619,7 @@ nngp_status knn_impl(const T *ref, int64_t n_ref, const T *query, int64_t n_quer
             NNGP_CUDA_TRY(cudaGetLastError());
             p.tv.build<<<grid_for(p.n_ref_pad), 256, 0, stream>>>(refs, n_ref, p.n_ref_pad, acc, tiles, r2);
             NNGP_CUDA_TRY(cudaGetLastError());
-            NNGP_CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void *>(p.tv.fn),
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize, p.tv.smem));
-            NNGP_CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void *>(p.tv.fn),
-                                               cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+            NNGP_CUDA_TRY(ensure_smem_limit(reinterpret_cast<const void *>(p.tv.fn), p.tv.smem, 100));
             const int64_t n_items = (n_query + tc::kTcQueryTile - 1) / tc::kTcQueryTile;
             // persistent grid: the CTAs one SM holds (shared memory and TMEM sized for them) per SM;
             // CTAs that find no SM free start late and pick up no items, nothing waits on them
@@ -652,8 +649,7 @@ nngp_status knn_impl(const T *ref, int64_t n_ref, const T *query, int64_t n_quer
             p.v.rec<<<grid_for(p.n_ref_pad), 256, 0, stream>>>(refs, n_ref, p.n_ref_pad, acc, recs, r2);
             NNGP_CUDA_TRY(cudaGetLastError());
             const int grid = (int)((n_query + kKnnThreads - 1) / kKnnThreads);
-            NNGP_CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void *>(p.v.fn),
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize, p.v.smem));
+            NNGP_CUDA_TRY(ensure_smem_limit(reinterpret_cast<const void *>(p.v.fn), p.v.smem));
             const float4 *recs_c = recs;
             const float *q_c = qsc;
             const double *acc_c = acc;
@@ -668,8 +664,7 @@ nngp_status knn_impl(const T *ref, int64_t n_ref, const T *query, int64_t n_quer
         int32_t *lidx = reinterpret_cast<int32_t *>(base + p.off_lidx);
         const int grid = (int)((n_query + kGenThreads - 1) / kGenThreads);
         const size_t smem = (size_t)d * kGenThreads * sizeof(T) + (size_t)kGenTile * p.dp * sizeof(T);
-        NNGP_CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void *>(knn_generic_kernel<T>),
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        NNGP_CUDA_TRY(ensure_smem_limit(reinterpret_cast<const void *>(knn_generic_kernel<T>), (int)smem));
         knn_generic_kernel<T><<<grid, kGenThreads, smem, stream>>>(refs, qsc, n_query, n_ref, p.dp, d, has_cut, cut, m,
                                                                    ldist, lidx, out);
     }

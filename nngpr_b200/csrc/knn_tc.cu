@@ -679,6 +679,8 @@ tc::TcVariant tc_variant(int D, int M) {
         case 8: return tc::tc_make<8>();
         case 12: return tc::tc_make<12>();
         case 16: return tc::tc_make<16>();
+        case 20: return tc::tc_make<20>();
+        case 24: return tc::tc_make<24>();
     }
     return tc::TcVariant{};
 }

@@ -24,7 +24,7 @@ struct TcVariant {
 
 }  // namespace tc
 
-// Kernels for dimension D (exact for d <= 8, else round_up(d, 4)); num_nn <= 32 (M = 8, 16, 32);
+// Kernels for dimension D (exact for d <= 8, else round_up(d, 4): 12, 16, 20, 24); num_nn <= 32;
 // fn == nullptr when the shape has no tensor-core variant.
 tc::TcVariant tc_variant(int D, int M);
 

@@ -707,13 +707,11 @@ nngp_status launch_local(const LocalPlan &pl, const LocalArgs &a, const TIn *x_r
                          cudaStream_t stream) {
     if (pl.warp) {
         auto fn = local_warp_kernel<TIn, GRAD, PRED>;
-        NNGP_CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void *>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)pl.smem));
+        NNGP_CUDA_TRY(ensure_smem_limit(reinterpret_cast<const void *>(fn), (int)pl.smem));
         fn<<<pl.grid, kLocWarps * 32, pl.smem, stream>>>(a, x_ref, y_ref, x_pt, y_pt, nbr, block_out, mean, var, flags);
     } else {
         auto fn = local_block_kernel<TIn, GRAD, PRED>;
-        NNGP_CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void *>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)pl.smem));
+        NNGP_CUDA_TRY(ensure_smem_limit(reinterpret_cast<const void *>(fn), (int)pl.smem));
         fn<<<pl.grid, kBlkThreads, pl.smem, stream>>>(a, x_ref, y_ref, x_pt, y_pt, nbr, block_out, mean, var, flags);
     }
     NNGP_CUDA_TRY(cudaGetLastError());

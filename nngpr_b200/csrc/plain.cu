@@ -69,8 +69,7 @@ nngp_status plain_knn_f32(const float *ref, int64_t n_ref, const float *query, i
     if (n_query == 0) return NNGP_OK;
     if (!query || !out || (n_ref > 0 && !ref)) return fail(NNGP_ERR_INVALID_ARGUMENT, "plain_knn: null pointer");
     const size_t smem = (size_t)kPlainThreads * m * (sizeof(float) + sizeof(int32_t));
-    NNGP_CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void *>(plain_knn_kernel),
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    NNGP_CUDA_TRY(ensure_smem_limit(reinterpret_cast<const void *>(plain_knn_kernel), (int)smem));
     const int64_t grid = (n_query + kPlainThreads - 1) / kPlainThreads;
     plain_knn_kernel<<<(unsigned)grid, kPlainThreads, smem, stream>>>(ref, n_ref, query, n_query, d, m,
                                                                      has_cut ? 1 : 0, cut, out);

@@ -1,0 +1,315 @@
+"""Continuous-batching predict server for a fitted model held in HBM.
+
+The reference answers ``predict`` one call at a time: every call re-uploads the training set,
+searches, fills and solves in worker batches (``nngpr/base_nngpr.py:763-894, 1032-1135``).
+:class:`PredictServer` keeps the training set, its kernel parameters and the search copy
+resident and serves a stream of predict requests of uneven sizes:
+
+* requests are queued as they arrive (:meth:`PredictServer.submit` returns a future); a
+  scheduler thread packs the queued points, oldest first, into one batch per free *slot* (a
+  request larger than the biggest batch is split, a batch takes pieces of several requests);
+* a batch is padded to the smallest size bucket that holds it and run as one CUDA graph
+  captured for that bucket: cast, neighbour search, fused fill + Cholesky + solves, all on the
+  slot's stream, between an H2D copy of the batch and a D2H copy of its results (pinned host
+  buffers of the slot);
+* several slots are in flight at once on their own streams, so requests that arrive while
+  others run are admitted as soon as a slot is free and their work overlaps on the device; the
+  number of slots is bounded by the free device memory at start-up;
+* a completion thread waits for each batch's event, scatters the rows to their requests and
+  completes a request's future when all its rows are back.
+
+Every query row is computed independently (its own neighbour list and local system), so a
+request's result does not depend on what it was batched with (tests/test_gpu_serving.py checks
+it bit for bit).
+"""
+from __future__ import annotations
+
+import collections
+import concurrent.futures as cf
+import threading
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _lib, ops
+
+DEFAULT_BUCKETS = (256, 1024, 4096, 16384, 65536)
+
+
+@dataclass
+class _Request:
+    x: np.ndarray
+    future: cf.Future
+    t_submit: float
+    mean: np.ndarray
+    var: np.ndarray
+    left: int
+    t_done: float = 0.0
+
+
+@dataclass
+class _Batch:
+    pieces: list  # (request, row offset in request, rows, row offset in batch)
+    points: int
+    bucket: int
+    event: torch.cuda.Event = None
+
+
+@dataclass
+class _Slot:
+    stream: torch.cuda.Stream
+    x_in: torch.Tensor            # (max bucket, d) float64 device input
+    x_pin: torch.Tensor           # pinned staging of the input
+    mean_pin: torch.Tensor        # pinned results
+    var_pin: torch.Tensor
+    flags_pin: torch.Tensor
+    graphs: dict = field(default_factory=dict)   # bucket -> (graph, mean_out, var_out, flags)
+    busy: bool = False
+
+
+class PredictServer:
+    """Serve ``predict(X, return_std=True)`` of a fitted :class:`nngpr_b200.B200Nngpr`.
+
+    ``buckets``: batch sizes (query points) with a captured CUDA graph each; the largest is the
+    most points one batch takes.  ``slots``: batches in flight at most (lowered when the free
+    device memory does not hold that many).  ``use_graphs=False`` launches the kernels directly
+    (same results; for comparison).
+    """
+
+    def __init__(self, gpr, buckets=DEFAULT_BUCKETS, slots: int = 3, use_graphs: bool = True,
+                 memory_fraction: float = 0.5):
+        if not hasattr(gpr, 'X_train_'):
+            raise ValueError('PredictServer needs a fitted model')
+        self.gpr = gpr
+        self.buckets = tuple(sorted(int(b) for b in buckets))
+        self.max_batch = self.buckets[-1]
+        self.use_graphs = use_graphs
+        dev = torch.device(gpr._device)
+        self.device = dev if dev.index is not None else torch.device('cuda', torch.cuda.current_device())
+        torch.cuda.set_device(self.device)
+        kernel = gpr.kernel_
+        self.p = gpr._params(kernel)
+        self.search_dtype, self.local_dtype = gpr._dtypes()
+        self.xt, self.yt = gpr._train_tensors(self.local_dtype)  # resident (keep_resident)
+        self.xs_train = self.xt if self.search_dtype == self.local_dtype else self.xt.to(self.search_dtype)
+        self.ls = gpr._search_ls(self.p)
+        self.d = self.xt.shape[1]
+        self.ydim = self.yt.shape[1] if self.yt.dim() == 2 else 1
+        self.m = min(gpr._num_nn, self.xt.shape[0])
+        self.alpha = float(gpr.alpha)
+        self.pivot_tol = gpr.pivot_tol
+        self.y_std = np.asarray(gpr._y_train_std, dtype=np.float64).reshape(1, -1)
+        self.y_mean = np.asarray(gpr._y_train_mean, dtype=np.float64).reshape(1, -1)
+
+        # slots bounded by free memory: inputs, outputs and the graphs' workspaces of one slot
+        per_slot = self._slot_bytes()
+        free, _ = torch.cuda.mem_get_info(self.device)
+        self.n_slots = max(1, min(int(slots), int(free * memory_fraction // max(per_slot, 1))))
+        self.slots = [self._make_slot() for _ in range(self.n_slots)]
+
+        self._queue = collections.deque()   # (request, next row offset)
+        self._inflight = collections.deque()  # (slot, batch) in launch order
+        self._cv = threading.Condition()
+        self._stop = False
+        self._error = None
+        self.completed = []
+        self._sched = threading.Thread(target=self._schedule_loop, name='nngp-sched', daemon=True)
+        self._done = threading.Thread(target=self._complete_loop, name='nngp-done', daemon=True)
+        self._sched.start()
+        self._done.start()
+
+    # ---- set-up ---------------------------------------------------------------------------
+    def _slot_bytes(self) -> int:
+        b = self.max_batch
+        io = b * self.d * 8 + b * (self.ydim + 1) * 8
+        ws = int(_lib.lib().nngp_knn_workspace_size_f32(self.xt.shape[0], b, self.d, self.m)) + b * self.m * 4
+        return 2 * io + ws * len(self.buckets)
+
+    def _run(self, slot: _Slot, b: int, flags: torch.Tensor):
+        """Kernels of one batch of ``b`` points from ``slot.x_in`` (captured into the graphs)."""
+        xq = slot.x_in[:b]
+        xs = xq.to(self.search_dtype)
+        xl = xs if self.local_dtype == self.search_dtype else xq.to(self.local_dtype)
+        nbr = ops.knn(self.xs_train, xs, self.m, None, self.ls, flags=flags)
+        return ops.predict(self.xt, self.yt, xl, nbr, self.p, self.alpha, self.pivot_tol, flags=flags)
+
+    def _make_slot(self) -> _Slot:
+        b = self.max_batch
+        dev = self.device
+        slot = _Slot(stream=torch.cuda.Stream(dev),
+                     x_in=torch.zeros((b, self.d), dtype=torch.float64, device=dev),
+                     x_pin=torch.empty((b, self.d), dtype=torch.float64).pin_memory(),
+                     mean_pin=torch.empty((b, self.ydim), dtype=torch.float64).pin_memory(),
+                     var_pin=torch.empty((b,), dtype=torch.float64).pin_memory(),
+                     flags_pin=torch.zeros(1, dtype=torch.int32).pin_memory())
+        for bucket in self.buckets:
+            flags = ops.new_flags(dev)
+            mean_out = torch.zeros((bucket, self.ydim), dtype=torch.float64, device=dev)
+            var_out = torch.zeros((bucket,), dtype=torch.float64, device=dev)
+            graph = None
+            if self.use_graphs:
+                with torch.cuda.stream(slot.stream):
+                    self._run(slot, bucket, flags)  # warm-up outside the capture
+                slot.stream.synchronize()
+                graph = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(graph, stream=slot.stream):
+                    flags.zero_()
+                    mean, var = self._run(slot, bucket, flags)
+                    mean_out.copy_(mean)
+                    var_out.copy_(var)
+            slot.graphs[bucket] = (graph, mean_out, var_out, flags)
+        return slot
+
+    # ---- client side ----------------------------------------------------------------------
+    def submit(self, x) -> cf.Future:
+        """Queue one predict request; the future resolves to ``(mean, std)`` in the estimator's
+        output format (``B200Nngpr.predict(x, return_std=True)``)."""
+        x = np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(-1, self.d))
+        fut = cf.Future()
+        req = _Request(x=x, future=fut, t_submit=time.perf_counter(), mean=np.empty((x.shape[0], self.ydim)),
+                       var=np.empty(x.shape[0]), left=x.shape[0])
+        if x.shape[0] == 0:
+            self._finish(req)
+            return fut
+        with self._cv:
+            if self._error is not None:
+                raise RuntimeError('predict server failed') from self._error
+            self._queue.append([req, 0])
+            self._cv.notify_all()
+        return fut
+
+    def predict(self, x):
+        return self.submit(x).result()
+
+    def close(self):
+        with self._cv:
+            self._stop = True
+            self._cv.notify_all()
+        self._sched.join()
+        self._done.join()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- scheduler ------------------------------------------------------------------------
+    def _free_slot(self):
+        for s in self.slots:
+            if not s.busy:
+                return s
+        return None
+
+    def _take_batch(self) -> _Batch:
+        """Pieces of the queued requests, oldest first, up to the largest bucket (under the lock)."""
+        pieces, points = [], 0
+        while self._queue and points < self.max_batch:
+            entry = self._queue[0]
+            req, off = entry
+            rows = min(req.x.shape[0] - off, self.max_batch - points)
+            pieces.append((req, off, rows, points))
+            points += rows
+            if off + rows == req.x.shape[0]:
+                self._queue.popleft()
+            else:
+                entry[1] = off + rows
+        bucket = next(b for b in self.buckets if b >= points)
+        return _Batch(pieces=pieces, points=points, bucket=bucket)
+
+    def _schedule_loop(self):
+        torch.cuda.set_device(self.device)
+        try:
+            while True:
+                with self._cv:
+                    while not self._stop and (not self._queue or self._free_slot() is None):
+                        self._cv.wait()
+                    if self._stop and not self._queue:
+                        return
+                    slot = self._free_slot()
+                    batch = self._take_batch()
+                    slot.busy = True
+                self._launch(slot, batch)
+                with self._cv:
+                    self._inflight.append((slot, batch))
+                    self._cv.notify_all()
+        except BaseException as e:  # surfaced to the clients
+            self._fail(e)
+
+    def _launch(self, slot: _Slot, batch: _Batch):
+        for req, off, rows, at in batch.pieces:
+            slot.x_pin[at:at + rows].numpy()[...] = req.x[off:off + rows]
+        P = batch.points
+        graph, mean_out, var_out, flags = slot.graphs[batch.bucket]
+        with torch.cuda.stream(slot.stream):
+            slot.x_in[:P].copy_(slot.x_pin[:P], non_blocking=True)
+            if graph is not None:
+                graph.replay()
+            else:
+                flags.zero_()
+                mean, var = self._run(slot, batch.bucket, flags)
+                mean_out.copy_(mean)
+                var_out.copy_(var)
+            slot.mean_pin[:P].copy_(mean_out[:P], non_blocking=True)
+            slot.var_pin[:P].copy_(var_out[:P], non_blocking=True)
+            slot.flags_pin.copy_(flags, non_blocking=True)
+            batch.event = torch.cuda.Event()
+            batch.event.record(slot.stream)
+
+    # ---- completion -----------------------------------------------------------------------
+    def _complete_loop(self):
+        torch.cuda.set_device(self.device)
+        try:
+            while True:
+                with self._cv:
+                    while not self._inflight and not (self._stop and not self._queue and self._idle()):
+                        self._cv.wait()
+                    if not self._inflight:
+                        return
+                    slot, batch = self._inflight.popleft()
+                batch.event.synchronize()
+                fl = int(slot.flags_pin.item()) & ~(_lib.NNGP_FLAG_FP64_FALLBACK | _lib.NNGP_FLAG_NOT_PD)
+                mean = slot.mean_pin.numpy()
+                var = slot.var_pin.numpy()
+                finished = []
+                for req, off, rows, at in batch.pieces:
+                    req.mean[off:off + rows] = mean[at:at + rows]
+                    req.var[off:off + rows] = var[at:at + rows]
+                    req.left -= rows
+                    if req.left == 0:
+                        finished.append(req)
+                with self._cv:
+                    slot.busy = False
+                    self._cv.notify_all()
+                for req in finished:
+                    if fl:
+                        req.future.set_exception(_lib.NngpError(f'predict server: kernel status flags {fl}'))
+                    else:
+                        self._finish(req)
+        except BaseException as e:
+            self._fail(e)
+
+    def _idle(self) -> bool:
+        return all(not s.busy for s in self.slots)
+
+    def _finish(self, req: _Request):
+        mean = self.y_std * req.mean + self.y_mean
+        std = np.sqrt(req.var).reshape(-1, 1) * self.y_std
+        if mean.shape[1] == 1:
+            mean, std = mean[:, 0], std[:, 0]
+        req.t_done = time.perf_counter()
+        self.completed.append(req.t_done - req.t_submit)
+        req.future.set_result((mean, std))
+
+    def _fail(self, e):
+        with self._cv:
+            self._error = e
+            pending = [r for r, _ in self._queue] + [p[0] for _, b in self._inflight for p in b.pieces]
+            self._queue.clear()
+            self._stop = True
+            self._cv.notify_all()
+        for r in pending:
+            if not r.future.done():
+                r.future.set_exception(e)

@@ -28,7 +28,7 @@ def run_knn(ref, q, m, cut, ls, dtype=np.float32):
     return out.cpu().numpy()
 
 
-@pytest.mark.parametrize('d', [1, 2, 3, 5, 8, 12, 16, 18, 33])
+@pytest.mark.parametrize('d', [1, 2, 3, 5, 8, 12, 16, 18, 22, 33])
 @pytest.mark.parametrize('m', [1, 7, 16, 32, 48, 70])
 def test_knn_prefix_matches_oracle(d, m):
     """The fit-step search (ref = query, cut 0) across the register and generic kernels."""
