@@ -7,8 +7,9 @@ n = 434,874 training points, d = 3, x ~ U[-1, 1]^3 scaled per axis by (1, 0.7, 0
 y = sum_k sin(3 x_k) + N(0, 0.05^2), m = 32 neighbours, ConstantKernel(1) * RBF(0.2) +
 WhiteKernel(1e-3), alpha = 1e-10.  One step = one full fit step over all n points: the
 prefix neighbour search (point i among points [0, i)), the fused local systems with the
-adjoint gradient (FP64 systems, the default allow_downcast_f32='only-nn') and the FP64
-reduction.  Predict throughput at 100,000 test points is reported beside it.
+adjoint gradient (FP64 systems, the default allow_downcast_f32='only-nn': at this nugget
+almost every FP32 system would need the FP64 re-solve) and the FP64 reduction.  Predict
+throughput at 100,000 test points is reported beside it.
 
 --workload precision: the mixed-precision configuration instead (n = 1,000,000, d = 16, x from
 a 64-component Gaussian mixture with means ~ U[-3, 3]^16 and std 0.5, y = 256 random Fourier
@@ -59,10 +60,12 @@ N_PRED = 100_000
 METRIC = 'fit-step loglik+grad/s'
 UNIT = 'fit-steps/s'
 WORKLOAD = ('nngp fit step, n=434874 d=3 m=32, isotropic RBF l=0.2, noise 1e-3; '
-            'fp32 exact neighbour search, fp64 local systems (allow_downcast_f32=only-nn)')
-LOCAL = 'f64'  # precision of the local systems
+            'fp32 exact neighbour search (tensor-core screen), fp64 local systems (allow_downcast_f32=only-nn)')
+# precision of the local systems: at this nugget nearly every FP32 system has a pivot below the
+# re-solve threshold, so FP64 systems are the faster exact choice (FP32 + re-solve: 51.9 ms/step)
+LOCAL = 'f64'
 DATA = 'synthetic (seeded stand-in for 3droad: shape 434874 x 3)'
-DTYPE = 'f32 search + f64 local'
+DTYPE = 'f32 search (tf32-split tensor screen) + f64 local'
 
 WORKLOADS = {
     'fit3d': {},
@@ -663,7 +666,7 @@ def run_ours(args):
             flush.zero_()
             s0.record()
             nq = ops.knn(x32, xq32, M, None, LS, flags=flags)
-            mean, var = ops.predict(x64, y64, xq64, nq, p, ALPHA, flags=flags)
+            mean, var = ops.predict(xl, yl, xq64 if LOCAL == 'f64' else xq32, nq, p, ALPHA, flags=flags)
             s1.record()
             torch.cuda.synchronize()
             pred_ms = s0.elapsed_time(s1)
