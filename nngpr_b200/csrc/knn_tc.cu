@@ -21,10 +21,12 @@
 //     allows (small d), so that each scheduler has two epilogue warps;
 //   * epilogue: each 32-column chunk of a row is one tcgen05.ld (issued one chunk ahead into a
 //     second register set), screened with three-input min over groups of 8 columns against the
-//     row's threshold (a rolled loop: the code stays small enough for the instruction cache).
-//     When a chunk has candidates each lane walks its own candidate columns, one per warp
-//     iteration, and rescores them exactly (exact coordinates from the same smem stage, the
-//     oracle's arithmetic); survivors of the row's current bound are compacted with ballots into a
+//     row's threshold into a candidate mask (skipped when no row of the warp has one); the
+//     accumulator buffer is freed as soon as the tile's four chunks are read.  Then each lane
+//     walks the candidates of its row in the whole tile, one per warp iteration (so one
+//     iteration serves every row that has a candidate), and rescores them exactly (exact
+//     coordinates from the same smem stage, the oracle's arithmetic); survivors of the row's
+//     current bound are compacted with ballots into a
 //     per-warp queue.  Once 32 entries are queued the warp drains them into the rows' lists: each
 //     row keeps its best m as a max-heap of 64-bit keys (distance bits << 32 | index) in shared
 //     memory, 32 entries go in per pass, one per lane, entries of one row serialised by match_any.
@@ -471,8 +473,9 @@ __global__ void __launch_bounds__(THREADS, Cfg<D>::CTAS_PER_SM) knn_tc_kernel(co
                 const float *exs = reinterpret_cast<const float *>(sB + s * C::STAGE_BYTES + C::OP_BYTES);
                 const int64_t j0 = (int64_t)t * RT;
                 const uint32_t taddr = tmem_base + ((uint32_t)(warp * 32) << 16) + b * RT;
-                // screen one 32-column chunk (scores in v) and queue its candidates
-                auto chunk = [&](const uint32_t (&v)[32], const int c) {
+                // screen one 32-column chunk (scores in v): this row's candidate mask, 0 when no row
+                // of the warp has one (the common case, a handful of instructions)
+                auto screen = [&](const uint32_t (&v)[32]) -> uint32_t {
                     float gmin[4];  // minimum of each group of 8 columns
 #pragma unroll
                     for (int gi = 0; gi < 4; ++gi) {
@@ -482,73 +485,93 @@ __global__ void __launch_bounds__(THREADS, Cfg<D>::CTAS_PER_SM) knn_tc_kernel(co
 #undef NNGP_V
                     }
                     const float mn = fminf(min3f(gmin[0], gmin[1], gmin[2]), gmin[3]);
-                    if (!__any_sync(FULL, mn < tq)) return;
-                    // rare path: candidate mask of this row (only groups whose minimum passes)
                     uint32_t cm = 0;
+                    if (!__any_sync(FULL, mn < tq)) return cm;
 #pragma unroll
                     for (int gi = 0; gi < 4; ++gi) {
-                        if (gmin[gi] < tq) {
+                        if (gmin[gi] < tq) {  // only groups whose minimum passes
 #pragma unroll
                             for (int k = 0; k < 8; ++k)
                                 cm |= (__uint_as_float(v[gi * 8 + k]) < tq ? 1u : 0u) << (gi * 8 + k);
                         }
                     }
-                    const int64_t jc = j0 + c * 32;
-                    const int64_t room = limit - jc;  // columns with j < limit
-                    if (room < 32) cm &= room <= 0 ? 0u : ((1u << (uint32_t)room) - 1u);
-                    // each lane walks its own candidates, one per warp iteration (the cost follows the
-                    // busiest row), rescoring them exactly from the stage's coordinates; survivors of the
-                    // row's current bound are queued and drained into the heaps in batches
-                    while (__any_sync(FULL, cm != 0)) {
-                        if (qcount > QCAP - 32) drain();
-                        bool keep = false;
-                        float d2 = 0.f;
-                        int k = 0;
-                        if (cm != 0) {
-                            k = __ffs(cm) - 1;
-                            cm &= cm - 1;
-                            // the oracle's arithmetic: ((x0 - q0)^2 + (x1 - q1)^2) + ..., each step rounded
-                            const float *rp = exs + (c * 32 + k) * C::DP;
-                            const float t0 = sub_rn(rp[0], qo[0]);
-                            d2 = mul_rn(t0, t0);
-#pragma unroll
-                            for (int f = 1; f < D; ++f) {
-                                const float tf = sub_rn(rp[f], qo[f]);
-                                d2 = add_rn(d2, mul_rn(tf, tf));
-                            }
-                            keep = d2 <= worst;  // NaN never kept
-                        }
-                        const unsigned mk = __ballot_sync(FULL, keep);
-                        if (keep) {
-                            const int pos = qcount + __popc(mk & ((1u << lane) - 1u));
-                            qd[pos] = d2;
-                            qj[pos] = (int32_t)(jc + k);
-                            qr[pos] = (uint8_t)lane;
-                        }
-                        qcount += __popc(mk);
-                    }
-                    if (qcount >= DRAIN_AT) drain();
+                    return cm;
                 };
-                // chunks in flight one ahead of the one being screened (two register sets)
+                // 1) screen the tile's four chunks (loads one chunk ahead, two register sets) into
+                //    per-chunk candidate masks; the accumulator buffer is freed once all four are read
                 uint32_t va[32], vb[32];
                 tmem_ld32_nowait(taddr, va);
                 tmem_wait_ld(va);
-#pragma unroll 1
-                for (int cp = 0; cp < RT / 64; ++cp) {
-                    tmem_ld32_nowait(taddr + (2 * cp + 1) * 32, vb);
-                    chunk(va, 2 * cp);
-                    tmem_wait_ld(vb);
-                    if (cp + 1 < RT / 64) {
-                        tmem_ld32_nowait(taddr + (2 * cp + 2) * 32, va);
-                    } else {
-                        // every chunk is in registers: the accumulator buffer is free
-                        tc_fence_before();
-                        __syncwarp();
-                        if (lane == 0) mbar_arrive(&t_empty[b]);
+                tmem_ld32_nowait(taddr + 32, vb);
+                uint32_t cm0 = screen(va);
+                tmem_wait_ld(vb);
+                tmem_ld32_nowait(taddr + 64, va);
+                uint32_t cm1 = screen(vb);
+                tmem_wait_ld(va);
+                tmem_ld32_nowait(taddr + 96, vb);
+                uint32_t cm2 = screen(va);
+                tmem_wait_ld(vb);
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&t_empty[b]);
+                uint32_t cm3 = screen(vb);
+                {  // columns with j < limit only
+                    const int64_t room = limit - j0;
+                    if (room < RT) {
+                        auto cut = [&](uint32_t &cm, int c) {
+                            const int64_t r = room - c * 32;
+                            if (r < 32) cm &= r <= 0 ? 0u : ((1u << (uint32_t)r) - 1u);
+                        };
+                        cut(cm0, 0);
+                        cut(cm1, 1);
+                        cut(cm2, 2);
+                        cut(cm3, 3);
                     }
-                    chunk(vb, 2 * cp + 1);
-                    if (cp + 1 < RT / 64) tmem_wait_ld(va);
                 }
+                // 2) candidates of the whole tile: each lane walks its own (chunk by chunk, column by
+                //    column), one per warp iteration, so a warp iteration serves every row that has one;
+                //    each is rescored exactly from the stage's coordinates and survivors of the row's
+                //    current bound are queued, then drained into the heaps in batches
+                while (__any_sync(FULL, (cm0 | cm1 | cm2 | cm3) != 0)) {
+                    if (qcount > QCAP - 32) drain();
+                    bool keep = false;
+                    float d2 = 0.f;
+                    int col = 0;
+                    if ((cm0 | cm1 | cm2 | cm3) != 0) {
+                        if (cm0) {
+                            col = __ffs(cm0) - 1;
+                            cm0 &= cm0 - 1;
+                        } else if (cm1) {
+                            col = 32 + __ffs(cm1) - 1;
+                            cm1 &= cm1 - 1;
+                        } else if (cm2) {
+                            col = 64 + __ffs(cm2) - 1;
+                            cm2 &= cm2 - 1;
+                        } else {
+                            col = 96 + __ffs(cm3) - 1;
+                            cm3 &= cm3 - 1;
+                        }
+                        // the oracle's arithmetic: ((x0 - q0)^2 + (x1 - q1)^2) + ..., each step rounded
+                        const float *rp = exs + col * C::DP;
+                        const float t0 = sub_rn(rp[0], qo[0]);
+                        d2 = mul_rn(t0, t0);
+#pragma unroll
+                        for (int f = 1; f < D; ++f) {
+                            const float tf = sub_rn(rp[f], qo[f]);
+                            d2 = add_rn(d2, mul_rn(tf, tf));
+                        }
+                        keep = d2 <= worst;  // NaN never kept
+                    }
+                    const unsigned mk = __ballot_sync(FULL, keep);
+                    if (keep) {
+                        const int pos = qcount + __popc(mk & ((1u << lane) - 1u));
+                        qd[pos] = d2;
+                        qj[pos] = (int32_t)(j0 + col);
+                        qr[pos] = (uint8_t)lane;
+                    }
+                    qcount += __popc(mk);
+                }
+                if (qcount >= DRAIN_AT) drain();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&b_empty[s]);
             }
