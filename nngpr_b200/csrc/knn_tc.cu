@@ -14,11 +14,13 @@
 //     adds at most K' ulps; eps = 2^-16 (|qc| + max|rc|)^2 covers both with a margin of 4 or more,
 //     so every ref the exact algorithm inserts still passes the screen;
 //   * persistent CTAs (work items = query tiles handed out heaviest first through a global
-//     counter), 160 threads: warp 4 allocates TMEM (256 columns = two 128-column accumulators) and
+//     counter), 160 threads: warp 4 allocates TMEM (two 128-column accumulators, or one when
+//     three CTAs share the SM) and
 //     one of its lanes issues the TMA bulk copies of ref tiles into a shared-memory ring (operands
 //     and exact coordinates in one copy) and the MMAs; warps 0-3 are the epilogue, warp w owning
-//     query rows 32w..32w+31 (its TMEM lane quadrant).  Two CTAs share an SM when shared memory
-//     allows (small d), so that each scheduler has two epilogue warps;
+//     query rows 32w..32w+31 (its TMEM lane quadrant).  Up to three CTAs share an SM when shared
+//     memory allows (small d): the epilogue is latency-bound, and every extra warp per scheduler
+//     shows (d = 3: 30.8 ms with two CTAs per SM, 23.1 ms with three, n = 434,874);
 //   * epilogue: each 32-column chunk of a row is one tcgen05.ld (issued one chunk ahead into a
 //     second register set), screened with three-input min over groups of 8 columns against the
 //     row's threshold into a candidate mask (skipped when no row of the warp has one); the
@@ -56,8 +58,8 @@ static_assert(THREADS == kTcThreads, "thread count");
 constexpr int LIST = 32;       // largest num_nn
 constexpr int HS = 33;         // heap row stride in 64-bit keys (odd: rows of a warp hit distinct banks)
 constexpr int DRAIN_AT = 32;   // queued entries that trigger a drain at the end of a chunk
-constexpr int QCAP = 512;      // candidate queue entries per epilogue warp
-constexpr uint32_t TMEM_COLS = 2 * RT;
+constexpr int QCAP = 256;      // candidate queue entries per epilogue warp
+constexpr uint32_t kSelftestCols = 2 * RT;  // TMEM columns of the layout self-test
 constexpr float kEpsTc = 1.52587890625e-05f;       // 2^-16
 constexpr float kPadNorm = 1.7014118346046923e38f;  // 2^127: padded refs never pass a finite screen
 // list key: FP32 distance bits (non-negative, so integer order = float order) << 32 | index;
@@ -78,13 +80,18 @@ struct Cfg {
     static constexpr int QUEUE_BYTES = EPI_WARPS * QCAP * (4 + 4 + 1);
     static constexpr int BAR_BYTES = 256;
     static constexpr int FIXED = 1024 + A_BYTES + LIST_BYTES + QUEUE_BYTES + BAR_BYTES;
-    // two CTAs per SM if at least 2 stages fit in half an SM's shared memory, else one CTA
-    static constexpr int HALF_SM = 112 * 1024;
-    static constexpr int ST2 = (HALF_SM - FIXED) / STAGE_BYTES;
+    // as many CTAs per SM (up to 3) as hold at least 2 stages each: more epilogue warps per
+    // scheduler.  Three CTAs share TMEM with one accumulator buffer each (the epilogue frees it
+    // as soon as a tile's scores are in registers); one or two CTAs double-buffer it.
+    static constexpr int ST3 = (75 * 1024 - FIXED) / STAGE_BYTES;
+    static constexpr int ST2 = (112 * 1024 - FIXED) / STAGE_BYTES;
     static constexpr int ST1 = (220 * 1024 - FIXED) / STAGE_BYTES;
-    static constexpr int STAGES = ST2 >= 2 ? (ST2 > 4 ? 4 : ST2) : (ST1 > 4 ? 4 : ST1);
+    static constexpr int CTAS_PER_SM = ST3 >= 2 ? 3 : (ST2 >= 2 ? 2 : 1);
+    static constexpr int STN = CTAS_PER_SM == 3 ? ST3 : (CTAS_PER_SM == 2 ? ST2 : ST1);
+    static constexpr int STAGES = STN > 4 ? 4 : STN;
     static constexpr int SMEM = FIXED + STAGES * STAGE_BYTES;
-    static constexpr int CTAS_PER_SM = ST2 >= 2 ? 2 : 1;
+    static constexpr int NBUF = CTAS_PER_SM == 3 ? 1 : 2;  // accumulator buffers in TMEM
+    static constexpr uint32_t TMEM_COLS = NBUF * RT;       // a power of two >= 32
     static_assert(STAGES >= 2, "ref tile too large for two stages");
     // K-major no-swizzle canonical layout: 8-row x 16-byte core matrices, SBO = 128 B between
     // 8-row groups, LBO between 16-byte K chunks
@@ -287,7 +294,7 @@ __global__ void __launch_bounds__(THREADS, Cfg<D>::CTAS_PER_SM) knn_tc_kernel(co
             mbar_init(&b_full[s], 1);
             mbar_init(&b_empty[s], 1 + EPI_WARPS);  // the MMA commit + the epilogue warps (exact coordinates)
         }
-        for (int b = 0; b < 2; ++b) {
+        for (int b = 0; b < C::NBUF; ++b) {
             mbar_init(&t_full[b], 1);
             mbar_init(&t_empty[b], EPI_WARPS);
         }
@@ -298,7 +305,7 @@ __global__ void __launch_bounds__(THREADS, Cfg<D>::CTAS_PER_SM) knn_tc_kernel(co
     if (producer_warp) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                          smem_addr(const_cast<uint32_t *>(tmem_slot))),
-                     "r"(TMEM_COLS));
+                     "r"(C::TMEM_COLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     tc_fence_before();
@@ -355,13 +362,13 @@ __global__ void __launch_bounds__(THREADS, Cfg<D>::CTAS_PER_SM) knn_tc_kernel(co
                 const uint32_t a_addr = smem_addr(sA);
                 for (uint32_t t = 0; t < ntiles && !aborted; ++t) {
                     const uint32_t g = G + t;
-                    const uint32_t s = g % S, b = g & 1;
+                    const uint32_t s = g % S, b = g % C::NBUF, use = g / C::NBUF;
                     if (!mbar_wait_bounded(&b_full[s], (g / S) & 1)) {
                         aborted = true;
                         break;
                     }
                     tma_landed = g + 1;
-                    if (!mbar_wait_bounded(&t_empty[b], ((g >> 1) & 1) ^ 1)) {
+                    if (!mbar_wait_bounded(&t_empty[b], (use & 1) ^ 1)) {
                         aborted = true;
                         break;
                     }
@@ -463,8 +470,8 @@ __global__ void __launch_bounds__(THREADS, Cfg<D>::CTAS_PER_SM) knn_tc_kernel(co
             const uint32_t G = g_tile;
             for (uint32_t t = 0; t < ntiles; ++t) {
                 const uint32_t g = G + t;
-                const uint32_t s = g % S, b = g & 1;
-                if (!mbar_wait_bounded(&t_full[b], (g >> 1) & 1)) aborted = true;
+                const uint32_t s = g % S, b = g % C::NBUF;
+                if (!mbar_wait_bounded(&t_full[b], (g / C::NBUF) & 1)) aborted = true;
                 if (__any_sync(FULL, aborted)) {
                     aborted = true;
                     break;
@@ -608,14 +615,16 @@ __global__ void __launch_bounds__(THREADS, Cfg<D>::CTAS_PER_SM) knn_tc_kernel(co
         // copies issued but never waited for: let them land before the CTA's shared memory goes
         for (uint32_t g = tma_landed; g < tma_issued; ++g) mbar_wait_bounded(&b_full[g % S], (g / S) & 1);
         // MMAs in flight: the last t_full phase of each accumulator buffer
-        if (g_tile > 0) mbar_wait_bounded(&t_full[(g_tile - 1) & 1], ((g_tile - 1) >> 1) & 1);
-        if (g_tile > 1) mbar_wait_bounded(&t_full[(g_tile - 2) & 1], ((g_tile - 2) >> 1) & 1);
+        for (uint32_t i = 1; i <= (uint32_t)C::NBUF && i <= g_tile; ++i) {
+            const uint32_t g = g_tile - i;
+            mbar_wait_bounded(&t_full[g % C::NBUF], (g / C::NBUF) & 1);
+        }
     }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     if (producer_warp) {
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(C::TMEM_COLS));
     }
 }
 
@@ -642,7 +651,7 @@ __global__ void __launch_bounds__(THREADS) tc_layout_selftest_kernel(const float
     }
     if (warp == EPI_WARPS) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_slot)),
-                     "r"(TMEM_COLS));
+                     "r"(kSelftestCols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     tc_fence_before();
@@ -672,7 +681,7 @@ __global__ void __launch_bounds__(THREADS) tc_layout_selftest_kernel(const float
     __syncthreads();
     tc_fence_after();
     if (warp == EPI_WARPS) {
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(kSelftestCols));
     }
 }
 
