@@ -426,8 +426,9 @@ def run_plain(args, torch, x32, y64, xq32, p, flags, flush, lml_ours):
     c.record()
     torch.cuda.synchronize()
     pred_ms = a.elapsed_time(c)
-    step_ms = float(np.mean(ms))
-    return {'value': 1e3 / step_ms, 'unit': UNIT, 'ms_per_step': step_ms, 'knn_ms': float(np.mean(knn_ms)),
+    step_ms = float(np.min(ms))  # the comparator's best step (its torch batched solvers vary run to run)
+    return {'value': 1e3 / step_ms, 'unit': UNIT, 'ms_per_step': step_ms, 'knn_ms': float(np.min(knn_ms)),
+            'ms_all_steps': [float(v) for v in ms],
             'steps': args.plain_steps, 'lists_identical': same, 'lml': lml,
             'lml_rel_diff_vs_ours': abs(lml - lml_ours) / abs(lml_ours),
             'predict': {'value': N_PRED / (pred_ms * 1e-3), 'unit': 'points/s', 'ms': pred_ms},
@@ -774,7 +775,7 @@ def main():
     ap.add_argument('--no-e2e', action='store_true', help='skip the end-to-end API timing')
     ap.add_argument('--no-predict', action='store_true', help='skip the predict timing')
     ap.add_argument('--no-plain', action='store_true', help='skip the plain FP32 GPU comparator')
-    ap.add_argument('--plain-steps', type=int, default=2, help='timed steps of the plain comparator')
+    ap.add_argument('--plain-steps', type=int, default=3, help='timed steps of the plain comparator (best reported)')
     ap.add_argument('--requests', type=int, default=400, help='serving workload: requests in the stream')
     ap.add_argument('--rate', type=float, default=200.0, help='serving workload: mean arrivals per second')
     ap.add_argument('--plain-requests', type=int, default=100, help='serving workload: requests the plain form runs')

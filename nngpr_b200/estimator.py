@@ -343,4 +343,40 @@ class B200Nngpr(GaussianProcessRegressor):
         return mean, std
 
     def sample_y(self, X, n_samples=1, random_state=0, conditioning_method=None):
-        raise NotImplementedError("sample_y is not part of the B200 hot path")
+        """Samples of the predictive marginals at ``X``, ``base_nngpr.py:616-689`` with
+        ``conditioning_method='only-train'``: every query point is conditioned on the training
+        set only, so its samples are independent draws ``mean + std * N(0, 1)`` (the reference's
+        own fast path, ``:672-689``).  The normal draws come from a device generator seeded by
+        ``random_state`` (an int, a ``RandomState`` or ``None``), so they differ from the
+        reference's worker streams, not in distribution.  Shape ``(n_samples_X, n_samples)`` or
+        ``(n_samples_X, n_targets, n_samples)``."""
+        conditioning_method = 'only-train' if conditioning_method is None else conditioning_method
+        if conditioning_method not in {'only-train', 'full', 'full-double-nn'}:
+            raise ValueError(f"unknown conditioning_method {conditioning_method!r}")
+        if conditioning_method != 'only-train':
+            raise NotImplementedError("B200Nngpr implements sample_y(conditioning_method='only-train')")
+        mean, std = self.predict(X, return_std=True)
+        mu = np.asarray(mean, dtype=np.float64)
+        sd = np.asarray(std, dtype=np.float64)
+        single = mu.ndim == 1
+        if single:
+            mu, sd = mu[:, None], sd[:, None]
+        rs = check_random_state(random_state)
+        seed = int(rs.randint(0, 2 ** 31))
+        dev = self._device
+        gen = torch.Generator(device=dev)
+        gen.manual_seed(seed)
+        z = torch.randn((mu.shape[0], mu.shape[1], int(n_samples)), generator=gen, device=dev, dtype=torch.float64)
+        out = torch.from_numpy(mu).to(dev)[..., None] + torch.from_numpy(sd).to(dev)[..., None] * z
+        out = out.cpu().numpy()
+        return out[:, 0, :] if single else out
+
+    # ---- persistence ------------------------------------------------------------------------
+    def __getstate__(self):
+        """Pickle without the device and pinned copies of the training set: they are rebuilt
+        from ``X_train_``/``y_train_`` on first use after loading."""
+        state = super().__getstate__() if hasattr(super(), '__getstate__') else self.__dict__.copy()
+        state = dict(state)
+        state.pop('_device_cache', None)
+        state.pop('_pinned_cache', None)
+        return state

@@ -93,3 +93,37 @@ def test_fit_with_optimizer_default_settings():
     a = B200Nngpr(**kw).fit(g['x'], g['y'])
     b = B200Nngpr(allow_downcast_f32='no', **kw).fit(g['x'], g['y'])
     assert np.max(np.abs(a.kernel_.theta - b.kernel_.theta)) < 1e-6
+
+
+def test_sample_y_only_train_shapes_seed_and_moments():
+    """sample_y (base_nngpr.py:616-689, only-train): independent draws mean + std * N(0, 1)."""
+    g = load('ard_n400_d5_m12_y2')
+    gpr = make('ard_n400_d5_m12_y2', g).fit(g['x'], g['y'])
+    xq = g['xq'][:40]
+    mean, std = gpr.predict(xq, return_std=True)
+    s = gpr.sample_y(xq, n_samples=6000, random_state=3)
+    assert s.shape == (40, 2, 6000)
+    np.testing.assert_array_equal(s, gpr.sample_y(xq, n_samples=6000, random_state=3))
+    assert not np.array_equal(s[..., :10], gpr.sample_y(xq, n_samples=10, random_state=4))
+    se = std / np.sqrt(6000)
+    assert np.all(np.abs(s.mean(-1) - mean) < 6 * se)
+    assert np.all(np.abs(s.std(-1) / std - 1) < 0.06)
+    g1 = load('cpu_n2000_d3_m16')
+    gpr1 = make('cpu_n2000_d3_m16', g1).fit(g1['x'], g1['y'])
+    assert gpr1.sample_y(g1['xq'][:7], n_samples=3).shape == (7, 3)
+    with pytest.raises(NotImplementedError):
+        gpr1.sample_y(g1['xq'][:7], conditioning_method='full')
+
+
+def test_pickle_round_trip():
+    import pickle
+    g = load('cpu_n2000_d3_m16')
+    gpr = make('cpu_n2000_d3_m16', g).fit(g['x'], g['y'])
+    mean, std = gpr.predict(g['xq'], return_std=True)
+    blob = pickle.dumps(gpr)
+    assert len(blob) < 2 * (g['x'].nbytes + g['y'].nbytes) + 200_000  # no device or pinned copies inside
+    back = pickle.loads(blob)
+    m2, s2 = back.predict(g['xq'], return_std=True)
+    np.testing.assert_array_equal(mean, m2)
+    np.testing.assert_array_equal(std, s2)
+    assert back.log_marginal_likelihood(back.kernel_.theta) == gpr.log_marginal_likelihood(gpr.kernel_.theta)
