@@ -43,7 +43,7 @@
 extern "C" {
 #endif
 
-#define NNGP_ABI_VERSION 1
+#define NNGP_ABI_VERSION 2
 
 typedef enum nngp_status {
     NNGP_OK = 0,
@@ -61,11 +61,14 @@ typedef enum nngp_status {
 #define NNGP_FLAG_FP64_FALLBACK 8  /* some FP32 systems were re-solved in FP64 (informational) */
 
 /*
- * Kernel  k(a, b) = rbf_level * exp(-sum_f (a_f - b_f)^2 / (2 l_f^2)) + const_value
- *                   + noise_level * [a is b]
- * i.e. the WhiteKernel + ConstantKernel + ConstantKernel*RBF family that the reference
- * accelerates (nngpr/cuda_kernel_accelerators.py:169-194, parameters from
- * get_kernel_params :520-581).  `alpha` is the GaussianProcessRegressor jitter added to
+ * Kernel  k(a, b) = rbf_level * s(r) + const_value + noise_level * [a is b],
+ * r^2 = sum_f (a_f - b_f)^2 / l_f^2, with the stationary part s chosen by `family`:
+ * NNGP_FAMILY_RBF s = exp(-r^2 / 2) -- the WhiteKernel + ConstantKernel + ConstantKernel*RBF
+ * family that the reference accelerates on CUDA (nngpr/cuda_kernel_accelerators.py:169-194,
+ * parameters from get_kernel_params :520-581) -- or the Matern kernels the reference
+ * evaluates on its generic path (nngpr/batched_kernels.py:1070-1131): nu = 1/2
+ * s = exp(-r); nu = 3/2 s = (1 + sqrt3 r) exp(-sqrt3 r); nu = 5/2
+ * s = (1 + sqrt5 r + 5 r^2 / 3) exp(-sqrt5 r).  `alpha` is the GaussianProcessRegressor jitter added to
  * every valid diagonal slot (base_nngpr.py:555-556; training slots only in predict,
  * :1106-1107).  The idx_* fields give the position of each free hyperparameter in
  * kernel.theta (get_kernel_theta_mapping, :583-649), -1 when fixed or absent; the
@@ -78,13 +81,19 @@ typedef struct nngp_kernel {
     double noise_level;
     double alpha;
     const double *length_scale; /* HOST pointer: n_ls values, 1 (isotropic) or d (ARD) */
-    int32_t n_ls;               /* 0 = no RBF term (rbf_level must then be 0) */
+    int32_t n_ls;               /* 0 = no stationary term (rbf_level must then be 0) */
     int32_t idx_rbf_level;
     int32_t idx_const;
     int32_t idx_noise;
     int32_t idx_ls;
     int32_t n_theta;
+    int32_t family;             /* NNGP_FAMILY_* (0 = RBF) */
 } nngp_kernel;
+
+#define NNGP_FAMILY_RBF 0
+#define NNGP_FAMILY_MATERN12 1
+#define NNGP_FAMILY_MATERN32 2
+#define NNGP_FAMILY_MATERN52 3
 
 /* ---------------------------------------------------------------------------------------
  * Library information

@@ -44,6 +44,7 @@ class NngpKernel(ctypes.Structure):
         ('idx_noise', ctypes.c_int32),
         ('idx_ls', ctypes.c_int32),
         ('n_theta', ctypes.c_int32),
+        ('family', ctypes.c_int32),
     ]
 
 

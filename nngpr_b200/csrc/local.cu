@@ -50,6 +50,7 @@ struct LocalArgs {
     int64_t n_points;
     int d, ydim, m;
     int ard;  // 1: per-feature length scales
+    int family;  // stationary part: NNGP_FAMILY_RBF or a Matern (include/nngp_b200.h)
     int idx_rbf, idx_const, idx_noise, idx_ls, n_theta;
     double inv_ls[kMaxDimLocal];
 };
@@ -57,6 +58,33 @@ struct LocalArgs {
 template <typename T> __device__ __forceinline__ T dsqrt(T v) { return sqrt(v); }
 template <typename T> __device__ __forceinline__ T dexp(T v) { return exp(v); }
 template <> __device__ __forceinline__ float dexp<float>(float v) { return expf(v); }
+
+// Unit-amplitude stationary part s of the kernel at squared scaled distance sq (formulas of
+// nngpr/batched_kernels.py:1070-1088 for the Matern kernels; RBF exp(-sq / 2)).
+template <bool MATERN, typename T> __device__ __forceinline__ T kern_s(int family, T sq) {
+    if (!MATERN || family == NNGP_FAMILY_RBF) return dexp<T>(T(-0.5) * sq);
+    if (family == NNGP_FAMILY_MATERN12) return dexp<T>(-dsqrt<T>(sq));
+    if (family == NNGP_FAMILY_MATERN32) {
+        const T r = dsqrt<T>(T(3) * sq);
+        return (T(1) + r) * dexp<T>(-r);
+    }
+    const T r = dsqrt<T>(T(5) * sq);
+    return (T(1) + r + r * r / T(3)) * dexp<T>(-r);
+}
+
+// g with d s / d log l_f = g * t_f^2 (t_f the scaled difference of feature f); isotropic:
+// d s / d log l = g * sq.  `s` is kern_s at the same sq.  Reference gradients:
+// nngpr/batched_kernels.py:1108-1120 (Matern), :895-898 (RBF).
+template <bool MATERN, typename T> __device__ __forceinline__ T kern_g(int family, T sq, T s) {
+    if (!MATERN || family == NNGP_FAMILY_RBF) return s;
+    if (family == NNGP_FAMILY_MATERN12) {
+        const T r = dsqrt<T>(sq);
+        return r > T(0) ? s / r : T(0);  // every t_f is 0 where r is
+    }
+    if (family == NNGP_FAMILY_MATERN32) return T(3) * dexp<T>(-dsqrt<T>(T(3) * sq));
+    const T r = dsqrt<T>(T(5) * sq);
+    return T(5) / T(3) * (T(1) + r) * dexp<T>(-r);
+}
 
 // ---------------------------------------------------------------------------------------
 // Warp kernel
@@ -80,7 +108,7 @@ struct WarpSmem {
 
 // Solves point p's system in precision TC.  Returns false (and commits nothing) when TC is
 // float and a pivot fell below the FP64 threshold.
-template <typename TC, typename TIn, bool GRAD, bool PRED>
+template <typename TC, typename TIn, bool GRAD, bool PRED, bool MATERN>
 __device__ __forceinline__ bool warp_system(const LocalArgs &a, int64_t p, int lane, const TIn *__restrict__ x_ref,
                                             const TIn *__restrict__ y_ref, const TIn *__restrict__ x_pt,
                                             const TIn *__restrict__ y_pt, const int32_t *__restrict__ nbr,
@@ -136,12 +164,12 @@ __device__ __forceinline__ bool warp_system(const LocalArgs &a, int64_t p, int l
 #pragma unroll
     for (int k = 0; k < M; ++k) {
         const bool vk = (vmask >> k) & 1u;
-        const TC e = rbf * dexp<TC>(TC(-0.5) * r[k]);
+        const TC e = rbf * kern_s<MATERN>(a.family, r[k]);
         TC kv = (valid && vk) ? e + cst : TC(0);
         if (k == lane) kv = valid ? kv + diag_add : TC(1);
         r[k] = kv;
     }
-    TC kvec = valid ? rbf * dexp<TC>(TC(-0.5) * rp) + cst : TC(0);  // K[p][lane]
+    TC kvec = valid ? rbf * kern_s<MATERN>(a.family, rp) + cst : TC(0);  // K[p][lane]
     const TC kpp = rbf + cst + (TC)a.noise + (PRED ? TC(0) : (TC)a.alpha);
 
     // ---- Cholesky of the neighbour block fused with l = L^-1 k ----------------------------
@@ -252,22 +280,24 @@ __device__ __forceinline__ bool warp_system(const LocalArgs &a, int64_t p, int l
         const bool vk_ok = (vmask >> k) & 1u;
         const TC G = wsum * b_own * bk - TC(0.5) * (b_own * vk + v_own * bk);
         const TC wgt = (valid && vk_ok) ? (k < lane ? TC(2) : (k == lane ? TC(1) : TC(0))) : TC(0);
-        const TC e = rbf * dexp<TC>(TC(-0.5) * r[k]);
+        const TC s = kern_s<MATERN>(a.family, r[k]);
         const TC gw = wgt * G;
-        const TC ge = gw * e;
+        const TC ge = gw * (rbf * s);
+        const TC gl = MATERN ? gw * (rbf * kern_g<MATERN>(a.family, r[k], s)) : ge;
         g_amp += ge;
         g_cst += gw;
-        g_iso = fma(ge, r[k], g_iso);
+        g_iso = fma(gl, r[k], g_iso);
         if (k == lane && valid) g_noise += G;
-        r[k] = ge;  // kept for the per-feature length-scale terms
+        r[k] = gl;  // kept for the per-feature length-scale terms
     }
     // pair (p, lane), weight 2, and (p, p)
     const TC Gp = valid ? TC(0.5) * v_own - wsum * b_own : TC(0);
-    const TC ep = rbf * dexp<TC>(TC(-0.5) * rp);
-    const TC gpe = TC(2) * Gp * ep;
+    const TC sp = kern_s<MATERN>(a.family, rp);
+    const TC gpe = TC(2) * Gp * (rbf * sp);
+    const TC gpl = MATERN ? TC(2) * Gp * (rbf * kern_g<MATERN>(a.family, rp, sp)) : gpe;
     g_amp += gpe;
     g_cst += TC(2) * Gp;
-    g_iso = fma(gpe, rp, g_iso);
+    g_iso = fma(gpl, rp, g_iso);
     const double amp_t = (double)warp_sum(g_amp) + (double)wsum * a.rbf;
     const double cst_t = (double)warp_sum(g_cst) + (double)wsum;
     const double noi_t = (double)warp_sum(g_noise) + (double)wsum;
@@ -289,7 +319,7 @@ __device__ __forceinline__ bool warp_system(const LocalArgs &a, int64_t p, int l
                 acc = fma(r[k] * t, t, acc);
             }
             const TC t = xi - xs[M * ds + f];
-            acc = fma(gpe * t, t, acc);
+            acc = fma(gpl * t, t, acc);
             const double s = (double)warp_sum(acc);
             if (lane == 0) gacc[a.idx_ls + f] += s;
         }
@@ -298,7 +328,7 @@ __device__ __forceinline__ bool warp_system(const LocalArgs &a, int64_t p, int l
     return true;
 }
 
-template <typename TIn, bool GRAD, bool PRED>
+template <typename TIn, bool GRAD, bool PRED, bool MATERN>
 __global__ void __launch_bounds__(kLocWarps * 32) local_warp_kernel(
     const __grid_constant__ LocalArgs a, const TIn *__restrict__ x_ref, const TIn *__restrict__ y_ref,
     const TIn *__restrict__ x_pt, const TIn *__restrict__ y_pt, const int32_t *__restrict__ nbr,
@@ -316,12 +346,12 @@ __global__ void __launch_bounds__(kLocWarps * 32) local_warp_kernel(
     for (int64_t p = (int64_t)blockIdx.x * kLocWarps + warp; p < a.n_points; p += nwarps) {
         bool done = false;
         if constexpr (std::is_same<TIn, float>::value) {
-            done = warp_system<float, TIn, GRAD, PRED>(a, p, lane, x_ref, y_ref, x_pt, y_pt, nbr, wsm, ll_acc, mean,
+            done = warp_system<float, TIn, GRAD, PRED, MATERN>(a, p, lane, x_ref, y_ref, x_pt, y_pt, nbr, wsm, ll_acc, mean,
                                                        var, flags);
         }
         if (!done) {
             if constexpr (std::is_same<TIn, float>::value) used_fp64 = true;
-            warp_system<double, TIn, GRAD, PRED>(a, p, lane, x_ref, y_ref, x_pt, y_pt, nbr, wsm, ll_acc, mean, var,
+            warp_system<double, TIn, GRAD, PRED, MATERN>(a, p, lane, x_ref, y_ref, x_pt, y_pt, nbr, wsm, ll_acc, mean, var,
                                                  flags);
         }
     }
@@ -445,7 +475,7 @@ __global__ void __launch_bounds__(kBlkThreads) local_block_kernel(
                     const double t = xs[i * d + f] - xs[jx * d + f];
                     r = fma(t, t, r);
                 }
-                kv = a.rbf * exp(-0.5 * r) + a.cst;
+                kv = a.rbf * kern_s<true>(a.family, r) + a.cst;
                 if (i == jx) kv += a.noise + ((i == m && PRED) ? 0.0 : a.alpha);
             } else {
                 kv = (i == jx) ? 1.0 : 0.0;
@@ -550,11 +580,11 @@ __global__ void __launch_bounds__(kBlkThreads) local_block_kernel(
                 const double t = xs[i * d + f] - xs[jx * d + f];
                 r = fma(t, t, r);
             }
-            const double e0 = a.rbf * exp(-0.5 * r);
-            t_amp += wgt * G * e0;
+            const double s0 = kern_s<true>(a.family, r);
+            t_amp += wgt * G * a.rbf * s0;
             t_cst += wgt * G;
             if (i == jx) t_noise += G;
-            t_iso += wgt * G * e0 * r;
+            t_iso += wgt * G * a.rbf * kern_g<true>(a.family, r, s0) * r;
         }
         g_loc[0] += t_amp;
         g_loc[1] += t_cst;
@@ -576,7 +606,7 @@ __global__ void __launch_bounds__(kBlkThreads) local_block_kernel(
                         r = fma(t, t, r);
                     }
                     const double t = xs[i * d + f] - xs[jx * d + f];
-                    acc += 2.0 * G * a.rbf * exp(-0.5 * r) * t * t;
+                    acc += 2.0 * G * a.rbf * kern_g<true>(a.family, r, kern_s<true>(a.family, r)) * t * t;
                 }
                 const double s = block_sum(acc, scratch);
                 if (tid == 0) o[1 + a.idx_ls + f] += s;
@@ -682,6 +712,9 @@ nngp_status fill_args(LocalArgs &a, const nngp_kernel *k, int d, int ydim, int m
     a.ydim = ydim;
     a.m = m;
     a.ard = k->n_ls == d && d > 1;
+    if (k->family < NNGP_FAMILY_RBF || k->family > NNGP_FAMILY_MATERN52)
+        return fail(NNGP_ERR_INVALID_ARGUMENT, "kernel family must be one of NNGP_FAMILY_*");
+    a.family = k->family;
     a.idx_rbf = grad ? k->idx_rbf_level : -1;
     a.idx_const = grad ? k->idx_const : -1;
     a.idx_noise = grad ? k->idx_noise : -1;
@@ -706,7 +739,8 @@ nngp_status launch_local(const LocalPlan &pl, const LocalArgs &a, const TIn *x_r
                          const TIn *y_pt, const int32_t *nbr, double *block_out, TIn *mean, TIn *var, int32_t *flags,
                          cudaStream_t stream) {
     if (pl.warp) {
-        auto fn = local_warp_kernel<TIn, GRAD, PRED>;
+        auto fn = a.family == NNGP_FAMILY_RBF ? local_warp_kernel<TIn, GRAD, PRED, false>
+                                              : local_warp_kernel<TIn, GRAD, PRED, true>;
         NNGP_CUDA_TRY(ensure_smem_limit(reinterpret_cast<const void *>(fn), (int)pl.smem));
         fn<<<pl.grid, kLocWarps * 32, pl.smem, stream>>>(a, x_ref, y_ref, x_pt, y_pt, nbr, block_out, mean, var, flags);
     } else {

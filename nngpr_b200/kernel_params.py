@@ -1,12 +1,14 @@
-"""Reduction of a kernel tree to ``White + const + rbf_level * RBF(length_scale)``.
+"""Reduction of a kernel tree to ``White + const + rbf_level * S(length_scale)``.
 
-The GPU path evaluates one kernel family, the one the reference accelerates on CUDA:
-sums and products of ``WhiteKernel``, ``ConstantKernel`` and one ``RBF``
-(``nngpr/cuda_kernel_accelerators.py:169-194``).  This module walks a scikit-learn
-kernel tree (the reference's ``nngpr.batched_kernels`` classes subclass the
-scikit-learn ones, so both are accepted) and returns
+The GPU path evaluates one kernel family: sums and products of ``WhiteKernel``,
+``ConstantKernel`` and one stationary kernel ``S``, either the ``RBF`` the reference
+accelerates on CUDA (``nngpr/cuda_kernel_accelerators.py:169-194``) or a ``Matern`` with
+nu = 1/2, 3/2 or 5/2 that the reference evaluates on its generic path
+(``nngpr/batched_kernels.py:1070-1131``).  This module walks a scikit-learn kernel tree (the
+reference's ``nngpr.batched_kernels`` classes subclass the scikit-learn ones, so both are
+accepted) and returns
 
-* the four parameter values (``extract``; rules of ``RbfAccelerator.get_kernel_params``,
+* the parameter values (``extract``; rules of ``RbfAccelerator.get_kernel_params``,
   ``cuda_kernel_accelerators.py:520-581``), and
 * the position of each free hyperparameter in ``kernel.theta`` (``theta_map``; rules of
   ``get_kernel_theta_mapping``, ``:583-649``: clone the kernel with known theta values
@@ -38,6 +40,7 @@ class RbfParams:
     const_value: float = 0.0
     noise_level: float = 0.0
     length_scale: object = None  # None (no RBF), float, or 1-D float64 array
+    family: int = 0  # stationary part: 0 RBF, 1/2/3 Matern nu = 1/2, 3/2, 5/2 (NNGP_FAMILY_*)
     idx_rbf_level: int = -1
     idx_const: int = -1
     idx_noise: int = -1
@@ -66,6 +69,10 @@ class RbfParams:
         return ls
 
 
+# nngp_kernel.family of the Matern smoothness values (include/nngp_b200.h, NNGP_FAMILY_*)
+MATERN_FAMILY = {0.5: 1, 1.5: 2, 2.5: 3}
+
+
 def _unsupported(msg: str):
     return NotImplementedError("Cannot accelerate this kernel: " + msg)
 
@@ -78,9 +85,17 @@ def _values(kernel) -> dict:
     if isinstance(kernel, skk.ConstantKernel):
         return {'constant_value': float(kernel.constant_value)}
     if isinstance(kernel, skk.Matern):
-        # Matern subclasses RBF in scikit-learn (and in nngpr.batched_kernels); the reference's
-        # issubclass(..., RBF) test would evaluate it as an RBF.  It is a different kernel.
-        raise _unsupported("Matern kernels are not in the accelerated family")
+        # Matern subclasses RBF in scikit-learn (and in nngpr.batched_kernels), so it is tested
+        # first; the reference's generic path evaluates nu = 1/2, 3/2, 5/2 and inf
+        # (batched_kernels.py:1070-1131), nu = inf being the RBF
+        nu = float(kernel.nu)
+        family = 0 if np.isinf(nu) else MATERN_FAMILY.get(nu)
+        if family is None:
+            raise _unsupported(f"Matern with nu = {nu} (only 0.5, 1.5, 2.5 and inf)")
+        ls = kernel.length_scale
+        if isinstance(ls, numbers.Number) or np.ndim(ls) == 0:
+            return {'length_scale': float(ls), 'family': family}
+        return {'length_scale': np.asarray(ls, dtype=np.float64).reshape(-1).copy(), 'family': family}
     if isinstance(kernel, skk.RBF):
         ls = kernel.length_scale
         if isinstance(ls, numbers.Number) or np.ndim(ls) == 0:
@@ -91,7 +106,7 @@ def _values(kernel) -> dict:
         a_rbf = bool(set(a) - {'noise_level', 'constant_value'})
         b_rbf = bool(set(b) - {'noise_level', 'constant_value'})
         if a_rbf and b_rbf:
-            raise _unsupported("a sum of two RBF kernels")
+            raise _unsupported("a sum of two stationary (RBF / Matern) kernels")
         if a_rbf:
             a, b = b, a
         # a has no RBF part: fold its white/constant terms into b
@@ -191,6 +206,7 @@ def extract(kernel) -> RbfParams:
     if 'length_scale' in vals:
         p.length_scale = vals['length_scale']
         p.rbf_level = float(vals.get('rbf_level', 1.0))
+        p.family = int(vals.get('family', 0))
     else:
         p.length_scale = None
         p.rbf_level = 0.0

@@ -118,6 +118,7 @@ def _kernel_struct(p: RbfParams, alpha: float, d: int, keep: list) -> _lib.NngpK
     k.idx_noise = p.idx_noise
     k.idx_ls = p.idx_ls
     k.n_theta = p.n_theta
+    k.family = int(p.family)
     return k
 
 

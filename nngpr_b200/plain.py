@@ -56,6 +56,24 @@ def plain_knn(ref, query, num_nn: int, ref_cut_index, length_scale) -> 'torch.Te
     return out
 
 
+def _stationary(family: int, sq):
+    """Stationary part and its length-scale gradient factor (RBF, ``batched_kernels.py:884-898``;
+    Matern nu = 1/2, 3/2, 5/2, ``:1070-1120``)."""
+    torch = _torch()
+    if family == 0:
+        S = torch.exp(-0.5 * sq)
+        return S, S
+    r = torch.sqrt(sq)
+    if family == 1:
+        S = torch.exp(-r)
+        return S, torch.where(r > 0, S / torch.where(r > 0, r, 1.0), 0.0)
+    if family == 2:
+        a = math.sqrt(3.0) * r
+        return (1.0 + a) * torch.exp(-a), 3.0 * torch.exp(-a)
+    a = math.sqrt(5.0) * r
+    return (1.0 + a + a * a / 3.0) * torch.exp(-a), 5.0 / 3.0 * (1.0 + a) * torch.exp(-a)
+
+
 def _fill(xn, valid, p: RbfParams, ls, eval_gradient: bool):
     """``K (b, k, k)`` and, with ``eval_gradient``, ``dK (b, k, k, n_theta)`` of gathered points
     ``xn (b, k, d)`` -- the reference's fill (``cuda_kernel_accelerators.py:748-863``)."""
@@ -63,7 +81,9 @@ def _fill(xn, valid, p: RbfParams, ls, eval_gradient: bool):
     k = xn.shape[1]
     diff = (xn[:, :, None, :] - xn[:, None, :, :]) / ls
     sq = diff * diff
-    E = p.rbf_level * torch.exp(-0.5 * sq.sum(-1))
+    S, Sg = _stationary(p.family, sq.sum(-1))
+    E = p.rbf_level * S
+    Eg = p.rbf_level * Sg  # d E / d log l_f = Eg * sq_f
     eye = torch.eye(k, dtype=torch.bool, device=xn.device)[None]
     pair = valid[:, :, None] & valid[:, None, :]
     K = torch.where(pair, E + p.const_value + torch.where(eye, p.noise_level, 0.0), 0.0)
@@ -80,9 +100,9 @@ def _fill(xn, valid, p: RbfParams, ls, eval_gradient: bool):
     if p.idx_ls >= 0:
         if p.ard:
             for f in range(xn.shape[2]):
-                G[..., p.idx_ls + f] = torch.where(pair, E * sq[..., f], 0.0)
+                G[..., p.idx_ls + f] = torch.where(pair, Eg * sq[..., f], 0.0)
         else:
-            G[..., p.idx_ls] = torch.where(pair, E * sq.sum(-1), 0.0)
+            G[..., p.idx_ls] = torch.where(pair, Eg * sq.sum(-1), 0.0)
     return K, G
 
 

@@ -48,6 +48,7 @@ class KernelParams:
     idx_noise: int = -1
     idx_ls: int = -1
     n_theta: int = 0
+    family: int = 0  # stationary part: 0 RBF, 1/2/3 Matern nu = 1/2, 3/2, 5/2
 
     @property
     def ard(self) -> bool:
@@ -171,6 +172,28 @@ def fit_neighbours(x: np.ndarray, num_nn: int, length_scale=1.0, dtype=np.float3
 # Local covariance fill
 # ----------------------------------------------------------------------------------------------
 
+def stationary(family: int, sq: np.ndarray):
+    """Unit-amplitude stationary kernel ``S`` at squared scaled distance ``sq`` and the factor
+    ``Sg`` of its length-scale gradient, ``d S / d log l_f = Sg * sq_f``: RBF
+    (``batched_kernels.py:884-898``) or Matern nu = 1/2, 3/2, 5/2 (``:1070-1120``; at distance 0
+    the nu = 1/2 factor is taken as 0, its numerator vanishing there, as the reference does with
+    its unit denominator)."""
+    if family == 0:
+        S = np.exp(-0.5 * sq)
+        return S, S
+    r = np.sqrt(sq)
+    if family == 1:
+        S = np.exp(-r)
+        return S, np.where(r > 0, S / np.where(r > 0, r, 1.0), 0.0)
+    if family == 2:
+        a = np.sqrt(3.0) * r
+        return (1.0 + a) * np.exp(-a), 3.0 * np.exp(-a)
+    if family == 3:
+        a = np.sqrt(5.0) * r
+        return (1.0 + a + a * a / 3.0) * np.exp(-a), 5.0 / 3.0 * (1.0 + a) * np.exp(-a)
+    raise ValueError(f'unknown kernel family {family}')
+
+
 def fill_nn_kernel(x_full: np.ndarray, nn_indices: np.ndarray, p: KernelParams, eval_gradient: bool):
     """Local covariance ``K (b, k, k)`` and gradient ``dK (b, k, k, n_theta)`` of a neighbour list.
 
@@ -191,8 +214,9 @@ def fill_nn_kernel(x_full: np.ndarray, nn_indices: np.ndarray, p: KernelParams, 
     ls = p.ls_vector(d)
     diff = (xn[:, :, None, :] - xn[:, None, :, :]) / ls  # (b, k, k, d)
     sq = diff * diff
-    dist = 0.5 * sq.sum(-1)
-    E = p.rbf_level * np.exp(-dist)
+    S, Sg = stationary(p.family, sq.sum(-1))
+    E = p.rbf_level * S
+    Eg = p.rbf_level * Sg  # d E / d log l_f = Eg * sq_f
     eye = np.eye(k, dtype=bool)[None]
     pair = valid[:, :, None] & valid[:, None, :]
     K = np.where(pair, E + p.const_value + np.where(eye, p.noise_level, 0.0), 0.0)
@@ -209,9 +233,9 @@ def fill_nn_kernel(x_full: np.ndarray, nn_indices: np.ndarray, p: KernelParams, 
     if p.idx_ls >= 0:
         if p.ard:
             for f in range(d):
-                G[..., p.idx_ls + f] = np.where(pair, E * sq[..., f], 0.0)
+                G[..., p.idx_ls + f] = np.where(pair, Eg * sq[..., f], 0.0)
         else:
-            G[..., p.idx_ls] = np.where(pair, E * sq.sum(-1), 0.0)
+            G[..., p.idx_ls] = np.where(pair, Eg * sq.sum(-1), 0.0)
     return K, G
 
 

@@ -17,6 +17,9 @@ KERNELS = {
     + skk.WhiteKernel(0.05),
     'const_n300_d2_m10': lambda: skk.ConstantKernel(0.5) + skk.ConstantKernel(1.3) * skk.RBF(0.4)
     + skk.WhiteKernel(0.02),
+    'matern12_n500_d3_m16': lambda: skk.ConstantKernel(0.9) * skk.Matern(0.4, nu=0.5) + skk.WhiteKernel(0.01),
+    'matern32_n450_d4_m12': lambda: skk.ConstantKernel(1.2) * skk.Matern(0.7, nu=1.5) + skk.WhiteKernel(0.02),
+    'matern52_n400_d2_m10': lambda: skk.ConstantKernel(1.0) * skk.Matern(0.6, nu=2.5) + skk.WhiteKernel(0.005),
 }
 CASES = sorted(KERNELS)
 
@@ -30,7 +33,7 @@ def oracle_params(p):
     return O.KernelParams(rbf_level=p.rbf_level, const_value=p.const_value, noise_level=p.noise_level,
                           length_scale=1.0 if p.length_scale is None else p.length_scale,
                           idx_rbf_level=p.idx_rbf_level, idx_const=p.idx_const, idx_noise=p.idx_noise,
-                          idx_ls=p.idx_ls, n_theta=p.n_theta)
+                          idx_ls=p.idx_ls, n_theta=p.n_theta, family=p.family)
 
 
 def normalized_y(g):

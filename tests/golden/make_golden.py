@@ -72,8 +72,12 @@ def case(name, NumpyNngpr, NumpyWorker, kernel_fn, x, y, xq, m, theta_eval=None,
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--ref', default='/root/reference')
+    ap.add_argument('--only', default='', help='comma-separated case groups to (re)generate: rbf,matern')
     args = ap.parse_args()
     NumpyNngpr, NumpyWorker, bk = _import_reference(args.ref)
+    only = set(filter(None, args.only.split(',')))
+    if only and 'rbf' not in only:
+        return matern_cases(NumpyNngpr, NumpyWorker, bk)
 
     # 1. CPU-oracle workload: n=2000, x~U[0,1]^3, y=sin(2 pi x1)+cos(2 pi x2) x3+N(0,0.1^2), m=16,
     #    C(1.0)*RBF(0.3)+White(0.01), 500 test points, seed 0
@@ -129,6 +133,34 @@ def main():
     case('const_n300_d2_m10', NumpyNngpr, NumpyWorker,
          lambda: bk.ConstantKernel(0.5) + bk.ConstantKernel(1.3) * bk.RBF(0.4) + bk.WhiteKernel(0.02),
          x, y, xq, 10, alpha=1e-6)
+    if not only or 'matern' in only:
+        matern_cases(NumpyNngpr, NumpyWorker, bk)
+
+
+def matern_cases(NumpyNngpr, NumpyWorker, bk):
+    """5-7. Matern nu = 1/2, 3/2, 5/2 (isotropic; the last with normalised y), evaluated
+    by the reference's generic path (batched_kernels.py:1070-1131)."""
+    rng = np.random.default_rng(5)
+    x = rng.uniform(0, 1, (500, 3))
+    y = np.sin(4 * x[:, 0]) + x[:, 1] * x[:, 2] + rng.normal(0, 0.05, 500)
+    xq = rng.uniform(0, 1, (120, 3))
+    case('matern12_n500_d3_m16', NumpyNngpr, NumpyWorker,
+         lambda: bk.ConstantKernel(0.9) * bk.Matern(0.4, nu=0.5) + bk.WhiteKernel(0.01), x, y, xq, 16)
+    rng = np.random.default_rng(6)
+    x = rng.uniform(-1, 1, (450, 4))
+    y = np.cos(2 * x[:, 0]) * x[:, 1] + 0.5 * x[:, 2] ** 2 + rng.normal(0, 0.05, 450)
+    xq = rng.uniform(-1, 1, (90, 4))
+    # isotropic: the reference's batched Matern checks an ARD length scale against the
+    # neighbour axis of its (batch, k, d) input (batched_kernels.py:1033) and raises
+    case('matern32_n450_d4_m12', NumpyNngpr, NumpyWorker,
+         lambda: bk.ConstantKernel(1.2) * bk.Matern(0.7, nu=1.5) + bk.WhiteKernel(0.02), x, y, xq, 12)
+    rng = np.random.default_rng(7)
+    x = rng.uniform(0, 2, (400, 2))
+    y = 3.0 + np.sin(3 * x[:, 0]) * np.exp(-x[:, 1]) + rng.normal(0, 0.05, 400)
+    xq = rng.uniform(0, 2, (100, 2))
+    case('matern52_n400_d2_m10', NumpyNngpr, NumpyWorker,
+         lambda: bk.ConstantKernel(1.0) * bk.Matern(0.6, nu=2.5) + bk.WhiteKernel(0.005), x, y, xq, 10,
+         normalize_y=True)
 
 
 if __name__ == '__main__':

@@ -122,3 +122,26 @@ def test_bad_neighbour_index_is_flagged_not_read():
     assert flags & _lib.NNGP_FLAG_BAD_INDEX
     with pytest.raises(IndexError):
         ops.raise_on_flags(flags, 'loglik')
+
+
+@pytest.mark.parametrize('nu', [0.5, 1.5, 2.5])
+@pytest.mark.parametrize('m', [16, 40])
+def test_matern_ard_loglik_matches_oracle(nu, m):
+    """ARD Matern (the reference's batched Matern cannot take ARD length scales on its batched
+    input, so this is pinned by the oracle): warp kernel (m <= 32) and block kernel (m > 32)."""
+    rng = np.random.default_rng(int(nu * 10) + m)
+    n, d = 600, 3
+    x = rng.uniform(-1, 1, (n, d))
+    y = np.sin(2 * x[:, 0]) * x[:, 1] + rng.normal(0, 0.05, n)
+    kernel = skk.ConstantKernel(0.8) * skk.Matern(np.array([0.4, 0.9, 1.7]), nu=nu) + skk.WhiteKernel(0.02)
+    p = extract(kernel)
+    nbr = O.knn(x, x, m, 0, p.length_scale)
+    want_l, want_g = O.log_marginal_likelihood(x, y[:, None], nbr, oracle_params(p), 1e-10, True)
+    out, flags = gpu_loglik(x, y, nbr, p, 1e-10, True, np.float64)
+    assert flags == 0
+    assert abs(out[0] / want_l - 1) < F64_LML
+    assert rel(out[1:], want_g) < F64_GRAD
+    out32, flags32 = gpu_loglik(x, y, nbr, p, 1e-10, True, np.float32)
+    assert flags32 & ~_lib.NNGP_FLAG_FP64_FALLBACK == 0
+    assert abs(out32[0] / want_l - 1) < F32_LML
+    assert rel(out32[1:], want_g) < F32_GRAD

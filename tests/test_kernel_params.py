@@ -48,7 +48,7 @@ def test_rbf_alone_and_white_alone():
 @pytest.mark.parametrize('kernel', [
     skk.RBF(1.0) + skk.RBF(2.0),
     skk.RBF(1.0) * skk.RBF(2.0),
-    skk.Matern(1.0),
+    skk.Matern(1.0, nu=2.0),
     skk.ConstantKernel(1.0) * skk.ConstantKernel(2.0) * skk.RBF(1.0),
 ])
 def test_unsupported_kernels_raise(kernel):
@@ -100,3 +100,12 @@ def test_params_from_theta_equals_clone_with_theta(kernel):
         np.testing.assert_allclose(np.asarray(got.length_scale), np.asarray(want.length_scale), rtol=1e-14)
     assert (got.idx_rbf_level, got.idx_const, got.idx_noise, got.idx_ls, got.n_theta) == (
         want.idx_rbf_level, want.idx_const, want.idx_noise, want.idx_ls, want.n_theta)
+
+
+@pytest.mark.parametrize('nu,family', [(0.5, 1), (1.5, 2), (2.5, 3), (np.inf, 0)])
+def test_matern_families(nu, family):
+    k = skk.ConstantKernel(0.7) * skk.Matern(np.array([0.3, 0.9]), nu=nu) + skk.WhiteKernel(0.05)
+    p = extract(k)
+    assert p.family == family and p.ard and p.rbf_level == pytest.approx(0.7)
+    assert (p.idx_rbf_level, p.idx_ls, p.idx_noise, p.n_theta) == (0, 1, 3, 4)
+    assert extract(skk.RBF(1.0)).family == 0
