@@ -53,3 +53,20 @@ def format_std(std, y_std, shape):
 def rel(a, b):
     a, b = np.asarray(a, dtype=np.float64), np.asarray(b, dtype=np.float64)
     return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+_SCALE = {}
+
+
+def lml_scale(name):
+    """Sum over points of |per-point log-likelihood| of a golden case (oracle, FP64): the scale
+    the FP32 paths' error is measured against (the total lml can be a heavily cancelled sum)."""
+    if name not in _SCALE:
+        from nngpr_b200.kernel_params import extract
+        g = load(name)
+        p = extract(KERNELS[name]().clone_with_theta(g['theta']))
+        y, _, _ = normalized_y(g)
+        y2 = y if y.ndim == 2 else y[:, None]
+        ll, _ = O.loglik_terms(g['x'], y2, g['nbr_fit_f64'], oracle_params(p), float(g['alpha']), False)
+        _SCALE[name] = max(float(np.abs(ll).sum()), abs(float(g['lml'])))
+    return _SCALE[name]

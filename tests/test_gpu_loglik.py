@@ -1,7 +1,9 @@
 """Fit-step log-likelihood and gradient through the C ABI vs the oracle / golden vectors.
 
 Tolerances: FP64 entry point 1e-10 relative (lml) and 1e-9 (gradient, max-norm relative);
-FP32 entry point 1e-5 relative for the lml and the gradient (max-norm relative).
+FP32 entry point 1e-5 for the lml relative to the sum of the per-point terms' magnitudes (the
+total can be a cancelled sum; on the golden cases that scale is 1-12x |lml|) and 1e-5 for the
+gradient (max-norm relative).
 """
 import numpy as np
 import pytest
@@ -12,7 +14,7 @@ from nngpr_b200.kernel_params import extract
 from oracle import nngp_oracle as O
 from sklearn.gaussian_process import kernels as skk
 
-from _common import CASES, KERNELS, load, normalized_y, oracle_params, rel
+from _common import CASES, KERNELS, lml_scale, load, normalized_y, oracle_params, rel
 
 pytestmark = pytest.mark.gpu
 
@@ -39,8 +41,12 @@ def test_loglik_golden(name, dtype):
     nbr = g['nbr_fit_f32']
     out, flags = gpu_loglik(g['x'], y, nbr, p, float(g['alpha']), True, dtype)
     assert flags & ~_lib.NNGP_FLAG_FP64_FALLBACK == 0
-    tol_l, tol_g = (F64_LML, F64_GRAD) if dtype == np.float64 else (F32_LML, F32_GRAD)
-    assert abs(out[0] / g['lml'] - 1) < tol_l, (out[0], g['lml'])
+    if dtype == np.float64:
+        tol_g = F64_GRAD
+        assert abs(out[0] / g['lml'] - 1) < F64_LML, (out[0], g['lml'])
+    else:
+        tol_g = F32_GRAD
+        assert abs(out[0] - g['lml']) < F32_LML * lml_scale(name), (out[0], g['lml'])
     assert rel(out[1:], g['grad']) < tol_g, (out[1:], g['grad'])
 
 
