@@ -620,7 +620,7 @@ nngp_status knn_impl(const T *ref, int64_t n_ref, const T *query, int64_t n_quer
             p.tv.build<<<grid_for(p.n_ref_pad), 256, 0, stream>>>(refs, n_ref, p.n_ref_pad, acc, tiles, r2);
             NNGP_CUDA_TRY(cudaGetLastError());
             NNGP_CUDA_TRY(ensure_smem_limit(reinterpret_cast<const void *>(p.tv.fn), p.tv.smem, 100));
-            const int64_t n_items = (n_query + tc::kTcQueryTile - 1) / tc::kTcQueryTile;
+            const int64_t n_items = (n_query + p.tv.rows_per_item - 1) / p.tv.rows_per_item;
             // persistent grid: the CTAs one SM holds (shared memory and TMEM sized for them) per SM;
             // CTAs that find no SM free start late and pick up no items, nothing waits on them
             const int per_sm = p.tv.ctas_per_sm;
@@ -636,7 +636,7 @@ nngp_status knn_impl(const T *ref, int64_t n_ref, const T *query, int64_t n_quer
                             (void *)&n_query, (void *)&n_ref, (void *)&has_cut, (void *)&cut, (void *)&m,
                             (void *)&out, (void *)&flags};
             NNGP_CUDA_TRY(cudaLaunchKernel(reinterpret_cast<const void *>(p.tv.fn), dim3(grid),
-                                           dim3(tc::kTcThreads), args, (size_t)p.tv.smem, stream));
+                                           dim3(p.tv.threads), args, (size_t)p.tv.smem, stream));
         }
     } else if (p.path == KnnPath::Simt) {
         if constexpr (std::is_same<T, float>::value) {

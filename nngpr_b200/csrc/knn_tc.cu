@@ -20,7 +20,9 @@
 //     and exact coordinates in one copy) and the MMAs; warps 0-3 are the epilogue, warp w owning
 //     query rows 32w..32w+31 (its TMEM lane quadrant).  Up to three CTAs share an SM when shared
 //     memory allows (small d): the epilogue is latency-bound, and every extra warp per scheduler
-//     shows (d = 3: 30.8 ms with two CTAs per SM, 23.1 ms with three, n = 434,874);
+//     shows (d = 3: 30.8 ms with two CTAs per SM, 23.1 ms with three, n = 434,874).  For d = 12
+//     and 16, where one CTA fills an SM, a work item is two query tiles: both MMA chains read the
+//     same staged ref tile and 8 epilogue warps share the SM (d = 16, n = 1M: 235 -> 173 ms);
 //   * epilogue: each 32-column chunk of a row is one tcgen05.ld (issued one chunk ahead into a
 //     second register set), screened with three-input min over groups of 8 columns against the
 //     row's threshold into a candidate mask (skipped when no row of the warp has one); the
@@ -52,9 +54,7 @@ namespace tc {
 constexpr int QT = kTcQueryTile;  // queries per tile (UMMA M)
 constexpr int RT = kTcRefTile;    // refs per tile (UMMA N)
 static_assert(RT == 128, "the epilogue screens a ref tile as four 32-column chunks");
-constexpr int EPI_WARPS = 4;      // one per TMEM lane quadrant
-constexpr int THREADS = (EPI_WARPS + 1) * 32;
-static_assert(THREADS == kTcThreads, "thread count");
+constexpr int THREADS = 5 * 32;   // layout self-test: 4 epilogue warps + the MMA warp
 constexpr int LIST = 32;       // largest num_nn
 constexpr int HS = 33;         // heap row stride in 64-bit keys (odd: rows of a warp hit distinct banks)
 constexpr int DRAIN_AT = 32;   // queued entries that trigger a drain at the end of a chunk
@@ -66,8 +66,13 @@ constexpr float kPadNorm = 1.7014118346046923e38f;  // 2^127: padded refs never 
 // an empty slot is (+inf, 0xffffffff), larger than every real entry, read back as index -1
 constexpr uint64_t kEmptyKey = (uint64_t)0x7F800000u << 32 | 0xFFFFFFFFu;
 
-template <int D>
+// D: padded dimension; QTILES: 128-query tiles per work item (their MMAs share each staged ref
+// tile; 4 epilogue warps per query tile, one per TMEM lane quadrant)
+template <int D, int QTILES>
 struct Cfg {
+    static constexpr int EPI_WARPS = 4 * QTILES;
+    static constexpr int THREADS = (EPI_WARPS + 1) * 32;
+    static constexpr int ROWS = QT * QTILES;        // queries per work item
     static constexpr int U = D + 1;                 // coordinates + the norm column
     static constexpr int KP = (3 * U + 7) / 8 * 8;  // split operand width (tf32), multiple of 8
     static constexpr int NMMA = KP / 8;             // UMMA K = 8 for tf32
@@ -75,8 +80,9 @@ struct Cfg {
     static constexpr int OP_BYTES = RT * KP * 4;    // B operand block of a ref tile
     static constexpr int EX_BYTES = RT * DP * 4;    // exact coordinates of a ref tile
     static constexpr int STAGE_BYTES = OP_BYTES + EX_BYTES;
-    static constexpr int A_BYTES = QT * KP * 4;
-    static constexpr int LIST_BYTES = QT * HS * 8;  // one heap of keys per query
+    static constexpr int A_TILE = QT * KP * 4;      // query operand of one query tile
+    static constexpr int A_BYTES = A_TILE * QTILES;
+    static constexpr int LIST_BYTES = ROWS * HS * 8;  // one heap of keys per query
     static constexpr int QUEUE_BYTES = EPI_WARPS * QCAP * (4 + 4 + 1);
     static constexpr int BAR_BYTES = 256;
     static constexpr int FIXED = 1024 + A_BYTES + LIST_BYTES + QUEUE_BYTES + BAR_BYTES;
@@ -91,7 +97,10 @@ struct Cfg {
     static constexpr int STAGES = STN > 4 ? 4 : STN;
     static constexpr int SMEM = FIXED + STAGES * STAGE_BYTES;
     static constexpr int NBUF = CTAS_PER_SM == 3 ? 1 : 2;  // accumulator buffers in TMEM
-    static constexpr uint32_t TMEM_COLS = NBUF * RT;       // a power of two >= 32
+    static constexpr uint32_t BUF_COLS = RT * QTILES;       // one buffer: a tile per query tile
+    static constexpr uint32_t TMEM_COLS = NBUF * BUF_COLS;  // a power of two >= 32, <= 512
+    static_assert(TMEM_COLS <= 512 && (TMEM_COLS & (TMEM_COLS - 1)) == 0, "TMEM columns");
+    static_assert(CTAS_PER_SM * TMEM_COLS <= 512, "TMEM of the CTAs sharing an SM");
     static_assert(STAGES >= 2, "ref tile too large for two stages");
     // K-major no-swizzle canonical layout: 8-row x 16-byte core matrices, SBO = 128 B between
     // 8-row groups, LBO between 16-byte K chunks
@@ -205,7 +214,7 @@ template <int D>
 __global__ void build_tc_tiles_kernel(const float *__restrict__ xs, int64_t n, int64_t n_pad,
                                       const double *__restrict__ acc, unsigned char *__restrict__ tiles,
                                       unsigned int *__restrict__ r2max_bits) {
-    using C = Cfg<D>;
+    using C = Cfg<D, 1>;  // the ref-tile layout does not depend on the query tiles
     float c[D];
 #pragma unroll
     for (int f = 0; f < D; ++f) c[f] = n > 0 ? (float)(acc[f] / (double)n) : 0.f;
@@ -257,24 +266,26 @@ __global__ void build_tc_tiles_kernel(const float *__restrict__ xs, int64_t n, i
     if ((threadIdx.x & 31) == 0) atomicMax(r2max_bits, __float_as_uint(mx));
 }
 
-template <int D>
-__global__ void __launch_bounds__(THREADS, Cfg<D>::CTAS_PER_SM) knn_tc_kernel(const unsigned char *__restrict__ tiles_g,
+template <int D, int QTILES>
+__global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_PER_SM)
+    knn_tc_kernel(const unsigned char *__restrict__ tiles_g,
                                                          const float *__restrict__ qs,
                                                          const double *__restrict__ acc,
                                                          const unsigned int *__restrict__ r2max_bits,
                                                          int *__restrict__ work_counter, int64_t n_query,
                                                          int64_t n_ref, int has_cut, int64_t cut, int m,
                                                          int32_t *__restrict__ out, int32_t *__restrict__ flags) {
-    using C = Cfg<D>;
+    using C = Cfg<D, QTILES>;
     constexpr int S = C::STAGES;
+    constexpr int EPI_WARPS = C::EPI_WARPS;
     constexpr unsigned FULL = 0xffffffffu;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char *sm =
         reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     unsigned char *sA = sm;
     unsigned char *sB = sA + C::A_BYTES;
-    uint64_t *H = reinterpret_cast<uint64_t *>(sB + S * C::STAGE_BYTES);  // [QT][HS] heaps
-    unsigned char *qbase = reinterpret_cast<unsigned char *>(H + QT * HS);
+    uint64_t *H = reinterpret_cast<uint64_t *>(sB + S * C::STAGE_BYTES);  // [ROWS][HS] heaps
+    unsigned char *qbase = reinterpret_cast<unsigned char *>(H + C::ROWS * HS);
     uint64_t *bars = reinterpret_cast<uint64_t *>(qbase + C::QUEUE_BYTES);
     uint64_t *b_full = bars;        // [S <= 4]
     uint64_t *b_empty = bars + 4;   // [S <= 4]
@@ -287,7 +298,7 @@ __global__ void __launch_bounds__(THREADS, Cfg<D>::CTAS_PER_SM) knn_tc_kernel(co
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const bool producer_warp = warp == EPI_WARPS;
-    const int64_t n_items = (n_query + QT - 1) / QT;
+    const int64_t n_items = (n_query + C::ROWS - 1) / C::ROWS;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < S; ++s) {
@@ -333,8 +344,8 @@ __global__ void __launch_bounds__(THREADS, Cfg<D>::CTAS_PER_SM) knn_tc_kernel(co
         __syncthreads();
         if (stop) break;
         const int64_t qtile = has_cut ? (n_items - 1 - item) : item;  // heaviest first for the prefix search
-        const int64_t q0 = qtile * QT;
-        const int64_t block_limit = limit_of(min(q0 + QT, n_query) - 1);
+        const int64_t q0 = qtile * C::ROWS;
+        const int64_t block_limit = limit_of(min(q0 + C::ROWS, n_query) - 1);
         const uint32_t ntiles = (uint32_t)((block_limit + RT - 1) / RT);
 
         if (producer_warp) {
@@ -374,12 +385,16 @@ __global__ void __launch_bounds__(THREADS, Cfg<D>::CTAS_PER_SM) knn_tc_kernel(co
                     }
                     tc_fence_after();
                     const uint32_t b_addr = smem_addr(sB + s * C::STAGE_BYTES);
-                    const uint32_t d_tmem = tmem_base + b * RT;
 #pragma unroll
-                    for (int i = 0; i < C::NMMA; ++i) {
-                        const uint64_t ad = smem_desc(a_addr + i * 2 * C::A_LBO, C::A_LBO, 128);
-                        const uint64_t bd = smem_desc(b_addr + i * 2 * C::B_LBO, C::B_LBO, 128);
-                        mma_tf32(d_tmem, ad, bd, i > 0 ? 1u : 0u);
+                    for (int qt = 0; qt < QTILES; ++qt) {  // every query tile against the same ref tile
+                        const uint32_t d_tmem = tmem_base + b * C::BUF_COLS + qt * RT;
+                        const uint32_t aq = a_addr + qt * C::A_TILE;
+#pragma unroll
+                        for (int i = 0; i < C::NMMA; ++i) {
+                            const uint64_t ad = smem_desc(aq + i * 2 * C::A_LBO, C::A_LBO, 128);
+                            const uint64_t bd = smem_desc(b_addr + i * 2 * C::B_LBO, C::B_LBO, 128);
+                            mma_tf32(d_tmem, ad, bd, i > 0 ? 1u : 0u);
+                        }
                     }
                     mma_commit(&t_full[b]);
                     mma_commit(&b_empty[s]);
@@ -396,7 +411,10 @@ __global__ void __launch_bounds__(THREADS, Cfg<D>::CTAS_PER_SM) knn_tc_kernel(co
             __syncwarp();
         } else {
             // ---------------- epilogue warps ----------------
-            const int row = warp * 32 + lane;  // query row in the tile = TMEM lane
+            // warp w serves query tile w / 4 through TMEM lane quadrant w % 4 (a warp reaches the
+            // lanes of its own quadrant only)
+            const int qtw = warp >> 2, quad = warp & 3;
+            const int row = warp * 32 + lane;  // query row in the work item
             const int64_t q = q0 + row;
             const bool active = q < n_query;
             const int64_t limit = active ? limit_of(q) : 0;
@@ -423,7 +441,7 @@ __global__ void __launch_bounds__(THREADS, Cfg<D>::CTAS_PER_SM) knn_tc_kernel(co
                         const float hi = tf32_round(a[f]);
                         v = (blk == 2) ? (a[f] - hi) : hi;
                     }
-                    *reinterpret_cast<float *>(sA + op_offset(row, k, QT)) = v;
+                    *reinterpret_cast<float *>(sA + qtw * C::A_TILE + op_offset(quad * 32 + lane, k, QT)) = v;
                 }
             }
             fence_proxy_async_smem();
@@ -479,7 +497,7 @@ __global__ void __launch_bounds__(THREADS, Cfg<D>::CTAS_PER_SM) knn_tc_kernel(co
                 tc_fence_after();
                 const float *exs = reinterpret_cast<const float *>(sB + s * C::STAGE_BYTES + C::OP_BYTES);
                 const int64_t j0 = (int64_t)t * RT;
-                const uint32_t taddr = tmem_base + ((uint32_t)(warp * 32) << 16) + b * RT;
+                const uint32_t taddr = tmem_base + ((uint32_t)(quad * 32) << 16) + b * C::BUF_COLS + qtw * RT;
                 // screen one 32-column chunk (scores in v): this row's candidate mask, 0 when no row
                 // of the warp has one (the common case, a handful of instructions)
                 auto screen = [&](const uint32_t (&v)[32]) -> uint32_t {
@@ -649,7 +667,7 @@ __global__ void __launch_bounds__(THREADS) tc_layout_selftest_kernel(const float
         mbar_init(&bar, 1);
         fence_mbar_init();
     }
-    if (warp == EPI_WARPS) {
+    if (warp == 4) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_slot)),
                      "r"(kSelftestCols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
@@ -658,7 +676,7 @@ __global__ void __launch_bounds__(THREADS) tc_layout_selftest_kernel(const float
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem_base = tmem_slot;
-    if (warp == EPI_WARPS && lane == 0) {
+    if (warp == 4 && lane == 0) {
         constexpr uint32_t A_LBO = (QT / 8) * 128, B_LBO = (RT / 8) * 128;
 #pragma unroll
         for (int i = 0; i < KP / 8; ++i)
@@ -669,7 +687,7 @@ __global__ void __launch_bounds__(THREADS) tc_layout_selftest_kernel(const float
     const bool ok = mbar_wait_bounded(&bar, 0);
     if (!ok && threadIdx.x == 0) flag_or(flags, NNGP_FLAG_TIMEOUT);
     tc_fence_after();
-    if (warp < EPI_WARPS && ok) {
+    if (warp < 4 && ok) {
         uint32_t v[32];
         for (int c = 0; c < RT / 32; ++c) {
             tmem_ld32_nowait(tmem_base + ((uint32_t)(warp * 32) << 16) + c * 32, v);
@@ -680,19 +698,24 @@ __global__ void __launch_bounds__(THREADS) tc_layout_selftest_kernel(const float
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    if (warp == EPI_WARPS) {
+    if (warp == 4) {
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(kSelftestCols));
     }
 }
 
-template <int D> TcVariant tc_make() {
+// d 12 and 16 fill an SM with one CTA: two query tiles per work item give it 8 epilogue warps
+// and halve the ref-tile stream per query
+template <int D, int QTILES = (D == 12 || D == 16) ? 2 : 1> TcVariant tc_make() {
+    using C = Cfg<D, QTILES>;
     TcVariant v;
-    v.fn = knn_tc_kernel<D>;
+    v.fn = knn_tc_kernel<D, QTILES>;
     v.build = build_tc_tiles_kernel<D>;
-    v.smem = Cfg<D>::SMEM;
-    v.stage_bytes = Cfg<D>::STAGE_BYTES;
-    v.dp = Cfg<D>::DP;
-    v.ctas_per_sm = Cfg<D>::CTAS_PER_SM;
+    v.smem = C::SMEM;
+    v.stage_bytes = C::STAGE_BYTES;
+    v.dp = C::DP;
+    v.ctas_per_sm = C::CTAS_PER_SM;
+    v.threads = C::THREADS;
+    v.rows_per_item = C::ROWS;
     return v;
 }
 

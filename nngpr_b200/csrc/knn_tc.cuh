@@ -9,7 +9,6 @@ namespace tc {
 
 constexpr int kTcRefTile = 128;    // refs per tile (UMMA N)
 constexpr int kTcQueryTile = 128;  // queries per tile (UMMA M)
-constexpr int kTcThreads = 160;    // 4 epilogue warps + 1 producer/MMA warp
 
 using TcFn = void (*)(const unsigned char *, const float *, const double *, const unsigned int *, int *, int64_t,
                       int64_t, int, int64_t, int, int32_t *, int32_t *);
@@ -19,7 +18,9 @@ struct TcVariant {
     TcFn fn = nullptr;
     TcBuildFn build = nullptr;
     int smem = 0, stage_bytes = 0, dp = 0;
-    int ctas_per_sm = 1;  // CTAs the shared memory of one SM holds (the kernel's launch bounds)
+    int ctas_per_sm = 1;     // CTAs the shared memory of one SM holds (the kernel's launch bounds)
+    int threads = 160;       // epilogue warps (4 per query tile) + the producer/MMA warp
+    int rows_per_item = 128;  // queries per work item (128 per query tile)
 };
 
 }  // namespace tc
