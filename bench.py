@@ -64,13 +64,14 @@ WORKLOAD = ('nngp fit step, n=434874 d=3 m=32, isotropic RBF l=0.2, noise 1e-3; 
 # precision of the local systems: at this nugget nearly every FP32 system has a pivot below the
 # re-solve threshold, so FP64 systems are the faster exact choice (FP32 + re-solve: 51.9 ms/step)
 LOCAL = 'f64'
+ROOF = 'fp32'  # roofline of the search kernel: 'fp32' (the screen's issue) or 'tensor'
 DATA = 'synthetic (seeded stand-in for 3droad: shape 434874 x 3)'
 DTYPE = 'f32 search (tf32-split tensor screen) + f64 local'
 
 WORKLOADS = {
     'fit3d': {},
     'precision': dict(
-        N_TRAIN=1_000_000, D=16, M=32, LS=0.8, NOISE=1e-4, ALPHA=1e-10, LOCAL='f32',
+        N_TRAIN=1_000_000, D=16, M=32, LS=0.8, NOISE=1e-4, ALPHA=1e-10, LOCAL='f32', ROOF='tensor',
         WORKLOAD=('nngp fit step, n=1000000 d=16 m=32, 64-component Gaussian mixture, isotropic RBF l=0.8, '
                   'noise 1e-4; tensor-core fp32 exact neighbour search, fp32 local systems with fp64 re-solve of '
                   'small pivots, fp64 reductions'),
@@ -366,6 +367,17 @@ def read_profile_traffic():
     except OSError:
         pass
     return None
+
+
+def tf32_peak_tflops():
+    """Dense TF32 tensor rate: half the BF16 dense rate measured on this pool's B200s
+    (MEASURED_PEAKS.json, burst), the ratio of NVIDIA's dense figures (1.1 vs 2.25 PFLOP/s)."""
+    try:
+        with open(os.path.join(ROOT, 'MEASURED_PEAKS.json')) as f:
+            bf16 = float(json.load(f)['bf16_tflops'])
+        return bf16 / 2.0, 'MEASURED_PEAKS.json bf16_tflops (burst) / 2: the TF32 dense rate'
+    except Exception:
+        return 1590.0 / 2.0, 'fallback 1.59 PFLOP/s BF16 dense / 2: the TF32 dense rate'
 
 
 def fp32_peak_tflops(torch, L, stream_ptr):
@@ -706,6 +718,20 @@ def run_ours(args):
         knn_avg_ms = float(np.mean(knn_ms))
         achieved = 2.0 * D * pairs / (knn_avg_ms * 1e-3) / 1e12
         ms_per_step = tot_ms / args.steps
+        # the pipe that bounds the search: the FP32/ALU issue of the screen at small d (the distance
+        # work is cheap), the tensor pipe at d = 16 (the survey's roofline for that configuration)
+        kp = (3 * (D + 1) + 7) // 8 * 8  # TF32 split width of the tensor-core operands
+        issued = 2.0 * kp * pairs / (knn_avg_ms * 1e-3) / 1e12
+        if ROOF == 'tensor':
+            tpk, tsrc = tf32_peak_tflops()
+            roof = {'bound': 'tensor', 'achieved': achieved, 'peak': tpk, 'unit': 'TFLOP/s', 'frac': achieved / tpk,
+                    'peak_source': tsrc, 'issued_mma_tflops': issued, 'issued_frac': issued / tpk,
+                    'fp32_fma_equivalent': {'peak': peak, 'frac': achieved / peak,
+                                            'peak_source': 'FP32 FMA probe measured in this run'}}
+        else:
+            roof = {'bound': 'fp32', 'achieved': achieved, 'peak': peak, 'unit': 'TFLOP/s', 'frac': achieved / peak,
+                    'peak_source': 'FP32 FMA probe measured in this run (MEASURED_PEAKS.json has no FP32 figure)',
+                    'issued_mma_tflops': issued}
         line = {
             'metric': METRIC, 'value': 1e3 / ms_per_step, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
             'warmup': args.warmup, 'ms_per_step': ms_per_step, 'higher_is_better': True,
@@ -715,12 +741,11 @@ def run_ours(args):
                        'l2': 'flushed (256 MB write) before every timed step', 'lml': lml_val,
                        'lml_rel_err_vs_fp64_local': lml_err},
             'e2e': e2e,
-            'roofline': {'bound': 'fp32', 'achieved': achieved, 'peak': peak, 'unit': 'TFLOP/s',
-                         'frac': achieved / peak, 'traffic': read_profile_traffic(),
-                         'kernel': f'knn_tc_kernel<{D}> (prefix search: tcgen05 TF32-split screen, exact FP32 rescoring)',
-                         'work': '2*d flops per (query, ref) pair, n(n-1)/2 pairs, whichever pipe computes them',
-                         'peak_source': 'FP32 FMA probe measured in this run (MEASURED_PEAKS.json has no FP32 figure)',
-                         'knn_ms': knn_avg_ms},
+            'roofline': dict(roof, traffic=read_profile_traffic(),
+                             kernel=f'knn_tc_kernel<{D}> (prefix search: tcgen05 TF32-split screen, exact FP32 rescoring)',
+                             work='2*d flops per (query, ref) pair, n(n-1)/2 pairs, whichever pipe computes them; '
+                                  'issued_mma = 2*K\' per pair with the split width K\'',
+                             knn_ms=knn_avg_ms),
             'cpu_baseline': cpu,
             'plain_gpu': plain,
             'lbfgs': lbfgs,
