@@ -56,6 +56,8 @@ struct LocalArgs {
 };
 
 template <typename T> __device__ __forceinline__ T dsqrt(T v) { return sqrt(v); }
+template <typename T> __device__ __forceinline__ T drsqrt(T v) { return rsqrt(v); }
+template <> __device__ __forceinline__ float drsqrt<float>(float v) { return rsqrtf(v); }
 template <typename T> __device__ __forceinline__ T dexp(T v) { return exp(v); }
 template <> __device__ __forceinline__ float dexp<float>(float v) { return expf(v); }
 
@@ -90,10 +92,11 @@ template <bool MATERN, typename T> __device__ __forceinline__ T kern_g(int famil
 // Warp kernel
 // ---------------------------------------------------------------------------------------
 // Shared memory per warp (bytes): xs (kWarpM + 1) x ds doubles | L kWarpM x (kWarpM + 1) doubles |
-// inverse diagonal kWarpM doubles | gradient accumulator n_theta doubles.
+// inverse diagonal kWarpM doubles | gradient accumulator n_theta doubles | the fill's kernel values
+// kWarpM x (kWarpM + 1) doubles (kept for the gradient, which would otherwise recompute them).
 struct WarpSmem {
     int ds;  // row stride of xs (d + 1)
-    size_t xs_bytes, l_bytes, idg_bytes, g_bytes, total;
+    size_t xs_bytes, l_bytes, idg_bytes, g_bytes, e_bytes, total;
     __host__ __device__ static WarpSmem make(int d, int n_theta) {
         WarpSmem s;
         s.ds = d + 1;
@@ -101,7 +104,8 @@ struct WarpSmem {
         s.l_bytes = (size_t)kWarpM * (kWarpM + 1) * 8;
         s.idg_bytes = (size_t)kWarpM * 8;
         s.g_bytes = (size_t)(n_theta > 0 ? n_theta : 1) * 8;
-        s.total = (s.xs_bytes + s.l_bytes + s.idg_bytes + s.g_bytes + 15) / 16 * 16;
+        s.e_bytes = (size_t)kWarpM * (kWarpM + 1) * 8;
+        s.total = (s.xs_bytes + s.l_bytes + s.idg_bytes + s.g_bytes + s.e_bytes + 15) / 16 * 16;
         return s;
     }
 };
@@ -121,6 +125,8 @@ __device__ __forceinline__ bool warp_system(const LocalArgs &a, int64_t p, int l
     TC *Ls = reinterpret_cast<TC *>(wsm + lay.xs_bytes);
     TC *idg = reinterpret_cast<TC *>(wsm + lay.xs_bytes + lay.l_bytes);
     double *gacc = reinterpret_cast<double *>(wsm + lay.xs_bytes + lay.l_bytes + lay.idg_bytes);
+    TC *Es = reinterpret_cast<TC *>(wsm + lay.xs_bytes + lay.l_bytes + lay.idg_bytes + lay.g_bytes);
+    constexpr bool STASH = GRAD && !MATERN;  // RBF gradient: reuse the fill's exponentials
     const int d = a.d, ds = lay.ds;
 
     // ---- neighbour of this lane --------------------------------------------------------
@@ -165,11 +171,13 @@ __device__ __forceinline__ bool warp_system(const LocalArgs &a, int64_t p, int l
     for (int k = 0; k < M; ++k) {
         const bool vk = (vmask >> k) & 1u;
         const TC e = rbf * kern_s<MATERN>(a.family, r[k]);
+        if (STASH) Es[lane * (M + 1) + k] = e;
         TC kv = (valid && vk) ? e + cst : TC(0);
         if (k == lane) kv = valid ? kv + diag_add : TC(1);
         r[k] = kv;
     }
-    TC kvec = valid ? rbf * kern_s<MATERN>(a.family, rp) + cst : TC(0);  // K[p][lane]
+    const TC ep0 = rbf * kern_s<MATERN>(a.family, rp);  // kept for the gradient
+    TC kvec = valid ? ep0 + cst : TC(0);                 // K[p][lane]
     const TC kpp = rbf + cst + (TC)a.noise + (PRED ? TC(0) : (TC)a.alpha);
 
     // ---- Cholesky of the neighbour block fused with l = L^-1 k ----------------------------
@@ -181,8 +189,8 @@ __device__ __forceinline__ bool warp_system(const LocalArgs &a, int64_t p, int l
     for (int k = 0; k < M; ++k) {
         const TC piv = __shfl_sync(FULL, r[k], k);
         minpiv = piv < minpiv ? piv : minpiv;
-        const TC sq = dsqrt<TC>(piv);
-        const TC inv = TC(1) / sq;
+        const TC inv = drsqrt<TC>(piv);  // 1 / L_kk
+        const TC sq = piv * inv;         // L_kk
         r[k] = (lane == k) ? sq : r[k] * inv;
         if (lane == k) dg_own = sq;
         const TC lk = __shfl_sync(FULL, kvec, k) * inv;
@@ -280,9 +288,9 @@ __device__ __forceinline__ bool warp_system(const LocalArgs &a, int64_t p, int l
         const bool vk_ok = (vmask >> k) & 1u;
         const TC G = wsum * b_own * bk - TC(0.5) * (b_own * vk + v_own * bk);
         const TC wgt = (valid && vk_ok) ? (k < lane ? TC(2) : (k == lane ? TC(1) : TC(0))) : TC(0);
-        const TC s = kern_s<MATERN>(a.family, r[k]);
+        const TC s = STASH ? TC(0) : kern_s<MATERN>(a.family, r[k]);
         const TC gw = wgt * G;
-        const TC ge = gw * (rbf * s);
+        const TC ge = gw * (STASH ? Es[lane * (M + 1) + k] : rbf * s);
         const TC gl = MATERN ? gw * (rbf * kern_g<MATERN>(a.family, r[k], s)) : ge;
         g_amp += ge;
         g_cst += gw;
@@ -292,8 +300,8 @@ __device__ __forceinline__ bool warp_system(const LocalArgs &a, int64_t p, int l
     }
     // pair (p, lane), weight 2, and (p, p)
     const TC Gp = valid ? TC(0.5) * v_own - wsum * b_own : TC(0);
-    const TC sp = kern_s<MATERN>(a.family, rp);
-    const TC gpe = TC(2) * Gp * (rbf * sp);
+    const TC sp = MATERN ? kern_s<MATERN>(a.family, rp) : TC(0);
+    const TC gpe = TC(2) * Gp * (MATERN ? rbf * sp : ep0);
     const TC gpl = MATERN ? TC(2) * Gp * (rbf * kern_g<MATERN>(a.family, rp, sp)) : gpe;
     g_amp += gpe;
     g_cst += TC(2) * Gp;
