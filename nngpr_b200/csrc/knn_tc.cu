@@ -83,7 +83,7 @@ struct Cfg {
     static constexpr int A_TILE = QT * KP * 4;      // query operand of one query tile
     static constexpr int A_BYTES = A_TILE * QTILES;
     static constexpr int LIST_BYTES = ROWS * HS * 8;  // one heap of keys per query
-    static constexpr int QUEUE_BYTES = EPI_WARPS * QCAP * (4 + 4 + 1);
+    static constexpr int QUEUE_BYTES = EPI_WARPS * QCAP * (8 + 1);  // key + row
     static constexpr int BAR_BYTES = 256;
     static constexpr int FIXED = 1024 + A_BYTES + LIST_BYTES + QUEUE_BYTES + BAR_BYTES;
     // as many CTAs per SM (up to 3) as hold at least 2 stages each: more epilogue warps per
@@ -450,9 +450,8 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
             // this warp's rows: row rr's heap at heap[rr * HS .. + m)
             uint64_t *heap = H + (warp * 32) * HS;
             for (int rr = 0; rr < 32; ++rr) heap[rr * HS + lane] = kEmptyKey;
-            float *qd = reinterpret_cast<float *>(qbase) + warp * QCAP;
-            int32_t *qj = reinterpret_cast<int32_t *>(qbase + EPI_WARPS * QCAP * 4) + warp * QCAP;
-            uint8_t *qr = qbase + EPI_WARPS * QCAP * 8 + warp * QCAP;
+            uint64_t *qk = reinterpret_cast<uint64_t *>(qbase) + warp * QCAP;  // queued keys
+            uint8_t *qr = qbase + EPI_WARPS * QCAP * 8 + warp * QCAP;           // their rows
             __syncwarp();
             // rows past the last query never take candidates
             const float tq_off = active ? pos_inf<float>() : neg_inf<float>();
@@ -467,7 +466,7 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
                     const int e = base + lane;
                     bool pend = e < qcount;
                     const int r = pend ? (int)qr[e] : 32 + lane;  // idle lanes: distinct dummy rows
-                    const uint64_t x = pend ? ((uint64_t)__float_as_uint(qd[e]) << 32 | (uint32_t)qj[e]) : 0;
+                    const uint64_t x = pend ? qk[e] : 0;
                     const unsigned grp = __match_any_sync(FULL, r);
                     unsigned todo = __ballot_sync(FULL, pend);
                     while (todo) {
@@ -553,45 +552,47 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
                         cut(cm3, 3);
                     }
                 }
-                // 2) candidates of the whole tile: each lane walks its own (chunk by chunk, column by
-                //    column), one per warp iteration, so a warp iteration serves every row that has one;
+                // 2) candidates of the whole tile: each lane walks its own (column by column, chunks in
+                //    order), one per warp iteration, so a warp iteration serves every row that has one;
                 //    each is rescored exactly from the stage's coordinates and survivors of the row's
-                //    current bound are queued, then drained into the heaps in batches
-                while (__any_sync(FULL, (cm0 | cm1 | cm2 | cm3) != 0)) {
+                //    current bound are queued as keys, then drained into the heaps in batches
+                uint64_t lo = (uint64_t)cm0 | (uint64_t)cm1 << 32, hi = (uint64_t)cm2 | (uint64_t)cm3 << 32;
+                while (__any_sync(FULL, (lo | hi) != 0)) {
                     if (qcount > QCAP - 32) drain();
                     bool keep = false;
-                    float d2 = 0.f;
-                    int col = 0;
-                    if ((cm0 | cm1 | cm2 | cm3) != 0) {
-                        if (cm0) {
-                            col = __ffs(cm0) - 1;
-                            cm0 &= cm0 - 1;
-                        } else if (cm1) {
-                            col = 32 + __ffs(cm1) - 1;
-                            cm1 &= cm1 - 1;
-                        } else if (cm2) {
-                            col = 64 + __ffs(cm2) - 1;
-                            cm2 &= cm2 - 1;
-                        } else {
-                            col = 96 + __ffs(cm3) - 1;
-                            cm3 &= cm3 - 1;
-                        }
+                    uint64_t key = 0;
+                    if ((lo | hi) != 0) {
+                        const bool use_lo = lo != 0;  // branch-free pick of the lowest remaining column
+                        const uint64_t w = use_lo ? lo : hi;
+                        const int col = __ffsll((long long)w) - 1 + (use_lo ? 0 : 64);
+                        const uint64_t w2 = w & (w - 1);
+                        lo = use_lo ? w2 : lo;
+                        hi = use_lo ? hi : w2;
                         // the oracle's arithmetic: ((x0 - q0)^2 + (x1 - q1)^2) + ..., each step rounded
-                        const float *rp = exs + col * C::DP;
-                        const float t0 = sub_rn(rp[0], qo[0]);
-                        d2 = mul_rn(t0, t0);
+                        const float4 *rp4 = reinterpret_cast<const float4 *>(exs + col * C::DP);
+                        float rv[C::DP];
+#pragma unroll
+                        for (int f4 = 0; f4 < C::DP / 4; ++f4) {
+                            const float4 t = rp4[f4];
+                            rv[4 * f4] = t.x;
+                            rv[4 * f4 + 1] = t.y;
+                            rv[4 * f4 + 2] = t.z;
+                            rv[4 * f4 + 3] = t.w;
+                        }
+                        const float t0 = sub_rn(rv[0], qo[0]);
+                        float d2 = mul_rn(t0, t0);
 #pragma unroll
                         for (int f = 1; f < D; ++f) {
-                            const float tf = sub_rn(rp[f], qo[f]);
+                            const float tf = sub_rn(rv[f], qo[f]);
                             d2 = add_rn(d2, mul_rn(tf, tf));
                         }
                         keep = d2 <= worst;  // NaN never kept
+                        key = (uint64_t)__float_as_uint(d2) << 32 | (uint32_t)(j0 + col);
                     }
                     const unsigned mk = __ballot_sync(FULL, keep);
                     if (keep) {
                         const int pos = qcount + __popc(mk & ((1u << lane) - 1u));
-                        qd[pos] = d2;
-                        qj[pos] = (int32_t)(j0 + col);
+                        qk[pos] = key;
                         qr[pos] = (uint8_t)lane;
                     }
                     qcount += __popc(mk);
