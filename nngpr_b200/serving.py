@@ -7,7 +7,9 @@ resident and serves a stream of predict requests of uneven sizes:
 
 * requests are queued as they arrive (:meth:`PredictServer.submit` returns a future); a
   scheduler thread packs the queued points, oldest first, into one batch per free *slot* (a
-  request larger than the biggest batch is split, a batch takes pieces of several requests);
+  request larger than the biggest batch is split, a batch takes pieces of several requests).
+  Small requests (at most ``small_points``) have their own queue and one slot of their own,
+  so they never wait behind a batch of large ones;
 * a batch is padded to the smallest size bucket that holds it and run as one CUDA graph
   captured for that bucket: cast, neighbour search, fused fill + Cholesky + solves, all on the
   slot's stream, between an H2D copy of the batch and a D2H copy of its results (pinned host
@@ -15,8 +17,8 @@ resident and serves a stream of predict requests of uneven sizes:
 * several slots are in flight at once on their own streams, so requests that arrive while
   others run are admitted as soon as a slot is free and their work overlaps on the device; the
   number of slots is bounded by the free device memory at start-up;
-* a completion thread waits for each batch's event, scatters the rows to their requests and
-  completes a request's future when all its rows are back.
+* a completion thread polls the batches' events, in any order, scatters the rows of each
+  finished batch to their requests and completes a request's future when all its rows are back.
 
 Every query row is computed independently (its own neighbour list and local system), so a
 request's result does not depend on what it was batched with (tests/test_gpu_serving.py checks
@@ -35,7 +37,9 @@ import torch
 
 from . import _lib, ops
 
-DEFAULT_BUCKETS = (256, 1024, 4096, 16384, 65536)
+# batch sizes with a captured graph; the largest bounds one batch (a larger request is split), which
+# also bounds how long a batch holds the SMs while small requests wait
+DEFAULT_BUCKETS = (256, 1024, 4096, 16384)
 
 
 @dataclass
@@ -78,8 +82,8 @@ class PredictServer:
     (same results; for comparison).
     """
 
-    def __init__(self, gpr, buckets=DEFAULT_BUCKETS, slots: int = 3, use_graphs: bool = True,
-                 memory_fraction: float = 0.5):
+    def __init__(self, gpr, buckets=DEFAULT_BUCKETS, slots: int = 4, use_graphs: bool = True,
+                 memory_fraction: float = 0.5, small_points: int = 4096):
         if not hasattr(gpr, 'X_train_'):
             raise ValueError('PredictServer needs a fitted model')
         self.gpr = gpr
@@ -107,10 +111,14 @@ class PredictServer:
         per_slot = self._slot_bytes()
         free, _ = torch.cuda.mem_get_info(self.device)
         self.n_slots = max(1, min(int(slots), int(free * memory_fraction // max(per_slot, 1))))
-        self.slots = [self._make_slot() for _ in range(self.n_slots)]
+        # slot 0 (the small requests' lane when there are several slots) runs on a high-priority
+        # stream: its blocks are scheduled ahead of queued blocks of the large batches
+        self.slots = [self._make_slot(high_priority=(i == 0 and self.n_slots > 1)) for i in range(self.n_slots)]
 
-        self._queue = collections.deque()   # (request, next row offset)
-        self._inflight = collections.deque()  # (slot, batch) in launch order
+        self._queue = collections.deque()        # large requests: [request, next row offset]
+        self._small = collections.deque()        # requests of at most small_points rows
+        self.small_points = int(small_points)
+        self._inflight = []                      # (slot, batch) launched, not yet completed
         self._cv = threading.Condition()
         self._stop = False
         self._error = None
@@ -135,10 +143,10 @@ class PredictServer:
         nbr = ops.knn(self.xs_train, xs, self.m, None, self.ls, flags=flags)
         return ops.predict(self.xt, self.yt, xl, nbr, self.p, self.alpha, self.pivot_tol, flags=flags)
 
-    def _make_slot(self) -> _Slot:
+    def _make_slot(self, high_priority: bool = False) -> _Slot:
         b = self.max_batch
         dev = self.device
-        slot = _Slot(stream=torch.cuda.Stream(dev),
+        slot = _Slot(stream=torch.cuda.Stream(dev, priority=-1 if high_priority else 0),
                      x_in=torch.zeros((b, self.d), dtype=torch.float64, device=dev),
                      x_pin=torch.empty((b, self.d), dtype=torch.float64).pin_memory(),
                      mean_pin=torch.empty((b, self.ydim), dtype=torch.float64).pin_memory(),
@@ -176,7 +184,7 @@ class PredictServer:
         with self._cv:
             if self._error is not None:
                 raise RuntimeError('predict server failed') from self._error
-            self._queue.append([req, 0])
+            (self._small if x.shape[0] <= self.small_points else self._queue).append([req, 0])
             self._cv.notify_all()
         return fut
 
@@ -197,23 +205,36 @@ class PredictServer:
         self.close()
 
     # ---- scheduler ------------------------------------------------------------------------
-    def _free_slot(self):
-        for s in self.slots:
-            if not s.busy:
-                return s
+    def _pick(self):
+        """(slot, queue) to launch next, or None (under the lock).  Slot 0 serves the small
+        queue only (when there are two or more slots); the others take large requests first."""
+        for i, sl in enumerate(self.slots):
+            if sl.busy:
+                continue
+            if i == 0 and len(self.slots) > 1:
+                if self._small:
+                    return sl, self._small
+                continue
+            if self._queue:
+                return sl, self._queue
+            if self._small:
+                return sl, self._small
         return None
 
-    def _take_batch(self) -> _Batch:
-        """Pieces of the queued requests, oldest first, up to the largest bucket (under the lock)."""
+    def _pending(self) -> bool:
+        return bool(self._queue or self._small)
+
+    def _take_batch(self, queue) -> _Batch:
+        """Pieces of the requests in ``queue``, oldest first, up to the largest bucket."""
         pieces, points = [], 0
-        while self._queue and points < self.max_batch:
-            entry = self._queue[0]
+        while queue and points < self.max_batch:
+            entry = queue[0]
             req, off = entry
             rows = min(req.x.shape[0] - off, self.max_batch - points)
             pieces.append((req, off, rows, points))
             points += rows
             if off + rows == req.x.shape[0]:
-                self._queue.popleft()
+                queue.popleft()
             else:
                 entry[1] = off + rows
         bucket = next(b for b in self.buckets if b >= points)
@@ -224,12 +245,17 @@ class PredictServer:
         try:
             while True:
                 with self._cv:
-                    while not self._stop and (not self._queue or self._free_slot() is None):
+                    pick = self._pick()
+                    while not self._stop and pick is None:
                         self._cv.wait()
-                    if self._stop and not self._queue:
-                        return
-                    slot = self._free_slot()
-                    batch = self._take_batch()
+                        pick = self._pick()
+                    if pick is None:  # stopping and nothing left to launch
+                        if not self._pending():
+                            return
+                        self._cv.wait(0.001)
+                        continue
+                    slot, queue = pick
+                    batch = self._take_batch(queue)
                     slot.busy = True
                 self._launch(slot, batch)
                 with self._cv:
@@ -264,30 +290,35 @@ class PredictServer:
         try:
             while True:
                 with self._cv:
-                    while not self._inflight and not (self._stop and not self._queue and self._idle()):
+                    while not self._inflight and not (self._stop and not self._pending() and self._idle()):
                         self._cv.wait()
                     if not self._inflight:
                         return
-                    slot, batch = self._inflight.popleft()
-                batch.event.synchronize()
-                fl = int(slot.flags_pin.item()) & ~(_lib.NNGP_FLAG_FP64_FALLBACK | _lib.NNGP_FLAG_NOT_PD)
-                mean = slot.mean_pin.numpy()
-                var = slot.var_pin.numpy()
-                finished = []
-                for req, off, rows, at in batch.pieces:
-                    req.mean[off:off + rows] = mean[at:at + rows]
-                    req.var[off:off + rows] = var[at:at + rows]
-                    req.left -= rows
-                    if req.left == 0:
-                        finished.append(req)
-                with self._cv:
-                    slot.busy = False
-                    self._cv.notify_all()
-                for req in finished:
-                    if fl:
-                        req.future.set_exception(_lib.NngpError(f'predict server: kernel status flags {fl}'))
-                    else:
-                        self._finish(req)
+                    batches = list(self._inflight)
+                done = [sb for sb in batches if sb[1].event.query()]
+                if not done:  # nothing finished yet: poll again shortly (batches finish out of order)
+                    time.sleep(2e-5)
+                    continue
+                for slot, batch in done:
+                    fl = int(slot.flags_pin.item()) & ~(_lib.NNGP_FLAG_FP64_FALLBACK | _lib.NNGP_FLAG_NOT_PD)
+                    mean = slot.mean_pin.numpy()
+                    var = slot.var_pin.numpy()
+                    finished = []
+                    for req, off, rows, at in batch.pieces:
+                        req.mean[off:off + rows] = mean[at:at + rows]
+                        req.var[off:off + rows] = var[at:at + rows]
+                        req.left -= rows
+                        if req.left == 0:
+                            finished.append(req)
+                    with self._cv:
+                        self._inflight.remove((slot, batch))
+                        slot.busy = False
+                        self._cv.notify_all()
+                    for req in finished:
+                        if fl:
+                            req.future.set_exception(_lib.NngpError(f'predict server: kernel status flags {fl}'))
+                        else:
+                            self._finish(req)
         except BaseException as e:
             self._fail(e)
 
@@ -306,8 +337,10 @@ class PredictServer:
     def _fail(self, e):
         with self._cv:
             self._error = e
-            pending = [r for r, _ in self._queue] + [p[0] for _, b in self._inflight for p in b.pieces]
+            pending = ([r for r, _ in self._queue] + [r for r, _ in self._small] +
+                       [p[0] for _, b in self._inflight for p in b.pieces])
             self._queue.clear()
+            self._small.clear()
             self._stop = True
             self._cv.notify_all()
         for r in pending:
