@@ -351,7 +351,8 @@ class ClockSampler:
 # ------------------------------------------------------------------------------------------
 # Our arm
 # ------------------------------------------------------------------------------------------
-PROFILE = {'fit3d': 'knn_tc_kernel_fit_n434874_d3_m32.md', 'precision': 'knn_tc_kernel_fit_n1000000_d16_m32.md'}
+PROFILE = {'fit3d': 'knn_tc_kernel_fit_n434874_d3_m32.md', 'precision': 'knn_tc_kernel_fit_n1000000_d16_m32.md',
+           'differentiation': 'knn_tc_kernel_fit_n434874_d8_m32.md'}
 
 
 def read_profile_traffic():
