@@ -133,6 +133,25 @@ nngp_status nngp_knn_f64(const double *ref, int64_t n_ref, const double *query, 
                          int32_t *status_flags, void *workspace, size_t workspace_bytes,
                          void *stream);
 
+/* Neighbour-list reuse across fit steps (isotropic or no length scale, FP32 search): the
+ * reference recomputes the fit step's search on every log-likelihood call (base_nngpr.py:532);
+ * an isotropic length scale only rescales every distance, so the lists can change only through
+ * FP32 rounding.  With n_cand > num_nn candidates per point from one prefix search
+ * (nngp_knn_f32, ref_cut_index 0, at length scale l0, ascending), nngp_knn_reuse_prepare_f32
+ * stores per point the normalised distance of its last candidate minus twice a rounding bound,
+ * 2 (d + 6) 2^-24 (|x_i| + max_norm)^2 (max_norm >= every row's 2-norm); nngp_knn_reuse_rank_f32
+ * then ranks the candidates at a new length scale l in the search's exact arithmetic and writes
+ * the top num_nn.  A point whose num_nn-th distance l^2 D is not below its threshold is counted
+ * in *n_failed (device int, accumulated): only when *n_failed stays 0 are the lists proven equal
+ * to nngp_knn_f32's at l; otherwise run the full search.  x: the unscaled FP32 points (n, d);
+ * n_cand <= 64, num_nn <= 32. */
+nngp_status nngp_knn_reuse_prepare_f32(const float *x, int64_t n, int32_t d, double length_scale,
+                                       const int32_t *cand, int32_t n_cand, double max_norm, double *thr,
+                                       void *stream);
+nngp_status nngp_knn_reuse_rank_f32(const float *x, int64_t n, int32_t d, double length_scale,
+                                    const int32_t *cand, int32_t n_cand, const double *thr,
+                                    int32_t num_nn, int32_t *out_idx, int32_t *n_failed, void *stream);
+
 /* ---------------------------------------------------------------------------------------
  * Log-likelihood (+ gradient) of the fit step
  *

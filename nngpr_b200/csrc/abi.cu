@@ -33,6 +33,10 @@ nngp_status loglik_f64_noalloc(const double *, const double *, int64_t, int, int
                                const nngp_kernel *, int, double *, int32_t *, cudaStream_t);
 nngp_status plain_knn_f32(const float *, int64_t, const float *, int64_t, int, int, bool, int64_t, int32_t *,
                           cudaStream_t);
+nngp_status reuse_prepare_f32(const float *, int64_t, int, double, const int32_t *, int, double, double *,
+                              cudaStream_t);
+nngp_status reuse_rank_f32(const float *, int64_t, int, double, const int32_t *, int, const double *, int, int32_t *,
+                           int32_t *, cudaStream_t);
 nngp_status predict_f32(const float *, const float *, int64_t, const float *, int64_t, int, int, const int32_t *, int,
                         const nngp_kernel *, double, float *, float *, int32_t *, cudaStream_t);
 nngp_status predict_f64(const double *, const double *, int64_t, const double *, int64_t, int, int, const int32_t *,
@@ -164,6 +168,23 @@ nngp_status nngp_plain_knn_f32(const float *ref_scaled, int64_t n_ref, const flo
     return guarded([&] {
         return plain_knn_f32(ref_scaled, n_ref, query_scaled, n_query, d, num_nn, has_ref_cut != 0, ref_cut_index,
                              out_idx, as_stream(stream));
+    });
+}
+
+nngp_status nngp_knn_reuse_prepare_f32(const float *x, int64_t n, int32_t d, double length_scale,
+                                       const int32_t *cand, int32_t n_cand, double max_norm, double *thr,
+                                       void *stream) {
+    return guarded([&] {
+        return reuse_prepare_f32(x, n, d, length_scale, cand, n_cand, max_norm, thr, as_stream(stream));
+    });
+}
+
+nngp_status nngp_knn_reuse_rank_f32(const float *x, int64_t n, int32_t d, double length_scale, const int32_t *cand,
+                                    int32_t n_cand, const double *thr, int32_t num_nn, int32_t *out_idx,
+                                    int32_t *n_failed, void *stream) {
+    return guarded([&] {
+        return reuse_rank_f32(x, n, d, length_scale, cand, n_cand, thr, num_nn, out_idx, n_failed,
+                              as_stream(stream));
     });
 }
 

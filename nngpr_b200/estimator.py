@@ -54,6 +54,12 @@ class B200Nngpr(GaussianProcessRegressor):
     keep_resident : bool, default True
         Keep the training set in HBM between calls.  ``False`` uploads it on every call, the
         reference's behaviour.
+    reuse_neighbours : bool, default False
+        Reuse the fit step's neighbour lists across calls whose length scale changes
+        (isotropic or no length scale, FP32 search): one wider search keeps 16 candidates more
+        per point, later calls rank the candidates at the new length scale and keep the result
+        only where a rounding bound proves it equal to a fresh search (``ops.knn_reuse_rank``);
+        otherwise the search runs again.  Results are identical either way.
     optimizer : 'fmin_l_bfgs_b', 'device-lbfgs', callable or None
         As scikit-learn's, plus ``'device-lbfgs'``: ``torch.optim.LBFGS`` on the device through
         the differentiable log-likelihood (``nngpr_b200.autograd``).
@@ -78,6 +84,7 @@ class B200Nngpr(GaussianProcessRegressor):
         "device": [str, torch.device, None],
         "pivot_tol": [Interval(Real, 0, None, closed="left")],
         "keep_resident": ["boolean"],
+        "reuse_neighbours": ["boolean"],
         "optimizer": [StrOptions({"fmin_l_bfgs_b", "device-lbfgs"}), callable, None],
     }
 
@@ -85,7 +92,7 @@ class B200Nngpr(GaussianProcessRegressor):
                  normalize_y=False, copy_X_train=True, n_targets=None, random_state=None, num_nn=None,
                  nn_type=None, batch_size=None, allow_downcast_f32=None, distribute_method=None,
                  mp_start_method=None, random_gen_batch_byte_size=None, distribute_environ=None,
-                 device=None, pivot_tol=1e-2, keep_resident=True):
+                 device=None, pivot_tol=1e-2, keep_resident=True, reuse_neighbours=False):
         super().__init__(kernel=kernel, alpha=alpha, optimizer=optimizer,
                          n_restarts_optimizer=n_restarts_optimizer, normalize_y=normalize_y,
                          copy_X_train=copy_X_train, n_targets=n_targets, random_state=random_state)
@@ -100,6 +107,7 @@ class B200Nngpr(GaussianProcessRegressor):
         self.device = device
         self.pivot_tol = pivot_tol
         self.keep_resident = keep_resident
+        self.reuse_neighbours = reuse_neighbours
 
     # ---- resolved settings ----------------------------------------------------------------
     @property
@@ -165,6 +173,7 @@ class B200Nngpr(GaussianProcessRegressor):
         return xh.to(dev, non_blocking=True), yh.to(dev, non_blocking=True)
 
     def _drop_device_copies(self):
+        self.__dict__.pop('_nn_cache', None)
         self.__dict__.pop('_device_cache', None)
         self.__dict__.pop('_pinned_cache', None)
 
@@ -257,7 +266,29 @@ class B200Nngpr(GaussianProcessRegressor):
             x_search = self._train_tensors(self._dtypes()[0])[0]
         n = x_search.shape[0]
         m = min(self._num_nn, max(n - 1, 0))
-        return ops.knn(x_search, x_search, m, ref_cut_index=0, length_scale=self._search_ls(p), flags=flags)
+        ls = self._search_ls(p)
+        if (self.reuse_neighbours and x_search.dtype == torch.float32 and 0 < m <= 32
+                and (ls is None or np.ndim(ls) == 0 or np.size(ls) == 1)):
+            return self._reused_neighbours(x_search, m, ls, flags)
+        return ops.knn(x_search, x_search, m, ref_cut_index=0, length_scale=ls, flags=flags)
+
+    def _reused_neighbours(self, xs, m, ls, flags):
+        """Fit-step lists through the reuse cache (see ``reuse_neighbours``)."""
+        n = xs.shape[0]
+        cache = self.__dict__.get('_nn_cache')
+        if cache is not None and cache['m'] == m and cache['n'] == n:
+            if ls is None:  # input space: the lists do not depend on theta
+                return cache['cand'][:, :m].contiguous()
+            nbr, failed = ops.knn_reuse_rank(xs, cache['cand'], cache['thr'], ls, m)
+            if int(failed.item()) == 0:
+                return nbr
+        # (re)build at this length scale: a wider search, the first m columns are its lists
+        c = min(m + 16, 64, n - 1)
+        cand = ops.knn(xs, xs, c, ref_cut_index=0, length_scale=ls, flags=flags)
+        max_norm = float(torch.linalg.vector_norm(xs.double(), dim=1).max()) if n else 0.0
+        thr = ops.knn_reuse_prepare(xs, cand, ls, max_norm)
+        self.__dict__['_nn_cache'] = {'m': m, 'n': n, 'cand': cand, 'thr': thr}
+        return cand[:, :m].contiguous()
 
     def log_marginal_likelihood(self, theta=None, eval_gradient=False, clone_kernel=True):
         """Log-likelihood of ``theta`` (and its gradient), ``base_nngpr.py:385-451``."""
@@ -379,4 +410,5 @@ class B200Nngpr(GaussianProcessRegressor):
         state = dict(state)
         state.pop('_device_cache', None)
         state.pop('_pinned_cache', None)
+        state.pop('_nn_cache', None)
         return state

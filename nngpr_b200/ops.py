@@ -54,6 +54,37 @@ def new_flags(device) -> torch.Tensor:
     return torch.zeros(1, dtype=torch.int32, device=device)
 
 
+def knn_reuse_prepare(x: torch.Tensor, cand: torch.Tensor, length_scale, max_norm: float) -> torch.Tensor:
+    """Per-point thresholds (float64 ``(n,)``) that let :func:`knn_reuse_rank` prove a reused
+    list exact: ``cand`` is the FP32 prefix search of ``x`` (float32 ``(n, d)``) at the scalar
+    ``length_scale`` (``None``: input space) with more slots than the lists will need;
+    ``max_norm`` bounds every row's 2-norm."""
+    _check_tensor(x, 'x', (torch.float32,))
+    _check_tensor(cand, 'cand', (torch.int32,))
+    n, d = x.shape
+    thr = torch.empty(n, dtype=torch.float64, device=x.device)
+    ls = 1.0 if length_scale is None else float(np.asarray(length_scale).reshape(-1)[0])
+    st = _lib.lib().nngp_knn_reuse_prepare_f32(_ptr(x), n, d, ls, _ptr(cand), cand.shape[1], float(max_norm),
+                                              _ptr(thr), _stream())
+    _lib.check(st, 'nngp_knn_reuse_prepare_f32')
+    return thr
+
+
+def knn_reuse_rank(x: torch.Tensor, cand: torch.Tensor, thr: torch.Tensor, length_scale, num_nn: int):
+    """Top-``num_nn`` of the candidates at a new scalar length scale, and a device int32 count
+    of the points whose list is not proven equal to :func:`knn`'s (0: every list is exact)."""
+    _check_tensor(x, 'x', (torch.float32,))
+    _check_tensor(cand, 'cand', (torch.int32,))
+    n, d = x.shape
+    out = torch.empty((n, num_nn), dtype=torch.int32, device=x.device)
+    failed = torch.zeros(1, dtype=torch.int32, device=x.device)
+    ls = 1.0 if length_scale is None else float(np.asarray(length_scale).reshape(-1)[0])
+    st = _lib.lib().nngp_knn_reuse_rank_f32(_ptr(x), n, d, ls, _ptr(cand), cand.shape[1], _ptr(thr), num_nn,
+                                           _ptr(out), _ptr(failed), _stream())
+    _lib.check(st, 'nngp_knn_reuse_rank_f32')
+    return out, failed
+
+
 def raise_on_flags(flags: int, what: str) -> None:
     """Turn a status word into an exception (bad index / timeout) or a LinAlgError."""
     if flags & _lib.NNGP_FLAG_TIMEOUT:

@@ -353,3 +353,67 @@ def predict(x_train, y_train, x_query, nbr, p: KernelParams, alpha: float):
     mean = (K_xn @ _chol_solve(L, y_nn))[:, 0, :]
     var = K[:, 0, 0] - (K_xn @ _chol_solve(L, np.swapaxes(K_xn, 1, 2)))[:, 0, 0]
     return mean, np.sqrt(var)
+
+
+# ----------------------------------------------------------------------------------------------
+# Neighbour-list reuse across length scales (restates nngpr_b200/csrc/knn_reuse.cu)
+# ----------------------------------------------------------------------------------------------
+
+UNIT_ROUNDOFF_F32 = 2.0 ** -24
+
+
+def _scale_of(length_scale) -> np.float32:
+    return np.float32(1.0) if length_scale is None else np.float32(np.asarray(length_scale).reshape(-1)[0])
+
+
+def _cand_sqdist(xs: np.ndarray, rows: np.ndarray, cols: np.ndarray) -> np.ndarray:
+    """Squared distances of the pairs (rows[k], cols[k]) in the search arithmetic (float32,
+    ``ref - query`` per feature, accumulated feature by feature)."""
+    out = np.zeros(rows.shape, dtype=xs.dtype)
+    for f in range(xs.shape[1]):
+        t = xs[cols, f] - xs[rows, f]
+        out += t * t
+    return out
+
+
+def reuse_thresholds(x: np.ndarray, cand: np.ndarray, length_scale, max_norm: float) -> np.ndarray:
+    """Per point: ``l0^2 D_l0(i, last candidate) - 2 * 2 (d + 6) u (|x_i| + max_norm)^2``, +inf
+    when the candidate list holds every earlier point (its last slot is -1).  ``cand`` is the
+    exact prefix search at ``length_scale`` (float32) with more slots than the lists need."""
+    x32 = np.asarray(x, dtype=np.float32)
+    n, d = x32.shape
+    xs = scale_for_search(x32, length_scale)
+    ls2 = float(_scale_of(length_scale)) ** 2
+    thr = np.full(n, np.inf)
+    last = np.asarray(cand)[:, -1]
+    rows = np.nonzero(last >= 0)[0]
+    tau = ls2 * _cand_sqdist(xs, rows, last[rows]).astype(np.float64)
+    r = np.sqrt((x32[rows].astype(np.float64) ** 2).sum(1)) * (1 + 1e-12) + max_norm
+    thr[rows] = tau - 2.0 * (2.0 * (d + 6) * UNIT_ROUNDOFF_F32) * r * r
+    return thr
+
+
+def reuse_rank(x: np.ndarray, cand: np.ndarray, thr: np.ndarray, length_scale, num_nn: int):
+    """Exact top-``num_nn`` of each point's candidates at ``length_scale`` (ascending distance,
+    lower index first) and the number of points whose ``num_nn``-th distance does not clear the
+    threshold (for those the lists are not proven exact)."""
+    x32 = np.asarray(x, dtype=np.float32)
+    n = x32.shape[0]
+    xs = scale_for_search(x32, length_scale)
+    ls2 = float(_scale_of(length_scale)) ** 2
+    cand = np.asarray(cand)
+    out = np.full((n, num_nn), -1, dtype=np.int32)
+    failed = 0
+    rr, cc = np.nonzero(cand >= 0)
+    dist = np.full(cand.shape, np.inf, dtype=np.float32)
+    dist[rr, cc] = _cand_sqdist(xs, rr, cand[rr, cc])
+    for i in range(n):
+        ok = cand[i] >= 0
+        js, ds = cand[i][ok], dist[i][ok]
+        order = np.lexsort((js, ds))[:num_nn]
+        out[i, :order.size] = js[order]
+        if np.isinf(thr[i]):
+            continue
+        if order.size < num_nn or not (ls2 * float(ds[order[-1]]) * (1 + 1e-12) < thr[i]):
+            failed += 1
+    return out, failed
