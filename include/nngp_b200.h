@@ -261,6 +261,24 @@ nngp_status nngp_plain_knn_f32(const float *ref_scaled, int64_t n_ref, const flo
                                int64_t n_query, int32_t d, int32_t num_nn, int32_t has_ref_cut,
                                int64_t ref_cut_index, int32_t *out_idx, void *stream);
 
+/* Predict with conditioning_method='full' (Nngpr.predict's sequential algorithm,
+ * base_nngpr.py:896-1030): query i conditions on the training set and on the queries before it.
+ * x_full = [x_train; x_query] (n_train + n_query rows), nbr (n_query, num_nn) indices into
+ * x_full from nngp_knn_f64/_f32 with ref = x_full, query = x_query, ref_cut_index = n_train
+ * (-1 padded; an index >= n_train + i is flagged and ignored).  Each query's local system gives
+ * its conditioning weights in parallel (alpha on training neighbours only, :952-954); one warp
+ * then walks the queries in order: the mean uses the predicted means of query neighbours, the
+ * variance adds their covariance, which is tracked only between a query and its own query
+ * neighbours, as the reference's sparse partial covariance does (:923-930, :1002-1008).  mean:
+ * (n_query, ydim); var (n_query) when want_var.  FP64, num_nn <= 32; the recursion is serial in
+ * the queries (tens of microseconds per hundred queries). */
+size_t nngp_predict_full_workspace_size(int64_t n_query, int32_t num_nn);
+nngp_status nngp_predict_full_f64(const double *x_full, const double *y_train, int64_t n_train,
+                                  int64_t n_query, int32_t d, int32_t ydim, const int32_t *nbr,
+                                  int32_t num_nn, const nngp_kernel *kernel, int32_t want_var,
+                                  double *mean, double *var, int32_t *status_flags, void *workspace,
+                                  size_t workspace_bytes, void *stream);
+
 /* Self-test of the tensor-core operand layout used by the search (no counterpart in the
  * reference): d (128 x 128) = a (128 x kp) * b (128 x kp)^T in TF32 with FP32 accumulation,
  * a and b row-major device arrays, kp = 8, 16 or 32, through the same shared-memory layout,

@@ -33,6 +33,9 @@ nngp_status loglik_f64_noalloc(const double *, const double *, int64_t, int, int
                                const nngp_kernel *, int, double *, int32_t *, cudaStream_t);
 nngp_status plain_knn_f32(const float *, int64_t, const float *, int64_t, int, int, bool, int64_t, int32_t *,
                           cudaStream_t);
+size_t predict_full_workspace_size(int64_t, int);
+nngp_status predict_full(const double *, const double *, int64_t, int64_t, int, int, const int32_t *, int,
+                         const nngp_kernel *, int, double *, double *, int32_t *, void *, size_t, cudaStream_t);
 nngp_status reuse_prepare_f32(const float *, int64_t, int, double, const int32_t *, int, double, double *,
                               cudaStream_t);
 nngp_status reuse_rank_f32(const float *, int64_t, int, double, const int32_t *, int, const double *, int, int32_t *,
@@ -168,6 +171,20 @@ nngp_status nngp_plain_knn_f32(const float *ref_scaled, int64_t n_ref, const flo
     return guarded([&] {
         return plain_knn_f32(ref_scaled, n_ref, query_scaled, n_query, d, num_nn, has_ref_cut != 0, ref_cut_index,
                              out_idx, as_stream(stream));
+    });
+}
+
+size_t nngp_predict_full_workspace_size(int64_t n_query, int32_t num_nn) {
+    return predict_full_workspace_size(n_query, num_nn);
+}
+
+nngp_status nngp_predict_full_f64(const double *x_full, const double *y_train, int64_t n_train, int64_t n_query,
+                                  int32_t d, int32_t ydim, const int32_t *nbr, int32_t num_nn,
+                                  const nngp_kernel *kernel, int32_t want_var, double *mean, double *var,
+                                  int32_t *status_flags, void *workspace, size_t workspace_bytes, void *stream) {
+    return guarded([&] {
+        return predict_full(x_full, y_train, n_train, n_query, d, ydim, nbr, num_nn, kernel, want_var, mean, var,
+                            status_flags, workspace, workspace_bytes, as_stream(stream));
     });
 }
 

@@ -51,6 +51,8 @@ struct LocalArgs {
     int d, ydim, m;
     int ard;  // 1: per-feature length scales
     int family;  // stationary part: NNGP_FAMILY_RBF or a Matern (include/nngp_b200.h)
+    int64_t alpha_below;  // alpha goes on the diagonal slots of neighbours with index < alpha_below
+    int weights_out;      // predict: write w = K_nn^-1 k (a.m per point) to `mean` instead of the mean
     int idx_rbf, idx_const, idx_noise, idx_ls, n_theta;
     double inv_ls[kMaxDimLocal];
 };
@@ -166,7 +168,7 @@ __device__ __forceinline__ bool warp_system(const LocalArgs &a, int64_t p, int l
         rp = fma(t, t, rp);
     }
     const TC rbf = (TC)a.rbf, cst = (TC)a.cst;
-    const TC diag_add = (TC)a.noise + (TC)a.alpha;
+    const TC diag_add = (TC)a.noise + ((int64_t)j < a.alpha_below ? (TC)a.alpha : TC(0));
 #pragma unroll
     for (int k = 0; k < M; ++k) {
         const bool vk = (vmask >> k) & 1u;
@@ -214,6 +216,22 @@ __device__ __forceinline__ bool warp_system(const LocalArgs &a, int64_t p, int l
     for (int k = 0; k < M; ++k) Ls[lane * (M + 1) + k] = r[k];
     idg[lane] = TC(1) / dg_own;
     __syncwarp();
+
+    if (PRED && a.weights_out) {
+        // conditioning weights w = L^-T l = K_nn^-1 k and the variance term s2 (no outputs yet:
+        // the full-conditioning recursion combines them with earlier predictions)
+        TC bv = l_own, b_own = TC(0);
+#pragma unroll
+        for (int k = M - 1; k >= 0; --k) {
+            const TC bk = __shfl_sync(FULL, bv, k) * idg[k];
+            if (lane == k) b_own = bk;
+            const TC lkj = Ls[k * (M + 1) + lane];
+            if (lane < k) bv = fma(-lkj, bk, bv);
+        }
+        if (lane < a.m) mean[p * a.m + lane] = (TIn)b_own;
+        if (lane == 0) var[p] = (TIn)s2;
+        return true;
+    }
 
     // ---- outputs ------------------------------------------------------------------------
     TC zw = TC(0);
@@ -720,6 +738,8 @@ nngp_status fill_args(LocalArgs &a, const nngp_kernel *k, int d, int ydim, int m
     a.ydim = ydim;
     a.m = m;
     a.ard = k->n_ls == d && d > 1;
+    a.alpha_below = n_rows;
+    a.weights_out = 0;
     if (k->family < NNGP_FAMILY_RBF || k->family > NNGP_FAMILY_MATERN52)
         return fail(NNGP_ERR_INVALID_ARGUMENT, "kernel family must be one of NNGP_FAMILY_*");
     a.family = k->family;
@@ -806,7 +826,111 @@ nngp_status predict_impl(const TIn *xt, const TIn *yt, int64_t nt, const TIn *xq
     return launch_local<TIn, false, true>(pl, a, xt, yt, xq, nullptr, nbr, nullptr, mean, var, flags, stream);
 }
 
+// ---------------------------------------------------------------------------------------
+// Predict conditioned on the training set and the earlier queries ('full', the sequential
+// algorithm of base_nngpr.py:896-1030)
+// ---------------------------------------------------------------------------------------
+// Covariance between two earlier queries a != b as the reference tracks it: only the pairs
+// where the later one has the earlier one among its neighbours hold a value (the sparse
+// partial covariance, :923-930, :1002-1008); every other pair counts as 0.
+__device__ __forceinline__ double full_pair_cov(const int32_t *__restrict__ nbr, const double *pc, int m, int64_t nt,
+                                               int64_t a, int64_t b) {
+    const int64_t hi = a > b ? a : b, lo = a > b ? b : a;
+    for (int u = 0; u < m; ++u)
+        if ((int64_t)nbr[hi * m + u] == nt + lo) return pc[hi * m + u];
+    return 0.0;
+}
+
+// One warp walks the queries in order (query i may condition on queries < i).  Lane s owns
+// neighbour slot s: mean_i = sum_s w_is v_s (v = y of a training neighbour or the mean already
+// predicted for a query neighbour); var_i = max(0, max(0, s2_i) + w_q^T C w_q) with C the
+// covariance of the query neighbours (variances on the diagonal, tracked pairs elsewhere);
+// the covariances of query i with its query neighbours, (C w)_s, are kept for later queries.
+__global__ void __launch_bounds__(32) full_recursion_kernel(const int32_t *__restrict__ nbr,
+                                                            const double *__restrict__ w,
+                                                            const double *__restrict__ s2,
+                                                            const double *__restrict__ y, int64_t nt, int64_t nq,
+                                                            int m, int ydim, int want_var, double *mean, double *var,
+                                                            double *pc, int32_t *__restrict__ flags) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x;
+    for (int64_t i = 0; i < nq; ++i) {
+        int32_t j = lane < m ? nbr[i * m + lane] : -1;
+        if (j >= 0 && (int64_t)j >= nt + i) {  // not an earlier point: treated as missing
+            flag_or(flags, NNGP_FLAG_BAD_INDEX);
+            j = -1;
+        }
+        const double ws = (lane < m && j >= 0) ? w[i * m + lane] : 0.0;
+        const bool q = j >= 0 && (int64_t)j >= nt;  // a query neighbour
+        for (int c = 0; c < ydim; ++c) {
+            double v = 0.0;
+            if (j >= 0) v = q ? mean[((int64_t)j - nt) * ydim + c] : y[(int64_t)j * ydim + c];
+            const double mu = warp_sum(ws * v);
+            if (lane == 0) mean[i * ydim + c] = mu;
+        }
+        if (want_var) {
+            const int64_t a = q ? (int64_t)j - nt : -1;
+            double cw = q ? var[a] * ws : 0.0;
+            for (int t = 0; t < m; ++t) {
+                const int32_t jt = __shfl_sync(FULL, j, t);
+                const double wt = __shfl_sync(FULL, ws, t);
+                if (q && t != lane && jt >= 0 && (int64_t)jt >= nt)
+                    cw += full_pair_cov(nbr, pc, m, nt, a, (int64_t)jt - nt) * wt;
+            }
+            const double quad = warp_sum(ws * cw);
+            if (lane < m) pc[i * m + lane] = q ? cw : 0.0;
+            if (lane == 0) {
+                const double raw = s2[i] > 0.0 ? s2[i] : 0.0;
+                const double vi = raw + quad;
+                var[i] = vi > 0.0 ? vi : 0.0;
+            }
+        }
+        __syncwarp();  // this query's mean, variance and covariances are visible to the next ones
+    }
+}
+
+size_t predict_full_workspace(int64_t nq, int m) { return (size_t)(2 * nq * (int64_t)m + nq) * sizeof(double) + 256; }
+
+nngp_status predict_full_f64(const double *x_full, const double *y_train, int64_t nt, int64_t nq, int d, int ydim,
+                             const int32_t *nbr, int m, const nngp_kernel *k, int want_var, double *mean, double *var,
+                             int32_t *flags, void *ws, size_t ws_bytes, cudaStream_t stream) {
+    if (nt < 0 || nq < 0) return fail(NNGP_ERR_INVALID_ARGUMENT, "predict_full: negative size");
+    if (m > kWarpM) return fail(NNGP_ERR_UNSUPPORTED, "predict_full: num_nn must be <= 32");
+    LocalArgs a;
+    nngp_status st = fill_args(a, k, d, ydim, m, nt + nq, nq, 0.0, false);
+    if (st != NNGP_OK) return st;
+    if (nq == 0) return NNGP_OK;
+    if (!x_full || !mean || (want_var && !var) || (m > 0 && !nbr) || (nt > 0 && !y_train))
+        return fail(NNGP_ERR_INVALID_ARGUMENT, "predict_full: null pointer");
+    if (!ws || ws_bytes < predict_full_workspace(nq, m))
+        return fail(NNGP_ERR_WORKSPACE, "predict_full: workspace missing or too small");
+    double *wts = reinterpret_cast<double *>(align_up(reinterpret_cast<uintptr_t>(ws), 256));
+    double *s2 = wts + nq * (int64_t)m;
+    double *pc = s2 + nq;
+    a.alpha_below = nt;  // alpha on training neighbours only (base_nngpr.py:952-954)
+    a.weights_out = 1;
+    if (m > 0) {
+        const LocalPlan pl = plan_local(nq, d, m, 0, false);
+        st = launch_local<double, false, true>(pl, a, x_full, y_train, x_full + nt * d, nullptr, nbr, nullptr, wts, s2,
+                                               flags, stream);
+        if (st != NNGP_OK) return st;
+    }
+    full_recursion_kernel<<<1, 32, 0, stream>>>(nbr, wts, s2, y_train, nt, nq, m, ydim, want_var, mean, var, pc,
+                                                flags);
+    NNGP_CUDA_TRY(cudaGetLastError());
+    return NNGP_OK;
+}
+
 }  // namespace
+
+size_t predict_full_workspace_size(int64_t nq, int m) { return predict_full_workspace(nq, m); }
+
+nngp_status predict_full(const double *x_full, const double *y_train, int64_t nt, int64_t nq, int d, int ydim,
+                         const int32_t *nbr, int m, const nngp_kernel *k, int want_var, double *mean, double *var,
+                         int32_t *flags, void *ws, size_t ws_bytes, cudaStream_t stream) {
+    return predict_full_f64(x_full, y_train, nt, nq, d, ydim, nbr, m, k, want_var, mean, var, flags, ws, ws_bytes,
+                            stream);
+}
 
 // ---------------------------------------------------------------------------------------
 // Allocation-free variant of the FP64 log-likelihood (nngp_loglik_f64_noalloc)

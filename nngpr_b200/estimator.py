@@ -326,8 +326,8 @@ class B200Nngpr(GaussianProcessRegressor):
         conditioning_method = 'only-train' if conditioning_method is None else conditioning_method
         if conditioning_method not in {'only-train', 'full', 'full-double-nn'}:
             raise ValueError(f"unknown conditioning_method {conditioning_method!r}")
-        if return_cov or conditioning_method != 'only-train':
-            raise NotImplementedError("B200Nngpr implements predict(conditioning_method='only-train') "
+        if return_cov or conditioning_method == 'full-double-nn':
+            raise NotImplementedError("B200Nngpr implements predict(conditioning_method='only-train' or 'full') "
                                       "without return_cov")
         if self.kernel is None or self.kernel.requires_vector_input:
             dtype, ensure_2d = "numeric", True
@@ -346,6 +346,8 @@ class B200Nngpr(GaussianProcessRegressor):
         p = self._params(kernel)
         dev = self._device
         search_dtype, local_dtype = self._dtypes()
+        if conditioning_method == 'full':
+            return self._predict_full(X, p, search_dtype, return_std)
         xt, yt = self._train_tensors(local_dtype)
         xs_train = xt if search_dtype == local_dtype else self._train_tensors(search_dtype)[0]
         xq_host = np.ascontiguousarray(X, dtype=np.float64)
@@ -369,6 +371,34 @@ class B200Nngpr(GaussianProcessRegressor):
         if not return_std:
             return mean
         std = np.sqrt(var).reshape(-1, 1) * y_std
+        if std.shape[1] == 1:
+            std = std[:, 0]
+        return mean, std
+
+    def _predict_full(self, X, p, search_dtype, return_std):
+        """``conditioning_method='full'`` (``base_nngpr.py:896-1030``): every query conditions on
+        the training set and on the queries before it; FP64 local systems."""
+        dev = self._device
+        xt, yt = self._train_tensors(torch.float64)
+        xq = torch.from_numpy(np.ascontiguousarray(X, dtype=np.float64)).to(dev)
+        nt, nq = xt.shape[0], xq.shape[0]
+        m = min(self._num_nn, nt + nq)
+        if m > 32:
+            raise NotImplementedError("predict(conditioning_method='full') supports num_nn <= 32")
+        flags = ops.new_flags(dev)
+        x_full_s = torch.cat([xt, xq]).to(search_dtype)
+        nbr = ops.knn(x_full_s, x_full_s[nt:], m, ref_cut_index=nt, length_scale=self._search_ls(p), flags=flags)
+        mean, var = ops.predict_full(xt, yt, xq, nbr, p, float(self.alpha), return_std, flags=flags)
+        mean = mean.cpu().numpy()
+        ops.raise_on_flags(int(flags.item()) & ~_lib.NNGP_FLAG_NOT_PD, 'predict')
+        y_std = np.asarray(self._y_train_std, dtype=np.float64).reshape(1, -1)
+        y_mean = np.asarray(self._y_train_mean, dtype=np.float64).reshape(1, -1)
+        mean = y_std * mean + y_mean
+        if mean.shape[1] == 1:
+            mean = mean[:, 0]
+        if not return_std:
+            return mean
+        std = np.sqrt(var.cpu().numpy()).reshape(-1, 1) * y_std
         if std.shape[1] == 1:
             std = std[:, 0]
         return mean, std

@@ -54,6 +54,36 @@ def new_flags(device) -> torch.Tensor:
     return torch.zeros(1, dtype=torch.int32, device=device)
 
 
+def predict_full(x_train: torch.Tensor, y_train: torch.Tensor, x_query: torch.Tensor, nbr: torch.Tensor,
+                 p: RbfParams, alpha: float, want_var: bool = True, flags: torch.Tensor | None = None):
+    """Predict with ``conditioning_method='full'`` (FP64): mean ``(nq, ydim)`` and variance ``(nq,)``
+    (``None`` without ``want_var``).  ``nbr`` indexes ``[x_train; x_query]``: the search of that
+    array for ``x_query`` with ``ref_cut_index = n_train``."""
+    for t, nm in ((x_train, 'x_train'), (y_train, 'y_train'), (x_query, 'x_query')):
+        _check_tensor(t, nm, (torch.float64,))
+    _check_tensor(nbr, 'nbr', (torch.int32,))
+    nt, d = x_train.shape
+    nq = x_query.shape[0]
+    y2 = y_train if y_train.dim() == 2 else y_train.reshape(nt, 1)
+    ydim = y2.shape[1]
+    m = nbr.shape[1] if nbr.dim() == 2 else 0
+    x_full = torch.cat([x_train, x_query]).contiguous()
+    mean = torch.empty((nq, ydim), dtype=torch.float64, device=x_query.device)
+    var = torch.empty((nq,), dtype=torch.float64, device=x_query.device) if want_var else None
+    if nq == 0:
+        return mean, var
+    keep = []
+    k = _kernel_struct(p, alpha, d, keep)
+    L = _lib.lib()
+    ws_bytes = int(L.nngp_predict_full_workspace_size(nq, m))
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device=x_query.device)
+    st = L.nngp_predict_full_f64(_ptr(x_full), _ptr(y2), nt, nq, d, ydim, _ptr(nbr), m, ctypes.byref(k),
+                                 1 if want_var else 0, _ptr(mean), _ptr(var), _ptr(flags), _ptr(ws), ws_bytes,
+                                 _stream())
+    _lib.check(st, 'nngp_predict_full_f64')
+    return mean, var
+
+
 def knn_reuse_prepare(x: torch.Tensor, cand: torch.Tensor, length_scale, max_norm: float) -> torch.Tensor:
     """Per-point thresholds (float64 ``(n,)``) that let :func:`knn_reuse_rank` prove a reused
     list exact: ``cand`` is the FP32 prefix search of ``x`` (float32 ``(n, d)``) at the scalar

@@ -417,3 +417,54 @@ def reuse_rank(x: np.ndarray, cand: np.ndarray, thr: np.ndarray, length_scale, n
         if order.size < num_nn or not (ls2 * float(ds[order[-1]]) * (1 + 1e-12) < thr[i]):
             failed += 1
     return out, failed
+
+
+def predict_full(x_train, y_train, x_query, nbr, p: KernelParams, alpha: float, return_std: bool = True):
+    """Predict with ``conditioning_method='full'``: restates the sequential algorithm of
+    ``Nngpr.predict`` (``base_nngpr.py:896-1030``) for ``return_cov=False``.  ``nbr`` is
+    ``(nq, m)`` of indices into ``x_full = [x_train; x_query]`` (query ``i`` may use indices below
+    ``nt + i``; ``-1`` padded).  Query neighbours contribute their predicted means; the variance
+    adds ``w^T C w`` with ``C`` the covariance of the query neighbours, known only between a query
+    and its own query neighbours (the reference's sparse partial covariance, ``:923-930``)."""
+    x_train = np.asarray(x_train, dtype=np.float64)
+    x_query = np.asarray(x_query, dtype=np.float64)
+    y_train = np.asarray(y_train, dtype=np.float64)
+    if y_train.ndim == 1:
+        y_train = y_train[:, None]
+    nt, nq = x_train.shape[0], x_query.shape[0]
+    x_full = np.concatenate([x_train, x_query])
+    nbr = np.asarray(nbr)
+    m = nbr.shape[1]
+    idx = np.concatenate([np.arange(nt, nt + nq)[:, None], nbr], axis=1)
+    K, _ = fill_nn_kernel(x_full, idx, p, False)
+    train = (idx >= 0) & (idx < nt)
+    ii = np.arange(idx.shape[1])
+    K[:, ii, ii] += np.where(train, alpha, 0.0)  # :952-954
+    mean = np.full((nt + nq, y_train.shape[1]), np.nan)
+    mean[:nt] = y_train
+    var = np.full(nq, np.nan)
+    pcov = {}  # (i, j) with j a query neighbour of query i (both query positions) -> covariance
+    for i in range(nq):
+        Kn = K[i, 1:, 1:]
+        kx = K[i, 0, 1:]
+        w = np.linalg.solve(Kn, kx)  # K_nn^-1 k (Kn symmetric)
+        js = nbr[i]
+        vals = np.where(js[:, None] >= 0, mean[np.where(js >= 0, js, 0)], 0.0)
+        mean[nt + i] = w @ vals
+        if not return_std:
+            continue
+        q = js >= nt
+        C = np.zeros((m, m))
+        for s in np.nonzero(q)[0]:
+            a = js[s] - nt
+            C[s, s] = var[a]
+            for t in np.nonzero(q)[0]:
+                b = js[t] - nt
+                if a > b:
+                    C[s, t] = C[t, s] = pcov.get((a, b), 0.0)
+        raw = max(0.0, K[i, 0, 0] - kx @ w)
+        var[i] = max(0.0, raw + w @ C @ w)
+        cw = C @ w
+        for s in np.nonzero(q)[0]:
+            pcov[(i, js[s] - nt)] = cw[s]
+    return mean[nt:], (np.sqrt(var) if return_std else None)

@@ -70,3 +70,11 @@ def lml_scale(name):
         ll, _ = O.loglik_terms(g['x'], y2, g['nbr_fit_f64'], oracle_params(p), float(g['alpha']), False)
         _SCALE[name] = max(float(np.abs(ll).sum()), abs(float(g['lml'])))
     return _SCALE[name]
+
+
+FULL_CASES = ['cpu_n2000_d3_m16', 'ard_n400_d5_m12_y2', 'matern52_n400_d2_m10']
+
+
+def load_full(name):
+    """The reference's predict(conditioning_method='full') on a golden case (make_golden.py)."""
+    return dict(np.load(os.path.join(GOLDEN, 'full_' + name + '.npz')))

@@ -76,6 +76,8 @@ def main():
     args = ap.parse_args()
     NumpyNngpr, NumpyWorker, bk = _import_reference(args.ref)
     only = set(filter(None, args.only.split(',')))
+    if 'full' in only:
+        return full_cases(NumpyNngpr, NumpyWorker, bk)
     if only and 'rbf' not in only:
         return matern_cases(NumpyNngpr, NumpyWorker, bk)
 
@@ -135,6 +137,34 @@ def main():
          x, y, xq, 10, alpha=1e-6)
     if not only or 'matern' in only:
         matern_cases(NumpyNngpr, NumpyWorker, bk)
+
+
+def full_cases(NumpyNngpr, NumpyWorker, bk):
+    """predict(conditioning_method='full') of the reference (the sequential algorithm,
+    base_nngpr.py:896-1030) on three of the cases above, written to full_<case>.npz with the
+    neighbour lists it used (indices into [x_train; x_query])."""
+    specs = {
+        'cpu_n2000_d3_m16': lambda: bk.ConstantKernel(1.0) * bk.RBF(0.3) + bk.WhiteKernel(0.01),
+        'ard_n400_d5_m12_y2': lambda: bk.ConstantKernel(0.7) * bk.RBF(np.array([0.3, 0.5, 0.8, 1.2, 2.0]))
+        + bk.WhiteKernel(0.05),
+        'matern52_n400_d2_m10': lambda: bk.ConstantKernel(1.0) * bk.Matern(0.6, nu=2.5) + bk.WhiteKernel(0.005),
+    }
+    for name, kernel_fn in specs.items():
+        g = dict(np.load(os.path.join(HERE, name + '.npz')))
+        m = int(g['num_nn'])
+        gpr = NumpyNngpr(kernel=kernel_fn(), num_nn=m, optimizer=None, alpha=float(g['alpha']),
+                         normalize_y=bool(g['normalize_y']), allow_downcast_f32='no', distribute_method='sequential',
+                         num_workers=1)
+        gpr.fit(g['x'], g['y'])
+        xq = g['xq']
+        mean, std = gpr.predict(xq, return_std=True, conditioning_method='full')
+        mean_only = gpr.predict(xq, return_std=False, conditioning_method='full')
+        worker = NumpyWorker()
+        nn, _ = gpr._find_nn_indices_for_train_and_eval(worker, gpr.kernel_, gpr.X_train_, xq, condition_on_eval=True,
+                                                         double_nn=False)
+        np.savez_compressed(os.path.join(HERE, 'full_' + name + '.npz'), mean=np.asarray(mean), std=np.asarray(std),
+                            mean_only=np.asarray(mean_only), nbr=np.asarray(nn)[:, 1:])
+        print('full', name, np.asarray(mean).ravel()[:3], np.asarray(std).ravel()[:3])
 
 
 def matern_cases(NumpyNngpr, NumpyWorker, bk):

@@ -83,7 +83,7 @@ def test_out_of_scope_calls_raise():
     with pytest.raises(NotImplementedError):
         gpr.predict(xe, return_cov=True)
     with pytest.raises(NotImplementedError):
-        gpr.predict(xe, conditioning_method='full')
+        gpr.predict(xe, conditioning_method='full-double-nn')
     with pytest.raises(NotImplementedError, match='Cannot accelerate'):
         B200Nngpr(kernel=skk.Matern(1.0, nu=2.0), optimizer=None).fit(x, y[:, 0])
 

@@ -1,0 +1,61 @@
+"""Predict with conditioning_method='full' through the C ABI and the estimator against the
+reference's own outputs (its sequential algorithm, base_nngpr.py:896-1030), FP64: 1e-10."""
+import numpy as np
+import pytest
+import torch
+
+from nngpr_b200 import B200Nngpr, _lib, ops
+from nngpr_b200 import kernel_params as KP
+
+from _common import FULL_CASES, KERNELS, format_std, load, load_full, normalized_y
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize('name', FULL_CASES)
+def test_predict_full_abi_matches_reference(name):
+    g, f = load(name), load_full(name)
+    y, ym, ys = normalized_y(g)
+    p = KP.extract(KERNELS[name]().clone_with_theta(g['theta_pred']))
+    dev = torch.device('cuda')
+    xt = torch.from_numpy(g['x']).to(dev)
+    yt = torch.from_numpy(np.ascontiguousarray(y.reshape(len(y), -1))).to(dev)
+    xq = torch.from_numpy(g['xq']).to(dev)
+    nbr = torch.from_numpy(np.ascontiguousarray(f['nbr'], dtype=np.int32)).to(dev)
+    flags = ops.new_flags(dev)
+    mean, var = ops.predict_full(xt, yt, xq, nbr, p, float(g['alpha']), True, flags=flags)
+    assert int(flags.item()) & ~_lib.NNGP_FLAG_NOT_PD == 0
+    mean = mean.cpu().numpy() * np.asarray(ys).reshape(1, -1) + np.asarray(ym).reshape(1, -1)
+    assert np.max(np.abs(mean - np.asarray(f['mean']).reshape(mean.shape))) < 1e-10
+    std = np.sqrt(var.cpu().numpy())
+    assert np.max(np.abs(format_std(std, ys, f['std'].shape) - f['std'])) < 1e-10
+    mean2, var2 = ops.predict_full(xt, yt, xq, nbr, p, float(g['alpha']), False)
+    assert var2 is None
+    np.testing.assert_array_equal(mean2.cpu().numpy() * np.asarray(ys).reshape(1, -1) + np.asarray(ym).reshape(1, -1),
+                                  mean)
+
+
+@pytest.mark.parametrize('name', FULL_CASES)
+def test_estimator_full_conditioning(name):
+    g, f = load(name), load_full(name)
+    gpr = B200Nngpr(kernel=KERNELS[name](), num_nn=int(g['num_nn']), alpha=float(g['alpha']),
+                    normalize_y=bool(g['normalize_y']), optimizer=None, allow_downcast_f32='no').fit(g['x'], g['y'])
+    gpr.kernel_ = gpr.kernel_.clone_with_theta(g['theta_pred'])
+    mean, std = gpr.predict(g['xq'], return_std=True, conditioning_method='full')
+    assert mean.shape == f['mean'].shape and std.shape == f['std'].shape
+    assert np.max(np.abs(mean - f['mean'])) < 1e-10
+    assert np.max(np.abs(std - f['std'])) < 1e-10
+    np.testing.assert_array_equal(gpr.predict(g['xq'], conditioning_method='full'), mean)
+
+
+def test_predict_full_flags_a_later_query_as_neighbour():
+    g, f = load('cpu_n2000_d3_m16'), load_full('cpu_n2000_d3_m16')
+    p = KP.extract(KERNELS['cpu_n2000_d3_m16']().clone_with_theta(g['theta_pred']))
+    dev = torch.device('cuda')
+    nbr = np.ascontiguousarray(f['nbr'], dtype=np.int32)
+    nt = g['x'].shape[0]
+    nbr[3, 0] = nt + 10  # query 3 cannot condition on query 10
+    flags = ops.new_flags(dev)
+    ops.predict_full(torch.from_numpy(g['x']).to(dev), torch.from_numpy(g['y'][:, None]).to(dev),
+                     torch.from_numpy(g['xq']).to(dev), torch.from_numpy(nbr).to(dev), p, 1e-10, True, flags=flags)
+    assert int(flags.item()) & _lib.NNGP_FLAG_BAD_INDEX

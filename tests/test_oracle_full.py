@@ -1,0 +1,33 @@
+"""The oracle's restatement of predict(conditioning_method='full') (the reference's sequential
+algorithm, base_nngpr.py:896-1030) against the reference's own outputs on three golden cases."""
+import numpy as np
+import pytest
+
+from nngpr_b200 import kernel_params as KP
+from oracle import nngp_oracle as O
+
+from _common import FULL_CASES, KERNELS, format_std, load, load_full, normalized_y, oracle_params
+
+
+@pytest.mark.parametrize('name', FULL_CASES)
+def test_oracle_full_predict_matches_reference(name):
+    g, f = load(name), load_full(name)
+    y, ym, ys = normalized_y(g)
+    p = oracle_params(KP.extract(KERNELS[name]().clone_with_theta(g['theta_pred'])))
+    mean, std = O.predict_full(g['x'], y, g['xq'], f['nbr'], p, float(g['alpha']), True)
+    mean = mean * np.asarray(ys).reshape(1, -1) + np.asarray(ym).reshape(1, -1)
+    want = np.asarray(f['mean']).reshape(mean.shape)
+    assert np.max(np.abs(mean - want)) < 1e-10
+    assert np.max(np.abs(format_std(std, ys, f['std'].shape) - f['std'])) < 1e-10
+    np.testing.assert_array_equal(np.asarray(f['mean_only']), np.asarray(f['mean']))
+
+
+@pytest.mark.parametrize('name', FULL_CASES)
+def test_full_neighbour_lists_are_the_prefix_search(name):
+    """The reference's lists for 'full' are the search of [x_train; x_query] where query i may
+    use the training set and the queries before it (ref_cut_index = n_train)."""
+    g, f = load(name), load_full(name)
+    x_full = np.concatenate([g['x'], g['xq']])
+    ls = KP.extract(KERNELS[name]().clone_with_theta(g['theta_pred'])).length_scale
+    got = O.knn(x_full, g['xq'], f['nbr'].shape[1], g['x'].shape[0], ls, np.float64)
+    assert np.array_equal(got, f['nbr'])
