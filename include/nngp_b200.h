@@ -279,6 +279,18 @@ nngp_status nngp_predict_full_f64(const double *x_full, const double *y_train, i
                                   double *mean, double *var, int32_t *status_flags, void *workspace,
                                   size_t workspace_bytes, void *stream);
 
+/* Samples with conditioning_method='full' (Nngpr.sample_y's sequential algorithm,
+ * base_nngpr.py:691-750): query i's samples condition on the training y and on the samples
+ * already drawn for the queries before it, sample = w . v + max(0, sqrt(s2)) z.  Same inputs and
+ * workspace as nngp_predict_full_f64; z: (n_query, ydim, n_samples) standard normals (device), in
+ * the order the reference draws them (query by query, then (ydim, n_samples) in C order), so the
+ * reference's own samples come back for its random stream; samples: same shape. */
+nngp_status nngp_sample_full_f64(const double *x_full, const double *y_train, int64_t n_train,
+                                 int64_t n_query, int32_t d, int32_t ydim, const int32_t *nbr,
+                                 int32_t num_nn, const nngp_kernel *kernel, int32_t n_samples,
+                                 const double *z, double *samples, int32_t *status_flags,
+                                 void *workspace, size_t workspace_bytes, void *stream);
+
 /* Self-test of the tensor-core operand layout used by the search (no counterpart in the
  * reference): d (128 x 128) = a (128 x kp) * b (128 x kp)^T in TF32 with FP32 accumulation,
  * a and b row-major device arrays, kp = 8, 16 or 32, through the same shared-memory layout,

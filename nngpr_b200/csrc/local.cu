@@ -889,18 +889,55 @@ __global__ void __launch_bounds__(32) full_recursion_kernel(const int32_t *__res
     }
 }
 
+// Samples conditioned on the training set and on the samples of the earlier queries (sample_y
+// with conditioning_method='full', base_nngpr.py:691-750): sample_i = sum_s w_is v_s +
+// max(0, sqrt(s2_i)) z_i, v the training y or the earlier query's sample of the same column.
+// One warp walks the queries in order; lanes share the ydim * n_samples columns.
+__global__ void __launch_bounds__(32) sample_recursion_kernel(const int32_t *__restrict__ nbr,
+                                                              const double *__restrict__ w,
+                                                              const double *__restrict__ s2,
+                                                              const double *__restrict__ y, int64_t nt, int64_t nq,
+                                                              int m, int ydim, int ns, const double *__restrict__ z,
+                                                              double *out, int32_t *__restrict__ flags) {
+    const int lane = threadIdx.x;
+    const int cols = ydim * ns;
+    for (int64_t i = 0; i < nq; ++i) {
+        const double sig = s2[i] > 0.0 ? sqrt(s2[i]) : 0.0;
+        for (int col = lane; col < cols; col += 32) {
+            const int c = col / ns;
+            double v = 0.0;
+            for (int sl = 0; sl < m; ++sl) {
+                const int32_t j = nbr[i * m + sl];
+                if (j < 0) continue;
+                if ((int64_t)j >= nt + i) {  // not an earlier point: treated as missing
+                    flag_or(flags, NNGP_FLAG_BAD_INDEX);
+                    continue;
+                }
+                const double val = (int64_t)j < nt ? y[(int64_t)j * ydim + c] : out[((int64_t)j - nt) * cols + col];
+                v = fma(w[i * m + sl], val, v);
+            }
+            out[i * cols + col] = v + sig * z[i * cols + col];
+        }
+        __syncwarp();  // this query's samples are visible to the next ones
+    }
+}
+
 size_t predict_full_workspace(int64_t nq, int m) { return (size_t)(2 * nq * (int64_t)m + nq) * sizeof(double) + 256; }
 
+// samples == false: predict (mean, and var when want_var); samples == true: want_var holds
+// n_samples, z the standard normals and mean receives the samples.
 nngp_status predict_full_f64(const double *x_full, const double *y_train, int64_t nt, int64_t nq, int d, int ydim,
                              const int32_t *nbr, int m, const nngp_kernel *k, int want_var, double *mean, double *var,
-                             int32_t *flags, void *ws, size_t ws_bytes, cudaStream_t stream) {
+                             int32_t *flags, void *ws, size_t ws_bytes, cudaStream_t stream, bool samples = false,
+                             const double *z = nullptr) {
     if (nt < 0 || nq < 0) return fail(NNGP_ERR_INVALID_ARGUMENT, "predict_full: negative size");
-    if (m > kWarpM) return fail(NNGP_ERR_UNSUPPORTED, "predict_full: num_nn must be <= 32");
+    if (m < 1 || m > kWarpM) return fail(NNGP_ERR_UNSUPPORTED, "predict_full: num_nn must be in [1, 32]");
     LocalArgs a;
     nngp_status st = fill_args(a, k, d, ydim, m, nt + nq, nq, 0.0, false);
     if (st != NNGP_OK) return st;
     if (nq == 0) return NNGP_OK;
-    if (!x_full || !mean || (want_var && !var) || (m > 0 && !nbr) || (nt > 0 && !y_train))
+    if (samples && (want_var < 1 || !z)) return fail(NNGP_ERR_INVALID_ARGUMENT, "sample_full: n_samples >= 1 and z");
+    if (!x_full || !mean || (want_var && !samples && !var) || !nbr || (nt > 0 && !y_train))
         return fail(NNGP_ERR_INVALID_ARGUMENT, "predict_full: null pointer");
     if (!ws || ws_bytes < predict_full_workspace(nq, m))
         return fail(NNGP_ERR_WORKSPACE, "predict_full: workspace missing or too small");
@@ -909,14 +946,17 @@ nngp_status predict_full_f64(const double *x_full, const double *y_train, int64_
     double *pc = s2 + nq;
     a.alpha_below = nt;  // alpha on training neighbours only (base_nngpr.py:952-954)
     a.weights_out = 1;
-    if (m > 0) {
-        const LocalPlan pl = plan_local(nq, d, m, 0, false);
-        st = launch_local<double, false, true>(pl, a, x_full, y_train, x_full + nt * d, nullptr, nbr, nullptr, wts, s2,
-                                               flags, stream);
-        if (st != NNGP_OK) return st;
+    const LocalPlan pl = plan_local(nq, d, m, 0, false);
+    st = launch_local<double, false, true>(pl, a, x_full, y_train, x_full + nt * d, nullptr, nbr, nullptr, wts, s2,
+                                           flags, stream);
+    if (st != NNGP_OK) return st;
+    if (samples) {
+        sample_recursion_kernel<<<1, 32, 0, stream>>>(nbr, wts, s2, y_train, nt, nq, m, ydim, want_var, z, mean,
+                                                      flags);
+    } else {
+        full_recursion_kernel<<<1, 32, 0, stream>>>(nbr, wts, s2, y_train, nt, nq, m, ydim, want_var, mean, var, pc,
+                                                    flags);
     }
-    full_recursion_kernel<<<1, 32, 0, stream>>>(nbr, wts, s2, y_train, nt, nq, m, ydim, want_var, mean, var, pc,
-                                                flags);
     NNGP_CUDA_TRY(cudaGetLastError());
     return NNGP_OK;
 }
@@ -930,6 +970,13 @@ nngp_status predict_full(const double *x_full, const double *y_train, int64_t nt
                          int32_t *flags, void *ws, size_t ws_bytes, cudaStream_t stream) {
     return predict_full_f64(x_full, y_train, nt, nq, d, ydim, nbr, m, k, want_var, mean, var, flags, ws, ws_bytes,
                             stream);
+}
+
+nngp_status sample_full(const double *x_full, const double *y_train, int64_t nt, int64_t nq, int d, int ydim,
+                        const int32_t *nbr, int m, const nngp_kernel *k, int n_samples, const double *z, double *out,
+                        int32_t *flags, void *ws, size_t ws_bytes, cudaStream_t stream) {
+    return predict_full_f64(x_full, y_train, nt, nq, d, ydim, nbr, m, k, n_samples, out, nullptr, flags, ws, ws_bytes,
+                            stream, true, z);
 }
 
 // ---------------------------------------------------------------------------------------

@@ -414,8 +414,10 @@ class B200Nngpr(GaussianProcessRegressor):
         conditioning_method = 'only-train' if conditioning_method is None else conditioning_method
         if conditioning_method not in {'only-train', 'full', 'full-double-nn'}:
             raise ValueError(f"unknown conditioning_method {conditioning_method!r}")
-        if conditioning_method != 'only-train':
-            raise NotImplementedError("B200Nngpr implements sample_y(conditioning_method='only-train')")
+        if conditioning_method == 'full-double-nn':
+            raise NotImplementedError("B200Nngpr implements sample_y(conditioning_method='only-train' or 'full')")
+        if conditioning_method == 'full':
+            return self._sample_full(X, n_samples, random_state)
         mean, std = self.predict(X, return_std=True)
         mu = np.asarray(mean, dtype=np.float64)
         sd = np.asarray(std, dtype=np.float64)
@@ -431,6 +433,41 @@ class B200Nngpr(GaussianProcessRegressor):
         out = torch.from_numpy(mu).to(dev)[..., None] + torch.from_numpy(sd).to(dev)[..., None] * z
         out = out.cpu().numpy()
         return out[:, 0, :] if single else out
+
+    def _sample_full(self, X, n_samples, random_state):
+        """``sample_y(conditioning_method='full')`` (``base_nngpr.py:691-750``): each query's samples
+        condition on the training y and on the samples of the queries before it.  The standard
+        normals are drawn on the host exactly as the reference draws them (scikit-learn's
+        ``check_random_state``, query by query, ``(n_targets, n_samples)`` each), so an int
+        ``random_state`` reproduces the reference's samples; the recursion runs on the device."""
+        if not hasattr(self, 'X_train_'):
+            raise NotImplementedError("sample_y(conditioning_method='full') needs a fitted model")
+        if self.kernel is None or self.kernel.requires_vector_input:
+            dtype, ensure_2d = "numeric", True
+        else:
+            dtype, ensure_2d = None, False
+        X = validate_data(self, X, ensure_2d=ensure_2d, dtype=dtype, reset=False)
+        p = self._params(self.kernel_)
+        dev = self._device
+        search_dtype, _ = self._dtypes()
+        xt, yt = self._train_tensors(torch.float64)
+        xq = torch.from_numpy(np.ascontiguousarray(X, dtype=np.float64)).to(dev)
+        nt, nq = xt.shape[0], xq.shape[0]
+        m = min(self._num_nn, nt + nq)
+        if m > 32:
+            raise NotImplementedError("sample_y(conditioning_method='full') supports num_nn <= 32")
+        ydim = yt.shape[1]
+        z = check_random_state(random_state).standard_normal((nq, ydim, int(n_samples)))
+        flags = ops.new_flags(dev)
+        x_full_s = torch.cat([xt, xq]).to(search_dtype)
+        nbr = ops.knn(x_full_s, x_full_s[nt:], m, ref_cut_index=nt, length_scale=self._search_ls(p), flags=flags)
+        out = ops.sample_full(xt, yt, xq, nbr, p, float(self.alpha), torch.from_numpy(z).to(dev), flags=flags)
+        out = out.cpu().numpy()
+        ops.raise_on_flags(int(flags.item()) & ~_lib.NNGP_FLAG_NOT_PD, 'sample_y')
+        y_std = np.asarray(self._y_train_std, dtype=np.float64).reshape(1, -1, 1)
+        y_mean = np.asarray(self._y_train_mean, dtype=np.float64).reshape(1, -1, 1)
+        out = out * y_std + y_mean
+        return out[:, 0, :] if ydim == 1 else out
 
     # ---- persistence ------------------------------------------------------------------------
     def __getstate__(self):

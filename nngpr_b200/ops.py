@@ -84,6 +84,37 @@ def predict_full(x_train: torch.Tensor, y_train: torch.Tensor, x_query: torch.Te
     return mean, var
 
 
+def sample_full(x_train: torch.Tensor, y_train: torch.Tensor, x_query: torch.Tensor, nbr: torch.Tensor,
+                p: RbfParams, alpha: float, z: torch.Tensor, flags: torch.Tensor | None = None) -> torch.Tensor:
+    """Samples with ``conditioning_method='full'`` (FP64) from the standard normals ``z``
+    ``(nq, ydim, n_samples)``: query ``i`` conditions on the training y and on the samples of the
+    queries before it.  ``nbr`` as for :func:`predict_full`."""
+    for t, nm in ((x_train, 'x_train'), (y_train, 'y_train'), (x_query, 'x_query'), (z, 'z')):
+        _check_tensor(t, nm, (torch.float64,))
+    _check_tensor(nbr, 'nbr', (torch.int32,))
+    nt, d = x_train.shape
+    nq = x_query.shape[0]
+    y2 = y_train if y_train.dim() == 2 else y_train.reshape(nt, 1)
+    ydim = y2.shape[1]
+    if z.dim() != 3 or z.shape[0] != nq or z.shape[1] != ydim:
+        raise ValueError('z must be (n_query, ydim, n_samples)')
+    ns = z.shape[2]
+    m = nbr.shape[1] if nbr.dim() == 2 else 0
+    x_full = torch.cat([x_train, x_query]).contiguous()
+    out = torch.empty_like(z)
+    if nq == 0 or ns == 0:
+        return out
+    keep = []
+    k = _kernel_struct(p, alpha, d, keep)
+    L = _lib.lib()
+    ws_bytes = int(L.nngp_predict_full_workspace_size(nq, m))
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device=x_query.device)
+    st = L.nngp_sample_full_f64(_ptr(x_full), _ptr(y2), nt, nq, d, ydim, _ptr(nbr), m, ctypes.byref(k), ns,
+                                _ptr(z.contiguous()), _ptr(out), _ptr(flags), _ptr(ws), ws_bytes, _stream())
+    _lib.check(st, 'nngp_sample_full_f64')
+    return out
+
+
 def knn_reuse_prepare(x: torch.Tensor, cand: torch.Tensor, length_scale, max_norm: float) -> torch.Tensor:
     """Per-point thresholds (float64 ``(n,)``) that let :func:`knn_reuse_rank` prove a reused
     list exact: ``cand`` is the FP32 prefix search of ``x`` (float32 ``(n, d)``) at the scalar

@@ -468,3 +468,35 @@ def predict_full(x_train, y_train, x_query, nbr, p: KernelParams, alpha: float, 
         for s in np.nonzero(q)[0]:
             pcov[(i, js[s] - nt)] = cw[s]
     return mean[nt:], (np.sqrt(var) if return_std else None)
+
+
+def sample_full(x_train, y_train, x_query, nbr, p: KernelParams, alpha: float, z: np.ndarray) -> np.ndarray:
+    """Samples with ``conditioning_method='full'``: restates ``Nngpr.sample_y``'s sequential
+    algorithm (``base_nngpr.py:691-750``) with the standard normals ``z (nq, ydim, n_samples)``
+    given: query ``i``'s samples are ``w . v + max(0, sqrt(K_00 - k^T w)) z_i`` where ``v`` holds
+    the training y and the samples of earlier query neighbours (normalised y units)."""
+    x_train = np.asarray(x_train, dtype=np.float64)
+    x_query = np.asarray(x_query, dtype=np.float64)
+    y_train = np.asarray(y_train, dtype=np.float64)
+    if y_train.ndim == 1:
+        y_train = y_train[:, None]
+    nt, nq = x_train.shape[0], x_query.shape[0]
+    x_full = np.concatenate([x_train, x_query])
+    nbr = np.asarray(nbr)
+    idx = np.concatenate([np.arange(nt, nt + nq)[:, None], nbr], axis=1)
+    K, _ = fill_nn_kernel(x_full, idx, p, False)
+    train = (idx >= 0) & (idx < nt)
+    ii = np.arange(idx.shape[1])
+    K[:, ii, ii] += np.where(train, alpha, 0.0)
+    out = np.full(z.shape, np.nan)
+    for i in range(nq):
+        w = np.linalg.solve(K[i, 1:, 1:], K[i, 0, 1:])
+        v = np.zeros((nbr.shape[1],) + z.shape[1:])
+        for s, j in enumerate(nbr[i]):
+            if j < 0:
+                continue
+            v[s] = y_train[j][:, None] if j < nt else out[j - nt]
+        s2 = K[i, 0, 0] - K[i, 0, 1:] @ w
+        sig = np.sqrt(s2) if s2 > 0 else 0.0
+        out[i] = np.einsum('i,ijk->jk', w, v) + sig * z[i]
+    return out

@@ -141,8 +141,9 @@ def main():
 
 def full_cases(NumpyNngpr, NumpyWorker, bk):
     """predict(conditioning_method='full') of the reference (the sequential algorithm,
-    base_nngpr.py:896-1030) on three of the cases above, written to full_<case>.npz with the
-    neighbour lists it used (indices into [x_train; x_query])."""
+    base_nngpr.py:896-1030) on three of the cases above, and sample_y(conditioning_method='full',
+    n_samples=4, random_state=11) on the first 60 query points (:691-750), written to
+    full_<case>.npz with the neighbour lists they used (indices into [x_train; x_query])."""
     specs = {
         'cpu_n2000_d3_m16': lambda: bk.ConstantKernel(1.0) * bk.RBF(0.3) + bk.WhiteKernel(0.01),
         'ard_n400_d5_m12_y2': lambda: bk.ConstantKernel(0.7) * bk.RBF(np.array([0.3, 0.5, 0.8, 1.2, 2.0]))
@@ -162,8 +163,12 @@ def full_cases(NumpyNngpr, NumpyWorker, bk):
         worker = NumpyWorker()
         nn, _ = gpr._find_nn_indices_for_train_and_eval(worker, gpr.kernel_, gpr.X_train_, xq, condition_on_eval=True,
                                                          double_nn=False)
+        samples = gpr.sample_y(xq[:60], n_samples=4, random_state=11, conditioning_method='full')
+        nn60, _ = gpr._find_nn_indices_for_train_and_eval(worker, gpr.kernel_, gpr.X_train_, xq[:60],
+                                                           condition_on_eval=True, double_nn=False)
         np.savez_compressed(os.path.join(HERE, 'full_' + name + '.npz'), mean=np.asarray(mean), std=np.asarray(std),
-                            mean_only=np.asarray(mean_only), nbr=np.asarray(nn)[:, 1:])
+                            mean_only=np.asarray(mean_only), nbr=np.asarray(nn)[:, 1:],
+                            samples60=np.asarray(samples), nbr60=np.asarray(nn60)[:, 1:])
         print('full', name, np.asarray(mean).ravel()[:3], np.asarray(std).ravel()[:3])
 
 

@@ -114,7 +114,7 @@ def test_sample_y_only_train_shapes_seed_and_moments():
     gpr1 = make('cpu_n2000_d3_m16', g1).fit(g1['x'], g1['y'])
     assert gpr1.sample_y(g1['xq'][:7], n_samples=3).shape == (7, 3)
     with pytest.raises(NotImplementedError):
-        gpr1.sample_y(g1['xq'][:7], conditioning_method='full')
+        gpr1.sample_y(g1['xq'][:7], conditioning_method='full-double-nn')
 
 
 def test_pickle_round_trip():

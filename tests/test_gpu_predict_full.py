@@ -59,3 +59,15 @@ def test_predict_full_flags_a_later_query_as_neighbour():
     ops.predict_full(torch.from_numpy(g['x']).to(dev), torch.from_numpy(g['y'][:, None]).to(dev),
                      torch.from_numpy(g['xq']).to(dev), torch.from_numpy(nbr).to(dev), p, 1e-10, True, flags=flags)
     assert int(flags.item()) & _lib.NNGP_FLAG_BAD_INDEX
+
+
+@pytest.mark.parametrize('name', FULL_CASES)
+def test_sample_y_full_reproduces_the_reference(name):
+    """sample_y(conditioning_method='full', random_state=11) returns the reference's own samples
+    (same normals, drawn as the reference draws them; recursion on the device)."""
+    g, f = load(name), load_full(name)
+    gpr = B200Nngpr(kernel=KERNELS[name](), num_nn=int(g['num_nn']), alpha=float(g['alpha']),
+                    normalize_y=bool(g['normalize_y']), optimizer=None, allow_downcast_f32='no').fit(g['x'], g['y'])
+    s = gpr.sample_y(g['xq'][:60], n_samples=4, random_state=11, conditioning_method='full')
+    assert s.shape == f['samples60'].shape
+    assert np.max(np.abs(s - f['samples60'])) < 1e-9

@@ -31,3 +31,19 @@ def test_full_neighbour_lists_are_the_prefix_search(name):
     ls = KP.extract(KERNELS[name]().clone_with_theta(g['theta_pred'])).length_scale
     got = O.knn(x_full, g['xq'], f['nbr'].shape[1], g['x'].shape[0], ls, np.float64)
     assert np.array_equal(got, f['nbr'])
+
+
+@pytest.mark.parametrize('name', FULL_CASES)
+def test_oracle_full_samples_reproduce_the_reference_stream(name):
+    """sample_y(conditioning_method='full', random_state=11): the reference draws its normals
+    query by query from sklearn's check_random_state(11), a numpy RandomState; with the same
+    normals the restatement gives the reference's samples."""
+    g, f = load(name), load_full(name)
+    y, ym, ys = normalized_y(g)
+    y2 = y if y.ndim == 2 else y[:, None]
+    p = oracle_params(KP.extract(KERNELS[name]().clone_with_theta(g['theta_pred'])))
+    z = np.random.RandomState(11).standard_normal((60, y2.shape[1], 4))
+    out = O.sample_full(g['x'], y2, g['xq'][:60], f['nbr60'], p, float(g['alpha']), z)
+    out = out * np.asarray(ys).reshape(1, -1, 1) + np.asarray(ym).reshape(1, -1, 1)
+    want = np.asarray(f['samples60']).reshape(out.shape)
+    assert np.max(np.abs(out - want)) < 1e-9
