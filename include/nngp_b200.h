@@ -279,6 +279,17 @@ nngp_status nngp_predict_full_f64(const double *x_full, const double *y_train, i
                                   double *mean, double *var, int32_t *status_flags, void *workspace,
                                   size_t workspace_bytes, void *stream);
 
+/* Predict with conditioning_method='full' and the dense predictive covariance (Nngpr.predict
+ * with return_cov, base_nngpr.py:989-1000): as nngp_predict_full_f64, but the covariance of every
+ * pair of queries is kept, so each query's variance uses the full covariance of its query
+ * neighbours.  cov: (n_query, n_query), symmetric, variances on the diagonal (normalised y
+ * units).  One CTA walks the queries in order: O(n_query^2 num_nn) work, n_query^2 doubles. */
+nngp_status nngp_predict_cov_full_f64(const double *x_full, const double *y_train, int64_t n_train,
+                                      int64_t n_query, int32_t d, int32_t ydim, const int32_t *nbr,
+                                      int32_t num_nn, const nngp_kernel *kernel, double *mean, double *cov,
+                                      int32_t *status_flags, void *workspace, size_t workspace_bytes,
+                                      void *stream);
+
 /* Samples with conditioning_method='full' (Nngpr.sample_y's sequential algorithm,
  * base_nngpr.py:691-750): query i's samples condition on the training y and on the samples
  * already drawn for the queries before it, sample = w . v + max(0, sqrt(s2)) z.  Same inputs and

@@ -28,6 +28,7 @@ EXPORTED = (
     'nngp_predict_f32', 'nngp_predict_f64', 'nngp_fma_probe', 'nngp_tc_layout_selftest',
     'nngp_plain_knn_f32', 'nngp_knn_reuse_prepare_f32', 'nngp_knn_reuse_rank_f32',
     'nngp_predict_full_workspace_size', 'nngp_predict_full_f64', 'nngp_sample_full_f64',
+    'nngp_predict_cov_full_f64',
 )
 
 
@@ -85,6 +86,8 @@ _SIGS = {
     'nngp_predict_full_workspace_size': ([_i64, _i32], ctypes.c_size_t),
     'nngp_predict_full_f64': ([_vp, _vp, _i64, _i64, _i32, _i32, _vp, _i32, ctypes.POINTER(NngpKernel), _i32, _vp,
                                _vp, _vp, _vp, ctypes.c_size_t, _vp], ctypes.c_int),
+    'nngp_predict_cov_full_f64': ([_vp, _vp, _i64, _i64, _i32, _i32, _vp, _i32, ctypes.POINTER(NngpKernel), _vp,
+                                   _vp, _vp, _vp, ctypes.c_size_t, _vp], ctypes.c_int),
     'nngp_sample_full_f64': ([_vp, _vp, _i64, _i64, _i32, _i32, _vp, _i32, ctypes.POINTER(NngpKernel), _i32, _vp,
                               _vp, _vp, _vp, ctypes.c_size_t, _vp], ctypes.c_int),
     'nngp_knn_reuse_prepare_f32': ([_vp, _i64, _i32, ctypes.c_double, _vp, _i32, ctypes.c_double, _vp, _vp],

@@ -36,6 +36,8 @@ nngp_status plain_knn_f32(const float *, int64_t, const float *, int64_t, int, i
 size_t predict_full_workspace_size(int64_t, int);
 nngp_status predict_full(const double *, const double *, int64_t, int64_t, int, int, const int32_t *, int,
                          const nngp_kernel *, int, double *, double *, int32_t *, void *, size_t, cudaStream_t);
+nngp_status predict_cov_full(const double *, const double *, int64_t, int64_t, int, int, const int32_t *, int,
+                             const nngp_kernel *, double *, double *, int32_t *, void *, size_t, cudaStream_t);
 nngp_status sample_full(const double *, const double *, int64_t, int64_t, int, int, const int32_t *, int,
                         const nngp_kernel *, int, const double *, double *, int32_t *, void *, size_t, cudaStream_t);
 nngp_status reuse_prepare_f32(const float *, int64_t, int, double, const int32_t *, int, double, double *,
@@ -187,6 +189,16 @@ nngp_status nngp_predict_full_f64(const double *x_full, const double *y_train, i
     return guarded([&] {
         return predict_full(x_full, y_train, n_train, n_query, d, ydim, nbr, num_nn, kernel, want_var, mean, var,
                             status_flags, workspace, workspace_bytes, as_stream(stream));
+    });
+}
+
+nngp_status nngp_predict_cov_full_f64(const double *x_full, const double *y_train, int64_t n_train, int64_t n_query,
+                                      int32_t d, int32_t ydim, const int32_t *nbr, int32_t num_nn,
+                                      const nngp_kernel *kernel, double *mean, double *cov, int32_t *status_flags,
+                                      void *workspace, size_t workspace_bytes, void *stream) {
+    return guarded([&] {
+        return predict_cov_full(x_full, y_train, n_train, n_query, d, ydim, nbr, num_nn, kernel, mean, cov,
+                                status_flags, workspace, workspace_bytes, as_stream(stream));
     });
 }
 

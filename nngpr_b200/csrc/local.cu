@@ -922,14 +922,84 @@ __global__ void __launch_bounds__(32) sample_recursion_kernel(const int32_t *__r
     }
 }
 
+// Predict with the dense predictive covariance (return_cov with 'full' conditioning,
+// base_nngpr.py:989-1000): like full_recursion_kernel, but the covariance of every pair of
+// queries is kept (cov, nq x nq, symmetric), so the query neighbours' covariance C is dense:
+// cov[i, j] = sum_s w_is cov[a_s, j] over the query neighbours a_s of i, for every j < i, and
+// cov[i, i] = max(0, max(0, s2_i) + w^T C w).  One CTA walks the queries in order; its threads
+// share the row.
+constexpr int kCovThreads = 256;
+__global__ void __launch_bounds__(kCovThreads) cov_recursion_kernel(const int32_t *__restrict__ nbr,
+                                                                    const double *__restrict__ w,
+                                                                    const double *__restrict__ s2,
+                                                                    const double *__restrict__ y, int64_t nt,
+                                                                    int64_t nq, int m, int ydim, double *mean,
+                                                                    double *cov, int32_t *__restrict__ flags) {
+    __shared__ int64_t sa[32];   // query position of each slot's neighbour, or -1
+    __shared__ int32_t sj[32];   // neighbour index (-1: missing)
+    __shared__ double sw[32];
+    __shared__ double svar;
+    const unsigned FULL = 0xffffffffu;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int64_t i = 0; i < nq; ++i) {
+        if (tid < 32) {
+            int32_t j = tid < m ? nbr[i * m + tid] : -1;
+            if (j >= 0 && (int64_t)j >= nt + i) {
+                flag_or(flags, NNGP_FLAG_BAD_INDEX);
+                j = -1;
+            }
+            sj[tid] = j;
+            sw[tid] = (tid < m && j >= 0) ? w[i * m + tid] : 0.0;
+            sa[tid] = (j >= 0 && (int64_t)j >= nt) ? (int64_t)j - nt : -1;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            const int32_t j = sj[lane];
+            const double ws = sw[lane];
+            const int64_t a = sa[lane];
+            for (int c = 0; c < ydim; ++c) {
+                double v = 0.0;
+                if (j >= 0) v = a >= 0 ? mean[a * ydim + c] : y[(int64_t)j * ydim + c];
+                const double mu = warp_sum(ws * v);
+                if (lane == 0) mean[i * ydim + c] = mu;
+            }
+            double cw = 0.0;  // (C w)_s for a query-neighbour slot s
+            if (a >= 0)
+                for (int t = 0; t < m; ++t) {
+                    const int64_t b = sa[t];
+                    if (b >= 0) cw += cov[a * nq + b] * sw[t];
+                }
+            const double quad = warp_sum(ws * cw);
+            if (lane == 0) {
+                const double raw = s2[i] > 0.0 ? s2[i] : 0.0;
+                const double vi = raw + quad;
+                svar = vi > 0.0 ? vi : 0.0;
+            }
+        }
+        for (int64_t jj = tid; jj < i; jj += blockDim.x) {
+            double r = 0.0;
+            for (int t = 0; t < m; ++t) {
+                const int64_t b = sa[t];
+                if (b >= 0) r += sw[t] * cov[b * nq + jj];
+            }
+            cov[i * nq + jj] = r;
+            cov[jj * nq + i] = r;
+        }
+        __syncthreads();
+        if (tid == 0) cov[i * nq + i] = svar;
+        __syncthreads();  // row i (and the diagonal) are complete before query i + 1 reads them
+    }
+}
+
 size_t predict_full_workspace(int64_t nq, int m) { return (size_t)(2 * nq * (int64_t)m + nq) * sizeof(double) + 256; }
 
-// samples == false: predict (mean, and var when want_var); samples == true: want_var holds
-// n_samples, z the standard normals and mean receives the samples.
+// samples == false: predict (mean, and var when want_var; with dense_cov, var receives the
+// nq x nq covariance); samples == true: want_var holds n_samples, z the standard normals and
+// mean receives the samples.
 nngp_status predict_full_f64(const double *x_full, const double *y_train, int64_t nt, int64_t nq, int d, int ydim,
                              const int32_t *nbr, int m, const nngp_kernel *k, int want_var, double *mean, double *var,
                              int32_t *flags, void *ws, size_t ws_bytes, cudaStream_t stream, bool samples = false,
-                             const double *z = nullptr) {
+                             const double *z = nullptr, bool dense_cov = false) {
     if (nt < 0 || nq < 0) return fail(NNGP_ERR_INVALID_ARGUMENT, "predict_full: negative size");
     if (m < 1 || m > kWarpM) return fail(NNGP_ERR_UNSUPPORTED, "predict_full: num_nn must be in [1, 32]");
     LocalArgs a;
@@ -953,6 +1023,8 @@ nngp_status predict_full_f64(const double *x_full, const double *y_train, int64_
     if (samples) {
         sample_recursion_kernel<<<1, 32, 0, stream>>>(nbr, wts, s2, y_train, nt, nq, m, ydim, want_var, z, mean,
                                                       flags);
+    } else if (dense_cov) {
+        cov_recursion_kernel<<<1, kCovThreads, 0, stream>>>(nbr, wts, s2, y_train, nt, nq, m, ydim, mean, var, flags);
     } else {
         full_recursion_kernel<<<1, 32, 0, stream>>>(nbr, wts, s2, y_train, nt, nq, m, ydim, want_var, mean, var, pc,
                                                     flags);
@@ -970,6 +1042,13 @@ nngp_status predict_full(const double *x_full, const double *y_train, int64_t nt
                          int32_t *flags, void *ws, size_t ws_bytes, cudaStream_t stream) {
     return predict_full_f64(x_full, y_train, nt, nq, d, ydim, nbr, m, k, want_var, mean, var, flags, ws, ws_bytes,
                             stream);
+}
+
+nngp_status predict_cov_full(const double *x_full, const double *y_train, int64_t nt, int64_t nq, int d, int ydim,
+                             const int32_t *nbr, int m, const nngp_kernel *k, double *mean, double *cov, int32_t *flags,
+                             void *ws, size_t ws_bytes, cudaStream_t stream) {
+    return predict_full_f64(x_full, y_train, nt, nq, d, ydim, nbr, m, k, 1, mean, cov, flags, ws, ws_bytes, stream,
+                            false, nullptr, true);
 }
 
 nngp_status sample_full(const double *x_full, const double *y_train, int64_t nt, int64_t nq, int d, int ydim,

@@ -15,9 +15,10 @@ Precision follows the reference's ``allow_downcast_f32`` (``base_nngpr.py:66-72`
 ``'only-nn'`` (default) searches neighbours in FP32 and solves the local systems in FP64;
 ``'yes'`` solves them in FP32 (FP64 re-solve below ``pivot_tol``); ``'no'`` is FP64 throughout.
 
-Not provided (out of scope of this backend): ``predict(return_cov=True)``, the
-``'full'``/``'full-double-nn'`` conditioning methods and ``sample_y``; they raise
-``NotImplementedError``.  Kernels outside the accelerated family raise
+``predict`` and ``sample_y`` support ``conditioning_method='only-train'`` and ``'full'`` (the
+reference's sequential algorithms, on the device), ``return_std`` and ``return_cov``.  Not
+provided: ``'full-double-nn'`` (raises ``NotImplementedError``).  Kernels outside the accelerated
+family raise
 ``NotImplementedError("Cannot accelerate this kernel ...")`` as the reference's CUDA path does.
 """
 
@@ -326,9 +327,10 @@ class B200Nngpr(GaussianProcessRegressor):
         conditioning_method = 'only-train' if conditioning_method is None else conditioning_method
         if conditioning_method not in {'only-train', 'full', 'full-double-nn'}:
             raise ValueError(f"unknown conditioning_method {conditioning_method!r}")
-        if return_cov or conditioning_method == 'full-double-nn':
-            raise NotImplementedError("B200Nngpr implements predict(conditioning_method='only-train' or 'full') "
-                                      "without return_cov")
+        if conditioning_method == 'full-double-nn':
+            raise NotImplementedError("B200Nngpr implements predict(conditioning_method='only-train' or 'full')")
+        if return_std:
+            return_cov = False  # the reference returns the standard deviation when both are asked for
         if self.kernel is None or self.kernel.requires_vector_input:
             dtype, ensure_2d = "numeric", True
         else:
@@ -339,6 +341,11 @@ class B200Nngpr(GaussianProcessRegressor):
             kernel = self.kernel if self.kernel is not None else self.get_default_kernel()
             p = self._params(kernel)
             mean = np.zeros(X.shape[0])
+            if return_cov:
+                if conditioning_method != 'only-train':
+                    raise NotImplementedError("predict(return_cov=True, conditioning_method='full') needs a "
+                                              "fitted model")
+                return mean, np.diag(np.full(X.shape[0], p.rbf_level + p.const_value + p.noise_level))
             if return_std:
                 return mean, np.full(X.shape[0], np.sqrt(p.rbf_level + p.const_value + p.noise_level))
             return mean
@@ -347,7 +354,7 @@ class B200Nngpr(GaussianProcessRegressor):
         dev = self._device
         search_dtype, local_dtype = self._dtypes()
         if conditioning_method == 'full':
-            return self._predict_full(X, p, search_dtype, return_std)
+            return self._predict_full(X, p, search_dtype, return_std, return_cov)
         xt, yt = self._train_tensors(local_dtype)
         xs_train = xt if search_dtype == local_dtype else self._train_tensors(search_dtype)[0]
         xq_host = np.ascontiguousarray(X, dtype=np.float64)
@@ -368,6 +375,8 @@ class B200Nngpr(GaussianProcessRegressor):
         mean = y_std * mean + y_mean
         if mean.shape[1] == 1:
             mean = mean[:, 0]
+        if return_cov:  # queries conditioned on the training set only are independent
+            return mean, self._format_cov(np.diag(np.maximum(var, 0.0)))
         if not return_std:
             return mean
         std = np.sqrt(var).reshape(-1, 1) * y_std
@@ -375,7 +384,7 @@ class B200Nngpr(GaussianProcessRegressor):
             std = std[:, 0]
         return mean, std
 
-    def _predict_full(self, X, p, search_dtype, return_std):
+    def _predict_full(self, X, p, search_dtype, return_std, return_cov=False):
         """``conditioning_method='full'`` (``base_nngpr.py:896-1030``): every query conditions on
         the training set and on the queries before it; FP64 local systems."""
         dev = self._device
@@ -388,7 +397,10 @@ class B200Nngpr(GaussianProcessRegressor):
         flags = ops.new_flags(dev)
         x_full_s = torch.cat([xt, xq]).to(search_dtype)
         nbr = ops.knn(x_full_s, x_full_s[nt:], m, ref_cut_index=nt, length_scale=self._search_ls(p), flags=flags)
-        mean, var = ops.predict_full(xt, yt, xq, nbr, p, float(self.alpha), return_std, flags=flags)
+        if return_cov:
+            mean, cov = ops.predict_cov_full(xt, yt, xq, nbr, p, float(self.alpha), flags=flags)
+        else:
+            mean, var = ops.predict_full(xt, yt, xq, nbr, p, float(self.alpha), return_std, flags=flags)
         mean = mean.cpu().numpy()
         ops.raise_on_flags(int(flags.item()) & ~_lib.NNGP_FLAG_NOT_PD, 'predict')
         y_std = np.asarray(self._y_train_std, dtype=np.float64).reshape(1, -1)
@@ -396,12 +408,20 @@ class B200Nngpr(GaussianProcessRegressor):
         mean = y_std * mean + y_mean
         if mean.shape[1] == 1:
             mean = mean[:, 0]
+        if return_cov:
+            return mean, self._format_cov(cov)
         if not return_std:
             return mean
         std = np.sqrt(var.cpu().numpy()).reshape(-1, 1) * y_std
         if std.shape[1] == 1:
             std = std[:, 0]
         return mean, std
+
+    def _format_cov(self, cov):
+        """Covariance in y units, ``(nq, nq)`` or ``(nq, nq, n_targets)`` (``base_nngpr.py:1017-1022``)."""
+        ys = np.asarray(self._y_train_std, dtype=np.float64).reshape(1, 1, -1)
+        c = (cov.cpu().numpy() if torch.is_tensor(cov) else np.asarray(cov))[:, :, None] * ys ** 2
+        return c[:, :, 0] if c.shape[2] == 1 else c
 
     def sample_y(self, X, n_samples=1, random_state=0, conditioning_method=None):
         """Samples of the predictive marginals at ``X``, ``base_nngpr.py:616-689`` with

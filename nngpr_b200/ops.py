@@ -84,6 +84,34 @@ def predict_full(x_train: torch.Tensor, y_train: torch.Tensor, x_query: torch.Te
     return mean, var
 
 
+def predict_cov_full(x_train: torch.Tensor, y_train: torch.Tensor, x_query: torch.Tensor, nbr: torch.Tensor,
+                     p: RbfParams, alpha: float, flags: torch.Tensor | None = None):
+    """Predict with ``conditioning_method='full'`` and the dense predictive covariance (FP64):
+    mean ``(nq, ydim)`` and covariance ``(nq, nq)`` (normalised y units)."""
+    for t, nm in ((x_train, 'x_train'), (y_train, 'y_train'), (x_query, 'x_query')):
+        _check_tensor(t, nm, (torch.float64,))
+    _check_tensor(nbr, 'nbr', (torch.int32,))
+    nt, d = x_train.shape
+    nq = x_query.shape[0]
+    y2 = y_train if y_train.dim() == 2 else y_train.reshape(nt, 1)
+    ydim = y2.shape[1]
+    m = nbr.shape[1] if nbr.dim() == 2 else 0
+    x_full = torch.cat([x_train, x_query]).contiguous()
+    mean = torch.empty((nq, ydim), dtype=torch.float64, device=x_query.device)
+    cov = torch.empty((nq, nq), dtype=torch.float64, device=x_query.device)
+    if nq == 0:
+        return mean, cov
+    keep = []
+    k = _kernel_struct(p, alpha, d, keep)
+    L = _lib.lib()
+    ws_bytes = int(L.nngp_predict_full_workspace_size(nq, m))
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device=x_query.device)
+    st = L.nngp_predict_cov_full_f64(_ptr(x_full), _ptr(y2), nt, nq, d, ydim, _ptr(nbr), m, ctypes.byref(k),
+                                     _ptr(mean), _ptr(cov), _ptr(flags), _ptr(ws), ws_bytes, _stream())
+    _lib.check(st, 'nngp_predict_cov_full_f64')
+    return mean, cov
+
+
 def sample_full(x_train: torch.Tensor, y_train: torch.Tensor, x_query: torch.Tensor, nbr: torch.Tensor,
                 p: RbfParams, alpha: float, z: torch.Tensor, flags: torch.Tensor | None = None) -> torch.Tensor:
     """Samples with ``conditioning_method='full'`` (FP64) from the standard normals ``z``

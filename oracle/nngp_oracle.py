@@ -500,3 +500,42 @@ def sample_full(x_train, y_train, x_query, nbr, p: KernelParams, alpha: float, z
         sig = np.sqrt(s2) if s2 > 0 else 0.0
         out[i] = np.einsum('i,ijk->jk', w, v) + sig * z[i]
     return out
+
+
+def predict_cov_full(x_train, y_train, x_query, nbr, p: KernelParams, alpha: float):
+    """Predict with ``conditioning_method='full'`` and ``return_cov=True``: restates the dense
+    branch of the sequential algorithm (``base_nngpr.py:896-1030``): the covariance of every pair
+    of queries is kept, ``cov[i, :i] = w_q^T cov[q-neighbours, :i]``, ``cov[i, i]`` the variance
+    (normalised y units)."""
+    x_train = np.asarray(x_train, dtype=np.float64)
+    x_query = np.asarray(x_query, dtype=np.float64)
+    y_train = np.asarray(y_train, dtype=np.float64)
+    if y_train.ndim == 1:
+        y_train = y_train[:, None]
+    nt, nq = x_train.shape[0], x_query.shape[0]
+    x_full = np.concatenate([x_train, x_query])
+    nbr = np.asarray(nbr)
+    idx = np.concatenate([np.arange(nt, nt + nq)[:, None], nbr], axis=1)
+    K, _ = fill_nn_kernel(x_full, idx, p, False)
+    train = (idx >= 0) & (idx < nt)
+    ii = np.arange(idx.shape[1])
+    K[:, ii, ii] += np.where(train, alpha, 0.0)
+    mean = np.full((nt + nq, y_train.shape[1]), np.nan)
+    mean[:nt] = y_train
+    cov = np.zeros((nq, nq))
+    for i in range(nq):
+        w = np.linalg.solve(K[i, 1:, 1:], K[i, 0, 1:])
+        js = nbr[i]
+        vals = np.where(js[:, None] >= 0, mean[np.where(js >= 0, js, 0)], 0.0)
+        mean[nt + i] = w @ vals
+        q = np.nonzero(js >= nt)[0]
+        a = js[q] - nt
+        C = cov[np.ix_(a, a)]
+        raw = max(0.0, K[i, 0, 0] - K[i, 0, 1:] @ w)
+        var = max(0.0, raw + w[q] @ C @ w[q])
+        if i > 0 and q.size:
+            row = w[q] @ cov[a, :i]
+            cov[i, :i] = row
+            cov[:i, i] = row
+        cov[i, i] = var
+    return mean[nt:], cov

@@ -142,7 +142,8 @@ def main():
 def full_cases(NumpyNngpr, NumpyWorker, bk):
     """predict(conditioning_method='full') of the reference (the sequential algorithm,
     base_nngpr.py:896-1030) on three of the cases above, and sample_y(conditioning_method='full',
-    n_samples=4, random_state=11) on the first 60 query points (:691-750), written to
+    n_samples=4, random_state=11) on the first 60 query points (:691-750) and predict with
+    return_cov on the first 80 (full and only-train), written to
     full_<case>.npz with the neighbour lists they used (indices into [x_train; x_query])."""
     specs = {
         'cpu_n2000_d3_m16': lambda: bk.ConstantKernel(1.0) * bk.RBF(0.3) + bk.WhiteKernel(0.01),
@@ -163,12 +164,18 @@ def full_cases(NumpyNngpr, NumpyWorker, bk):
         worker = NumpyWorker()
         nn, _ = gpr._find_nn_indices_for_train_and_eval(worker, gpr.kernel_, gpr.X_train_, xq, condition_on_eval=True,
                                                          double_nn=False)
+        _, cov_full = gpr.predict(xq[:80], return_cov=True, conditioning_method='full')
+        _, cov_train = gpr.predict(xq[:80], return_cov=True, conditioning_method='only-train')
+        nn80, _ = gpr._find_nn_indices_for_train_and_eval(worker, gpr.kernel_, gpr.X_train_, xq[:80],
+                                                           condition_on_eval=True, double_nn=False)
         samples = gpr.sample_y(xq[:60], n_samples=4, random_state=11, conditioning_method='full')
         nn60, _ = gpr._find_nn_indices_for_train_and_eval(worker, gpr.kernel_, gpr.X_train_, xq[:60],
                                                            condition_on_eval=True, double_nn=False)
         np.savez_compressed(os.path.join(HERE, 'full_' + name + '.npz'), mean=np.asarray(mean), std=np.asarray(std),
                             mean_only=np.asarray(mean_only), nbr=np.asarray(nn)[:, 1:],
-                            samples60=np.asarray(samples), nbr60=np.asarray(nn60)[:, 1:])
+                            samples60=np.asarray(samples), nbr60=np.asarray(nn60)[:, 1:],
+                            cov80_full=np.asarray(cov_full), cov80_train=np.asarray(cov_train),
+                            nbr80=np.asarray(nn80)[:, 1:])
         print('full', name, np.asarray(mean).ravel()[:3], np.asarray(std).ravel()[:3])
 
 

@@ -81,9 +81,10 @@ def test_out_of_scope_calls_raise():
     gpr = B200Nngpr(kernel=skk.ConstantKernel(1.0) * skk.RBF(1.0) + skk.WhiteKernel(0.1), optimizer=None,
                     num_nn=8).fit(x, y[:, 0])
     with pytest.raises(NotImplementedError):
-        gpr.predict(xe, return_cov=True)
-    with pytest.raises(NotImplementedError):
         gpr.predict(xe, conditioning_method='full-double-nn')
+    with pytest.raises(NotImplementedError):
+        B200Nngpr(kernel=skk.RBF(1.0), num_nn=40, optimizer=None).fit(x, y[:, 0]).predict(
+            xe, conditioning_method='full')  # more than 32 neighbours in the full recursion
     with pytest.raises(NotImplementedError, match='Cannot accelerate'):
         B200Nngpr(kernel=skk.Matern(1.0, nu=2.0), optimizer=None).fit(x, y[:, 0])
 

@@ -71,3 +71,22 @@ def test_sample_y_full_reproduces_the_reference(name):
     s = gpr.sample_y(g['xq'][:60], n_samples=4, random_state=11, conditioning_method='full')
     assert s.shape == f['samples60'].shape
     assert np.max(np.abs(s - f['samples60'])) < 1e-9
+
+
+@pytest.mark.parametrize('name', FULL_CASES)
+@pytest.mark.parametrize('method', ['full', 'only-train'])
+def test_return_cov_matches_reference(name, method):
+    """predict(return_cov=True): the dense predictive covariance of the sequential algorithm
+    ('full'), diagonal for 'only-train' (its queries are independent); the reference's outputs
+    on the first 80 queries, FP64: 1e-10."""
+    g, f = load(name), load_full(name)
+    gpr = B200Nngpr(kernel=KERNELS[name](), num_nn=int(g['num_nn']), alpha=float(g['alpha']),
+                    normalize_y=bool(g['normalize_y']), optimizer=None, allow_downcast_f32='no').fit(g['x'], g['y'])
+    mean, cov = gpr.predict(g['xq'][:80], return_cov=True, conditioning_method=method)
+    want = f['cov80_full'] if method == 'full' else f['cov80_train']
+    assert cov.shape == want.shape
+    assert np.max(np.abs(cov - want)) < 1e-10
+    want_mean = gpr.predict(g['xq'][:80], conditioning_method=method)
+    np.testing.assert_array_equal(mean, want_mean)
+    _, std = gpr.predict(g['xq'][:80], return_std=True, return_cov=True, conditioning_method=method)
+    assert std.shape == want_mean.shape  # both asked for: the standard deviation, as the reference

@@ -47,3 +47,16 @@ def test_oracle_full_samples_reproduce_the_reference_stream(name):
     out = out * np.asarray(ys).reshape(1, -1, 1) + np.asarray(ym).reshape(1, -1, 1)
     want = np.asarray(f['samples60']).reshape(out.shape)
     assert np.max(np.abs(out - want)) < 1e-9
+
+
+@pytest.mark.parametrize('name', FULL_CASES)
+def test_oracle_dense_covariance_matches_reference(name):
+    """predict(return_cov=True, conditioning_method='full') on the first 80 queries."""
+    g, f = load(name), load_full(name)
+    y, ym, ys = normalized_y(g)
+    p = oracle_params(KP.extract(KERNELS[name]().clone_with_theta(g['theta_pred'])))
+    _, cov = O.predict_cov_full(g['x'], y, g['xq'][:80], f['nbr80'], p, float(g['alpha']))
+    c = cov[:, :, None] * np.asarray(ys).reshape(1, 1, -1) ** 2
+    want = np.asarray(f['cov80_full']).reshape(c.shape)
+    assert np.max(np.abs(c - want)) < 1e-10
+    assert np.abs(want[~np.eye(80, dtype=bool)]).max() > 0  # the covariance is dense
