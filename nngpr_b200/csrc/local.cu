@@ -502,7 +502,8 @@ __global__ void __launch_bounds__(kBlkThreads) local_block_kernel(
                     r = fma(t, t, r);
                 }
                 kv = a.rbf * kern_s<true>(a.family, r) + a.cst;
-                if (i == jx) kv += a.noise + ((i == m && PRED) ? 0.0 : a.alpha);
+                if (i == jx)
+                    kv += a.noise + (((i == m && PRED) || (i < m && (int64_t)ids[i] >= a.alpha_below)) ? 0.0 : a.alpha);
             } else {
                 kv = (i == jx) ? 1.0 : 0.0;
             }
@@ -531,6 +532,23 @@ __global__ void __launch_bounds__(kBlkThreads) local_block_kernel(
         if (notpd && tid == 0) flag_or(flags, NNGP_FLAG_NOT_PD);
         const double sigma = A[m * lda + m];
         const double s2 = sigma * sigma;
+        if (PRED && a.weights_out) {
+            // conditioning weights w = L^-T l (l: row m of the augmented factor), by warp 0
+            if (tid < 32) {
+                for (int k = m - 1; k >= 0; --k) {
+                    double part = 0.0;
+                    for (int jx = k + 1 + tid; jx < m; jx += 32) part = fma(A[jx * lda + k], zw[jx], part);
+                    part = warp_sum(part);
+                    if (tid == 0) zw[k] = (A[m * lda + k] - part) / A[k * lda + k];
+                    __syncwarp();
+                }
+            }
+            __syncthreads();
+            for (int i = tid; i < m; i += blockDim.x) mean[p * m + i] = (TIn)zw[i];
+            if (tid == 0) var[p] = (TIn)s2;
+            __syncthreads();
+            continue;
+        }
         double wsum = 0.0, ll = 0.0;
         for (int i = tid; i < n1; i += blockDim.x) zw[i] = 0.0;
         for (int c = 0; c < a.ydim; ++c) {
@@ -841,10 +859,10 @@ __device__ __forceinline__ double full_pair_cov(const int32_t *__restrict__ nbr,
     return 0.0;
 }
 
-// One warp walks the queries in order (query i may condition on queries < i).  Lane s owns
-// neighbour slot s: mean_i = sum_s w_is v_s (v = y of a training neighbour or the mean already
-// predicted for a query neighbour); var_i = max(0, max(0, s2_i) + w_q^T C w_q) with C the
-// covariance of the query neighbours (variances on the diagonal, tracked pairs elsewhere);
+// One warp walks the queries in order (query i may condition on queries < i).  Lane l owns
+// neighbour slots l and l + 32: mean_i = sum_s w_is v_s (v = y of a training neighbour or the
+// mean already predicted for a query neighbour); var_i = max(0, max(0, s2_i) + w_q^T C w_q) with
+// C the covariance of the query neighbours (variances on the diagonal, tracked pairs elsewhere);
 // the covariances of query i with its query neighbours, (C w)_s, are kept for later queries.
 __global__ void __launch_bounds__(32) full_recursion_kernel(const int32_t *__restrict__ nbr,
                                                             const double *__restrict__ w,
@@ -855,30 +873,50 @@ __global__ void __launch_bounds__(32) full_recursion_kernel(const int32_t *__res
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x;
     for (int64_t i = 0; i < nq; ++i) {
-        int32_t j = lane < m ? nbr[i * m + lane] : -1;
-        if (j >= 0 && (int64_t)j >= nt + i) {  // not an earlier point: treated as missing
-            flag_or(flags, NNGP_FLAG_BAD_INDEX);
-            j = -1;
+        int32_t j[2];
+        double ws[2];
+        bool q[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int sl = lane + 32 * h;
+            int32_t jj = sl < m ? nbr[i * m + sl] : -1;
+            if (jj >= 0 && (int64_t)jj >= nt + i) {  // not an earlier point: treated as missing
+                flag_or(flags, NNGP_FLAG_BAD_INDEX);
+                jj = -1;
+            }
+            j[h] = jj;
+            ws[h] = (sl < m && jj >= 0) ? w[i * m + sl] : 0.0;
+            q[h] = jj >= 0 && (int64_t)jj >= nt;  // a query neighbour
         }
-        const double ws = (lane < m && j >= 0) ? w[i * m + lane] : 0.0;
-        const bool q = j >= 0 && (int64_t)j >= nt;  // a query neighbour
         for (int c = 0; c < ydim; ++c) {
-            double v = 0.0;
-            if (j >= 0) v = q ? mean[((int64_t)j - nt) * ydim + c] : y[(int64_t)j * ydim + c];
-            const double mu = warp_sum(ws * v);
+            double acc = 0.0;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                if (j[h] < 0) continue;
+                const double v = q[h] ? mean[((int64_t)j[h] - nt) * ydim + c] : y[(int64_t)j[h] * ydim + c];
+                acc = fma(ws[h], v, acc);
+            }
+            const double mu = warp_sum(acc);
             if (lane == 0) mean[i * ydim + c] = mu;
         }
         if (want_var) {
-            const int64_t a = q ? (int64_t)j - nt : -1;
-            double cw = q ? var[a] * ws : 0.0;
+            double cw[2] = {0.0, 0.0};
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+                if (q[h]) cw[h] = var[(int64_t)j[h] - nt] * ws[h];
             for (int t = 0; t < m; ++t) {
-                const int32_t jt = __shfl_sync(FULL, j, t);
-                const double wt = __shfl_sync(FULL, ws, t);
-                if (q && t != lane && jt >= 0 && (int64_t)jt >= nt)
-                    cw += full_pair_cov(nbr, pc, m, nt, a, (int64_t)jt - nt) * wt;
+                const int32_t jt = __shfl_sync(FULL, t < 32 ? j[0] : j[1], t & 31);
+                const double wt = __shfl_sync(FULL, t < 32 ? ws[0] : ws[1], t & 31);
+                if (jt < 0 || (int64_t)jt < nt) continue;
+#pragma unroll
+                for (int h = 0; h < 2; ++h)
+                    if (q[h] && t != lane + 32 * h)
+                        cw[h] += full_pair_cov(nbr, pc, m, nt, (int64_t)j[h] - nt, (int64_t)jt - nt) * wt;
             }
-            const double quad = warp_sum(ws * cw);
-            if (lane < m) pc[i * m + lane] = q ? cw : 0.0;
+            const double quad = warp_sum(ws[0] * cw[0] + ws[1] * cw[1]);
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+                if (lane + 32 * h < m) pc[i * m + lane + 32 * h] = q[h] ? cw[h] : 0.0;
             if (lane == 0) {
                 const double raw = s2[i] > 0.0 ? s2[i] : 0.0;
                 const double vi = raw + quad;
@@ -935,14 +973,13 @@ __global__ void __launch_bounds__(kCovThreads) cov_recursion_kernel(const int32_
                                                                     const double *__restrict__ y, int64_t nt,
                                                                     int64_t nq, int m, int ydim, double *mean,
                                                                     double *cov, int32_t *__restrict__ flags) {
-    __shared__ int64_t sa[32];   // query position of each slot's neighbour, or -1
-    __shared__ int32_t sj[32];   // neighbour index (-1: missing)
-    __shared__ double sw[32];
+    __shared__ int64_t sa[64];   // query position of each slot's neighbour, or -1
+    __shared__ int32_t sj[64];   // neighbour index (-1: missing)
+    __shared__ double sw[64];
     __shared__ double svar;
-    const unsigned FULL = 0xffffffffu;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (int64_t i = 0; i < nq; ++i) {
-        if (tid < 32) {
+        if (tid < 64) {
             int32_t j = tid < m ? nbr[i * m + tid] : -1;
             if (j >= 0 && (int64_t)j >= nt + i) {
                 flag_or(flags, NNGP_FLAG_BAD_INDEX);
@@ -954,22 +991,33 @@ __global__ void __launch_bounds__(kCovThreads) cov_recursion_kernel(const int32_
         }
         __syncthreads();
         if (warp == 0) {
-            const int32_t j = sj[lane];
-            const double ws = sw[lane];
-            const int64_t a = sa[lane];
             for (int c = 0; c < ydim; ++c) {
-                double v = 0.0;
-                if (j >= 0) v = a >= 0 ? mean[a * ydim + c] : y[(int64_t)j * ydim + c];
-                const double mu = warp_sum(ws * v);
+                double acc = 0.0;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int sl = lane + 32 * h;
+                    const int32_t j = sj[sl];
+                    if (j < 0) continue;
+                    const double v = sa[sl] >= 0 ? mean[sa[sl] * ydim + c] : y[(int64_t)j * ydim + c];
+                    acc = fma(sw[sl], v, acc);
+                }
+                const double mu = warp_sum(acc);
                 if (lane == 0) mean[i * ydim + c] = mu;
             }
-            double cw = 0.0;  // (C w)_s for a query-neighbour slot s
-            if (a >= 0)
+            double part = 0.0;  // sum over this lane's slots s of w_s (C w)_s
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int sl = lane + 32 * h;
+                const int64_t a = sa[sl];
+                if (a < 0) continue;
+                double cw = 0.0;
                 for (int t = 0; t < m; ++t) {
                     const int64_t b = sa[t];
                     if (b >= 0) cw += cov[a * nq + b] * sw[t];
                 }
-            const double quad = warp_sum(ws * cw);
+                part = fma(sw[sl], cw, part);
+            }
+            const double quad = warp_sum(part);
             if (lane == 0) {
                 const double raw = s2[i] > 0.0 ? s2[i] : 0.0;
                 const double vi = raw + quad;
@@ -1001,7 +1049,7 @@ nngp_status predict_full_f64(const double *x_full, const double *y_train, int64_
                              int32_t *flags, void *ws, size_t ws_bytes, cudaStream_t stream, bool samples = false,
                              const double *z = nullptr, bool dense_cov = false) {
     if (nt < 0 || nq < 0) return fail(NNGP_ERR_INVALID_ARGUMENT, "predict_full: negative size");
-    if (m < 1 || m > kWarpM) return fail(NNGP_ERR_UNSUPPORTED, "predict_full: num_nn must be in [1, 32]");
+    if (m < 1 || m > 2 * kWarpM) return fail(NNGP_ERR_UNSUPPORTED, "predict_full: num_nn must be in [1, 64]");
     LocalArgs a;
     nngp_status st = fill_args(a, k, d, ydim, m, nt + nq, nq, 0.0, false);
     if (st != NNGP_OK) return st;

@@ -15,10 +15,11 @@ Precision follows the reference's ``allow_downcast_f32`` (``base_nngpr.py:66-72`
 ``'only-nn'`` (default) searches neighbours in FP32 and solves the local systems in FP64;
 ``'yes'`` solves them in FP32 (FP64 re-solve below ``pivot_tol``); ``'no'`` is FP64 throughout.
 
-``predict`` and ``sample_y`` support ``conditioning_method='only-train'`` and ``'full'`` (the
-reference's sequential algorithms, on the device), ``return_std`` and ``return_cov``.  Not
-provided: ``'full-double-nn'`` (raises ``NotImplementedError``).  Kernels outside the accelerated
-family raise
+``predict`` and ``sample_y`` support ``conditioning_method='only-train'``, ``'full'`` and
+``'full-double-nn'`` (the reference's sequential algorithms, on the device), ``return_std`` and
+``return_cov``; the sequential ones take up to 64 neighbour slots (``num_nn <= 64`` for
+``'full'``, ``<= 32`` for ``'full-double-nn'``) and raise ``NotImplementedError`` above.
+Kernels outside the accelerated family raise
 ``NotImplementedError("Cannot accelerate this kernel ...")`` as the reference's CUDA path does.
 """
 
@@ -322,13 +323,12 @@ class B200Nngpr(GaussianProcessRegressor):
 
     # ---- predict --------------------------------------------------------------------------
     def predict(self, X, return_std=False, return_cov=False, conditioning_method=None):
-        """Predictive mean (and std) conditioned on the training set, ``base_nngpr.py:763-894``
-        (``conditioning_method='only-train'``)."""
+        """Predictive mean (and std or covariance), ``base_nngpr.py:763-1030``: conditioned on the
+        training set (``'only-train'``, the default) or, query by query, on the training set and
+        the earlier queries (``'full'``, ``'full-double-nn'``)."""
         conditioning_method = 'only-train' if conditioning_method is None else conditioning_method
         if conditioning_method not in {'only-train', 'full', 'full-double-nn'}:
             raise ValueError(f"unknown conditioning_method {conditioning_method!r}")
-        if conditioning_method == 'full-double-nn':
-            raise NotImplementedError("B200Nngpr implements predict(conditioning_method='only-train' or 'full')")
         if return_std:
             return_cov = False  # the reference returns the standard deviation when both are asked for
         if self.kernel is None or self.kernel.requires_vector_input:
@@ -343,8 +343,8 @@ class B200Nngpr(GaussianProcessRegressor):
             mean = np.zeros(X.shape[0])
             if return_cov:
                 if conditioning_method != 'only-train':
-                    raise NotImplementedError("predict(return_cov=True, conditioning_method='full') needs a "
-                                              "fitted model")
+                    raise NotImplementedError(f"predict(return_cov=True, conditioning_method={conditioning_method!r}) "
+                                              "needs a fitted model")
                 return mean, np.diag(np.full(X.shape[0], p.rbf_level + p.const_value + p.noise_level))
             if return_std:
                 return mean, np.full(X.shape[0], np.sqrt(p.rbf_level + p.const_value + p.noise_level))
@@ -353,8 +353,9 @@ class B200Nngpr(GaussianProcessRegressor):
         p = self._params(kernel)
         dev = self._device
         search_dtype, local_dtype = self._dtypes()
-        if conditioning_method == 'full':
-            return self._predict_full(X, p, search_dtype, return_std, return_cov)
+        if conditioning_method != 'only-train':
+            return self._predict_full(X, p, search_dtype, return_std, return_cov,
+                                      conditioning_method == 'full-double-nn')
         xt, yt = self._train_tensors(local_dtype)
         xs_train = xt if search_dtype == local_dtype else self._train_tensors(search_dtype)[0]
         xq_host = np.ascontiguousarray(X, dtype=np.float64)
@@ -384,19 +385,45 @@ class B200Nngpr(GaussianProcessRegressor):
             std = std[:, 0]
         return mean, std
 
-    def _predict_full(self, X, p, search_dtype, return_std, return_cov=False):
-        """``conditioning_method='full'`` (``base_nngpr.py:896-1030``): every query conditions on
-        the training set and on the queries before it; FP64 local systems."""
+    def _full_lists(self, xt, xq, p, search_dtype, double_nn, flags):
+        """Neighbour lists of the sequential algorithm, ``(nq, m)`` int32 indices into
+        ``[x_train; x_query]`` (``base_nngpr.py:1370-1464``).  ``'full'``: the prefix search of the
+        queries over the training set and the earlier queries (``ref_cut_index = n_train``).
+        ``'full-double-nn'``: ``num_nn`` training neighbours plus ``num_nn`` earlier-query
+        neighbours, each row packed as valid training entries, valid query entries, then ``-1``
+        (``:1418-1449``).  At most 64 slots (the device recursions' limit)."""
+        nt, nq = xt.shape[0], xq.shape[0]
+        ls = self._search_ls(p)
+        k = self._num_nn
+        if not double_nn:
+            m = min(k, nt + nq)
+            if m > 64:
+                raise NotImplementedError("conditioning_method='full' supports num_nn <= 64")
+            x_full_s = torch.cat([xt, xq]).to(search_dtype)
+            return ops.knn(x_full_s, x_full_s[nt:], m, ref_cut_index=nt, length_scale=ls, flags=flags)
+        mt, mq = (min(k, nt) if nt > 0 else 0), max(0, min(k, nq - 1))
+        if mt + mq > 64:
+            raise NotImplementedError("conditioning_method='full-double-nn' supports num_nn <= 32")
+        xq_s = xq.to(search_dtype)
+        q = ops.knn(xq_s, xq_s, mq, ref_cut_index=0, length_scale=ls, flags=flags)
+        q = torch.where(q >= 0, q + nt, q)
+        if mt == 0:
+            return q
+        t = ops.knn(xt.to(search_dtype), xq_s, mt, None, length_scale=ls, flags=flags)
+        both = torch.cat([t, q], dim=1)
+        # stable sort on "missing": valid entries keep their order (training first), -1 last
+        order = torch.sort((both < 0).to(torch.int8), dim=1, stable=True).indices
+        return torch.gather(both, 1, order).contiguous()
+
+    def _predict_full(self, X, p, search_dtype, return_std, return_cov=False, double_nn=False):
+        """``conditioning_method='full'`` or ``'full-double-nn'`` (``base_nngpr.py:896-1030``):
+        every query conditions on the training set and on the queries before it; FP64 local
+        systems."""
         dev = self._device
         xt, yt = self._train_tensors(torch.float64)
         xq = torch.from_numpy(np.ascontiguousarray(X, dtype=np.float64)).to(dev)
-        nt, nq = xt.shape[0], xq.shape[0]
-        m = min(self._num_nn, nt + nq)
-        if m > 32:
-            raise NotImplementedError("predict(conditioning_method='full') supports num_nn <= 32")
         flags = ops.new_flags(dev)
-        x_full_s = torch.cat([xt, xq]).to(search_dtype)
-        nbr = ops.knn(x_full_s, x_full_s[nt:], m, ref_cut_index=nt, length_scale=self._search_ls(p), flags=flags)
+        nbr = self._full_lists(xt, xq, p, search_dtype, double_nn, flags)
         if return_cov:
             mean, cov = ops.predict_cov_full(xt, yt, xq, nbr, p, float(self.alpha), flags=flags)
         else:
@@ -429,15 +456,15 @@ class B200Nngpr(GaussianProcessRegressor):
         set only, so its samples are independent draws ``mean + std * N(0, 1)`` (the reference's
         own fast path, ``:672-689``).  The normal draws come from a device generator seeded by
         ``random_state`` (an int, a ``RandomState`` or ``None``), so they differ from the
-        reference's worker streams, not in distribution.  Shape ``(n_samples_X, n_samples)`` or
+        reference's worker streams, not in distribution.  With ``'full'`` or ``'full-double-nn'``
+        the samples follow the sequential algorithm (``:691-750``, :meth:`_sample_full`) and an
+        int ``random_state`` reproduces the reference's.  Shape ``(n_samples_X, n_samples)`` or
         ``(n_samples_X, n_targets, n_samples)``."""
         conditioning_method = 'only-train' if conditioning_method is None else conditioning_method
         if conditioning_method not in {'only-train', 'full', 'full-double-nn'}:
             raise ValueError(f"unknown conditioning_method {conditioning_method!r}")
-        if conditioning_method == 'full-double-nn':
-            raise NotImplementedError("B200Nngpr implements sample_y(conditioning_method='only-train' or 'full')")
-        if conditioning_method == 'full':
-            return self._sample_full(X, n_samples, random_state)
+        if conditioning_method != 'only-train':
+            return self._sample_full(X, n_samples, random_state, conditioning_method == 'full-double-nn')
         mean, std = self.predict(X, return_std=True)
         mu = np.asarray(mean, dtype=np.float64)
         sd = np.asarray(std, dtype=np.float64)
@@ -454,14 +481,15 @@ class B200Nngpr(GaussianProcessRegressor):
         out = out.cpu().numpy()
         return out[:, 0, :] if single else out
 
-    def _sample_full(self, X, n_samples, random_state):
-        """``sample_y(conditioning_method='full')`` (``base_nngpr.py:691-750``): each query's samples
-        condition on the training y and on the samples of the queries before it.  The standard
+    def _sample_full(self, X, n_samples, random_state, double_nn=False):
+        """``sample_y`` with ``conditioning_method='full'`` or ``'full-double-nn'``
+        (``base_nngpr.py:691-750``): each query's samples condition on the training y and on the
+        samples of the queries before it.  The standard
         normals are drawn on the host exactly as the reference draws them (scikit-learn's
         ``check_random_state``, query by query, ``(n_targets, n_samples)`` each), so an int
         ``random_state`` reproduces the reference's samples; the recursion runs on the device."""
         if not hasattr(self, 'X_train_'):
-            raise NotImplementedError("sample_y(conditioning_method='full') needs a fitted model")
+            raise NotImplementedError("sample_y with conditioning on the queries needs a fitted model")
         if self.kernel is None or self.kernel.requires_vector_input:
             dtype, ensure_2d = "numeric", True
         else:
@@ -472,15 +500,11 @@ class B200Nngpr(GaussianProcessRegressor):
         search_dtype, _ = self._dtypes()
         xt, yt = self._train_tensors(torch.float64)
         xq = torch.from_numpy(np.ascontiguousarray(X, dtype=np.float64)).to(dev)
-        nt, nq = xt.shape[0], xq.shape[0]
-        m = min(self._num_nn, nt + nq)
-        if m > 32:
-            raise NotImplementedError("sample_y(conditioning_method='full') supports num_nn <= 32")
+        nq = xq.shape[0]
         ydim = yt.shape[1]
         z = check_random_state(random_state).standard_normal((nq, ydim, int(n_samples)))
         flags = ops.new_flags(dev)
-        x_full_s = torch.cat([xt, xq]).to(search_dtype)
-        nbr = ops.knn(x_full_s, x_full_s[nt:], m, ref_cut_index=nt, length_scale=self._search_ls(p), flags=flags)
+        nbr = self._full_lists(xt, xq, p, search_dtype, double_nn, flags)
         out = ops.sample_full(xt, yt, xq, nbr, p, float(self.alpha), torch.from_numpy(z).to(dev), flags=flags)
         out = out.cpu().numpy()
         ops.raise_on_flags(int(flags.item()) & ~_lib.NNGP_FLAG_NOT_PD, 'sample_y')

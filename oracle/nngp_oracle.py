@@ -419,6 +419,28 @@ def reuse_rank(x: np.ndarray, cand: np.ndarray, thr: np.ndarray, length_scale, n
     return out, failed
 
 
+def double_nn_lists(x_train, x_query, num_nn: int, length_scale=1.0, dtype=np.float32) -> np.ndarray:
+    """Neighbour lists of ``conditioning_method='full-double-nn'``
+    (``base_nngpr.py:1418-1449``): ``min(num_nn, nt)`` nearest training points and
+    ``min(num_nn, nq - 1)`` nearest earlier queries (indices offset by ``nt``), packed per row as
+    the valid training entries, then the valid query entries, then ``-1``."""
+    x_train = np.asarray(x_train)
+    x_query = np.asarray(x_query)
+    nt, nq = x_train.shape[0], x_query.shape[0]
+    mq = max(0, min(num_nn, nq - 1))
+    q = knn(x_query, x_query, mq, 0, length_scale, dtype) if mq > 0 else np.empty((nq, 0), np.int32)
+    q = np.where(q >= 0, q + nt, -1).astype(np.int32)
+    if nt == 0:
+        return q
+    t = knn(x_train, x_query, min(num_nn, nt), None, length_scale, dtype)
+    both = np.concatenate([t, q], axis=1)
+    out = np.full_like(both, -1)
+    for i in range(nq):
+        v = both[i][both[i] >= 0]
+        out[i, :v.size] = v
+    return out
+
+
 def predict_full(x_train, y_train, x_query, nbr, p: KernelParams, alpha: float, return_std: bool = True):
     """Predict with ``conditioning_method='full'``: restates the sequential algorithm of
     ``Nngpr.predict`` (``base_nngpr.py:896-1030``) for ``return_cov=False``.  ``nbr`` is

@@ -143,7 +143,8 @@ def full_cases(NumpyNngpr, NumpyWorker, bk):
     """predict(conditioning_method='full') of the reference (the sequential algorithm,
     base_nngpr.py:896-1030) on three of the cases above, and sample_y(conditioning_method='full',
     n_samples=4, random_state=11) on the first 60 query points (:691-750) and predict with
-    return_cov on the first 80 (full and only-train), written to
+    return_cov on the first 80 (full and only-train); the same for 'full-double-nn' (samples with
+    random_state=12); on the first case also 'full' with num_nn=48.  Written to
     full_<case>.npz with the neighbour lists they used (indices into [x_train; x_query])."""
     specs = {
         'cpu_n2000_d3_m16': lambda: bk.ConstantKernel(1.0) * bk.RBF(0.3) + bk.WhiteKernel(0.01),
@@ -171,11 +172,32 @@ def full_cases(NumpyNngpr, NumpyWorker, bk):
         samples = gpr.sample_y(xq[:60], n_samples=4, random_state=11, conditioning_method='full')
         nn60, _ = gpr._find_nn_indices_for_train_and_eval(worker, gpr.kernel_, gpr.X_train_, xq[:60],
                                                            condition_on_eval=True, double_nn=False)
+        # 'full-double-nn': num_nn neighbours from the training set plus num_nn from the earlier
+        # queries (base_nngpr.py:1418-1449)
+        dn_mean, dn_std = gpr.predict(xq, return_std=True, conditioning_method='full-double-nn')
+        dn_nn, _ = gpr._find_nn_indices_for_train_and_eval(worker, gpr.kernel_, gpr.X_train_, xq,
+                                                            condition_on_eval=True, double_nn=True)
+        _, dn_cov = gpr.predict(xq[:80], return_cov=True, conditioning_method='full-double-nn')
+        dn_samples = gpr.sample_y(xq[:60], n_samples=4, random_state=12, conditioning_method='full-double-nn')
+        extra = {}
+        if name == 'cpu_n2000_d3_m16':
+            # 'full' with 48 neighbours (more than one warp's 32 slots) on the first 150 queries
+            gpr48 = NumpyNngpr(kernel=kernel_fn(), num_nn=48, optimizer=None, alpha=float(g['alpha']),
+                               normalize_y=bool(g['normalize_y']), allow_downcast_f32='no',
+                               distribute_method='sequential', num_workers=1)
+            gpr48.fit(g['x'], g['y'])
+            f48_mean, f48_std = gpr48.predict(xq[:150], return_std=True, conditioning_method='full')
+            f48_nn, _ = gpr48._find_nn_indices_for_train_and_eval(worker, gpr48.kernel_, gpr48.X_train_, xq[:150],
+                                                                   condition_on_eval=True, double_nn=False)
+            extra = dict(f48_mean=np.asarray(f48_mean), f48_std=np.asarray(f48_std),
+                         f48_nbr=np.asarray(f48_nn)[:, 1:])
         np.savez_compressed(os.path.join(HERE, 'full_' + name + '.npz'), mean=np.asarray(mean), std=np.asarray(std),
                             mean_only=np.asarray(mean_only), nbr=np.asarray(nn)[:, 1:],
                             samples60=np.asarray(samples), nbr60=np.asarray(nn60)[:, 1:],
                             cov80_full=np.asarray(cov_full), cov80_train=np.asarray(cov_train),
-                            nbr80=np.asarray(nn80)[:, 1:])
+                            nbr80=np.asarray(nn80)[:, 1:], dn_mean=np.asarray(dn_mean), dn_std=np.asarray(dn_std),
+                            dn_nbr=np.asarray(dn_nn)[:, 1:], dn_cov80=np.asarray(dn_cov),
+                            dn_samples60=np.asarray(dn_samples), **extra)
         print('full', name, np.asarray(mean).ravel()[:3], np.asarray(std).ravel()[:3])
 
 

@@ -78,13 +78,9 @@ def test_prior_predict():
 
 def test_out_of_scope_calls_raise():
     x, xe, y = _fixture()
-    gpr = B200Nngpr(kernel=skk.ConstantKernel(1.0) * skk.RBF(1.0) + skk.WhiteKernel(0.1), optimizer=None,
-                    num_nn=8).fit(x, y[:, 0])
-    with pytest.raises(NotImplementedError):
-        gpr.predict(xe, conditioning_method='full-double-nn')
     with pytest.raises(NotImplementedError):
         B200Nngpr(kernel=skk.RBF(1.0), num_nn=40, optimizer=None).fit(x, y[:, 0]).predict(
-            xe, conditioning_method='full')  # more than 32 neighbours in the full recursion
+            xe, conditioning_method='full-double-nn')  # 80 slots: more than the recursions' 64
     with pytest.raises(NotImplementedError, match='Cannot accelerate'):
         B200Nngpr(kernel=skk.Matern(1.0, nu=2.0), optimizer=None).fit(x, y[:, 0])
 
@@ -114,8 +110,7 @@ def test_sample_y_only_train_shapes_seed_and_moments():
     g1 = load('cpu_n2000_d3_m16')
     gpr1 = make('cpu_n2000_d3_m16', g1).fit(g1['x'], g1['y'])
     assert gpr1.sample_y(g1['xq'][:7], n_samples=3).shape == (7, 3)
-    with pytest.raises(NotImplementedError):
-        gpr1.sample_y(g1['xq'][:7], conditioning_method='full-double-nn')
+    assert gpr1.sample_y(g1['xq'][:7], n_samples=3, conditioning_method='full-double-nn').shape == (7, 3)
 
 
 def test_pickle_round_trip():

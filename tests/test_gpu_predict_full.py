@@ -90,3 +90,75 @@ def test_return_cov_matches_reference(name, method):
     np.testing.assert_array_equal(mean, want_mean)
     _, std = gpr.predict(g['xq'][:80], return_std=True, return_cov=True, conditioning_method=method)
     assert std.shape == want_mean.shape  # both asked for: the standard deviation, as the reference
+
+
+def _fitted(name, g, **kw):
+    return B200Nngpr(kernel=KERNELS[name](), num_nn=int(g['num_nn']), alpha=float(g['alpha']),
+                     normalize_y=bool(g['normalize_y']), optimizer=None, allow_downcast_f32='no',
+                     **kw).fit(g['x'], g['y'])
+
+
+@pytest.mark.parametrize('name', FULL_CASES)
+def test_double_nn_matches_reference(name):
+    """conditioning_method='full-double-nn' (base_nngpr.py:1418-1449): the device lists are the
+    reference's (training search + prefix search of the queries, packed valid-first), and predict
+    (mean, std, dense covariance of the first 80) and sample_y (random_state=12, first 60) give
+    the reference's outputs, FP64: 1e-10 (samples 1e-9)."""
+    g, f = load(name), load_full(name)
+    gpr = _fitted(name, g)
+    dev = torch.device('cuda')
+    p = gpr._params(gpr.kernel_)
+    xt, _ = gpr._train_tensors(torch.float64)
+    nbr = gpr._full_lists(xt, torch.from_numpy(g['xq']).to(dev), p, torch.float64, True, ops.new_flags(dev))
+    np.testing.assert_array_equal(nbr.cpu().numpy(), f['dn_nbr'])
+    mean, std = gpr.predict(g['xq'], return_std=True, conditioning_method='full-double-nn')
+    assert mean.shape == f['dn_mean'].shape and std.shape == f['dn_std'].shape
+    assert np.max(np.abs(mean - f['dn_mean'])) < 1e-10
+    assert np.max(np.abs(std - f['dn_std'])) < 1e-10
+    _, cov = gpr.predict(g['xq'][:80], return_cov=True, conditioning_method='full-double-nn')
+    assert cov.shape == f['dn_cov80'].shape
+    assert np.max(np.abs(cov - f['dn_cov80'])) < 1e-10
+    s = gpr.sample_y(g['xq'][:60], n_samples=4, random_state=12, conditioning_method='full-double-nn')
+    assert s.shape == f['dn_samples60'].shape
+    assert np.max(np.abs(s - f['dn_samples60'])) < 1e-9
+
+
+def test_full_with_48_neighbours_matches_reference():
+    """'full' with num_nn = 48: the local systems take the one-CTA-per-system kernel and the
+    recursions two slots per lane; the reference's mean and std on the first 150 queries
+    (1e-10), and the dense covariance and the samples against the oracle on the same lists."""
+    name = 'cpu_n2000_d3_m16'
+    g, f = load(name), load_full(name)
+    gpr = B200Nngpr(kernel=KERNELS[name](), num_nn=48, alpha=float(g['alpha']), normalize_y=bool(g['normalize_y']),
+                    optimizer=None, allow_downcast_f32='no').fit(g['x'], g['y'])
+    xq = g['xq'][:150]
+    mean, std = gpr.predict(xq, return_std=True, conditioning_method='full')
+    assert np.max(np.abs(mean - f['f48_mean'])) < 1e-10
+    assert np.max(np.abs(std - f['f48_std'])) < 1e-10
+    from oracle import nngp_oracle as O
+    from _common import oracle_params
+    y, ym, ys = normalized_y(g)
+    po = oracle_params(KP.extract(gpr.kernel_))
+    _, cov_o = O.predict_cov_full(g['x'], y, xq, f['f48_nbr'], po, float(g['alpha']))
+    _, cov = gpr.predict(xq, return_cov=True, conditioning_method='full')
+    assert np.max(np.abs(cov - cov_o * float(np.asarray(ys).reshape(-1)[0]) ** 2)) < 1e-10
+    z = np.random.RandomState(5).standard_normal((150, 1, 3))
+    s_o = O.sample_full(g['x'], y[:, None], xq, f['f48_nbr'], po, float(g['alpha']), z)
+    s = gpr.sample_y(xq, n_samples=3, random_state=5, conditioning_method='full')
+    assert np.max(np.abs(s - (s_o[:, 0, :] * float(np.asarray(ys).reshape(-1)[0]) + float(np.asarray(ym).reshape(-1)[0])))) < 1e-9
+
+
+def test_sequential_conditioning_slot_limit():
+    g = load('cpu_n2000_d3_m16')
+    x, y, xq = g['x'][:300], g['y'][:300], g['xq'][:20]
+    k = KERNELS['cpu_n2000_d3_m16']
+    with pytest.raises(NotImplementedError):
+        B200Nngpr(kernel=k(), num_nn=70, optimizer=None).fit(x, y).predict(xq, conditioning_method='full')
+    gpr40 = B200Nngpr(kernel=k(), num_nn=40, optimizer=None).fit(x, y)
+    with pytest.raises(NotImplementedError):  # 40 training + 29 query slots
+        gpr40.sample_y(g['xq'][:30], conditioning_method='full-double-nn')
+    assert gpr40.predict(xq, conditioning_method='full-double-nn').shape == (20,)  # 40 + 19 slots
+    # one query: no earlier query to condition on, the double lists are the training lists
+    gpr = B200Nngpr(kernel=k(), num_nn=8, optimizer=None, allow_downcast_f32='no').fit(x, y)
+    np.testing.assert_array_equal(gpr.predict(xq[:1], conditioning_method='full-double-nn'),
+                                  gpr.predict(xq[:1], conditioning_method='only-train'))
