@@ -270,8 +270,10 @@ nngp_status nngp_plain_knn_f32(const float *ref_scaled, int64_t n_ref, const flo
  * then walks the queries in order: the mean uses the predicted means of query neighbours, the
  * variance adds their covariance, which is tracked only between a query and its own query
  * neighbours, as the reference's sparse partial covariance does (:923-930, :1002-1008).  mean:
- * (n_query, ydim); var (n_query) when want_var.  FP64, num_nn <= 32; the recursion is serial in
- * the queries (tens of microseconds per hundred queries). */
+ * (n_query, ydim); var (n_query) when want_var.  FP64, num_nn <= 64 (for 'full-double-nn' pass
+ * the packed lists of the training search and the queries' prefix search, base_nngpr.py:1418-1449,
+ * num_nn = their combined width); the recursion is serial in the queries (tens of microseconds
+ * per hundred queries). */
 size_t nngp_predict_full_workspace_size(int64_t n_query, int32_t num_nn);
 nngp_status nngp_predict_full_f64(const double *x_full, const double *y_train, int64_t n_train,
                                   int64_t n_query, int32_t d, int32_t ydim, const int32_t *nbr,
