@@ -37,6 +37,7 @@
 #include <type_traits>
 
 #include "common.cuh"
+#include "knn_seed.cuh"
 #include "knn_tc.cuh"
 
 namespace nngp {
@@ -511,7 +512,7 @@ struct KnnPlan {
     int dp = 0;  // padded row length of the scaled arrays
     int64_t n_ref_pad = 0;
     size_t off_ref = 0, off_q = 0, off_rec = 0, off_acc = 0, off_r2 = 0, off_ctr = 0, off_ldist = 0, off_lidx = 0,
-           total = 0;
+           off_seed = 0, off_seed_ws = 0, seed_ws_bytes = 0, total = 0;
     ScreenVariant v{};
     tc::TcVariant tv{};
 };
@@ -550,6 +551,13 @@ KnnPlan make_plan(int64_t n_ref, int64_t n_query, int d, int m, bool same) {
         off = align_up(off + 16, 256);
         p.off_ctr = off;
         off = align_up(off + 16, 256);
+        if (p.path == KnnPath::Tc && seed::workspace(n_ref) > 0) {  // seeds of the prefix search
+            p.off_seed = off;
+            off = align_up(off + (size_t)n_ref * sizeof(float), 256);
+            p.off_seed_ws = off;
+            p.seed_ws_bytes = seed::workspace(n_ref);
+            off = align_up(off + p.seed_ws_bytes, 256);
+        }
     } else {
         p.off_ldist = off;
         off = align_up(off + (size_t)n_query * m * sizeof(T), 256);
@@ -626,15 +634,26 @@ nngp_status knn_impl(const T *ref, int64_t n_ref, const T *query, int64_t n_quer
             const int per_sm = p.tv.ctas_per_sm;
             const int grid = (int)std::min<int64_t>(n_items, (int64_t)num_sms_knn() * per_sm);
             if (const char *dbg = std::getenv("NNGP_KNN_DEBUG"); dbg && dbg[0] == '1')
-                std::fprintf(stderr, "nngp_knn: tensor-core path d=%d m=%d items=%lld ctas/sm=%d grid=%d smem=%d\n", d,
-                             m, (long long)n_items, per_sm, grid, p.tv.smem);
+                std::fprintf(stderr, "nngp_knn: tensor-core path d=%d m=%d items=%lld ctas/sm=%d grid=%d smem=%d seeded=%d\n",
+                             d, m, (long long)n_items, per_sm, grid, p.tv.smem,
+                             (int)(same && has_cut && cut == 0 && p.seed_ws_bytes > 0 && seed::window() > 0));
+            // the prefix search of a point set over itself (the fit step) starts every row from a
+            // proven bound of its m-th distance: the same lists, far fewer candidates
+            const float *seeds_c = nullptr;
+            if (same && has_cut && cut == 0 && p.seed_ws_bytes > 0 && seed::window() > 0) {
+                float *sd = reinterpret_cast<float *>(base + p.off_seed);
+                nngp_status sst = seed::prefix_seeds(refs, n_ref, d, round_d(d), p.dp, m, base + p.off_seed_ws,
+                                                     p.seed_ws_bytes, sd, stream);
+                if (sst != NNGP_OK) return sst;
+                seeds_c = sd;
+            }
             const unsigned char *tiles_c = tiles;
             const float *q_c = qsc;
             const double *acc_c = acc;
             const unsigned int *r2_c = r2;
-            void *args[] = {(void *)&tiles_c, (void *)&q_c, (void *)&acc_c, (void *)&r2_c, (void *)&ctr,
-                            (void *)&n_query, (void *)&n_ref, (void *)&has_cut, (void *)&cut, (void *)&m,
-                            (void *)&out, (void *)&flags};
+            void *args[] = {(void *)&tiles_c, (void *)&q_c, (void *)&acc_c, (void *)&r2_c, (void *)&seeds_c,
+                            (void *)&ctr, (void *)&n_query, (void *)&n_ref, (void *)&has_cut, (void *)&cut,
+                            (void *)&m, (void *)&out, (void *)&flags};
             NNGP_CUDA_TRY(cudaLaunchKernel(reinterpret_cast<const void *>(p.tv.fn), dim3(grid),
                                            dim3(p.tv.threads), args, (size_t)p.tv.smem, stream));
         }

@@ -1,0 +1,322 @@
+// Seed thresholds for the prefix neighbour search of the fit step.
+//
+// The search keeps, for every point i, the m nearest of the points j < i (calc_nn with
+// ref_cut_index = 0, nngpr/cuda_kernel_accelerators.py:663-743, as called by
+// nngpr/base_nngpr.py:530-535).  The tensor-core kernel streams the refs in index order and
+// screens each against the row's current bound, the m-th best distance found so far; in random
+// input order a row meets about m ln(i/m) list updates, and every one costs an exact rescoring
+// and a heap insert.  That candidate work, not the screen, dominates the kernel at small d.
+//
+// Any m distinct refs j < i bound the row from above: the m-th smallest of their distances is
+// >= the m-th smallest over all j < i.  This file finds such refs cheaply: two space-filling
+// (Morton) orders of the scaled points, the second on a shifted grid, and for each point the
+// refs within W positions of it in either order.  With the m-th smallest of those distances as
+// the row's starting bound the screen passes about 40 refs per row instead of about 300 (d = 3,
+// uniform data, W = 256).  The bound is computed with exactly the arithmetic of the search's
+// exact rescoring, so it never excludes a true neighbour and the lists are bit-identical with or
+// without seeds; only the number of candidates changes.
+//
+// Steps (all on the caller's stream): per-dimension bounds of the finite coordinates; 64-bit
+// Morton keys (b = min(10, 64 / d) bits per dimension, interleaved) for both grids; a radix sort
+// of each (CUB, key/index pairs); the inverse permutations; then one warp per point, points
+// taken in curve order so that neighbouring warps read the same windows.
+#include <cub/device/device_radix_sort.cuh>
+
+#include <algorithm>
+#include <cstdlib>
+#include <string>
+
+#include "common.cuh"
+#include "knn_seed.cuh"
+
+namespace nngp {
+namespace seed {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr uint32_t kInfBits = 0x7F800000u;
+constexpr uint32_t kTolBits = 1u << 12;  // stop the bisection within 2^12 ulp (5e-4 relative)
+
+// monotone unsigned image of a float (for atomic min / max) and back
+__device__ __forceinline__ uint32_t ord_of(float x) {
+    const uint32_t u = __float_as_uint(x);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float from_ord(uint32_t o) {
+    return __uint_as_float((o & 0x80000000u) ? (o & 0x7FFFFFFFu) : ~o);
+}
+
+__global__ void __launch_bounds__(kThreads) bounds_kernel(const float *__restrict__ xs, int64_t n, int d, int dp,
+                                                          uint32_t *__restrict__ lo, uint32_t *__restrict__ hi) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t i0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    for (int f = 0; f < d; ++f) {
+        uint32_t mn = 0xFFFFFFFFu, mx = 0u;
+        for (int64_t i = i0; i < n; i += stride) {
+            const float v = xs[i * dp + f];
+            if (isfinite(v)) {
+                const uint32_t o = ord_of(v);
+                mn = min(mn, o);
+                mx = max(mx, o);
+            }
+        }
+        mn = __reduce_min_sync(0xFFFFFFFFu, mn);
+        mx = __reduce_max_sync(0xFFFFFFFFu, mx);
+        if ((threadIdx.x & 31) == 0) {
+            atomicMin(lo + f, mn);
+            atomicMax(hi + f, mx);
+        }
+    }
+}
+
+// Morton key of every point on grid `curve` (0: cells aligned with the bounds; 1: shifted by
+// 1.23 % of the extent in every dimension); idx = 0..n-1.
+__global__ void __launch_bounds__(kThreads) keys_kernel(const float *__restrict__ xs, int64_t n, int d, int dp,
+                                                        const uint32_t *__restrict__ lo, const uint32_t *__restrict__ hi,
+                                                        int bits, int curve, uint64_t *__restrict__ keys,
+                                                        int32_t *__restrict__ idx) {
+    float span = 0.f;
+    for (int f = 0; f < d; ++f) {
+        if (hi[f] >= lo[f]) span = fmaxf(span, from_ord(hi[f]) - from_ord(lo[f]));
+    }
+    const float cells = (float)(1u << bits);
+    const float scale = span > 0.f && isfinite(span) ? 0.97f * cells / span : 0.f;
+    const float shift = curve == 0 ? 0.f : 0.0123f * cells;
+    const uint32_t qmax = (1u << bits) - 1u;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        uint64_t key = 0;
+        for (int f = 0; f < d; ++f) {
+            const float base = hi[f] >= lo[f] ? from_ord(lo[f]) : 0.f;
+            const float t = (xs[i * dp + f] - base) * scale + shift;
+            const uint32_t q = t > 0.f ? (t < (float)qmax ? (uint32_t)t : qmax) : 0u;  // NaN -> 0
+            for (int b = 0; b < bits; ++b) key |= (uint64_t)((q >> b) & 1u) << (b * d + f);
+        }
+        keys[i] = key;
+        idx[i] = (int32_t)i;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) inverse_kernel(const int32_t *__restrict__ order, int64_t n,
+                                                           int32_t *__restrict__ pos) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+        pos[order[k]] = (int32_t)k;
+}
+
+// Squared distance bits of refs j and the query coordinates qv in the search's exact arithmetic:
+// ((x_j0 - q0)^2 + (x_j1 - q1)^2) + ..., every step rounded, over the D padded features.
+template <int D>
+__device__ __forceinline__ uint32_t dist_bits(const float *__restrict__ xs, int dp, int64_t j, const float (&qv)[D]) {
+    constexpr int V = (D + 3) / 4;
+    const float4 *r4 = reinterpret_cast<const float4 *>(xs + j * dp);
+    float r[4 * V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+        const float4 t = __ldg(r4 + v);
+        r[4 * v] = t.x;
+        r[4 * v + 1] = t.y;
+        r[4 * v + 2] = t.z;
+        r[4 * v + 3] = t.w;
+    }
+    const float t0 = sub_rn(r[0], qv[0]);
+    float d2 = mul_rn(t0, t0);
+#pragma unroll
+    for (int f = 1; f < D; ++f) {
+        const float t = sub_rn(r[f], qv[f]);
+        d2 = add_rn(d2, mul_rn(t, t));
+    }
+    return __float_as_uint(d2);  // NaN bits lie above kInfBits and are never counted
+}
+
+// One warp per point (taken in curve-0 order).  Lane values: squared-distance bits of the refs
+// j < i in the window [p - W, p + W) of each curve (curve 1 skips refs inside curve 0's window,
+// so every ref counts once); 0xFFFFFFFF for the other slots.  The row's seed is the m-th
+// smallest value (bisection on the bit patterns, stopped within kTolBits above it), or +inf.
+template <int D, int VPL>
+__global__ void __launch_bounds__(kThreads) seed_kernel(const float *__restrict__ xs, int64_t n, int dp, int m,
+                                                        const int32_t *__restrict__ order0,
+                                                        const int32_t *__restrict__ pos0,
+                                                        const int32_t *__restrict__ order1,
+                                                        const int32_t *__restrict__ pos1,
+                                                        float *__restrict__ seeds) {
+    constexpr int W = VPL * 16;
+    constexpr unsigned FULL = 0xFFFFFFFFu;
+    const int lane = threadIdx.x & 31;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t k = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; k < n; k += nwarps) {
+        const int64_t i = order0[k];
+        if (i < m) {  // fewer than m earlier points: no bound
+            if (lane == 0) seeds[i] = __uint_as_float(kInfBits);
+            continue;
+        }
+        float qv[D];
+#pragma unroll
+        for (int f = 0; f < D; ++f) qv[f] = xs[i * dp + f];
+        uint32_t v[2 * VPL];
+#pragma unroll
+        for (int t = 0; t < VPL; ++t) {
+            const int64_t pk = k - W + lane + 32 * t;
+            uint32_t val = 0xFFFFFFFFu;
+            if (pk >= 0 && pk < n) {
+                const int64_t j = order0[pk];
+                if (j < i) val = dist_bits<D>(xs, dp, j, qv);
+            }
+            v[t] = val;
+        }
+        const int64_t p1 = pos1[i];
+#pragma unroll
+        for (int t = 0; t < VPL; ++t) {
+            const int64_t pk = p1 - W + lane + 32 * t;
+            uint32_t val = 0xFFFFFFFFu;
+            if (pk >= 0 && pk < n) {
+                const int64_t j = order1[pk];
+                if (j < i) {
+                    const int64_t pj = pos0[j];
+                    if (pj < k - W || pj >= k + W) val = dist_bits<D>(xs, dp, j, qv);
+                }
+            }
+            v[VPL + t] = val;
+        }
+        auto count_le = [&](uint32_t bound) -> int {
+            int c = 0;
+#pragma unroll
+            for (int e = 0; e < 2 * VPL; ++e) c += v[e] <= bound ? 1 : 0;
+            return (int)__reduce_add_sync(FULL, (unsigned)c);
+        };
+        uint32_t res = kInfBits;
+        if (count_le(kInfBits) >= m) {
+            uint32_t mn = 0xFFFFFFFFu, mx = 0u;
+#pragma unroll
+            for (int e = 0; e < 2 * VPL; ++e) {
+                if (v[e] <= kInfBits) {
+                    mn = min(mn, v[e]);
+                    mx = max(mx, v[e]);
+                }
+            }
+            uint32_t lo = __reduce_min_sync(FULL, mn), hi = __reduce_max_sync(FULL, mx);  // count_le(hi) >= m
+            while (hi - lo > kTolBits) {  // invariant: count_le(hi) >= m; warp-uniform
+                const uint32_t mid = lo + ((hi - lo) >> 1);
+                if (count_le(mid) >= m) hi = mid;
+                else lo = mid + 1;
+            }
+            res = hi;
+        }
+        if (lane == 0) seeds[i] = __uint_as_float(res);
+    }
+}
+
+struct Layout {
+    size_t keys_a, keys_b, idx0_a, idx0_b, idx1_a, idx1_b, pos0, pos1, bounds, cub, cub_bytes, total;
+};
+
+Layout layout(int64_t n) {
+    Layout L{};
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        const size_t o = off;
+        off = align_up(off + bytes, 256);
+        return o;
+    };
+    L.keys_a = take((size_t)n * 8);
+    L.keys_b = take((size_t)n * 8);
+    L.idx0_a = take((size_t)n * 4);
+    L.idx0_b = take((size_t)n * 4);
+    L.idx1_a = take((size_t)n * 4);
+    L.idx1_b = take((size_t)n * 4);
+    L.pos0 = take((size_t)n * 4);
+    L.pos1 = take((size_t)n * 4);
+    L.bounds = take(2 * 256 * 4);
+    L.cub_bytes = align_up((size_t)(4u << 20) + (size_t)n / 2, 256);  // radix-sort scratch budget
+    L.cub = take(L.cub_bytes);
+    L.total = off + 256;
+    return L;
+}
+
+template <int D, int VPL>
+void launch_seed(int grid, const float *xs, int64_t n, int dp, int m, const int32_t *o0, const int32_t *p0,
+                 const int32_t *o1, const int32_t *p1, float *seeds, cudaStream_t stream) {
+    seed_kernel<D, VPL><<<grid, kThreads, 0, stream>>>(xs, n, dp, m, o0, p0, o1, p1, seeds);
+}
+
+template <int VPL>
+bool dispatch_seed(int D, int grid, const float *xs, int64_t n, int dp, int m, const int32_t *o0, const int32_t *p0,
+                   const int32_t *o1, const int32_t *p1, float *seeds, cudaStream_t stream) {
+    switch (D) {
+        case 1: launch_seed<1, VPL>(grid, xs, n, dp, m, o0, p0, o1, p1, seeds, stream); return true;
+        case 2: launch_seed<2, VPL>(grid, xs, n, dp, m, o0, p0, o1, p1, seeds, stream); return true;
+        case 3: launch_seed<3, VPL>(grid, xs, n, dp, m, o0, p0, o1, p1, seeds, stream); return true;
+        case 4: launch_seed<4, VPL>(grid, xs, n, dp, m, o0, p0, o1, p1, seeds, stream); return true;
+        case 5: launch_seed<5, VPL>(grid, xs, n, dp, m, o0, p0, o1, p1, seeds, stream); return true;
+        case 6: launch_seed<6, VPL>(grid, xs, n, dp, m, o0, p0, o1, p1, seeds, stream); return true;
+        case 7: launch_seed<7, VPL>(grid, xs, n, dp, m, o0, p0, o1, p1, seeds, stream); return true;
+        case 8: launch_seed<8, VPL>(grid, xs, n, dp, m, o0, p0, o1, p1, seeds, stream); return true;
+        case 12: launch_seed<12, VPL>(grid, xs, n, dp, m, o0, p0, o1, p1, seeds, stream); return true;
+        case 16: launch_seed<16, VPL>(grid, xs, n, dp, m, o0, p0, o1, p1, seeds, stream); return true;
+        case 20: launch_seed<20, VPL>(grid, xs, n, dp, m, o0, p0, o1, p1, seeds, stream); return true;
+        case 24: launch_seed<24, VPL>(grid, xs, n, dp, m, o0, p0, o1, p1, seeds, stream); return true;
+    }
+    return false;
+}
+
+int grid_of(int64_t work) {
+    return (int)std::max<int64_t>(1, std::min<int64_t>((work + kThreads - 1) / kThreads, (int64_t)kNumSMsB200 * 8));
+}
+
+}  // namespace
+
+size_t workspace(int64_t n) { return n < kMinPoints ? 0 : layout(n).total; }
+
+int window() {
+    const char *env = std::getenv("NNGP_KNN_SEED_W");
+    if (!env) return 256;
+    const int w = std::atoi(env);
+    return (w == 0 || w == 128 || w == 256) ? w : 256;
+}
+
+nngp_status prefix_seeds(const float *xs, int64_t n, int d, int D, int dp, int m, void *ws, size_t ws_bytes,
+                         float *seeds, cudaStream_t stream) {
+    const int W = window();
+    if (W == 0 || n < kMinPoints || m < 1 || d < 1 || d > 24 || D < d || dp % 4 != 0 || dp < D)
+        return fail(NNGP_ERR_UNSUPPORTED, "knn seeds: shape outside the seeded search");
+    const Layout L = layout(n);
+    if (!ws || ws_bytes < L.total) return fail(NNGP_ERR_WORKSPACE, "knn seeds: workspace too small");
+    char *base = reinterpret_cast<char *>(align_up(reinterpret_cast<uintptr_t>(ws), 256));
+    auto at = [&](size_t off) { return reinterpret_cast<void *>(base + off); };
+    uint64_t *keys_a = static_cast<uint64_t *>(at(L.keys_a)), *keys_b = static_cast<uint64_t *>(at(L.keys_b));
+    int32_t *idx[2][2] = {{static_cast<int32_t *>(at(L.idx0_a)), static_cast<int32_t *>(at(L.idx0_b))},
+                          {static_cast<int32_t *>(at(L.idx1_a)), static_cast<int32_t *>(at(L.idx1_b))}};
+    int32_t *pos[2] = {static_cast<int32_t *>(at(L.pos0)), static_cast<int32_t *>(at(L.pos1))};
+    uint32_t *lo = static_cast<uint32_t *>(at(L.bounds)), *hi = lo + 256;
+    const int bits = std::min(10, 64 / d);
+
+    NNGP_CUDA_TRY(cudaMemsetAsync(lo, 0xFF, 256 * 4, stream));
+    NNGP_CUDA_TRY(cudaMemsetAsync(hi, 0x00, 256 * 4, stream));
+    bounds_kernel<<<grid_of(n), kThreads, 0, stream>>>(xs, n, d, dp, lo, hi);
+    NNGP_CUDA_TRY(cudaGetLastError());
+    const int32_t *order[2] = {nullptr, nullptr};
+    for (int c = 0; c < 2; ++c) {
+        keys_kernel<<<grid_of(n), kThreads, 0, stream>>>(xs, n, d, dp, lo, hi, bits, c, keys_a, idx[c][0]);
+        NNGP_CUDA_TRY(cudaGetLastError());
+        cub::DoubleBuffer<uint64_t> dk(keys_a, keys_b);
+        cub::DoubleBuffer<int32_t> dv(idx[c][0], idx[c][1]);
+        size_t need = 0;
+        NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, need, dk, dv, (int)n, 0, bits * d, stream));
+        if (need > L.cub_bytes)
+            return fail(NNGP_ERR_WORKSPACE, "knn seeds: radix-sort scratch " + std::to_string(need) +
+                                                " bytes exceeds the budget");
+        size_t have = L.cub_bytes;
+        NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(at(L.cub), have, dk, dv, (int)n, 0, bits * d, stream));
+        order[c] = dv.Current();
+        inverse_kernel<<<grid_of(n), kThreads, 0, stream>>>(order[c], n, pos[c]);
+        NNGP_CUDA_TRY(cudaGetLastError());
+    }
+    const int grid = (int)std::min<int64_t>((n + kThreads / 32 - 1) / (kThreads / 32), (int64_t)kNumSMsB200 * 16);
+    const bool ok = W == 128 ? dispatch_seed<8>(D, grid, xs, n, dp, m, order[0], pos[0], order[1], pos[1], seeds, stream)
+                             : dispatch_seed<16>(D, grid, xs, n, dp, m, order[0], pos[0], order[1], pos[1], seeds,
+                                                 stream);
+    if (!ok) return fail(NNGP_ERR_UNSUPPORTED, "knn seeds: no kernel for D = " + std::to_string(D));
+    NNGP_CUDA_TRY(cudaGetLastError());
+    return NNGP_OK;
+}
+
+}  // namespace seed
+}  // namespace nngp

@@ -272,6 +272,7 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
                                                          const float *__restrict__ qs,
                                                          const double *__restrict__ acc,
                                                          const unsigned int *__restrict__ r2max_bits,
+                                                         const float *__restrict__ seeds,
                                                          int *__restrict__ work_counter, int64_t n_query,
                                                          int64_t n_ref, int has_cut, int64_t cut, int m,
                                                          int32_t *__restrict__ out, int32_t *__restrict__ flags) {
@@ -455,8 +456,10 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
             __syncwarp();
             // rows past the last query never take candidates
             const float tq_off = active ? pos_inf<float>() : neg_inf<float>();
-            float tq = tq_off;                 // screening threshold of this row
-            float worst = pos_inf<float>();    // distance of this row's heap root (m-th best so far)
+            // a proven upper bound of the row's m-th distance (seeded prefix search), else +inf
+            const float seed_r = (active && seeds) ? seeds[q] : pos_inf<float>();
+            float worst = seed_r;  // min(seed, distance of the heap root = m-th best so far)
+            float tq = fminf((worst - nq) + eps, tq_off);  // screening threshold of this row
             int qcount = 0;
             // insert the queued entries: 32 at a time, each lane into its entry's row heap; entries
             // of one row go in one after the other (match_any groups), so any order gives the same heap set
@@ -480,7 +483,7 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
                     }
                 }
                 qcount = 0;
-                worst = __uint_as_float((uint32_t)(heap[lane * HS] >> 32));
+                worst = fminf(__uint_as_float((uint32_t)(heap[lane * HS] >> 32)), seed_r);
                 tq = fminf((worst - nq) + eps, tq_off);
             };
 

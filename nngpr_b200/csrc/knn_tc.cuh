@@ -10,8 +10,8 @@ namespace tc {
 constexpr int kTcRefTile = 128;    // refs per tile (UMMA N)
 constexpr int kTcQueryTile = 128;  // queries per tile (UMMA M)
 
-using TcFn = void (*)(const unsigned char *, const float *, const double *, const unsigned int *, int *, int64_t,
-                      int64_t, int, int64_t, int, int32_t *, int32_t *);
+using TcFn = void (*)(const unsigned char *, const float *, const double *, const unsigned int *, const float *, int *,
+                      int64_t, int64_t, int, int64_t, int, int32_t *, int32_t *);
 using TcBuildFn = void (*)(const float *, int64_t, int64_t, const double *, unsigned char *, unsigned int *);
 
 struct TcVariant {

@@ -1,0 +1,78 @@
+"""Seeded prefix search: the fit step's search (ref = query, cut 0) starts every row from a
+proven upper bound of its m-th distance, taken from the row's neighbours along two Morton
+orders.  The lists must be bit-identical to the unseeded search (NNGP_KNN_SEED_W=0) and to the
+oracle; only the amount of candidate work changes."""
+import numpy as np
+import pytest
+import torch
+
+from nngpr_b200 import ops
+from oracle import nngp_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def search(monkeypatch, x, m, ls, window):
+    monkeypatch.setenv('NNGP_KNN_SEED_W', str(window))
+    t = torch.from_numpy(np.ascontiguousarray(x, dtype=np.float32)).cuda()
+    flags = ops.new_flags(t.device)
+    out = ops.knn(t, t, m, 0, ls, flags=flags)
+    assert int(flags.item()) == 0
+    return out.cpu().numpy()
+
+
+def check_rows(x, got, m, ls, rng, k=200):
+    rows = np.sort(rng.choice(x.shape[0], k, replace=False))
+    rows = np.union1d(rows, np.arange(x.shape[0] - 50, x.shape[0]))  # the longest rows too
+    want = O.knn(x, x[rows], m, 0, ls, query_index=rows)
+    assert np.array_equal(got[rows], want)
+
+
+@pytest.mark.parametrize('d', [1, 2, 3, 5, 8, 12, 16, 20, 24])
+@pytest.mark.parametrize('m', [1, 16, 32])
+def test_seeded_lists_equal_unseeded_and_oracle(monkeypatch, d, m):
+    rng = np.random.default_rng(1000 * d + m)
+    n = 20000
+    x = rng.uniform(-1, 1, (n, d))
+    ls = rng.uniform(0.3, 2.0, d) if d % 2 else 0.4
+    plain = search(monkeypatch, x, m, ls, 0)
+    for w in (128, 256):
+        assert np.array_equal(search(monkeypatch, x, m, ls, w), plain)
+    check_rows(x, plain, m, ls, rng)
+
+
+def test_seeded_ties_duplicates_outlier_and_clusters(monkeypatch):
+    """Integer lattice with many duplicates (exact ties, lower index first); one far outlier
+    that squeezes every other point into a few Morton cells; a 16-d Gaussian mixture."""
+    rng = np.random.default_rng(3)
+    x = rng.integers(0, 6, (30000, 3)).astype(np.float64)
+    a = search(monkeypatch, x, 32, None, 256)
+    assert np.array_equal(a, search(monkeypatch, x, 32, None, 0))
+    check_rows(x, a, 32, None, rng)
+    y = rng.normal(size=(25000, 3))
+    y[12345] = 1e6
+    b = search(monkeypatch, y, 16, 0.5, 256)
+    assert np.array_equal(b, search(monkeypatch, y, 16, 0.5, 0))
+    check_rows(y, b, 16, 0.5, rng)
+    means = rng.uniform(-3, 3, (64, 16))
+    z = means[rng.integers(0, 64, 30000)] + 0.5 * rng.normal(size=(30000, 16))
+    c = search(monkeypatch, z, 32, 0.8, 256)
+    assert np.array_equal(c, search(monkeypatch, z, 32, 0.8, 0))
+    check_rows(z, c, 32, 0.8, rng, k=100)
+
+
+def test_seeding_engages_only_on_the_prefix_self_search(monkeypatch, capfd):
+    monkeypatch.setenv('NNGP_KNN_DEBUG', '1')
+    rng = np.random.default_rng(4)
+    x = rng.uniform(0, 1, (20000, 3))
+    search(monkeypatch, x, 32, 0.3, 256)
+    assert 'seeded=1' in capfd.readouterr().err
+    search(monkeypatch, x, 32, 0.3, 0)
+    assert 'seeded=0' in capfd.readouterr().err
+    monkeypatch.setenv('NNGP_KNN_SEED_W', '256')
+    t = torch.from_numpy(x.astype(np.float32)).cuda()
+    ops.knn(t, t[:5000].clone(), 32, None, 0.3)  # predict-style search: no seeds
+    assert 'seeded=0' in capfd.readouterr().err
+    small = torch.from_numpy(x[:5000].astype(np.float32)).cuda()
+    ops.knn(small, small, 32, 0, 0.3)  # below the size where seeding pays
+    assert 'seeded=0' in capfd.readouterr().err
