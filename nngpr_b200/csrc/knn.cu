@@ -37,6 +37,7 @@
 #include <type_traits>
 
 #include "common.cuh"
+#include "knn_prune.cuh"
 #include "knn_seed.cuh"
 #include "knn_tc.cuh"
 
@@ -512,7 +513,8 @@ struct KnnPlan {
     int dp = 0;  // padded row length of the scaled arrays
     int64_t n_ref_pad = 0;
     size_t off_ref = 0, off_q = 0, off_rec = 0, off_acc = 0, off_r2 = 0, off_ctr = 0, off_ldist = 0, off_lidx = 0,
-           off_seed = 0, off_seed_ws = 0, seed_ws_bytes = 0, total = 0;
+           off_seed = 0, off_seed_ws = 0, seed_ws_bytes = 0, off_tiles2 = 0, off_prune_ws = 0, prune_ws_bytes = 0,
+           total = 0;
     ScreenVariant v{};
     tc::TcVariant tv{};
 };
@@ -557,6 +559,13 @@ KnnPlan make_plan(int64_t n_ref, int64_t n_query, int d, int m, bool same) {
             p.off_seed_ws = off;
             p.seed_ws_bytes = seed::workspace(n_ref);
             off = align_up(off + p.seed_ws_bytes, 256);
+            if (prune::workspace(n_ref, d, p.tv.rows_per_item) > 0) {  // pruned search: curve-order tiles + lists
+                p.off_tiles2 = align_up(off, 1024);
+                off = align_up(p.off_tiles2 + rec_bytes, 1024);
+                p.off_prune_ws = off;
+                p.prune_ws_bytes = prune::workspace(n_ref, d, p.tv.rows_per_item);
+                off = align_up(off + p.prune_ws_bytes, 256);
+            }
         }
     } else {
         p.off_ldist = off;
@@ -625,37 +634,94 @@ nngp_status knn_impl(const T *ref, int64_t n_ref, const T *query, int64_t n_quer
             NNGP_CUDA_TRY(cudaMemsetAsync(base + p.off_acc, 0, p.off_ctr + 16 - p.off_acc, stream));
             center_sum_kernel<<<grid_for(n_ref), 256, 0, stream>>>(refs, n_ref, p.dp, d, acc);
             NNGP_CUDA_TRY(cudaGetLastError());
-            p.tv.build<<<grid_for(p.n_ref_pad), 256, 0, stream>>>(refs, n_ref, p.n_ref_pad, acc, tiles, r2);
+            const int32_t *no_perm = nullptr;
+            p.tv.build<<<grid_for(p.n_ref_pad), 256, 0, stream>>>(refs, n_ref, p.n_ref_pad, acc, no_perm, tiles, r2);
             NNGP_CUDA_TRY(cudaGetLastError());
             NNGP_CUDA_TRY(ensure_smem_limit(reinterpret_cast<const void *>(p.tv.fn), p.tv.smem, 100));
-            const int64_t n_items = (n_query + p.tv.rows_per_item - 1) / p.tv.rows_per_item;
-            // persistent grid: the CTAs one SM holds (shared memory and TMEM sized for them) per SM;
-            // CTAs that find no SM free start late and pick up no items, nothing waits on them
-            const int per_sm = p.tv.ctas_per_sm;
-            const int grid = (int)std::min<int64_t>(n_items, (int64_t)num_sms_knn() * per_sm);
-            if (const char *dbg = std::getenv("NNGP_KNN_DEBUG"); dbg && dbg[0] == '1')
-                std::fprintf(stderr, "nngp_knn: tensor-core path d=%d m=%d items=%lld ctas/sm=%d grid=%d smem=%d seeded=%d\n",
-                             d, m, (long long)n_items, per_sm, grid, p.tv.smem,
-                             (int)(same && has_cut && cut == 0 && p.seed_ws_bytes > 0 && seed::window() > 0));
             // the prefix search of a point set over itself (the fit step) starts every row from a
             // proven bound of its m-th distance: the same lists, far fewer candidates
+            const bool seeded = same && has_cut && cut == 0 && p.seed_ws_bytes > 0 && seed::window() > 0;
             const float *seeds_c = nullptr;
-            if (same && has_cut && cut == 0 && p.seed_ws_bytes > 0 && seed::window() > 0) {
+            const int32_t *order0 = nullptr, *pos0 = nullptr;
+            const uint64_t *keys0 = nullptr;
+            if (seeded) {
                 float *sd = reinterpret_cast<float *>(base + p.off_seed);
                 nngp_status sst = seed::prefix_seeds(refs, n_ref, d, round_d(d), p.dp, m, base + p.off_seed_ws,
-                                                     p.seed_ws_bytes, sd, stream);
+                                                     p.seed_ws_bytes, sd, stream, &order0, &pos0, &keys0);
                 if (sst != NNGP_OK) return sst;
                 seeds_c = sd;
             }
-            const unsigned char *tiles_c = tiles;
+            // and, for large low-dimensional sets, visits per group of rows only the ref tiles its
+            // seeds allow (rows and refs in curve order; loose and early rows stay in index order)
+            const bool pruned = seeded && p.prune_ws_bytes > 0 && prune::enabled();
+            prune::Lists lists;
+            unsigned char *tiles_curve = reinterpret_cast<unsigned char *>(base + p.off_tiles2);
+            if (pruned) {
+                p.tv.build<<<grid_for(p.n_ref_pad), 256, 0, stream>>>(refs, n_ref, p.n_ref_pad, acc, order0,
+                                                                      tiles_curve, r2);
+                NNGP_CUDA_TRY(cudaGetLastError());
+                nngp_status pst = prune::build(refs, n_ref, d, p.dp, p.tv.rows_per_item, seed::bits(d), seeds_c,
+                                               order0, pos0, keys0, base + p.off_prune_ws, p.prune_ws_bytes, &lists,
+                                               stream);
+                if (pst != NNGP_OK) return pst;
+                if (const char *dbg = std::getenv("NNGP_KNN_DEBUG"); dbg && dbg[0] == '1') {
+                    prune::DevSizes hs[2];  // diagnostics only (synchronises the stream)
+                    int32_t total = 0;
+                    NNGP_CUDA_TRY(cudaMemcpyAsync(hs, lists.pruned, sizeof(hs), cudaMemcpyDeviceToHost, stream));
+                    NNGP_CUDA_TRY(cudaStreamSynchronize(stream));
+                    NNGP_CUDA_TRY(cudaMemcpyAsync(&total, lists.offsets + hs[0].n_items, sizeof(total),
+                                                  cudaMemcpyDeviceToHost, stream));
+                    NNGP_CUDA_TRY(cudaStreamSynchronize(stream));
+                    std::fprintf(stderr,
+                                 "nngp_knn: pruned rows=%lld groups=%lld tiles listed=%d (%.1f per group of %lld); "
+                                 "index-order rows=%lld\n",
+                                 (long long)hs[0].n_rows, (long long)hs[0].n_items, total,
+                                 (double)total / (double)std::max<int64_t>(1, hs[0].n_items),
+                                 (long long)(p.n_ref_pad / tc::kTcRefTile), (long long)hs[1].n_rows);
+                }
+            }
+            // persistent grid: the CTAs one SM holds (shared memory and TMEM sized for them) per SM;
+            // CTAs that find no SM free start late and pick up no items, nothing waits on them
+            const int per_sm = p.tv.ctas_per_sm;
             const float *q_c = qsc;
             const double *acc_c = acc;
             const unsigned int *r2_c = r2;
-            void *args[] = {(void *)&tiles_c, (void *)&q_c, (void *)&acc_c, (void *)&r2_c, (void *)&seeds_c,
-                            (void *)&ctr, (void *)&n_query, (void *)&n_ref, (void *)&has_cut, (void *)&cut,
-                            (void *)&m, (void *)&out, (void *)&flags};
-            NNGP_CUDA_TRY(cudaLaunchKernel(reinterpret_cast<const void *>(p.tv.fn), dim3(grid),
-                                           dim3(p.tv.threads), args, (size_t)p.tv.smem, stream));
+            const int32_t *none = nullptr;
+            const int64_t *no_sizes = nullptr;
+            auto launch = [&](const unsigned char *tiles_c, int64_t items_bound, const int32_t *rows_perm,
+                              const int32_t *row_off, const int64_t *dev_sizes, const int32_t *item_order,
+                              const int32_t *ref_perm, const int32_t *tile_off, const int32_t *tile_list,
+                              int *counter) -> nngp_status {
+                if (items_bound == 0) return NNGP_OK;
+                const int grid = (int)std::min<int64_t>(items_bound, (int64_t)num_sms_knn() * per_sm);
+                if (const char *dbg = std::getenv("NNGP_KNN_DEBUG"); dbg && dbg[0] == '1')
+                    std::fprintf(stderr,
+                                 "nngp_knn: tensor-core path d=%d m=%d items<=%lld ctas/sm=%d grid=%d smem=%d seeded=%d "
+                                 "pruned=%d\n",
+                                 d, m, (long long)items_bound, per_sm, grid, p.tv.smem, (int)seeded,
+                                 (int)(tile_list != nullptr));
+                void *args[] = {(void *)&tiles_c,  (void *)&q_c,      (void *)&acc_c,      (void *)&r2_c,
+                                (void *)&seeds_c,  (void *)&rows_perm, (void *)&row_off,   (void *)&dev_sizes,
+                                (void *)&item_order, (void *)&ref_perm, (void *)&tile_off, (void *)&tile_list,
+                                (void *)&counter,  (void *)&n_query,  (void *)&n_ref,      (void *)&has_cut,
+                                (void *)&cut,      (void *)&m,        (void *)&out,        (void *)&flags};
+                NNGP_CUDA_TRY(cudaLaunchKernel(reinterpret_cast<const void *>(p.tv.fn), dim3(grid), dim3(p.tv.threads),
+                                               args, (size_t)p.tv.smem, stream));
+                return NNGP_OK;
+            };
+            nngp_status lst;
+            if (pruned) {
+                const int64_t *ps = reinterpret_cast<const int64_t *>(lists.pruned);
+                const int64_t *is = reinterpret_cast<const int64_t *>(lists.index_order);
+                lst = launch(tiles_curve, lists.max_groups, lists.rows, lists.row_off, ps, lists.item_order, order0,
+                             lists.offsets, lists.tiles, ctr + 1);
+                if (lst != NNGP_OK) return lst;
+                lst = launch(tiles, lists.max_index_items, lists.rows, none, is, none, none, none, none, ctr);
+            } else {
+                const int64_t items = (n_query + p.tv.rows_per_item - 1) / p.tv.rows_per_item;
+                lst = launch(tiles, items, none, none, no_sizes, none, none, none, none, ctr);
+            }
+            if (lst != NNGP_OK) return lst;
         }
     } else if (p.path == KnnPath::Simt) {
         if constexpr (std::is_same<T, float>::value) {

@@ -1,0 +1,483 @@
+// Pruned prefix search: which rows go together and which ref tiles each group has to visit.
+//
+// The prefix search (every point i against the points j < i, calc_nn with ref_cut_index = 0,
+// nngpr/cuda_kernel_accelerators.py:663-743) is brute force in the reference: n^2 / 2 pairs.
+// With every row's seed (a proven upper bound of its m-th distance, knn_seed.cu) most pairs can
+// be proven irrelevant in bulk: with points in space-filling-curve order, 128 consecutive points
+// (a ref tile) and a group of rows are compact regions with small bounding boxes, and a ref tile
+// whose box lies farther from the group's box than the largest seed of the group cannot hold a
+// neighbour of any row.  The tensor-core search then streams, per group, only the listed tiles
+// (d = 3, n = 434,874: about 125 tiles per group of 128 rows instead of about 1,700 on average)
+// and checks j < i per candidate.
+//
+// Exactness: the FP32 squared distance the search compares, ((t0^2 + t1^2) + ...) with every
+// step rounded and t_f = fl(x_jf - x_if), is at least (1 - u)^(D + 2) times the exact squared
+// distance of the same FP32 coordinates (all terms are non-negative), minus at most
+// (D + 2) 2^-150 from subnormal rounding; the box distance is at most the exact distance.  A tile
+// is dropped only if box_distance^2 (1 - gamma) - 1e-37 > seed, gamma = (D + 3) 2^-23, so every
+// ref in it has an FP32 distance above every row's bound and could never enter a list.
+//
+// Rows: band = floor(log2(n / i)) groups rows whose prefixes differ by less than a factor of
+// two, hence seeds of similar size.  A row whose seed exceeds 16 times its band's geometric mean
+// (its window held few earlier points) would inflate its group's reach, so it goes to the
+// index-order launch with the rows below n / 8, where it costs only its prefix.
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdlib>
+#include <string>
+
+#include "common.cuh"
+#include "knn_prune.cuh"
+
+namespace nngp {
+namespace prune {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kBands = 4;            // i >= n / 8: bands 0..2 (3 only at rounding edges)
+constexpr int kLooseLog2Q = 4 * 256;  // seed > 16 x band geometric mean (log2 in 1/256 units)
+constexpr uint64_t kIndexOrderTag = 15ull << 60;
+
+__device__ __forceinline__ int band_of(int64_t i, int64_t n) {
+    int b = 0;
+    while (b < kBands - 1 && (i << (b + 1)) < n) ++b;  // i < n / 2^(b + 1)
+    return b;
+}
+
+// log2 of a finite non-negative seed in units of 1/256, clamped below (zero seeds: duplicates)
+__device__ __forceinline__ long long log2q(float tau) {
+    return llrint(fmax(log2((double)tau), -160.0) * 256.0);
+}
+
+__global__ void __launch_bounds__(kThreads) tile_box_kernel(const float *__restrict__ xs, int64_t n, int d, int dp,
+                                                            const int32_t *__restrict__ order0, int64_t n_tiles,
+                                                            float *__restrict__ tlo, float *__restrict__ thi,
+                                                            int32_t *__restrict__ tmin) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n_tiles;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k0 = t * kTileRefs, k1 = min(n, k0 + kTileRefs);
+        int32_t mi = INT32_MAX;
+        for (int64_t k = k0; k < k1; ++k) mi = min(mi, order0[k]);
+        tmin[t] = mi;
+        for (int f = 0; f < d; ++f) {
+            float lo = pos_inf<float>(), hi = neg_inf<float>();  // NaN coordinates are skipped
+            for (int64_t k = k0; k < k1; ++k) {
+                const float v = xs[(int64_t)order0[k] * dp + f];
+                lo = fminf(lo, v);
+                hi = fmaxf(hi, v);
+            }
+            tlo[t * d + f] = lo;
+            thi[t * d + f] = hi;
+        }
+    }
+}
+
+// Per band: sum of log2q(seed) over the finite seeds of rows >= early, and their count
+// (integer sums: the result does not depend on the order of the atomics).
+__global__ void __launch_bounds__(kThreads) band_stats_kernel(int64_t n, int64_t early, const float *__restrict__ seeds,
+                                                              unsigned long long *__restrict__ sum,
+                                                              unsigned long long *__restrict__ cnt) {
+    long long s[kBands] = {0, 0, 0, 0};
+    unsigned long long c[kBands] = {0, 0, 0, 0};
+    for (int64_t i = early + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const float tau = seeds[i];
+        if (!isinf(tau)) {
+            const int b = band_of(i, n);
+            s[b] += log2q(tau);
+            c[b] += 1;
+        }
+    }
+#pragma unroll
+    for (int b = 0; b < kBands; ++b) {
+        long long sv = s[b];
+        unsigned long long cv = c[b];
+        for (int o = 16; o > 0; o >>= 1) {
+            sv += __shfl_xor_sync(0xFFFFFFFFu, sv, o);
+            cv += __shfl_xor_sync(0xFFFFFFFFu, cv, o);
+        }
+        if ((threadIdx.x & 31) == 0 && cv > 0) {
+            atomicAdd(sum + b, (unsigned long long)sv);  // two's complement: signed sums wrap correctly
+            atomicAdd(cnt + b, cv);
+        }
+    }
+}
+
+// Sort keys: pruned rows (band << 60 | curve position), the others (15 << 60 | index); counts
+// of pruned rows per band and in total.
+__global__ void __launch_bounds__(kThreads) classify_kernel(int64_t n, int64_t early, const float *__restrict__ seeds,
+                                                            const int32_t *__restrict__ pos0,
+                                                            const unsigned long long *__restrict__ sum,
+                                                            const unsigned long long *__restrict__ cnt,
+                                                            uint64_t *__restrict__ keys, int32_t *__restrict__ vals,
+                                                            unsigned long long *__restrict__ pruned_cnt) {
+    unsigned long long c[kBands] = {0, 0, 0, 0};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        bool pruned = false;
+        int b = 0;
+        if (i >= early) {
+            b = band_of(i, n);
+            const float tau = seeds[i];
+            if (!isinf(tau) && cnt[b] > 0) {
+                const long long mean = (long long)sum[b] / (long long)cnt[b];
+                pruned = log2q(tau) <= mean + kLooseLog2Q;
+            }
+        }
+        keys[i] = pruned ? ((uint64_t)b << 60 | (uint32_t)pos0[i]) : (kIndexOrderTag | (uint64_t)i);
+        vals[i] = (int32_t)i;
+        if (pruned) c[b] += 1;
+    }
+#pragma unroll
+    for (int b = 0; b < kBands; ++b) {
+        unsigned long long cv = c[b];
+        for (int o = 16; o > 0; o >>= 1) cv += __shfl_xor_sync(0xFFFFFFFFu, cv, o);
+        if ((threadIdx.x & 31) == 0 && cv > 0) atomicAdd(pruned_cnt + b, cv);
+    }
+}
+
+// Octree cell level of band b: cells of 2^(d L) per level hold about 256 of the band's pruned
+// rows, so a band has at most cnt / 256 cells (at least one).
+__device__ __forceinline__ int cell_level(unsigned long long cnt, int d, int bits) {
+    int L = 0;
+    while (L < bits && (cnt >> (d * (L + 1))) >= 256ull) ++L;
+    return L;
+}
+
+// headpos[r] = r where a new (band, cell) segment starts among the pruned rows, else 0.
+__global__ void __launch_bounds__(kThreads) segment_kernel(int64_t n, const uint64_t *__restrict__ skeys,
+                                                           const int32_t *__restrict__ rows,
+                                                           const int32_t *__restrict__ pos0,
+                                                           const uint64_t *__restrict__ keys0,
+                                                           const unsigned long long *__restrict__ pruned_cnt, int d,
+                                                           int bits, int32_t *__restrict__ headpos) {
+    unsigned long long total = 0;
+    for (int b = 0; b < kBands; ++b) total += pruned_cnt[b];
+    auto cell_of = [&](int64_t r, int b) -> uint64_t {
+        const int L = cell_level(pruned_cnt[b], d, bits);
+        const int shift = d * (bits - L);
+        const uint64_t key = keys0[pos0[rows[r]]];
+        return shift >= 64 ? 0ull : key >> shift;
+    };
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+        int32_t h = 0;
+        if (r < (int64_t)total) {
+            const int b = (int)(skeys[r] >> 60);
+            bool head = r == 0;
+            if (!head) {
+                const int bp = (int)(skeys[r - 1] >> 60);
+                head = bp != b || cell_of(r - 1, b) != cell_of(r, b);
+            }
+            h = head ? (int32_t)r : 0;
+        }
+        headpos[r] = h;
+    }
+}
+
+// gh[r] = 1 where a group starts (every G rows of a segment), for the pruned rows.
+__global__ void __launch_bounds__(kThreads) group_head_kernel(int64_t n, const int32_t *__restrict__ seg_start,
+                                                              const unsigned long long *__restrict__ pruned_cnt, int G,
+                                                              int32_t *__restrict__ gh) {
+    unsigned long long total = 0;
+    for (int b = 0; b < kBands; ++b) total += pruned_cnt[b];
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x)
+        gh[r] = (r < (int64_t)total && (r - seg_start[r]) % G == 0) ? 1 : 0;
+}
+
+__global__ void __launch_bounds__(kThreads) row_off_kernel(int64_t n, const int32_t *__restrict__ gh,
+                                                           const int32_t *__restrict__ gid,
+                                                           int32_t *__restrict__ row_off) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x)
+        if (gh[r]) row_off[gid[r]] = (int32_t)r;
+}
+
+__global__ void sizes_kernel(int64_t n, int G, const int32_t *__restrict__ gh, const int32_t *__restrict__ gid,
+                             const unsigned long long *__restrict__ pruned_cnt, int32_t *__restrict__ row_off,
+                             DevSizes *__restrict__ pruned, DevSizes *__restrict__ index_order) {
+    unsigned long long total = 0;
+    for (int b = 0; b < kBands; ++b) total += pruned_cnt[b];
+    const int64_t n_groups = (int64_t)gid[n - 1] + gh[n - 1];
+    row_off[n_groups] = (int32_t)total;
+    pruned->first_row = 0;
+    pruned->n_rows = (int64_t)total;
+    pruned->n_items = n_groups;
+    index_order->first_row = (int64_t)total;
+    index_order->n_rows = n - (int64_t)total;
+    index_order->n_items = (n - (int64_t)total + G - 1) / G;
+}
+
+__global__ void __launch_bounds__(kThreads) group_box_kernel(const float *__restrict__ xs, int d, int dp,
+                                                             const int32_t *__restrict__ rows,
+                                                             const int32_t *__restrict__ row_off,
+                                                             const DevSizes *__restrict__ pruned,
+                                                             const float *__restrict__ seeds, float *__restrict__ glo,
+                                                             float *__restrict__ ghi, float *__restrict__ gtau,
+                                                             int32_t *__restrict__ glim) {
+    const int64_t n_groups = pruned->n_items;
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n_groups;
+         g += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r0 = row_off[g], r1 = row_off[g + 1];
+        float tau = 0.f;
+        int32_t lim = -1;
+        for (int64_t r = r0; r < r1; ++r) {
+            const int32_t i = rows[r];
+            tau = fmaxf(tau, seeds[i]);
+            lim = max(lim, i);
+        }
+        gtau[g] = tau;
+        glim[g] = lim;  // refs j < lim can serve some row of the group
+        for (int f = 0; f < d; ++f) {
+            float lo = pos_inf<float>(), hi = neg_inf<float>();
+            for (int64_t r = r0; r < r1; ++r) {
+                const float v = xs[(int64_t)rows[r] * dp + f];
+                lo = fminf(lo, v);
+                hi = fmaxf(hi, v);
+            }
+            glo[g * d + f] = lo;
+            ghi[g * d + f] = hi;
+        }
+    }
+}
+
+struct Boxes {
+    const float *tlo, *thi, *glo, *ghi, *gtau;
+    const int32_t *tmin, *glim;
+    int d;
+    double gamma;
+};
+
+// May ref tile t hold a neighbour of a row of group g?
+__device__ __forceinline__ bool tile_needed(const Boxes &b, int64_t g, int64_t t) {
+    if (b.tmin[t] >= b.glim[g]) return false;  // every ref of the tile comes after every row
+    const double tau = (double)b.gtau[g];
+    if (isinf(tau)) return true;
+    double lb = 0.0;
+    for (int f = 0; f < b.d; ++f) {
+        const double gap = fmax(0.0, fmax((double)b.tlo[t * b.d + f] - (double)b.ghi[g * b.d + f],
+                                          (double)b.glo[g * b.d + f] - (double)b.thi[t * b.d + f]));  // NaN -> 0
+        lb += gap * gap;
+    }
+    return !(lb * (1.0 - b.gamma) - 1e-37 > tau);
+}
+
+// One warp per group: counts[g] = tiles needed (0 for the slots past the groups), and the
+// sort key of the group's place in the work order (longest list first).
+__global__ void __launch_bounds__(kThreads) count_kernel(Boxes b, const DevSizes *__restrict__ pruned,
+                                                         int64_t max_groups, int64_t n_tiles,
+                                                         int32_t *__restrict__ counts,
+                                                         uint32_t *__restrict__ order_keys,
+                                                         int32_t *__restrict__ order_vals) {
+    const int lane = threadIdx.x & 31;
+    const int64_t n_groups = pruned->n_items;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t g = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; g < max_groups; g += nw) {
+        int c = 0;
+        if (g < n_groups)
+            for (int64_t t = lane; t < n_tiles; t += 32) c += tile_needed(b, g, t) ? 1 : 0;
+        c = (int)__reduce_add_sync(0xFFFFFFFFu, (unsigned)c);
+        if (lane == 0) {
+            counts[g] = c;
+            order_keys[g] = g < n_groups ? 0xFFFFFFFEu - (uint32_t)c : 0xFFFFFFFFu;
+            order_vals[g] = (int32_t)g;
+        }
+    }
+}
+
+// One warp per group: the needed tiles in ascending order at list[offsets[g] ..).
+__global__ void __launch_bounds__(kThreads) fill_kernel(Boxes b, const DevSizes *__restrict__ pruned, int64_t n_tiles,
+                                                        const int32_t *__restrict__ offsets,
+                                                        int32_t *__restrict__ list) {
+    const int lane = threadIdx.x & 31;
+    const int64_t n_groups = pruned->n_items;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t g = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; g < n_groups; g += nw) {
+        int64_t o = offsets[g];
+        for (int64_t base = 0; base < n_tiles; base += 32) {
+            const int64_t t = base + lane;
+            const bool need = t < n_tiles && tile_needed(b, g, t);
+            const unsigned mask = __ballot_sync(0xFFFFFFFFu, need);
+            if (need) list[o + __popc(mask & ((1u << lane) - 1u))] = (int32_t)t;
+            o += __popc(mask);
+        }
+    }
+}
+
+struct Layout {
+    int64_t n_tiles, max_groups;
+    size_t tlo, thi, tmin, stats, keys_a, keys_b, vals_a, vals_b, headpos, seg_start, gh, gid, row_off, sizes, glo,
+        ghi, gtau, glim, counts, offsets, okeys_a, okeys_b, ovals_a, ovals_b, list, cub, cub_bytes, total;
+};
+
+// Groups: segments per band <= (pruned rows of the band) / 256 or 1, groups per segment
+// <= rows / G + 1, so max_groups = n / G + n / 256 + 2 kBands bounds the count.
+Layout layout(int64_t n, int d, int G) {
+    Layout L{};
+    L.n_tiles = (n + kTileRefs - 1) / kTileRefs;
+    L.max_groups = n / G + n / 256 + 2 * kBands + 1;
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        const size_t o = off;
+        off = align_up(off + bytes, 256);
+        return o;
+    };
+    L.tlo = take((size_t)L.n_tiles * d * 4);
+    L.thi = take((size_t)L.n_tiles * d * 4);
+    L.tmin = take((size_t)L.n_tiles * 4);
+    L.stats = take(3 * kBands * 8);
+    L.keys_a = take((size_t)n * 8);
+    L.keys_b = take((size_t)n * 8);
+    L.vals_a = take((size_t)n * 4);
+    L.vals_b = take((size_t)n * 4);
+    L.headpos = take((size_t)n * 4);
+    L.seg_start = take((size_t)n * 4);
+    L.gh = take((size_t)n * 4);
+    L.gid = take((size_t)n * 4);
+    L.row_off = take((size_t)(L.max_groups + 1) * 4);
+    L.sizes = take(2 * sizeof(DevSizes));
+    L.glo = take((size_t)L.max_groups * d * 4);
+    L.ghi = take((size_t)L.max_groups * d * 4);
+    L.gtau = take((size_t)L.max_groups * 4);
+    L.glim = take((size_t)L.max_groups * 4);
+    L.counts = take((size_t)(L.max_groups + 1) * 4);
+    L.offsets = take((size_t)(L.max_groups + 1) * 4);
+    L.okeys_a = take((size_t)L.max_groups * 4);
+    L.okeys_b = take((size_t)L.max_groups * 4);
+    L.ovals_a = take((size_t)L.max_groups * 4);
+    L.ovals_b = take((size_t)L.max_groups * 4);
+    L.list = take((size_t)L.max_groups * L.n_tiles * 4);
+    L.cub_bytes = align_up((size_t)(4u << 20) + (size_t)n / 2, 256);
+    L.cub = take(L.cub_bytes);
+    L.total = off + 256;
+    return L;
+}
+
+int grid_of(int64_t threads) {
+    return (int)std::max<int64_t>(1, std::min<int64_t>((threads + kThreads - 1) / kThreads, (int64_t)kNumSMsB200 * 8));
+}
+
+}  // namespace
+
+int64_t early_rows(int64_t n) { return n / 8; }
+
+bool enabled() {
+    const char *env = std::getenv("NNGP_KNN_PRUNE");
+    return !(env && env[0] == '0');
+}
+
+size_t workspace(int64_t n, int d, int rows_per_group) {
+    if (n < kMinPoints || n > INT32_MAX - 1 || d < 1 || d > kMaxDim || rows_per_group < 1) return 0;
+    return layout(n, d, rows_per_group).total;
+}
+
+nngp_status build(const float *xs, int64_t n, int d, int dp, int G, int bits, const float *seeds,
+                  const int32_t *order0, const int32_t *pos0, const uint64_t *keys0, void *ws, size_t ws_bytes,
+                  Lists *out, cudaStream_t stream) {
+    if (n < kMinPoints || n > INT32_MAX - 1 || d < 1 || d > kMaxDim || G < 1 || bits < 1 || d * bits > 60 || !xs ||
+        !seeds || !order0 || !pos0 || !keys0 || !out)
+        return fail(NNGP_ERR_UNSUPPORTED, "knn pruning: shape outside the pruned search");
+    const Layout L = layout(n, d, G);
+    if (!ws || ws_bytes < L.total) return fail(NNGP_ERR_WORKSPACE, "knn pruning: workspace too small");
+    char *base = reinterpret_cast<char *>(align_up(reinterpret_cast<uintptr_t>(ws), 256));
+    auto at = [&](size_t off) { return reinterpret_cast<void *>(base + off); };
+    float *tlo = static_cast<float *>(at(L.tlo)), *thi = static_cast<float *>(at(L.thi));
+    int32_t *tmin = static_cast<int32_t *>(at(L.tmin));
+    unsigned long long *sum = static_cast<unsigned long long *>(at(L.stats)), *cnt = sum + kBands,
+                       *pcnt = sum + 2 * kBands;
+    int32_t *headpos = static_cast<int32_t *>(at(L.headpos)), *seg_start = static_cast<int32_t *>(at(L.seg_start));
+    int32_t *gh = static_cast<int32_t *>(at(L.gh)), *gid = static_cast<int32_t *>(at(L.gid));
+    int32_t *row_off = static_cast<int32_t *>(at(L.row_off));
+    DevSizes *sizes = static_cast<DevSizes *>(at(L.sizes));
+    float *glo = static_cast<float *>(at(L.glo)), *ghi = static_cast<float *>(at(L.ghi));
+    float *gtau = static_cast<float *>(at(L.gtau));
+    int32_t *glim = static_cast<int32_t *>(at(L.glim));
+    int32_t *counts = static_cast<int32_t *>(at(L.counts)), *offsets = static_cast<int32_t *>(at(L.offsets));
+    int32_t *list = static_cast<int32_t *>(at(L.list));
+    const int64_t early = early_rows(n);
+    auto cub_check = [&](size_t need) -> nngp_status {
+        return need <= L.cub_bytes ? NNGP_OK
+                                   : fail(NNGP_ERR_WORKSPACE, "knn pruning: sort / scan scratch of " +
+                                                                  std::to_string(need) + " bytes exceeds the budget");
+    };
+
+    tile_box_kernel<<<grid_of(L.n_tiles), kThreads, 0, stream>>>(xs, n, d, dp, order0, L.n_tiles, tlo, thi, tmin);
+    NNGP_CUDA_TRY(cudaGetLastError());
+    NNGP_CUDA_TRY(cudaMemsetAsync(sum, 0, 3 * kBands * 8, stream));
+    band_stats_kernel<<<grid_of(n - early), kThreads, 0, stream>>>(n, early, seeds, sum, cnt);
+    NNGP_CUDA_TRY(cudaGetLastError());
+    classify_kernel<<<grid_of(n), kThreads, 0, stream>>>(n, early, seeds, pos0, sum, cnt,
+                                                         static_cast<uint64_t *>(at(L.keys_a)),
+                                                         static_cast<int32_t *>(at(L.vals_a)), pcnt);
+    NNGP_CUDA_TRY(cudaGetLastError());
+
+    // rows: pruned (band, curve position) first, then the index-order rows ascending
+    cub::DoubleBuffer<uint64_t> dk(static_cast<uint64_t *>(at(L.keys_a)), static_cast<uint64_t *>(at(L.keys_b)));
+    cub::DoubleBuffer<int32_t> dv(static_cast<int32_t *>(at(L.vals_a)), static_cast<int32_t *>(at(L.vals_b)));
+    size_t need = 0;
+    NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, need, dk, dv, (int)n, 0, 64, stream));
+    nngp_status st = cub_check(need);
+    if (st != NNGP_OK) return st;
+    size_t have = L.cub_bytes;
+    NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(at(L.cub), have, dk, dv, (int)n, 0, 64, stream));
+    const int32_t *rows = dv.Current();
+
+    // groups: segments of one band and one octree cell, cut every G rows
+    segment_kernel<<<grid_of(n), kThreads, 0, stream>>>(n, dk.Current(), rows, pos0, keys0, pcnt, d, bits, headpos);
+    NNGP_CUDA_TRY(cudaGetLastError());
+    need = 0;
+    NNGP_CUDA_TRY(cub::DeviceScan::InclusiveScan(nullptr, need, headpos, seg_start, cub::Max(), (int)n, stream));
+    if ((st = cub_check(need)) != NNGP_OK) return st;
+    have = L.cub_bytes;
+    NNGP_CUDA_TRY(cub::DeviceScan::InclusiveScan(at(L.cub), have, headpos, seg_start, cub::Max(), (int)n, stream));
+    group_head_kernel<<<grid_of(n), kThreads, 0, stream>>>(n, seg_start, pcnt, G, gh);
+    NNGP_CUDA_TRY(cudaGetLastError());
+    need = 0;
+    NNGP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, need, gh, gid, (int)n, stream));
+    if ((st = cub_check(need)) != NNGP_OK) return st;
+    have = L.cub_bytes;
+    NNGP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(at(L.cub), have, gh, gid, (int)n, stream));
+    row_off_kernel<<<grid_of(n), kThreads, 0, stream>>>(n, gh, gid, row_off);
+    NNGP_CUDA_TRY(cudaGetLastError());
+    sizes_kernel<<<1, 1, 0, stream>>>(n, G, gh, gid, pcnt, row_off, sizes, sizes + 1);
+    NNGP_CUDA_TRY(cudaGetLastError());
+
+    // tile lists, then the work order (longest list first)
+    group_box_kernel<<<grid_of(L.max_groups), kThreads, 0, stream>>>(xs, d, dp, rows, row_off, sizes, seeds, glo, ghi,
+                                                                     gtau, glim);
+    NNGP_CUDA_TRY(cudaGetLastError());
+    Boxes b{tlo, thi, glo, ghi, gtau, tmin, glim, d, (double)(d + 3) * 1.1920928955078125e-07};
+    cub::DoubleBuffer<uint32_t> ok(static_cast<uint32_t *>(at(L.okeys_a)), static_cast<uint32_t *>(at(L.okeys_b)));
+    cub::DoubleBuffer<int32_t> ov(static_cast<int32_t *>(at(L.ovals_a)), static_cast<int32_t *>(at(L.ovals_b)));
+    NNGP_CUDA_TRY(cudaMemsetAsync(counts + L.max_groups, 0, sizeof(int32_t), stream));
+    count_kernel<<<grid_of(L.max_groups * 32), kThreads, 0, stream>>>(b, sizes, L.max_groups, L.n_tiles, counts,
+                                                                      ok.Current(), ov.Current());
+    NNGP_CUDA_TRY(cudaGetLastError());
+    need = 0;
+    NNGP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, need, counts, offsets, (int)(L.max_groups + 1), stream));
+    if ((st = cub_check(need)) != NNGP_OK) return st;
+    have = L.cub_bytes;
+    NNGP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(at(L.cub), have, counts, offsets, (int)(L.max_groups + 1), stream));
+    fill_kernel<<<grid_of(L.max_groups * 32), kThreads, 0, stream>>>(b, sizes, L.n_tiles, offsets, list);
+    NNGP_CUDA_TRY(cudaGetLastError());
+    need = 0;
+    NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, need, ok, ov, (int)L.max_groups, 0, 32, stream));
+    if ((st = cub_check(need)) != NNGP_OK) return st;
+    have = L.cub_bytes;
+    NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(at(L.cub), have, ok, ov, (int)L.max_groups, 0, 32, stream));
+
+    out->rows = rows;
+    out->pruned = sizes;
+    out->index_order = sizes + 1;
+    out->row_off = row_off;
+    out->item_order = ov.Current();
+    out->offsets = offsets;
+    out->tiles = list;
+    out->max_groups = L.max_groups;
+    out->max_index_items = (n + G - 1) / G;
+    return NNGP_OK;
+}
+
+}  // namespace prune
+}  // namespace nngp

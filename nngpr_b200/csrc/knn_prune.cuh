@@ -1,0 +1,64 @@
+// Row groups and ref-tile lists of the pruned prefix search (knn_prune.cu), used by the
+// dispatcher in knn.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "nngp_b200.h"
+
+namespace nngp {
+namespace prune {
+
+constexpr int64_t kMinPoints = 65536;  // below this the index-order search is short enough
+constexpr int kMaxDim = 4;             // bounding boxes stop pruning in more dimensions
+constexpr int kTileRefs = 128;         // refs per tile (the tensor-core search's ref tile)
+
+// Rows [0, early_rows(n)) always take the index-order search: their prefixes are short, and
+// their seeds, drawn from windows where few points precede them, are loose.
+int64_t early_rows(int64_t n);
+
+// NNGP_KNN_PRUNE=0 turns pruning off (seeded index-order search only).
+bool enabled();
+
+// Device-side sizes of one launch of the search (written by build, read by the kernel).
+struct DevSizes {
+    int64_t first_row;  // position of the launch's first row in Lists::rows
+    int64_t n_rows;
+    int64_t n_items;    // work items (groups of rows)
+};
+
+struct Lists {
+    const int32_t *rows = nullptr;        // n point indices: the pruned rows group after group, then
+                                          // the index-order rows, ascending
+    const DevSizes *pruned = nullptr;     // the pruned launch
+    const DevSizes *index_order = nullptr;  // the index-order launch (rows_per_group rows per item)
+    const int32_t *row_off = nullptr;     // pruned group g: rows[row_off[g] .. row_off[g + 1])
+    const int32_t *item_order = nullptr;  // pruned groups, longest tile list first
+    const int32_t *offsets = nullptr;     // group g's tiles: tiles[offsets[g] .. offsets[g + 1])
+    const int32_t *tiles = nullptr;       // ref tile ids (curve positions / 128)
+    int64_t max_groups = 0;               // host-side bound of pruned->n_items
+    int64_t max_index_items = 0;          // host-side bound of index_order->n_items
+};
+
+size_t workspace(int64_t n, int d, int rows_per_group);
+
+// Plans the prefix search of n scaled points xs (row stride dp, d <= kMaxDim features) over
+// itself, from the seeds and the curve order of knn_seed.cu (order0, pos0, keys0 with
+// bits_per_dim bits per dimension).  Rows below early_rows(n) and rows whose seed is more than
+// 16 times the geometric mean of their band's seeds go to the index-order launch; the others
+// are sorted by (band = floor(log2(n / i)), curve position) and cut into groups of at most
+// rows_per_group rows that never straddle a band or an octree cell of the curve (a cell level
+// per band chosen so that cells hold about 256 of its rows).  A ref tile (128 consecutive
+// points of the curve order) is listed for a group unless (a) every point in it has an index
+// >= every row of the group, or (b) the distance between the two bounding boxes, shrunk by the
+// FP32 rounding bound, exceeds the largest seed of the group.  Neither excludes a neighbour of
+// any row, so the search returns the same lists.  No host synchronisation: sizes stay on the
+// device.
+nngp_status build(const float *xs, int64_t n, int d, int dp, int rows_per_group, int bits_per_dim,
+                  const float *seeds, const int32_t *order0, const int32_t *pos0, const uint64_t *keys0, void *ws,
+                  size_t ws_bytes, Lists *out, cudaStream_t stream);
+
+}  // namespace prune
+}  // namespace nngp

@@ -205,7 +205,7 @@ __global__ void __launch_bounds__(kThreads) seed_kernel(const float *__restrict_
 }
 
 struct Layout {
-    size_t keys_a, keys_b, idx0_a, idx0_b, idx1_a, idx1_b, pos0, pos1, bounds, cub, cub_bytes, total;
+    size_t keys_a, keys_b, keys0, idx0_a, idx0_b, idx1_a, idx1_b, pos0, pos1, bounds, cub, cub_bytes, total;
 };
 
 Layout layout(int64_t n) {
@@ -218,6 +218,7 @@ Layout layout(int64_t n) {
     };
     L.keys_a = take((size_t)n * 8);
     L.keys_b = take((size_t)n * 8);
+    L.keys0 = take((size_t)n * 8);
     L.idx0_a = take((size_t)n * 4);
     L.idx0_b = take((size_t)n * 4);
     L.idx1_a = take((size_t)n * 4);
@@ -267,13 +268,14 @@ size_t workspace(int64_t n) { return n < kMinPoints ? 0 : layout(n).total; }
 
 int window() {
     const char *env = std::getenv("NNGP_KNN_SEED_W");
-    if (!env) return 256;
+    if (!env) return 128;
     const int w = std::atoi(env);
-    return (w == 0 || w == 128 || w == 256) ? w : 256;
+    return (w == 0 || w == 128 || w == 256) ? w : 128;
 }
 
 nngp_status prefix_seeds(const float *xs, int64_t n, int d, int D, int dp, int m, void *ws, size_t ws_bytes,
-                         float *seeds, cudaStream_t stream) {
+                         float *seeds, cudaStream_t stream, const int32_t **order0_out, const int32_t **pos0_out,
+                         const uint64_t **keys0_out) {
     const int W = window();
     if (W == 0 || n < kMinPoints || m < 1 || d < 1 || d > 24 || D < d || dp % 4 != 0 || dp < D)
         return fail(NNGP_ERR_UNSUPPORTED, "knn seeds: shape outside the seeded search");
@@ -286,7 +288,7 @@ nngp_status prefix_seeds(const float *xs, int64_t n, int d, int D, int dp, int m
                           {static_cast<int32_t *>(at(L.idx1_a)), static_cast<int32_t *>(at(L.idx1_b))}};
     int32_t *pos[2] = {static_cast<int32_t *>(at(L.pos0)), static_cast<int32_t *>(at(L.pos1))};
     uint32_t *lo = static_cast<uint32_t *>(at(L.bounds)), *hi = lo + 256;
-    const int bits = std::min(10, 64 / d);
+    const int bits = seed::bits(d);
 
     NNGP_CUDA_TRY(cudaMemsetAsync(lo, 0xFF, 256 * 4, stream));
     NNGP_CUDA_TRY(cudaMemsetAsync(hi, 0x00, 256 * 4, stream));
@@ -306,6 +308,9 @@ nngp_status prefix_seeds(const float *xs, int64_t n, int d, int D, int dp, int m
         size_t have = L.cub_bytes;
         NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(at(L.cub), have, dk, dv, (int)n, 0, bits * d, stream));
         order[c] = dv.Current();
+        if (c == 0) {  // the curve-0 keys in curve order, for callers that cut the curve into cells
+            NNGP_CUDA_TRY(cudaMemcpyAsync(at(L.keys0), dk.Current(), (size_t)n * 8, cudaMemcpyDeviceToDevice, stream));
+        }
         inverse_kernel<<<grid_of(n), kThreads, 0, stream>>>(order[c], n, pos[c]);
         NNGP_CUDA_TRY(cudaGetLastError());
     }
@@ -315,6 +320,9 @@ nngp_status prefix_seeds(const float *xs, int64_t n, int d, int D, int dp, int m
                                                  stream);
     if (!ok) return fail(NNGP_ERR_UNSUPPORTED, "knn seeds: no kernel for D = " + std::to_string(D));
     NNGP_CUDA_TRY(cudaGetLastError());
+    if (order0_out) *order0_out = order[0];
+    if (pos0_out) *pos0_out = pos[0];
+    if (keys0_out) *keys0_out = static_cast<const uint64_t *>(at(L.keys0));
     return NNGP_OK;
 }
 

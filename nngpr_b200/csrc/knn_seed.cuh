@@ -15,16 +15,23 @@ constexpr int64_t kMinPoints = 8192;  // below this the search is short and seed
 // Workspace bytes of prefix_seeds for n points (0 when n < kMinPoints).
 size_t workspace(int64_t n);
 
-// Window half-width in curve positions: NNGP_KNN_SEED_W = 128 or 256 (default 256); 0 turns
-// seeding off.
+// Window half-width in curve positions: NNGP_KNN_SEED_W = 128 or 256 (default 128: the faster
+// fit step at d = 3, 8 and 16); 0 turns seeding off.
 int window();
 
 // seeds[i] >= the m-th smallest squared distance from point i to the points j < i, in the
 // search's FP32 arithmetic (the squared distance of the scaled coordinates, ((t0^2 + t1^2) + ...),
 // every step rounded), or +inf.  xs: n scaled points, row stride dp (zero padded), D the padded
 // dimension the search kernel loops over.  Runs on `stream`; ws of workspace(n) bytes.
+// order0 / pos0 / keys0 (optional): the curve-0 order of the points (a permutation of 0..n-1),
+// its inverse and the curve-0 Morton keys in that order (key of point i = keys0[pos0[i]];
+// bits() bits per dimension, interleaved), left in ws for the caller.
 nngp_status prefix_seeds(const float *xs, int64_t n, int d, int D, int dp, int m, void *ws, size_t ws_bytes,
-                         float *seeds, cudaStream_t stream);
+                         float *seeds, cudaStream_t stream, const int32_t **order0 = nullptr,
+                         const int32_t **pos0 = nullptr, const uint64_t **keys0 = nullptr);
+
+// Bits per dimension of the Morton keys for d features.
+inline int bits(int d) { return d < 7 ? 10 : 64 / d; }
 
 }  // namespace seed
 }  // namespace nngp

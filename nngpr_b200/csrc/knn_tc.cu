@@ -212,8 +212,8 @@ __device__ __forceinline__ float min3f(float a, float b, float c) {
 // xs: scaled refs (n_pad x DP, zero padded); acc: per-feature sums for the centre.
 template <int D>
 __global__ void build_tc_tiles_kernel(const float *__restrict__ xs, int64_t n, int64_t n_pad,
-                                      const double *__restrict__ acc, unsigned char *__restrict__ tiles,
-                                      unsigned int *__restrict__ r2max_bits) {
+                                      const double *__restrict__ acc, const int32_t *__restrict__ perm,
+                                      unsigned char *__restrict__ tiles, unsigned int *__restrict__ r2max_bits) {
     using C = Cfg<D, 1>;  // the ref-tile layout does not depend on the query tiles
     float c[D];
 #pragma unroll
@@ -231,7 +231,7 @@ __global__ void build_tc_tiles_kernel(const float *__restrict__ xs, int64_t n, i
             float nr = 0.f;
 #pragma unroll
             for (int f = 0; f < D; ++f) {
-                const float r = xs[i * C::DP + f];
+                const float r = xs[(perm ? (int64_t)perm[i] : i) * C::DP + f];
                 const float rc = r - c[f];
                 ex[f] = r;
                 b[f] = -2.f * rc;
@@ -273,6 +273,13 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
                                                          const double *__restrict__ acc,
                                                          const unsigned int *__restrict__ r2max_bits,
                                                          const float *__restrict__ seeds,
+                                                         const int32_t *__restrict__ rows_perm,
+                                                         const int32_t *__restrict__ row_off,
+                                                         const int64_t *__restrict__ dev_sizes,
+                                                         const int32_t *__restrict__ item_order,
+                                                         const int32_t *__restrict__ ref_perm,
+                                                         const int32_t *__restrict__ tile_off,
+                                                         const int32_t *__restrict__ tile_list,
                                                          int *__restrict__ work_counter, int64_t n_query,
                                                          int64_t n_ref, int has_cut, int64_t cut, int m,
                                                          int32_t *__restrict__ out, int32_t *__restrict__ flags) {
@@ -299,7 +306,18 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const bool producer_warp = warp == EPI_WARPS;
-    const int64_t n_items = (n_query + C::ROWS - 1) / C::ROWS;
+    // Rows: positions [first_row, first_row + n_rows) of rows_perm (point indices; the positions
+    // themselves when rows_perm is null), from dev_sizes = {first_row, n_rows, n_items} on the
+    // device or {0, n_query, ceil(n_query / ROWS)}; work item g is positions
+    // [row_off[g], row_off[g + 1]) (at most ROWS) or ROWS consecutive positions.  Refs: with
+    // tile_list (pruned search), item g streams the tiles tile_list[tile_off[g] .. tile_off[g + 1])
+    // of tiles_g, whose positions map to points through ref_perm, and j < limit(i) is checked per
+    // candidate; otherwise refs in index order up to the largest limit of the item's rows (the
+    // rows of an item ascend).  Items: item_order[k] or, for the prefix search, heaviest first.
+    const bool pruned = tile_list != nullptr;
+    const int64_t first_row = dev_sizes ? dev_sizes[0] : 0;
+    const int64_t n_rows = dev_sizes ? dev_sizes[1] : n_query;
+    const int64_t n_items = dev_sizes ? dev_sizes[2] : (n_query + C::ROWS - 1) / C::ROWS;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < S; ++s) {
@@ -344,10 +362,24 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
         const bool stop = (item >= n_items) || (*s_abort != 0);
         __syncthreads();
         if (stop) break;
-        const int64_t qtile = has_cut ? (n_items - 1 - item) : item;  // heaviest first for the prefix search
-        const int64_t q0 = qtile * C::ROWS;
-        const int64_t block_limit = limit_of(min(q0 + C::ROWS, n_query) - 1);
-        const uint32_t ntiles = (uint32_t)((block_limit + RT - 1) / RT);
+        const int64_t qtile = item_order ? (int64_t)item_order[item] : (has_cut ? (n_items - 1 - item) : item);
+        int64_t q0, n_item_rows;  // the item's first row position and its row count
+        if (row_off) {
+            q0 = row_off[qtile];
+            n_item_rows = row_off[qtile + 1] - q0;
+        } else {
+            q0 = first_row + qtile * C::ROWS;
+            n_item_rows = min((int64_t)C::ROWS, first_row + n_rows - q0);
+        }
+        auto point_of = [&](int64_t pos) -> int64_t { return rows_perm ? (int64_t)rows_perm[pos] : pos; };
+        const int32_t *tl = pruned ? tile_list + tile_off[qtile] : nullptr;  // this group's ref tiles
+        uint32_t ntiles;
+        if (pruned) {
+            ntiles = (uint32_t)(tile_off[qtile + 1] - tile_off[qtile]);
+        } else {
+            const int64_t block_limit = limit_of(point_of(q0 + n_item_rows - 1));
+            ntiles = (uint32_t)((block_limit + RT - 1) / RT);
+        }
 
         if (producer_warp) {
             if (lane == 0) {
@@ -359,7 +391,7 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
                 };
                 auto issue_tma = [&](uint32_t g) {
                     const uint32_t s = g % S;
-                    const int64_t t = (int64_t)(g - G);
+                    const int64_t t = pruned ? (int64_t)tl[g - G] : (int64_t)(g - G);
                     mbar_arrive_expect_tx(&b_full[s], C::STAGE_BYTES);
                     tma_bulk_g2s(sB + s * C::STAGE_BYTES, tiles_g + t * C::STAGE_BYTES, C::STAGE_BYTES, &b_full[s]);
                     tma_issued = g + 1;
@@ -416,8 +448,8 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
             // lanes of its own quadrant only)
             const int qtw = warp >> 2, quad = warp & 3;
             const int row = warp * 32 + lane;  // query row in the work item
-            const int64_t q = q0 + row;
-            const bool active = q < n_query;
+            const bool active = row < n_item_rows;
+            const int64_t q = active ? point_of(q0 + row) : 0;  // the point's index
             const int64_t limit = active ? limit_of(q) : 0;
             float qo[D], qc[D];
             float nq = 0.f;
@@ -498,7 +530,7 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
                 }
                 tc_fence_after();
                 const float *exs = reinterpret_cast<const float *>(sB + s * C::STAGE_BYTES + C::OP_BYTES);
-                const int64_t j0 = (int64_t)t * RT;
+                const int64_t j0 = (pruned ? (int64_t)tl[t] : (int64_t)t) * RT;  // first ref position of the tile
                 const uint32_t taddr = tmem_base + ((uint32_t)(quad * 32) << 16) + b * C::BUF_COLS + qtw * RT;
                 // screen one 32-column chunk (scores in v): this row's candidate mask, 0 when no row
                 // of the warp has one (the common case, a handful of instructions)
@@ -542,8 +574,8 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&t_empty[b]);
                 uint32_t cm3 = screen(vb);
-                {  // columns with j < limit only
-                    const int64_t room = limit - j0;
+                {  // columns with j < limit only (pruned: positions < n_ref; the index test is per candidate)
+                    const int64_t room = (pruned ? n_ref : limit) - j0;
                     if (room < RT) {
                         auto cut = [&](uint32_t &cm, int c) {
                             const int64_t r = room - c * 32;
@@ -589,8 +621,9 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
                             const float tf = sub_rn(rv[f], qo[f]);
                             d2 = add_rn(d2, mul_rn(tf, tf));
                         }
-                        keep = d2 <= worst;  // NaN never kept
-                        key = (uint64_t)__float_as_uint(d2) << 32 | (uint32_t)(j0 + col);
+                        const int64_t jo = pruned ? (int64_t)ref_perm[j0 + col] : j0 + col;  // the ref's index
+                        keep = d2 <= worst && jo < limit;  // NaN never kept
+                        key = (uint64_t)__float_as_uint(d2) << 32 | (uint32_t)jo;
                     }
                     const unsigned mk = __ballot_sync(FULL, keep);
                     if (keep) {
@@ -620,8 +653,8 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
                             x = take_min ? (o < x ? o : x) : (o > x ? o : x);
                         }
                     }
-                    const int64_t qq = q0 + warp * 32 + rr;
-                    if (qq < n_query && lane < m) out[qq * m + lane] = (int32_t)(uint32_t)x;
+                    const int64_t rq = warp * 32 + rr;
+                    if (rq < n_item_rows && lane < m) out[point_of(q0 + rq) * m + lane] = (int32_t)(uint32_t)x;
                 }
             }
         }

@@ -10,9 +10,13 @@ namespace tc {
 constexpr int kTcRefTile = 128;    // refs per tile (UMMA N)
 constexpr int kTcQueryTile = 128;  // queries per tile (UMMA M)
 
-using TcFn = void (*)(const unsigned char *, const float *, const double *, const unsigned int *, const float *, int *,
-                      int64_t, int64_t, int, int64_t, int, int32_t *, int32_t *);
-using TcBuildFn = void (*)(const float *, int64_t, int64_t, const double *, unsigned char *, unsigned int *);
+using TcFn = void (*)(const unsigned char *, const float *, const double *, const unsigned int *, const float *,
+                      const int32_t *, const int32_t *, const int64_t *, const int32_t *, const int32_t *,
+                      const int32_t *, const int32_t *, int *, int64_t, int64_t, int, int64_t, int, int32_t *,
+                      int32_t *);
+// build(xs, n, n_pad, acc, perm, tiles, r2max): tile position i holds point perm[i] (i when perm is null)
+using TcBuildFn = void (*)(const float *, int64_t, int64_t, const double *, const int32_t *, unsigned char *,
+                           unsigned int *);
 
 struct TcVariant {
     TcFn fn = nullptr;

@@ -76,3 +76,42 @@ def test_seeding_engages_only_on_the_prefix_self_search(monkeypatch, capfd):
     small = torch.from_numpy(x[:5000].astype(np.float32)).cuda()
     ops.knn(small, small, 32, 0, 0.3)  # below the size where seeding pays
     assert 'seeded=0' in capfd.readouterr().err
+
+
+def search_mode(monkeypatch, x, m, ls, prune):
+    monkeypatch.setenv('NNGP_KNN_PRUNE', '1' if prune else '0')
+    return search(monkeypatch, x, m, ls, 128)
+
+
+@pytest.mark.parametrize('d', [1, 2, 3, 5, 8, 16, 24])
+@pytest.mark.parametrize('m', [1, 32])
+def test_pruned_lists_equal_unpruned_and_oracle(monkeypatch, d, m):
+    """n >= 65,536: groups of rows visit only the ref tiles their seeds allow (bounding boxes
+    along the curve order); the lists stay bit-identical."""
+    rng = np.random.default_rng(50 * d + m)
+    n = 70000
+    x = rng.uniform(-1, 1, (n, d)) * rng.uniform(0.3, 1.0, d)
+    ls = rng.uniform(0.3, 2.0, d) if d % 2 else 0.4
+    a = search_mode(monkeypatch, x, m, ls, True)
+    assert np.array_equal(a, search_mode(monkeypatch, x, m, ls, False))
+    check_rows(x, a, m, ls, rng, k=150)
+
+
+def test_pruned_ties_outlier_and_clusters(monkeypatch, capfd):
+    rng = np.random.default_rng(9)
+    lattice = rng.integers(0, 8, (80000, 3)).astype(np.float64)  # duplicates: exact ties
+    monkeypatch.setenv('NNGP_KNN_DEBUG', '1')
+    a = search_mode(monkeypatch, lattice, 32, None, True)
+    assert 'pruned=1' in capfd.readouterr().err
+    assert np.array_equal(a, search_mode(monkeypatch, lattice, 32, None, False))
+    check_rows(lattice, a, 32, None, rng, k=100)
+    y = rng.normal(size=(70000, 3))
+    y[33333] = [1e7, -1e7, 5e6]  # squeezes the other points into a few curve cells
+    b = search_mode(monkeypatch, y, 16, 0.5, True)
+    assert np.array_equal(b, search_mode(monkeypatch, y, 16, 0.5, False))
+    check_rows(y, b, 16, 0.5, rng, k=100)
+    means = rng.uniform(-3, 3, (64, 16))
+    z = means[rng.integers(0, 64, 70000)] + 0.5 * rng.normal(size=(70000, 16))
+    c = search_mode(monkeypatch, z, 32, 0.8, True)
+    assert np.array_equal(c, search_mode(monkeypatch, z, 32, 0.8, False))
+    check_rows(z, c, 32, 0.8, rng, k=80)
