@@ -553,11 +553,11 @@ KnnPlan make_plan(int64_t n_ref, int64_t n_query, int d, int m, bool same) {
         off = align_up(off + 16, 256);
         p.off_ctr = off;
         off = align_up(off + 16, 256);
-        if (p.path == KnnPath::Tc && seed::workspace(n_ref) > 0) {  // seeds of the prefix search
+        if (p.path == KnnPath::Tc && seed::workspace(n_ref, p.dp) > 0) {  // seeds of the prefix search
             p.off_seed = off;
             off = align_up(off + (size_t)n_ref * sizeof(float), 256);
             p.off_seed_ws = off;
-            p.seed_ws_bytes = seed::workspace(n_ref);
+            p.seed_ws_bytes = seed::workspace(n_ref, p.dp);
             off = align_up(off + p.seed_ws_bytes, 256);
             if (prune::workspace(n_ref, d, p.tv.rows_per_item) > 0) {  // pruned search: curve-order tiles + lists
                 p.off_tiles2 = align_up(off, 1024);
@@ -657,13 +657,13 @@ nngp_status knn_impl(const T *ref, int64_t n_ref, const T *query, int64_t n_quer
             prune::Lists lists;
             unsigned char *tiles_curve = reinterpret_cast<unsigned char *>(base + p.off_tiles2);
             if (pruned) {
-                p.tv.build<<<grid_for(p.n_ref_pad), 256, 0, stream>>>(refs, n_ref, p.n_ref_pad, acc, order0,
-                                                                      tiles_curve, r2);
-                NNGP_CUDA_TRY(cudaGetLastError());
                 nngp_status pst = prune::build(refs, n_ref, d, p.dp, p.tv.rows_per_item, seed::bits(d), seeds_c,
                                                order0, pos0, keys0, base + p.off_prune_ws, p.prune_ws_bytes, &lists,
                                                stream);
                 if (pst != NNGP_OK) return pst;
+                p.tv.build<<<grid_for(p.n_ref_pad), 256, 0, stream>>>(refs, n_ref, p.n_ref_pad, acc, lists.ref_order,
+                                                                      tiles_curve, r2);
+                NNGP_CUDA_TRY(cudaGetLastError());
                 if (const char *dbg = std::getenv("NNGP_KNN_DEBUG"); dbg && dbg[0] == '1') {
                     prune::DevSizes hs[2];  // diagnostics only (synchronises the stream)
                     int32_t total = 0;
@@ -713,8 +713,8 @@ nngp_status knn_impl(const T *ref, int64_t n_ref, const T *query, int64_t n_quer
             if (pruned) {
                 const int64_t *ps = reinterpret_cast<const int64_t *>(lists.pruned);
                 const int64_t *is = reinterpret_cast<const int64_t *>(lists.index_order);
-                lst = launch(tiles_curve, lists.max_groups, lists.rows, lists.row_off, ps, lists.item_order, order0,
-                             lists.offsets, lists.tiles, ctr + 1);
+                lst = launch(tiles_curve, lists.max_groups, lists.rows, lists.row_off, ps, lists.item_order,
+                             lists.ref_order, lists.offsets, lists.tiles, ctr + 1);
                 if (lst != NNGP_OK) return lst;
                 lst = launch(tiles, lists.max_index_items, lists.rows, none, is, none, none, none, none, ctr);
             } else {

@@ -40,7 +40,7 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kBands = 4;            // i >= n / 8: bands 0..2 (3 only at rounding edges)
 constexpr int kLooseLog2Q = 4 * 256;  // seed > 16 x band geometric mean (log2 in 1/256 units)
-constexpr uint64_t kIndexOrderTag = 15ull << 60;
+constexpr uint64_t kIndexOrderTag = 1ull << 34;  // above (band << 32 | curve position) for bands < 4
 
 __device__ __forceinline__ int band_of(int64_t i, int64_t n) {
     int b = 0;
@@ -53,26 +53,55 @@ __device__ __forceinline__ long long log2q(float tau) {
     return llrint(fmax(log2((double)tau), -160.0) * 256.0);
 }
 
+// Box and smallest index of every ref tile (128 consecutive points of `order`); one warp per tile.
 __global__ void __launch_bounds__(kThreads) tile_box_kernel(const float *__restrict__ xs, int64_t n, int d, int dp,
-                                                            const int32_t *__restrict__ order0, int64_t n_tiles,
+                                                            const int32_t *__restrict__ order, int64_t n_tiles,
                                                             float *__restrict__ tlo, float *__restrict__ thi,
                                                             int32_t *__restrict__ tmin) {
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n_tiles;
-         t += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t k0 = t * kTileRefs, k1 = min(n, k0 + kTileRefs);
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t t = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; t < n_tiles; t += nw) {
+        int32_t pt[kTileRefs / 32];
         int32_t mi = INT32_MAX;
-        for (int64_t k = k0; k < k1; ++k) mi = min(mi, order0[k]);
-        tmin[t] = mi;
+#pragma unroll
+        for (int q = 0; q < kTileRefs / 32; ++q) {
+            const int64_t k = t * kTileRefs + q * 32 + lane;
+            pt[q] = k < n ? order[k] : -1;
+            if (pt[q] >= 0) mi = min(mi, pt[q]);
+        }
+        mi = __reduce_min_sync(0xFFFFFFFFu, mi);
+        if (lane == 0) tmin[t] = mi;
         for (int f = 0; f < d; ++f) {
             float lo = pos_inf<float>(), hi = neg_inf<float>();  // NaN coordinates are skipped
-            for (int64_t k = k0; k < k1; ++k) {
-                const float v = xs[(int64_t)order0[k] * dp + f];
-                lo = fminf(lo, v);
-                hi = fmaxf(hi, v);
+#pragma unroll
+            for (int q = 0; q < kTileRefs / 32; ++q) {
+                if (pt[q] >= 0) {
+                    const float v = xs[(int64_t)pt[q] * dp + f];
+                    lo = fminf(lo, v);
+                    hi = fmaxf(hi, v);
+                }
             }
-            tlo[t * d + f] = lo;
-            thi[t * d + f] = hi;
+            for (int o = 16; o > 0; o >>= 1) {
+                lo = fminf(lo, __shfl_xor_sync(0xFFFFFFFFu, lo, o));
+                hi = fmaxf(hi, __shfl_xor_sync(0xFFFFFFFFu, hi, o));
+            }
+            if (lane == 0) {
+                tlo[t * d + f] = lo;
+                thi[t * d + f] = hi;
+            }
         }
+    }
+}
+
+// Ref order: points sorted by (index class, curve position), class = 3 - band: [0, n/8),
+// [n/8, n/4), [n/4, n/2), [n/2, n).  A tile then holds refs of one class (up to the one tile at
+// each class boundary), so a group of rows of band b skips whole tiles whose refs all come
+// after its rows, and meets refs j > i only in its own class.
+__global__ void __launch_bounds__(kThreads) ref_keys_kernel(int64_t n, const int32_t *__restrict__ pos0,
+                                                            uint64_t *__restrict__ keys, int32_t *__restrict__ vals) {
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+        keys[j] = (uint64_t)(kBands - 1 - band_of(j, n)) << 32 | (uint32_t)pos0[j];
+        vals[j] = (int32_t)j;
     }
 }
 
@@ -107,7 +136,7 @@ __global__ void __launch_bounds__(kThreads) band_stats_kernel(int64_t n, int64_t
     }
 }
 
-// Sort keys: pruned rows (band << 60 | curve position), the others (15 << 60 | index); counts
+// Sort keys: pruned rows (band << 32 | curve position), the others (2^34 | index); counts
 // of pruned rows per band and in total.
 __global__ void __launch_bounds__(kThreads) classify_kernel(int64_t n, int64_t early, const float *__restrict__ seeds,
                                                             const int32_t *__restrict__ pos0,
@@ -127,7 +156,7 @@ __global__ void __launch_bounds__(kThreads) classify_kernel(int64_t n, int64_t e
                 pruned = log2q(tau) <= mean + kLooseLog2Q;
             }
         }
-        keys[i] = pruned ? ((uint64_t)b << 60 | (uint32_t)pos0[i]) : (kIndexOrderTag | (uint64_t)i);
+        keys[i] = pruned ? ((uint64_t)b << 32 | (uint32_t)pos0[i]) : (kIndexOrderTag | (uint64_t)i);
         vals[i] = (int32_t)i;
         if (pruned) c[b] += 1;
     }
@@ -165,10 +194,10 @@ __global__ void __launch_bounds__(kThreads) segment_kernel(int64_t n, const uint
     for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
         int32_t h = 0;
         if (r < (int64_t)total) {
-            const int b = (int)(skeys[r] >> 60);
+            const int b = (int)(skeys[r] >> 32);
             bool head = r == 0;
             if (!head) {
-                const int bp = (int)(skeys[r - 1] >> 60);
+                const int bp = (int)(skeys[r - 1] >> 32);
                 head = bp != b || cell_of(r - 1, b) != cell_of(r, b);
             }
             h = head ? (int32_t)r : 0;
@@ -209,6 +238,7 @@ __global__ void sizes_kernel(int64_t n, int G, const int32_t *__restrict__ gh, c
     index_order->n_items = (n - (int64_t)total + G - 1) / G;
 }
 
+// Box, largest seed and largest index of every pruned group; one warp per group.
 __global__ void __launch_bounds__(kThreads) group_box_kernel(const float *__restrict__ xs, int d, int dp,
                                                              const int32_t *__restrict__ rows,
                                                              const int32_t *__restrict__ row_off,
@@ -216,28 +246,39 @@ __global__ void __launch_bounds__(kThreads) group_box_kernel(const float *__rest
                                                              const float *__restrict__ seeds, float *__restrict__ glo,
                                                              float *__restrict__ ghi, float *__restrict__ gtau,
                                                              int32_t *__restrict__ glim) {
+    const int lane = threadIdx.x & 31;
     const int64_t n_groups = pruned->n_items;
-    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n_groups;
-         g += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t g = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; g < n_groups; g += nw) {
         const int64_t r0 = row_off[g], r1 = row_off[g + 1];
         float tau = 0.f;
         int32_t lim = -1;
-        for (int64_t r = r0; r < r1; ++r) {
+        for (int64_t r = r0 + lane; r < r1; r += 32) {
             const int32_t i = rows[r];
             tau = fmaxf(tau, seeds[i]);
             lim = max(lim, i);
         }
-        gtau[g] = tau;
-        glim[g] = lim;  // refs j < lim can serve some row of the group
+        lim = __reduce_max_sync(0xFFFFFFFFu, lim);
+        for (int o = 16; o > 0; o >>= 1) tau = fmaxf(tau, __shfl_xor_sync(0xFFFFFFFFu, tau, o));
+        if (lane == 0) {
+            gtau[g] = tau;
+            glim[g] = lim;  // refs j < lim can serve some row of the group
+        }
         for (int f = 0; f < d; ++f) {
             float lo = pos_inf<float>(), hi = neg_inf<float>();
-            for (int64_t r = r0; r < r1; ++r) {
+            for (int64_t r = r0 + lane; r < r1; r += 32) {
                 const float v = xs[(int64_t)rows[r] * dp + f];
                 lo = fminf(lo, v);
                 hi = fmaxf(hi, v);
             }
-            glo[g * d + f] = lo;
-            ghi[g * d + f] = hi;
+            for (int o = 16; o > 0; o >>= 1) {
+                lo = fminf(lo, __shfl_xor_sync(0xFFFFFFFFu, lo, o));
+                hi = fmaxf(hi, __shfl_xor_sync(0xFFFFFFFFu, hi, o));
+            }
+            if (lane == 0) {
+                glo[g * d + f] = lo;
+                ghi[g * d + f] = hi;
+            }
         }
     }
 }
@@ -263,6 +304,13 @@ __device__ __forceinline__ bool tile_needed(const Boxes &b, int64_t g, int64_t t
     return !(lb * (1.0 - b.gamma) - 1e-37 > tau);
 }
 
+// Do the boxes of ref tile t and group g intersect?
+__device__ __forceinline__ bool box_overlap(const Boxes &b, int64_t g, int64_t t) {
+    for (int f = 0; f < b.d; ++f)
+        if (b.tlo[t * b.d + f] > b.ghi[g * b.d + f] || b.glo[g * b.d + f] > b.thi[t * b.d + f]) return false;
+    return true;
+}
+
 // One warp per group: counts[g] = tiles needed (0 for the slots past the groups), and the
 // sort key of the group's place in the work order (longest list first).
 __global__ void __launch_bounds__(kThreads) count_kernel(Boxes b, const DevSizes *__restrict__ pruned,
@@ -286,7 +334,9 @@ __global__ void __launch_bounds__(kThreads) count_kernel(Boxes b, const DevSizes
     }
 }
 
-// One warp per group: the needed tiles in ascending order at list[offsets[g] ..).
+// One warp per group: the needed tiles at list[offsets[g] ..), first those whose box meets the
+// group's box (they hold most of the rows' nearest refs, so the rows' bounds tighten early),
+// then the others, each part in ascending order.
 __global__ void __launch_bounds__(kThreads) fill_kernel(Boxes b, const DevSizes *__restrict__ pruned, int64_t n_tiles,
                                                         const int32_t *__restrict__ offsets,
                                                         int32_t *__restrict__ list) {
@@ -295,19 +345,22 @@ __global__ void __launch_bounds__(kThreads) fill_kernel(Boxes b, const DevSizes 
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t g = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; g < n_groups; g += nw) {
         int64_t o = offsets[g];
-        for (int64_t base = 0; base < n_tiles; base += 32) {
-            const int64_t t = base + lane;
-            const bool need = t < n_tiles && tile_needed(b, g, t);
-            const unsigned mask = __ballot_sync(0xFFFFFFFFu, need);
-            if (need) list[o + __popc(mask & ((1u << lane) - 1u))] = (int32_t)t;
-            o += __popc(mask);
+        for (int pass = 0; pass < 2; ++pass) {
+            for (int64_t base = 0; base < n_tiles; base += 32) {
+                const int64_t t = base + lane;
+                bool need = t < n_tiles && tile_needed(b, g, t);
+                if (need) need = box_overlap(b, g, t) == (pass == 0);
+                const unsigned mask = __ballot_sync(0xFFFFFFFFu, need);
+                if (need) list[o + __popc(mask & ((1u << lane) - 1u))] = (int32_t)t;
+                o += __popc(mask);
+            }
         }
     }
 }
 
 struct Layout {
     int64_t n_tiles, max_groups;
-    size_t tlo, thi, tmin, stats, keys_a, keys_b, vals_a, vals_b, headpos, seg_start, gh, gid, row_off, sizes, glo,
+    size_t tlo, thi, tmin, stats, keys_a, keys_b, vals_a, vals_b, rvals_a, rvals_b, headpos, seg_start, gh, gid, row_off, sizes, glo,
         ghi, gtau, glim, counts, offsets, okeys_a, okeys_b, ovals_a, ovals_b, list, cub, cub_bytes, total;
 };
 
@@ -331,6 +384,8 @@ Layout layout(int64_t n, int d, int G) {
     L.keys_b = take((size_t)n * 8);
     L.vals_a = take((size_t)n * 4);
     L.vals_b = take((size_t)n * 4);
+    L.rvals_a = take((size_t)n * 4);
+    L.rvals_b = take((size_t)n * 4);
     L.headpos = take((size_t)n * 4);
     L.seg_start = take((size_t)n * 4);
     L.gh = take((size_t)n * 4);
@@ -402,7 +457,20 @@ nngp_status build(const float *xs, int64_t n, int d, int dp, int G, int bits, co
                                                                   std::to_string(need) + " bytes exceeds the budget");
     };
 
-    tile_box_kernel<<<grid_of(L.n_tiles), kThreads, 0, stream>>>(xs, n, d, dp, order0, L.n_tiles, tlo, thi, tmin);
+    // ref order (index class, curve position) and the boxes of its tiles
+    ref_keys_kernel<<<grid_of(n), kThreads, 0, stream>>>(n, pos0, static_cast<uint64_t *>(at(L.keys_a)),
+                                                         static_cast<int32_t *>(at(L.rvals_a)));
+    NNGP_CUDA_TRY(cudaGetLastError());
+    cub::DoubleBuffer<uint64_t> rk(static_cast<uint64_t *>(at(L.keys_a)), static_cast<uint64_t *>(at(L.keys_b)));
+    cub::DoubleBuffer<int32_t> rv(static_cast<int32_t *>(at(L.rvals_a)), static_cast<int32_t *>(at(L.rvals_b)));
+    size_t need0 = 0;
+    NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, need0, rk, rv, (int)n, 0, 34, stream));
+    if (need0 > L.cub_bytes) return fail(NNGP_ERR_WORKSPACE, "knn pruning: sort scratch exceeds the budget");
+    size_t have0 = L.cub_bytes;
+    NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(at(L.cub), have0, rk, rv, (int)n, 0, 34, stream));
+    const int32_t *ref_order = rv.Current();
+    tile_box_kernel<<<grid_of(L.n_tiles * 32), kThreads, 0, stream>>>(xs, n, d, dp, ref_order, L.n_tiles, tlo, thi,
+                                                                       tmin);
     NNGP_CUDA_TRY(cudaGetLastError());
     NNGP_CUDA_TRY(cudaMemsetAsync(sum, 0, 3 * kBands * 8, stream));
     band_stats_kernel<<<grid_of(n - early), kThreads, 0, stream>>>(n, early, seeds, sum, cnt);
@@ -416,11 +484,11 @@ nngp_status build(const float *xs, int64_t n, int d, int dp, int G, int bits, co
     cub::DoubleBuffer<uint64_t> dk(static_cast<uint64_t *>(at(L.keys_a)), static_cast<uint64_t *>(at(L.keys_b)));
     cub::DoubleBuffer<int32_t> dv(static_cast<int32_t *>(at(L.vals_a)), static_cast<int32_t *>(at(L.vals_b)));
     size_t need = 0;
-    NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, need, dk, dv, (int)n, 0, 64, stream));
+    NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, need, dk, dv, (int)n, 0, 35, stream));
     nngp_status st = cub_check(need);
     if (st != NNGP_OK) return st;
     size_t have = L.cub_bytes;
-    NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(at(L.cub), have, dk, dv, (int)n, 0, 64, stream));
+    NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(at(L.cub), have, dk, dv, (int)n, 0, 35, stream));
     const int32_t *rows = dv.Current();
 
     // groups: segments of one band and one octree cell, cut every G rows
@@ -444,8 +512,8 @@ nngp_status build(const float *xs, int64_t n, int d, int dp, int G, int bits, co
     NNGP_CUDA_TRY(cudaGetLastError());
 
     // tile lists, then the work order (longest list first)
-    group_box_kernel<<<grid_of(L.max_groups), kThreads, 0, stream>>>(xs, d, dp, rows, row_off, sizes, seeds, glo, ghi,
-                                                                     gtau, glim);
+    group_box_kernel<<<grid_of(L.max_groups * 32), kThreads, 0, stream>>>(xs, d, dp, rows, row_off, sizes, seeds, glo,
+                                                                          ghi, gtau, glim);
     NNGP_CUDA_TRY(cudaGetLastError());
     Boxes b{tlo, thi, glo, ghi, gtau, tmin, glim, d, (double)(d + 3) * 1.1920928955078125e-07};
     cub::DoubleBuffer<uint32_t> ok(static_cast<uint32_t *>(at(L.okeys_a)), static_cast<uint32_t *>(at(L.okeys_b)));
@@ -468,6 +536,7 @@ nngp_status build(const float *xs, int64_t n, int d, int dp, int G, int bits, co
     NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(at(L.cub), have, ok, ov, (int)L.max_groups, 0, 32, stream));
 
     out->rows = rows;
+    out->ref_order = ref_order;
     out->pruned = sizes;
     out->index_order = sizes + 1;
     out->row_off = row_off;

@@ -32,12 +32,13 @@ struct DevSizes {
 struct Lists {
     const int32_t *rows = nullptr;        // n point indices: the pruned rows group after group, then
                                           // the index-order rows, ascending
+    const int32_t *ref_order = nullptr;   // n point indices: tile position k holds point ref_order[k]
     const DevSizes *pruned = nullptr;     // the pruned launch
     const DevSizes *index_order = nullptr;  // the index-order launch (rows_per_group rows per item)
     const int32_t *row_off = nullptr;     // pruned group g: rows[row_off[g] .. row_off[g + 1])
     const int32_t *item_order = nullptr;  // pruned groups, longest tile list first
     const int32_t *offsets = nullptr;     // group g's tiles: tiles[offsets[g] .. offsets[g + 1])
-    const int32_t *tiles = nullptr;       // ref tile ids (curve positions / 128)
+    const int32_t *tiles = nullptr;       // ref tile ids (ref_order positions / 128)
     int64_t max_groups = 0;               // host-side bound of pruned->n_items
     int64_t max_index_items = 0;          // host-side bound of index_order->n_items
 };
@@ -50,12 +51,13 @@ size_t workspace(int64_t n, int d, int rows_per_group);
 // 16 times the geometric mean of their band's seeds go to the index-order launch; the others
 // are sorted by (band = floor(log2(n / i)), curve position) and cut into groups of at most
 // rows_per_group rows that never straddle a band or an octree cell of the curve (a cell level
-// per band chosen so that cells hold about 256 of its rows).  A ref tile (128 consecutive
-// points of the curve order) is listed for a group unless (a) every point in it has an index
-// >= every row of the group, or (b) the distance between the two bounding boxes, shrunk by the
-// FP32 rounding bound, exceeds the largest seed of the group.  Neither excludes a neighbour of
-// any row, so the search returns the same lists.  No host synchronisation: sizes stay on the
-// device.
+// per band chosen so that cells hold about 256 of its rows).  Refs are ordered by (index class
+// = 3 - band, curve position) and cut into tiles of 128 (ref_order; the caller builds the
+// search's tiles in that order).  A ref tile is listed for a group unless (a) every point in it
+// has an index >= every row of the group, or (b) the distance between the two bounding boxes,
+// shrunk by the FP32 rounding bound, exceeds the largest seed of the group; tiles whose box meets
+// the group's come first.  Neither rule excludes a neighbour of any row, so the search returns
+// the same lists.  No host synchronisation: sizes stay on the device.
 nngp_status build(const float *xs, int64_t n, int d, int dp, int rows_per_group, int bits_per_dim,
                   const float *seeds, const int32_t *order0, const int32_t *pos0, const uint64_t *keys0, void *ws,
                   size_t ws_bytes, Lists *out, cudaStream_t stream);

@@ -102,12 +102,33 @@ __global__ void __launch_bounds__(kThreads) inverse_kernel(const int32_t *__rest
         pos[order[k]] = (int32_t)k;
 }
 
-// Squared distance bits of refs j and the query coordinates qv in the search's exact arithmetic:
-// ((x_j0 - q0)^2 + (x_j1 - q1)^2) + ..., every step rounded, over the D padded features.
+// Coordinates in a curve's order (row k = point order[k], dp floats) and, for curve 1, the
+// curve-0 position of each of its points: the seed kernel's window reads become contiguous.
+__global__ void __launch_bounds__(kThreads) gather_kernel(const float *__restrict__ xs, int64_t n, int dp,
+                                                          const int32_t *__restrict__ order, float *__restrict__ xs_c) {
+    const int64_t total = n * (dp / 4);
+    const float4 *src = reinterpret_cast<const float4 *>(xs);
+    float4 *dst = reinterpret_cast<float4 *>(xs_c);
+    const int v4 = dp / 4;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k = e / v4, v = e - k * v4;
+        dst[e] = src[(int64_t)order[k] * v4 + v];
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) cross_pos_kernel(const int32_t *__restrict__ order1,
+                                                             const int32_t *__restrict__ pos0, int64_t n,
+                                                             int32_t *__restrict__ p0_of1) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+        p0_of1[k] = pos0[order1[k]];
+}
+
+// Squared distance bits of the ref row r and the query coordinates qv in the search's exact
+// arithmetic: ((r0 - q0)^2 + (r1 - q1)^2) + ..., every step rounded, over the D padded features.
 template <int D>
-__device__ __forceinline__ uint32_t dist_bits(const float *__restrict__ xs, int dp, int64_t j, const float (&qv)[D]) {
+__device__ __forceinline__ uint32_t dist_bits(const float *__restrict__ row, const float (&qv)[D]) {
     constexpr int V = (D + 3) / 4;
-    const float4 *r4 = reinterpret_cast<const float4 *>(xs + j * dp);
+    const float4 *r4 = reinterpret_cast<const float4 *>(row);
     float r[4 * V];
 #pragma unroll
     for (int v = 0; v < V; ++v) {
@@ -131,11 +152,12 @@ __device__ __forceinline__ uint32_t dist_bits(const float *__restrict__ xs, int 
 // j < i in the window [p - W, p + W) of each curve (curve 1 skips refs inside curve 0's window,
 // so every ref counts once); 0xFFFFFFFF for the other slots.  The row's seed is the m-th
 // smallest value (bisection on the bit patterns, stopped within kTolBits above it), or +inf.
+// xs0 / xs1: the coordinates in curve order; p0_of1[k] = curve-0 position of order1[k].
 template <int D, int VPL>
-__global__ void __launch_bounds__(kThreads) seed_kernel(const float *__restrict__ xs, int64_t n, int dp, int m,
-                                                        const int32_t *__restrict__ order0,
-                                                        const int32_t *__restrict__ pos0,
+__global__ void __launch_bounds__(kThreads) seed_kernel(const float *__restrict__ xs0, const float *__restrict__ xs1,
+                                                        int64_t n, int dp, int m, const int32_t *__restrict__ order0,
                                                         const int32_t *__restrict__ order1,
+                                                        const int32_t *__restrict__ p0_of1,
                                                         const int32_t *__restrict__ pos1,
                                                         float *__restrict__ seeds) {
     constexpr int W = VPL * 16;
@@ -150,7 +172,7 @@ __global__ void __launch_bounds__(kThreads) seed_kernel(const float *__restrict_
         }
         float qv[D];
 #pragma unroll
-        for (int f = 0; f < D; ++f) qv[f] = xs[i * dp + f];
+        for (int f = 0; f < D; ++f) qv[f] = xs0[k * dp + f];
         uint32_t v[2 * VPL];
 #pragma unroll
         for (int t = 0; t < VPL; ++t) {
@@ -158,7 +180,7 @@ __global__ void __launch_bounds__(kThreads) seed_kernel(const float *__restrict_
             uint32_t val = 0xFFFFFFFFu;
             if (pk >= 0 && pk < n) {
                 const int64_t j = order0[pk];
-                if (j < i) val = dist_bits<D>(xs, dp, j, qv);
+                if (j < i) val = dist_bits<D>(xs0 + pk * dp, qv);
             }
             v[t] = val;
         }
@@ -170,8 +192,8 @@ __global__ void __launch_bounds__(kThreads) seed_kernel(const float *__restrict_
             if (pk >= 0 && pk < n) {
                 const int64_t j = order1[pk];
                 if (j < i) {
-                    const int64_t pj = pos0[j];
-                    if (pj < k - W || pj >= k + W) val = dist_bits<D>(xs, dp, j, qv);
+                    const int64_t pj = p0_of1[pk];
+                    if (pj < k - W || pj >= k + W) val = dist_bits<D>(xs1 + pk * dp, qv);
                 }
             }
             v[VPL + t] = val;
@@ -205,10 +227,11 @@ __global__ void __launch_bounds__(kThreads) seed_kernel(const float *__restrict_
 }
 
 struct Layout {
-    size_t keys_a, keys_b, keys0, idx0_a, idx0_b, idx1_a, idx1_b, pos0, pos1, bounds, cub, cub_bytes, total;
+    size_t keys_a, keys_b, keys0, idx0_a, idx0_b, idx1_a, idx1_b, pos0, pos1, p0of1, xs0, xs1, bounds, cub, cub_bytes,
+        total;
 };
 
-Layout layout(int64_t n) {
+Layout layout(int64_t n, int dp) {
     Layout L{};
     size_t off = 0;
     auto take = [&](size_t bytes) {
@@ -225,6 +248,9 @@ Layout layout(int64_t n) {
     L.idx1_b = take((size_t)n * 4);
     L.pos0 = take((size_t)n * 4);
     L.pos1 = take((size_t)n * 4);
+    L.p0of1 = take((size_t)n * 4);
+    L.xs0 = take((size_t)n * dp * 4);
+    L.xs1 = take((size_t)n * dp * 4);
     L.bounds = take(2 * 256 * 4);
     L.cub_bytes = align_up((size_t)(4u << 20) + (size_t)n / 2, 256);  // radix-sort scratch budget
     L.cub = take(L.cub_bytes);
@@ -232,28 +258,35 @@ Layout layout(int64_t n) {
     return L;
 }
 
+struct SeedArgs {
+    const float *xs0, *xs1;
+    int64_t n;
+    int dp, m;
+    const int32_t *o0, *o1, *p0of1, *p1;
+    float *seeds;
+};
+
 template <int D, int VPL>
-void launch_seed(int grid, const float *xs, int64_t n, int dp, int m, const int32_t *o0, const int32_t *p0,
-                 const int32_t *o1, const int32_t *p1, float *seeds, cudaStream_t stream) {
-    seed_kernel<D, VPL><<<grid, kThreads, 0, stream>>>(xs, n, dp, m, o0, p0, o1, p1, seeds);
+void launch_seed(int grid, const SeedArgs &a, cudaStream_t stream) {
+    seed_kernel<D, VPL><<<grid, kThreads, 0, stream>>>(a.xs0, a.xs1, a.n, a.dp, a.m, a.o0, a.o1, a.p0of1, a.p1,
+                                                       a.seeds);
 }
 
 template <int VPL>
-bool dispatch_seed(int D, int grid, const float *xs, int64_t n, int dp, int m, const int32_t *o0, const int32_t *p0,
-                   const int32_t *o1, const int32_t *p1, float *seeds, cudaStream_t stream) {
+bool dispatch_seed(int D, int grid, const SeedArgs &a, cudaStream_t stream) {
     switch (D) {
-        case 1: launch_seed<1, VPL>(grid, xs, n, dp, m, o0, p0, o1, p1, seeds, stream); return true;
-        case 2: launch_seed<2, VPL>(grid, xs, n, dp, m, o0, p0, o1, p1, seeds, stream); return true;
-        case 3: launch_seed<3, VPL>(grid, xs, n, dp, m, o0, p0, o1, p1, seeds, stream); return true;
-        case 4: launch_seed<4, VPL>(grid, xs, n, dp, m, o0, p0, o1, p1, seeds, stream); return true;
-        case 5: launch_seed<5, VPL>(grid, xs, n, dp, m, o0, p0, o1, p1, seeds, stream); return true;
-        case 6: launch_seed<6, VPL>(grid, xs, n, dp, m, o0, p0, o1, p1, seeds, stream); return true;
-        case 7: launch_seed<7, VPL>(grid, xs, n, dp, m, o0, p0, o1, p1, seeds, stream); return true;
-        case 8: launch_seed<8, VPL>(grid, xs, n, dp, m, o0, p0, o1, p1, seeds, stream); return true;
-        case 12: launch_seed<12, VPL>(grid, xs, n, dp, m, o0, p0, o1, p1, seeds, stream); return true;
-        case 16: launch_seed<16, VPL>(grid, xs, n, dp, m, o0, p0, o1, p1, seeds, stream); return true;
-        case 20: launch_seed<20, VPL>(grid, xs, n, dp, m, o0, p0, o1, p1, seeds, stream); return true;
-        case 24: launch_seed<24, VPL>(grid, xs, n, dp, m, o0, p0, o1, p1, seeds, stream); return true;
+        case 1: launch_seed<1, VPL>(grid, a, stream); return true;
+        case 2: launch_seed<2, VPL>(grid, a, stream); return true;
+        case 3: launch_seed<3, VPL>(grid, a, stream); return true;
+        case 4: launch_seed<4, VPL>(grid, a, stream); return true;
+        case 5: launch_seed<5, VPL>(grid, a, stream); return true;
+        case 6: launch_seed<6, VPL>(grid, a, stream); return true;
+        case 7: launch_seed<7, VPL>(grid, a, stream); return true;
+        case 8: launch_seed<8, VPL>(grid, a, stream); return true;
+        case 12: launch_seed<12, VPL>(grid, a, stream); return true;
+        case 16: launch_seed<16, VPL>(grid, a, stream); return true;
+        case 20: launch_seed<20, VPL>(grid, a, stream); return true;
+        case 24: launch_seed<24, VPL>(grid, a, stream); return true;
     }
     return false;
 }
@@ -264,7 +297,7 @@ int grid_of(int64_t work) {
 
 }  // namespace
 
-size_t workspace(int64_t n) { return n < kMinPoints ? 0 : layout(n).total; }
+size_t workspace(int64_t n, int dp) { return n < kMinPoints ? 0 : layout(n, dp).total; }
 
 int window() {
     const char *env = std::getenv("NNGP_KNN_SEED_W");
@@ -279,7 +312,7 @@ nngp_status prefix_seeds(const float *xs, int64_t n, int d, int D, int dp, int m
     const int W = window();
     if (W == 0 || n < kMinPoints || m < 1 || d < 1 || d > 24 || D < d || dp % 4 != 0 || dp < D)
         return fail(NNGP_ERR_UNSUPPORTED, "knn seeds: shape outside the seeded search");
-    const Layout L = layout(n);
+    const Layout L = layout(n, dp);
     if (!ws || ws_bytes < L.total) return fail(NNGP_ERR_WORKSPACE, "knn seeds: workspace too small");
     char *base = reinterpret_cast<char *>(align_up(reinterpret_cast<uintptr_t>(ws), 256));
     auto at = [&](size_t off) { return reinterpret_cast<void *>(base + off); };
@@ -313,11 +346,17 @@ nngp_status prefix_seeds(const float *xs, int64_t n, int d, int D, int dp, int m
         }
         inverse_kernel<<<grid_of(n), kThreads, 0, stream>>>(order[c], n, pos[c]);
         NNGP_CUDA_TRY(cudaGetLastError());
+        gather_kernel<<<grid_of(n * (dp / 4)), kThreads, 0, stream>>>(xs, n, dp, order[c],
+                                                                      static_cast<float *>(at(c ? L.xs1 : L.xs0)));
+        NNGP_CUDA_TRY(cudaGetLastError());
     }
+    int32_t *p0of1 = static_cast<int32_t *>(at(L.p0of1));
+    cross_pos_kernel<<<grid_of(n), kThreads, 0, stream>>>(order[1], pos[0], n, p0of1);
+    NNGP_CUDA_TRY(cudaGetLastError());
     const int grid = (int)std::min<int64_t>((n + kThreads / 32 - 1) / (kThreads / 32), (int64_t)kNumSMsB200 * 16);
-    const bool ok = W == 128 ? dispatch_seed<8>(D, grid, xs, n, dp, m, order[0], pos[0], order[1], pos[1], seeds, stream)
-                             : dispatch_seed<16>(D, grid, xs, n, dp, m, order[0], pos[0], order[1], pos[1], seeds,
-                                                 stream);
+    const SeedArgs sa{static_cast<const float *>(at(L.xs0)), static_cast<const float *>(at(L.xs1)), n, dp, m,
+                      order[0], order[1], p0of1, pos[1], seeds};
+    const bool ok = W == 128 ? dispatch_seed<8>(D, grid, sa, stream) : dispatch_seed<16>(D, grid, sa, stream);
     if (!ok) return fail(NNGP_ERR_UNSUPPORTED, "knn seeds: no kernel for D = " + std::to_string(D));
     NNGP_CUDA_TRY(cudaGetLastError());
     if (order0_out) *order0_out = order[0];

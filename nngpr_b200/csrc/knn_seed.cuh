@@ -12,8 +12,8 @@ namespace seed {
 
 constexpr int64_t kMinPoints = 8192;  // below this the search is short and seeding does not pay
 
-// Workspace bytes of prefix_seeds for n points (0 when n < kMinPoints).
-size_t workspace(int64_t n);
+// Workspace bytes of prefix_seeds for n points of row stride dp (0 when n < kMinPoints).
+size_t workspace(int64_t n, int dp);
 
 // Window half-width in curve positions: NNGP_KNN_SEED_W = 128 or 256 (default 128: the faster
 // fit step at d = 3, 8 and 16); 0 turns seeding off.
