@@ -669,15 +669,16 @@ nngp_status knn_impl(const T *ref, int64_t n_ref, const T *query, int64_t n_quer
                     int32_t total = 0;
                     NNGP_CUDA_TRY(cudaMemcpyAsync(hs, lists.pruned, sizeof(hs), cudaMemcpyDeviceToHost, stream));
                     NNGP_CUDA_TRY(cudaStreamSynchronize(stream));
-                    NNGP_CUDA_TRY(cudaMemcpyAsync(&total, lists.offsets + hs[0].n_items, sizeof(total),
+                    NNGP_CUDA_TRY(cudaMemcpyAsync(&total, lists.offsets + hs[0].n_groups, sizeof(total),
                                                   cudaMemcpyDeviceToHost, stream));
                     NNGP_CUDA_TRY(cudaStreamSynchronize(stream));
                     std::fprintf(stderr,
-                                 "nngp_knn: pruned rows=%lld groups=%lld tiles listed=%d (%.1f per group of %lld); "
-                                 "index-order rows=%lld\n",
-                                 (long long)hs[0].n_rows, (long long)hs[0].n_items, total,
-                                 (double)total / (double)std::max<int64_t>(1, hs[0].n_items),
-                                 (long long)(p.n_ref_pad / tc::kTcRefTile), (long long)hs[1].n_rows);
+                                 "nngp_knn: pruned rows=%lld groups=%lld items=%lld tiles listed=%d (%.1f per group of "
+                                 "%lld); index-order rows=%lld items=%lld\n",
+                                 (long long)hs[0].n_rows, (long long)hs[0].n_groups, (long long)hs[0].n_items, total,
+                                 (double)total / (double)std::max<int64_t>(1, hs[0].n_groups),
+                                 (long long)(p.n_ref_pad / tc::kTcRefTile), (long long)hs[1].n_rows,
+                                 (long long)hs[1].n_items);
                 }
             }
             // persistent grid: the CTAs one SM holds (shared memory and TMEM sized for them) per SM;
@@ -689,7 +690,7 @@ nngp_status knn_impl(const T *ref, int64_t n_ref, const T *query, int64_t n_quer
             const int32_t *none = nullptr;
             const int64_t *no_sizes = nullptr;
             auto launch = [&](const unsigned char *tiles_c, int64_t items_bound, const int32_t *rows_perm,
-                              const int32_t *row_off, const int64_t *dev_sizes, const int32_t *item_order,
+                              const int32_t *row_off, const int64_t *dev_sizes, const tc::TcItems &items,
                               const int32_t *ref_perm, const int32_t *tile_off, const int32_t *tile_list,
                               int *counter) -> nngp_status {
                 if (items_bound == 0) return NNGP_OK;
@@ -702,7 +703,7 @@ nngp_status knn_impl(const T *ref, int64_t n_ref, const T *query, int64_t n_quer
                                  (int)(tile_list != nullptr));
                 void *args[] = {(void *)&tiles_c,  (void *)&q_c,      (void *)&acc_c,      (void *)&r2_c,
                                 (void *)&seeds_c,  (void *)&rows_perm, (void *)&row_off,   (void *)&dev_sizes,
-                                (void *)&item_order, (void *)&ref_perm, (void *)&tile_off, (void *)&tile_list,
+                                (void *)&items,    (void *)&ref_perm, (void *)&tile_off, (void *)&tile_list,
                                 (void *)&counter,  (void *)&n_query,  (void *)&n_ref,      (void *)&has_cut,
                                 (void *)&cut,      (void *)&m,        (void *)&out,        (void *)&flags};
                 NNGP_CUDA_TRY(cudaLaunchKernel(reinterpret_cast<const void *>(p.tv.fn), dim3(grid), dim3(p.tv.threads),
@@ -713,13 +714,17 @@ nngp_status knn_impl(const T *ref, int64_t n_ref, const T *query, int64_t n_quer
             if (pruned) {
                 const int64_t *ps = reinterpret_cast<const int64_t *>(lists.pruned);
                 const int64_t *is = reinterpret_cast<const int64_t *>(lists.index_order);
-                lst = launch(tiles_curve, lists.max_groups, lists.rows, lists.row_off, ps, lists.item_order,
+                lst = launch(tiles_curve, lists.max_items[0], lists.rows, lists.row_off, ps, lists.pruned_items,
                              lists.ref_order, lists.offsets, lists.tiles, ctr + 1);
                 if (lst != NNGP_OK) return lst;
-                lst = launch(tiles, lists.max_index_items, lists.rows, none, is, none, none, none, none, ctr);
+                if ((lst = prune::merge(lists, 0, p.tv.rows_per_item, m, out, stream)) != NNGP_OK) return lst;
+                lst = launch(tiles, lists.max_items[1], lists.rows, none, is, lists.index_items, none, none, none, ctr);
+                if (lst != NNGP_OK) return lst;
+                lst = prune::merge(lists, 1, p.tv.rows_per_item, m, out, stream);
             } else {
                 const int64_t items = (n_query + p.tv.rows_per_item - 1) / p.tv.rows_per_item;
-                lst = launch(tiles, items, none, none, no_sizes, none, none, none, none, ctr);
+                const tc::TcItems whole{};
+                lst = launch(tiles, items, none, none, no_sizes, whole, none, none, none, ctr);
             }
             if (lst != NNGP_OK) return lst;
         }

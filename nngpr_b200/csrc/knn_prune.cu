@@ -19,7 +19,7 @@
 //
 // Rows: band = floor(log2(n / i)) groups rows whose prefixes differ by less than a factor of
 // two, hence seeds of similar size.  A row whose seed exceeds 16 times its band's geometric mean
-// (its window held few earlier points) would inflate its group's reach, so it goes to the
+// (its windows held few nearby earlier points) would inflate its group's reach, so it goes to the
 // index-order launch with the rows below n / 8, where it costs only its prefix.
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
@@ -38,9 +38,10 @@ namespace prune {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kBands = 4;            // i >= n / 8: bands 0..2 (3 only at rounding edges)
+constexpr int kEarlyShift = 3;       // rows below n / 8 take the index-order search
+constexpr int kBands = kEarlyShift + 1;  // band b: rows [n / 2^(b + 1), n / 2^b) (the last only at rounding edges)
 constexpr int kLooseLog2Q = 4 * 256;  // seed > 16 x band geometric mean (log2 in 1/256 units)
-constexpr uint64_t kIndexOrderTag = 1ull << 34;  // above (band << 32 | curve position) for bands < 4
+constexpr uint64_t kIndexOrderTag = 1ull << 36;  // above (band << 32 | curve position) for bands < 16
 
 __device__ __forceinline__ int band_of(int64_t i, int64_t n) {
     int b = 0;
@@ -95,8 +96,8 @@ __global__ void __launch_bounds__(kThreads) tile_box_kernel(const float *__restr
 
 // Ref order: points sorted by (index class, curve position), class = 3 - band: [0, n/8),
 // [n/8, n/4), [n/4, n/2), [n/2, n).  A tile then holds refs of one class (up to the one tile at
-// each class boundary), so a group of rows of band b skips whole tiles whose refs all come
-// after its rows, and meets refs j > i only in its own class.
+// each class boundary), so a group of rows of band b skips whole tiles whose refs all come after
+// its rows, and meets refs j > i only in its own class.
 __global__ void __launch_bounds__(kThreads) ref_keys_kernel(int64_t n, const int32_t *__restrict__ pos0,
                                                             uint64_t *__restrict__ keys, int32_t *__restrict__ vals) {
     for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
@@ -110,8 +111,8 @@ __global__ void __launch_bounds__(kThreads) ref_keys_kernel(int64_t n, const int
 __global__ void __launch_bounds__(kThreads) band_stats_kernel(int64_t n, int64_t early, const float *__restrict__ seeds,
                                                               unsigned long long *__restrict__ sum,
                                                               unsigned long long *__restrict__ cnt) {
-    long long s[kBands] = {0, 0, 0, 0};
-    unsigned long long c[kBands] = {0, 0, 0, 0};
+    long long s[kBands] = {};
+    unsigned long long c[kBands] = {};
     for (int64_t i = early + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
         const float tau = seeds[i];
@@ -136,7 +137,7 @@ __global__ void __launch_bounds__(kThreads) band_stats_kernel(int64_t n, int64_t
     }
 }
 
-// Sort keys: pruned rows (band << 32 | curve position), the others (2^34 | index); counts
+// Sort keys: pruned rows (band << 32 | curve position), the others (2^36 | index); counts
 // of pruned rows per band and in total.
 __global__ void __launch_bounds__(kThreads) classify_kernel(int64_t n, int64_t early, const float *__restrict__ seeds,
                                                             const int32_t *__restrict__ pos0,
@@ -144,7 +145,7 @@ __global__ void __launch_bounds__(kThreads) classify_kernel(int64_t n, int64_t e
                                                             const unsigned long long *__restrict__ cnt,
                                                             uint64_t *__restrict__ keys, int32_t *__restrict__ vals,
                                                             unsigned long long *__restrict__ pruned_cnt) {
-    unsigned long long c[kBands] = {0, 0, 0, 0};
+    unsigned long long c[kBands] = {};
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         bool pruned = false;
         int b = 0;
@@ -194,10 +195,10 @@ __global__ void __launch_bounds__(kThreads) segment_kernel(int64_t n, const uint
     for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
         int32_t h = 0;
         if (r < (int64_t)total) {
-            const int b = (int)(skeys[r] >> 32);
+            const int b = (int)(skeys[r] >> 32) & 15;
             bool head = r == 0;
             if (!head) {
-                const int bp = (int)(skeys[r - 1] >> 32);
+                const int bp = (int)(skeys[r - 1] >> 32) & 15;
                 head = bp != b || cell_of(r - 1, b) != cell_of(r, b);
             }
             h = head ? (int32_t)r : 0;
@@ -233,9 +234,11 @@ __global__ void sizes_kernel(int64_t n, int G, const int32_t *__restrict__ gh, c
     pruned->first_row = 0;
     pruned->n_rows = (int64_t)total;
     pruned->n_items = n_groups;
+    pruned->n_groups = n_groups;
     index_order->first_row = (int64_t)total;
     index_order->n_rows = n - (int64_t)total;
-    index_order->n_items = (n - (int64_t)total + G - 1) / G;
+    index_order->n_groups = (n - (int64_t)total + G - 1) / G;
+    index_order->n_items = index_order->n_groups;
 }
 
 // Box, largest seed and largest index of every pruned group; one warp per group.
@@ -247,7 +250,7 @@ __global__ void __launch_bounds__(kThreads) group_box_kernel(const float *__rest
                                                              float *__restrict__ ghi, float *__restrict__ gtau,
                                                              int32_t *__restrict__ glim) {
     const int lane = threadIdx.x & 31;
-    const int64_t n_groups = pruned->n_items;
+    const int64_t n_groups = pruned->n_groups;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t g = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; g < n_groups; g += nw) {
         const int64_t r0 = row_off[g], r1 = row_off[g + 1];
@@ -311,26 +314,19 @@ __device__ __forceinline__ bool box_overlap(const Boxes &b, int64_t g, int64_t t
     return true;
 }
 
-// One warp per group: counts[g] = tiles needed (0 for the slots past the groups), and the
-// sort key of the group's place in the work order (longest list first).
+// One warp per group: counts[g] = tiles needed (0 for the slots past the groups).
 __global__ void __launch_bounds__(kThreads) count_kernel(Boxes b, const DevSizes *__restrict__ pruned,
                                                          int64_t max_groups, int64_t n_tiles,
-                                                         int32_t *__restrict__ counts,
-                                                         uint32_t *__restrict__ order_keys,
-                                                         int32_t *__restrict__ order_vals) {
+                                                         int32_t *__restrict__ counts) {
     const int lane = threadIdx.x & 31;
-    const int64_t n_groups = pruned->n_items;
+    const int64_t n_groups = pruned->n_groups;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t g = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; g < max_groups; g += nw) {
         int c = 0;
         if (g < n_groups)
             for (int64_t t = lane; t < n_tiles; t += 32) c += tile_needed(b, g, t) ? 1 : 0;
         c = (int)__reduce_add_sync(0xFFFFFFFFu, (unsigned)c);
-        if (lane == 0) {
-            counts[g] = c;
-            order_keys[g] = g < n_groups ? 0xFFFFFFFEu - (uint32_t)c : 0xFFFFFFFFu;
-            order_vals[g] = (int32_t)g;
-        }
+        if (lane == 0) counts[g] = c;
     }
 }
 
@@ -341,7 +337,7 @@ __global__ void __launch_bounds__(kThreads) fill_kernel(Boxes b, const DevSizes 
                                                         const int32_t *__restrict__ offsets,
                                                         int32_t *__restrict__ list) {
     const int lane = threadIdx.x & 31;
-    const int64_t n_groups = pruned->n_items;
+    const int64_t n_groups = pruned->n_groups;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t g = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; g < n_groups; g += nw) {
         int64_t o = offsets[g];
@@ -358,10 +354,128 @@ __global__ void __launch_bounds__(kThreads) fill_kernel(Boxes b, const DevSizes 
     }
 }
 
+// ---- work items (split long tile ranges) ----
+// Tiles of every group (0 past the groups): the list length (pruned) or the tiles below the
+// limit of the group's last row (index order; rows ascend, the prefix search has cut 0).
+__global__ void __launch_bounds__(kThreads) group_tiles_kernel(const DevSizes *__restrict__ sz, int64_t maxg,
+                                                               const int32_t *__restrict__ offsets,
+                                                               const int32_t *__restrict__ rows, int G, int64_t n,
+                                                               int32_t *__restrict__ cnt) {
+    const int64_t ng = sz->n_groups;
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g <= maxg; g += (int64_t)gridDim.x * blockDim.x) {
+        int64_t c = 0;
+        if (g < ng) {
+            if (offsets) {
+                c = offsets[g + 1] - offsets[g];
+            } else {
+                const int64_t last = sz->first_row + min((g + 1) * (int64_t)G, sz->n_rows) - 1;
+                const int64_t lim = min((int64_t)rows[last], n);
+                c = (lim + kTileRefs - 1) / kTileRefs;
+            }
+        }
+        cnt[g] = (int32_t)c;
+    }
+}
+
+// Items per group: K = ceil(tiles / C) with C = max(kChunkTiles, ceil(2 total / kMaxSlots)), so
+// the split groups need at most sum over them of (tiles / C + 1) < 2 total / C <= kMaxSlots
+// partial slots.  S = K for split groups (their slots), else 0.
+__global__ void __launch_bounds__(kThreads) split_kernel(const DevSizes *__restrict__ sz, int64_t maxg,
+                                                         const int32_t *__restrict__ cnt,
+                                                         const int32_t *__restrict__ cbase, int32_t *__restrict__ K,
+                                                         int32_t *__restrict__ S) {
+    const int64_t ng = sz->n_groups;
+    const int64_t total = cbase[maxg];
+    const int64_t C = max((int64_t)kChunkTiles, (2 * total + kMaxSlots - 1) / kMaxSlots);
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g <= maxg; g += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k = g < ng ? max((int64_t)1, (cnt[g] + C - 1) / C) : 0;
+        K[g] = (int32_t)k;
+        S[g] = k > 1 ? (int32_t)k : 0;
+    }
+}
+
+// Item descriptors (group, tile range, slot) and their sort keys (most tiles first; the slots
+// past the items last).
+__global__ void __launch_bounds__(kThreads) item_fill_kernel(const DevSizes *__restrict__ sz, int64_t maxg,
+                                                             int64_t max_items, const int32_t *__restrict__ cnt,
+                                                             const int32_t *__restrict__ K,
+                                                             const int32_t *__restrict__ kbase,
+                                                             const int32_t *__restrict__ sbase,
+                                                             int32_t *__restrict__ group, int32_t *__restrict__ t0,
+                                                             int32_t *__restrict__ t1, int32_t *__restrict__ slot,
+                                                             uint32_t *__restrict__ okey, int32_t *__restrict__ oval) {
+    const int64_t ng = sz->n_groups;
+    const int64_t T = kbase[maxg];
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < ng; g += stride) {
+        const int64_t k_n = K[g], c = cnt[g];
+        for (int64_t k = 0; k < k_n; ++k) {
+            const int64_t d = kbase[g] + k;
+            const int64_t a = c * k / k_n, b = c * (k + 1) / k_n;
+            group[d] = (int32_t)g;
+            t0[d] = (int32_t)a;
+            t1[d] = (int32_t)b;
+            slot[d] = k_n > 1 ? sbase[g] + (int32_t)k : -1;
+            okey[d] = 0xFFFFFFFFu - (uint32_t)(b - a);
+            oval[d] = (int32_t)d;
+        }
+    }
+    for (int64_t d = T + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; d < max_items; d += stride) {
+        okey[d] = 0xFFFFFFFFu;
+        oval[d] = (int32_t)d;
+    }
+}
+
+__global__ void items_size_kernel(DevSizes *__restrict__ sz, int64_t maxg, const int32_t *__restrict__ kbase) {
+    sz->n_items = kbase[maxg];
+}
+
+// One warp per (split group, row): the top m of the group's partial lists (each ascending).
+__global__ void __launch_bounds__(kThreads) merge_kernel(const DevSizes *__restrict__ sz, int64_t maxg, int G,
+                                                         const int32_t *__restrict__ K,
+                                                         const int32_t *__restrict__ sbase,
+                                                         const int32_t *__restrict__ row_off,
+                                                         const int32_t *__restrict__ rows,
+                                                         const unsigned long long *__restrict__ partial, int m,
+                                                         int32_t *__restrict__ out) {
+    const unsigned FULL = 0xFFFFFFFFu;
+    const int lane = threadIdx.x & 31;
+    const int64_t ng = sz->n_groups;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; w < maxg * G; w += nw) {
+        const int64_t g = w / G, r = w - g * G;
+        if (g >= ng || K[g] <= 1) continue;
+        int64_t r0, nr;
+        if (row_off) {
+            r0 = row_off[g];
+            nr = row_off[g + 1] - r0;
+        } else {
+            r0 = sz->first_row + g * G;
+            nr = min((int64_t)G, sz->first_row + sz->n_rows - r0);
+        }
+        if (r >= nr) continue;
+        const int64_t s0 = sbase[g];
+        unsigned long long cur = partial[(s0 * G + r) * 32 + lane];
+        for (int64_t k = 1; k < K[g]; ++k) {
+            const unsigned long long nx = partial[((s0 + k) * G + r) * 32 + (31 - lane)];
+            cur = nx < cur ? nx : cur;  // the 32 smallest of both lists, a bitonic sequence
+#pragma unroll
+            for (int j = 16; j > 0; j >>= 1) {
+                const unsigned long long o = __shfl_xor_sync(FULL, cur, j);
+                cur = ((lane & j) == 0) ? (o < cur ? o : cur) : (o > cur ? o : cur);
+            }
+        }
+        if (lane < m) out[(int64_t)rows[r0 + r] * m + lane] = (int32_t)(uint32_t)cur;
+    }
+}
+
 struct Layout {
     int64_t n_tiles, max_groups;
     size_t tlo, thi, tmin, stats, keys_a, keys_b, vals_a, vals_b, rvals_a, rvals_b, headpos, seg_start, gh, gid, row_off, sizes, glo,
-        ghi, gtau, glim, counts, offsets, okeys_a, okeys_b, ovals_a, ovals_b, list, cub, cub_bytes, total;
+        ghi, gtau, glim, counts, offsets, list, cub, cub_bytes, total;
+    int64_t maxg[2], max_items[2];
+    size_t cnt[2], cbase[2], K[2], kbase[2], S[2], sbase[2], igroup[2], it0[2], it1[2], islot[2], okey_a[2], okey_b[2],
+        oval_a[2], oval_b[2], partial[2];
 };
 
 // Groups: segments per band <= (pruned rows of the band) / 256 or 1, groups per segment
@@ -398,10 +512,22 @@ Layout layout(int64_t n, int d, int G) {
     L.glim = take((size_t)L.max_groups * 4);
     L.counts = take((size_t)(L.max_groups + 1) * 4);
     L.offsets = take((size_t)(L.max_groups + 1) * 4);
-    L.okeys_a = take((size_t)L.max_groups * 4);
-    L.okeys_b = take((size_t)L.max_groups * 4);
-    L.ovals_a = take((size_t)L.max_groups * 4);
-    L.ovals_b = take((size_t)L.max_groups * 4);
+    L.maxg[0] = L.max_groups;
+    L.maxg[1] = (n + G - 1) / G;
+    for (int p = 0; p < 2; ++p) {
+        const int64_t g1 = L.maxg[p] + 1;
+        L.max_items[p] = L.maxg[p] + kMaxSlots;
+        L.cnt[p] = take((size_t)g1 * 4);
+        L.cbase[p] = take((size_t)g1 * 4);
+        L.K[p] = take((size_t)g1 * 4);
+        L.kbase[p] = take((size_t)g1 * 4);
+        L.S[p] = take((size_t)g1 * 4);
+        L.sbase[p] = take((size_t)g1 * 4);
+        for (size_t *f : {&L.igroup[p], &L.it0[p], &L.it1[p], &L.islot[p], &L.okey_a[p], &L.okey_b[p], &L.oval_a[p],
+                          &L.oval_b[p]})
+            *f = take((size_t)L.max_items[p] * 4);
+        L.partial[p] = take((size_t)kMaxSlots * G * 32 * 8);
+    }
     L.list = take((size_t)L.max_groups * L.n_tiles * 4);
     L.cub_bytes = align_up((size_t)(4u << 20) + (size_t)n / 2, 256);
     L.cub = take(L.cub_bytes);
@@ -415,7 +541,7 @@ int grid_of(int64_t threads) {
 
 }  // namespace
 
-int64_t early_rows(int64_t n) { return n / 8; }
+int64_t early_rows(int64_t n) { return n >> kEarlyShift; }
 
 bool enabled() {
     const char *env = std::getenv("NNGP_KNN_PRUNE");
@@ -423,14 +549,14 @@ bool enabled() {
 }
 
 size_t workspace(int64_t n, int d, int rows_per_group) {
-    if (n < kMinPoints || n > INT32_MAX - 1 || d < 1 || d > kMaxDim || rows_per_group < 1) return 0;
+    if (n < kMinPoints || n > kMaxPoints || d < 1 || d > kMaxDim || rows_per_group < 1) return 0;
     return layout(n, d, rows_per_group).total;
 }
 
 nngp_status build(const float *xs, int64_t n, int d, int dp, int G, int bits, const float *seeds,
                   const int32_t *order0, const int32_t *pos0, const uint64_t *keys0, void *ws, size_t ws_bytes,
                   Lists *out, cudaStream_t stream) {
-    if (n < kMinPoints || n > INT32_MAX - 1 || d < 1 || d > kMaxDim || G < 1 || bits < 1 || d * bits > 60 || !xs ||
+    if (n < kMinPoints || n > kMaxPoints || d < 1 || d > kMaxDim || G < 1 || bits < 1 || d * bits > 60 || !xs ||
         !seeds || !order0 || !pos0 || !keys0 || !out)
         return fail(NNGP_ERR_UNSUPPORTED, "knn pruning: shape outside the pruned search");
     const Layout L = layout(n, d, G);
@@ -464,10 +590,10 @@ nngp_status build(const float *xs, int64_t n, int d, int dp, int G, int bits, co
     cub::DoubleBuffer<uint64_t> rk(static_cast<uint64_t *>(at(L.keys_a)), static_cast<uint64_t *>(at(L.keys_b)));
     cub::DoubleBuffer<int32_t> rv(static_cast<int32_t *>(at(L.rvals_a)), static_cast<int32_t *>(at(L.rvals_b)));
     size_t need0 = 0;
-    NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, need0, rk, rv, (int)n, 0, 34, stream));
+    NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, need0, rk, rv, (int)n, 0, 36, stream));
     if (need0 > L.cub_bytes) return fail(NNGP_ERR_WORKSPACE, "knn pruning: sort scratch exceeds the budget");
     size_t have0 = L.cub_bytes;
-    NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(at(L.cub), have0, rk, rv, (int)n, 0, 34, stream));
+    NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(at(L.cub), have0, rk, rv, (int)n, 0, 36, stream));
     const int32_t *ref_order = rv.Current();
     tile_box_kernel<<<grid_of(L.n_tiles * 32), kThreads, 0, stream>>>(xs, n, d, dp, ref_order, L.n_tiles, tlo, thi,
                                                                        tmin);
@@ -484,11 +610,11 @@ nngp_status build(const float *xs, int64_t n, int d, int dp, int G, int bits, co
     cub::DoubleBuffer<uint64_t> dk(static_cast<uint64_t *>(at(L.keys_a)), static_cast<uint64_t *>(at(L.keys_b)));
     cub::DoubleBuffer<int32_t> dv(static_cast<int32_t *>(at(L.vals_a)), static_cast<int32_t *>(at(L.vals_b)));
     size_t need = 0;
-    NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, need, dk, dv, (int)n, 0, 35, stream));
+    NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, need, dk, dv, (int)n, 0, 37, stream));
     nngp_status st = cub_check(need);
     if (st != NNGP_OK) return st;
     size_t have = L.cub_bytes;
-    NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(at(L.cub), have, dk, dv, (int)n, 0, 35, stream));
+    NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(at(L.cub), have, dk, dv, (int)n, 0, 37, stream));
     const int32_t *rows = dv.Current();
 
     // groups: segments of one band and one octree cell, cut every G rows
@@ -516,11 +642,8 @@ nngp_status build(const float *xs, int64_t n, int d, int dp, int G, int bits, co
                                                                           ghi, gtau, glim);
     NNGP_CUDA_TRY(cudaGetLastError());
     Boxes b{tlo, thi, glo, ghi, gtau, tmin, glim, d, (double)(d + 3) * 1.1920928955078125e-07};
-    cub::DoubleBuffer<uint32_t> ok(static_cast<uint32_t *>(at(L.okeys_a)), static_cast<uint32_t *>(at(L.okeys_b)));
-    cub::DoubleBuffer<int32_t> ov(static_cast<int32_t *>(at(L.ovals_a)), static_cast<int32_t *>(at(L.ovals_b)));
     NNGP_CUDA_TRY(cudaMemsetAsync(counts + L.max_groups, 0, sizeof(int32_t), stream));
-    count_kernel<<<grid_of(L.max_groups * 32), kThreads, 0, stream>>>(b, sizes, L.max_groups, L.n_tiles, counts,
-                                                                      ok.Current(), ov.Current());
+    count_kernel<<<grid_of(L.max_groups * 32), kThreads, 0, stream>>>(b, sizes, L.max_groups, L.n_tiles, counts);
     NNGP_CUDA_TRY(cudaGetLastError());
     need = 0;
     NNGP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, need, counts, offsets, (int)(L.max_groups + 1), stream));
@@ -529,22 +652,79 @@ nngp_status build(const float *xs, int64_t n, int d, int dp, int G, int bits, co
     NNGP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(at(L.cub), have, counts, offsets, (int)(L.max_groups + 1), stream));
     fill_kernel<<<grid_of(L.max_groups * 32), kThreads, 0, stream>>>(b, sizes, L.n_tiles, offsets, list);
     NNGP_CUDA_TRY(cudaGetLastError());
-    need = 0;
-    NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, need, ok, ov, (int)L.max_groups, 0, 32, stream));
-    if ((st = cub_check(need)) != NNGP_OK) return st;
-    have = L.cub_bytes;
-    NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(at(L.cub), have, ok, ov, (int)L.max_groups, 0, 32, stream));
+
+    // work items of both launches: long tile ranges split, most tiles first
+    for (int pl = 0; pl < 2; ++pl) {
+        const int64_t maxg = L.maxg[pl], g1 = maxg + 1, mi = L.max_items[pl];
+        int32_t *cnt = static_cast<int32_t *>(at(L.cnt[pl])), *cbase = static_cast<int32_t *>(at(L.cbase[pl]));
+        int32_t *K = static_cast<int32_t *>(at(L.K[pl])), *kbase = static_cast<int32_t *>(at(L.kbase[pl]));
+        int32_t *S = static_cast<int32_t *>(at(L.S[pl])), *sbase = static_cast<int32_t *>(at(L.sbase[pl]));
+        DevSizes *sz = sizes + pl;
+        group_tiles_kernel<<<grid_of(g1), kThreads, 0, stream>>>(sz, maxg, pl == 0 ? offsets : nullptr, rows, G, n,
+                                                                 cnt);
+        NNGP_CUDA_TRY(cudaGetLastError());
+        auto scan = [&](int32_t *src, int32_t *dst) -> nngp_status {
+            size_t nb = 0;
+            NNGP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, nb, src, dst, (int)g1, stream));
+            if (nb > L.cub_bytes) return fail(NNGP_ERR_WORKSPACE, "knn pruning: scan scratch exceeds the budget");
+            nb = L.cub_bytes;
+            NNGP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(at(L.cub), nb, src, dst, (int)g1, stream));
+            return NNGP_OK;
+        };
+        if ((st = scan(cnt, cbase)) != NNGP_OK) return st;
+        split_kernel<<<grid_of(g1), kThreads, 0, stream>>>(sz, maxg, cnt, cbase, K, S);
+        NNGP_CUDA_TRY(cudaGetLastError());
+        if ((st = scan(K, kbase)) != NNGP_OK) return st;
+        if ((st = scan(S, sbase)) != NNGP_OK) return st;
+        int32_t *ig = static_cast<int32_t *>(at(L.igroup[pl])), *i0 = static_cast<int32_t *>(at(L.it0[pl]));
+        int32_t *i1 = static_cast<int32_t *>(at(L.it1[pl])), *is = static_cast<int32_t *>(at(L.islot[pl]));
+        cub::DoubleBuffer<uint32_t> okb(static_cast<uint32_t *>(at(L.okey_a[pl])),
+                                        static_cast<uint32_t *>(at(L.okey_b[pl])));
+        cub::DoubleBuffer<int32_t> ovb(static_cast<int32_t *>(at(L.oval_a[pl])), static_cast<int32_t *>(at(L.oval_b[pl])));
+        item_fill_kernel<<<grid_of(mi), kThreads, 0, stream>>>(sz, maxg, mi, cnt, K, kbase, sbase, ig, i0, i1, is,
+                                                               okb.Current(), ovb.Current());
+        NNGP_CUDA_TRY(cudaGetLastError());
+        items_size_kernel<<<1, 1, 0, stream>>>(sz, maxg, kbase);
+        NNGP_CUDA_TRY(cudaGetLastError());
+        need = 0;
+        NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, need, okb, ovb, (int)mi, 0, 32, stream));
+        if ((st = cub_check(need)) != NNGP_OK) return st;
+        have = L.cub_bytes;
+        NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(at(L.cub), have, okb, ovb, (int)mi, 0, 32, stream));
+        tc::TcItems &ti = pl == 0 ? out->pruned_items : out->index_items;
+        ti.group = ig;
+        ti.t0 = i0;
+        ti.t1 = i1;
+        ti.slot = is;
+        ti.order = ovb.Current();
+        ti.partial = static_cast<unsigned long long *>(at(L.partial[pl]));
+        out->split_k[pl] = K;
+        out->slot_base[pl] = sbase;
+        out->max_groups_of[pl] = maxg;
+        out->max_items[pl] = mi;
+    }
 
     out->rows = rows;
     out->ref_order = ref_order;
     out->pruned = sizes;
     out->index_order = sizes + 1;
     out->row_off = row_off;
-    out->item_order = ov.Current();
     out->offsets = offsets;
     out->tiles = list;
     out->max_groups = L.max_groups;
-    out->max_index_items = (n + G - 1) / G;
+    return NNGP_OK;
+}
+
+nngp_status merge(const Lists &lists, int which, int G, int m, int32_t *out, cudaStream_t stream) {
+    if (which < 0 || which > 1 || !lists.split_k[which]) return fail(NNGP_ERR_INVALID_ARGUMENT, "knn merge: no plan");
+    const DevSizes *sz = which == 0 ? lists.pruned : lists.index_order;
+    const tc::TcItems &ti = which == 0 ? lists.pruned_items : lists.index_items;
+    const int64_t maxg = lists.max_groups_of[which];
+    merge_kernel<<<grid_of(maxg * G * 32), kThreads, 0, stream>>>(sz, maxg, G, lists.split_k[which],
+                                                                  lists.slot_base[which],
+                                                                  which == 0 ? lists.row_off : nullptr, lists.rows,
+                                                                  ti.partial, m, out);
+    NNGP_CUDA_TRY(cudaGetLastError());
     return NNGP_OK;
 }
 

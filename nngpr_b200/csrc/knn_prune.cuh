@@ -6,17 +6,19 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include "knn_tc.cuh"
 #include "nngp_b200.h"
 
 namespace nngp {
 namespace prune {
 
 constexpr int64_t kMinPoints = 65536;  // below this the index-order search is short enough
+constexpr int64_t kMaxPoints = 2000000;  // the tile lists' worst-case bound (groups x tiles) grows as n^2
 constexpr int kMaxDim = 4;             // bounding boxes stop pruning in more dimensions
 constexpr int kTileRefs = 128;         // refs per tile (the tensor-core search's ref tile)
 
-// Rows [0, early_rows(n)) always take the index-order search: their prefixes are short, and
-// their seeds, drawn from windows where few points precede them, are loose.
+// Rows [0, early_rows(n)) = [0, n / 8) always take the index-order search: their prefixes are
+// short, and the boxes of the sparse index classes they may use are large.
 int64_t early_rows(int64_t n);
 
 // NNGP_KNN_PRUNE=0 turns pruning off (seeded index-order search only).
@@ -26,8 +28,16 @@ bool enabled();
 struct DevSizes {
     int64_t first_row;  // position of the launch's first row in Lists::rows
     int64_t n_rows;
-    int64_t n_items;    // work items (groups of rows)
+    int64_t n_items;    // work items (a group's whole tile range or a chunk of it)
+    int64_t n_groups;   // groups of rows
 };
+
+// A group whose tile range exceeds C = max(kChunkTiles, 2 x total tiles / kMaxSlots) tiles is
+// split into items of about equal ranges, so that a launch with few groups still spreads over
+// every SM; each item writes its rows' partial lists and merge() combines them (any global top-m
+// ref is in the top-m of its item's range, so the merged lists are exact).
+constexpr int kChunkTiles = 16;
+constexpr int kMaxSlots = 1024;
 
 struct Lists {
     const int32_t *rows = nullptr;        // n point indices: the pruned rows group after group, then
@@ -36,11 +46,14 @@ struct Lists {
     const DevSizes *pruned = nullptr;     // the pruned launch
     const DevSizes *index_order = nullptr;  // the index-order launch (rows_per_group rows per item)
     const int32_t *row_off = nullptr;     // pruned group g: rows[row_off[g] .. row_off[g + 1])
-    const int32_t *item_order = nullptr;  // pruned groups, longest tile list first
+    tc::TcItems pruned_items, index_items;  // work items of the two launches (most tiles first)
+    const int32_t *split_k[2] = {nullptr, nullptr};     // items per group (pruned, index order)
+    const int32_t *slot_base[2] = {nullptr, nullptr};   // first partial slot per split group
+    int64_t max_groups_of[2] = {0, 0};
     const int32_t *offsets = nullptr;     // group g's tiles: tiles[offsets[g] .. offsets[g + 1])
     const int32_t *tiles = nullptr;       // ref tile ids (ref_order positions / 128)
-    int64_t max_groups = 0;               // host-side bound of pruned->n_items
-    int64_t max_index_items = 0;          // host-side bound of index_order->n_items
+    int64_t max_groups = 0;               // host-side bound of pruned->n_groups
+    int64_t max_items[2] = {0, 0};        // host-side bounds of the launches' n_items
 };
 
 size_t workspace(int64_t n, int d, int rows_per_group);
@@ -61,6 +74,10 @@ size_t workspace(int64_t n, int d, int rows_per_group);
 nngp_status build(const float *xs, int64_t n, int d, int dp, int rows_per_group, int bits_per_dim,
                   const float *seeds, const int32_t *order0, const int32_t *pos0, const uint64_t *keys0, void *ws,
                   size_t ws_bytes, Lists *out, cudaStream_t stream);
+
+// Combines the partial lists of the split groups of launch `which` (0 pruned, 1 index order)
+// into out (num_nn m).  Runs after that launch on the same stream.
+nngp_status merge(const Lists &lists, int which, int rows_per_group, int m, int32_t *out, cudaStream_t stream);
 
 }  // namespace prune
 }  // namespace nngp

@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(kThreads) seed_kernel(const float *__restrict_
                                                         int64_t n, int dp, int m, const int32_t *__restrict__ order0,
                                                         const int32_t *__restrict__ order1,
                                                         const int32_t *__restrict__ p0_of1,
-                                                        const int32_t *__restrict__ pos1,
+                                                        const int32_t *__restrict__ pos1, int combine,
                                                         float *__restrict__ seeds) {
     constexpr int W = VPL * 16;
     constexpr unsigned FULL = 0xFFFFFFFFu;
@@ -167,7 +167,7 @@ __global__ void __launch_bounds__(kThreads) seed_kernel(const float *__restrict_
     for (int64_t k = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; k < n; k += nwarps) {
         const int64_t i = order0[k];
         if (i < m) {  // fewer than m earlier points: no bound
-            if (lane == 0) seeds[i] = __uint_as_float(kInfBits);
+            if (lane == 0 && !combine) seeds[i] = __uint_as_float(kInfBits);
             continue;
         }
         float qv[D];
@@ -222,7 +222,7 @@ __global__ void __launch_bounds__(kThreads) seed_kernel(const float *__restrict_
             }
             res = hi;
         }
-        if (lane == 0) seeds[i] = __uint_as_float(res);
+        if (lane == 0) seeds[i] = combine ? fminf(seeds[i], __uint_as_float(res)) : __uint_as_float(res);
     }
 }
 
@@ -263,13 +263,14 @@ struct SeedArgs {
     int64_t n;
     int dp, m;
     const int32_t *o0, *o1, *p0of1, *p1;
+    int combine;
     float *seeds;
 };
 
 template <int D, int VPL>
 void launch_seed(int grid, const SeedArgs &a, cudaStream_t stream) {
     seed_kernel<D, VPL><<<grid, kThreads, 0, stream>>>(a.xs0, a.xs1, a.n, a.dp, a.m, a.o0, a.o1, a.p0of1, a.p1,
-                                                       a.seeds);
+                                                       a.combine, a.seeds);
 }
 
 template <int VPL>
@@ -295,26 +296,12 @@ int grid_of(int64_t work) {
     return (int)std::max<int64_t>(1, std::min<int64_t>((work + kThreads - 1) / kThreads, (int64_t)kNumSMsB200 * 8));
 }
 
-}  // namespace
 
-size_t workspace(int64_t n, int dp) { return n < kMinPoints ? 0 : layout(n, dp).total; }
-
-int window() {
-    const char *env = std::getenv("NNGP_KNN_SEED_W");
-    if (!env) return 128;
-    const int w = std::atoi(env);
-    return (w == 0 || w == 128 || w == 256) ? w : 128;
-}
-
-nngp_status prefix_seeds(const float *xs, int64_t n, int d, int D, int dp, int m, void *ws, size_t ws_bytes,
-                         float *seeds, cudaStream_t stream, const int32_t **order0_out, const int32_t **pos0_out,
-                         const uint64_t **keys0_out) {
-    const int W = window();
-    if (W == 0 || n < kMinPoints || m < 1 || d < 1 || d > 24 || D < d || dp % 4 != 0 || dp < D)
-        return fail(NNGP_ERR_UNSUPPORTED, "knn seeds: shape outside the seeded search");
-    const Layout L = layout(n, dp);
-    if (!ws || ws_bytes < L.total) return fail(NNGP_ERR_WORKSPACE, "knn seeds: workspace too small");
-    char *base = reinterpret_cast<char *>(align_up(reinterpret_cast<uintptr_t>(ws), 256));
+// One level: seeds of the points [0, n) from the windows of the curves of those points only
+// (combine: keep the smaller of the old and the new bound).
+nngp_status run_level(const float *xs, int64_t n, int d, int D, int dp, int m, int W, char *base, const Layout &L,
+                      int combine, float *seeds, cudaStream_t stream, const int32_t **order0_out,
+                      const int32_t **pos0_out, const uint64_t **keys0_out) {
     auto at = [&](size_t off) { return reinterpret_cast<void *>(base + off); };
     uint64_t *keys_a = static_cast<uint64_t *>(at(L.keys_a)), *keys_b = static_cast<uint64_t *>(at(L.keys_b));
     int32_t *idx[2][2] = {{static_cast<int32_t *>(at(L.idx0_a)), static_cast<int32_t *>(at(L.idx0_b))},
@@ -341,7 +328,7 @@ nngp_status prefix_seeds(const float *xs, int64_t n, int d, int D, int dp, int m
         size_t have = L.cub_bytes;
         NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(at(L.cub), have, dk, dv, (int)n, 0, bits * d, stream));
         order[c] = dv.Current();
-        if (c == 0) {  // the curve-0 keys in curve order, for callers that cut the curve into cells
+        if (c == 0 && keys0_out) {  // the curve-0 keys in curve order, for callers that cut the curve into cells
             NNGP_CUDA_TRY(cudaMemcpyAsync(at(L.keys0), dk.Current(), (size_t)n * 8, cudaMemcpyDeviceToDevice, stream));
         }
         inverse_kernel<<<grid_of(n), kThreads, 0, stream>>>(order[c], n, pos[c]);
@@ -355,13 +342,51 @@ nngp_status prefix_seeds(const float *xs, int64_t n, int d, int D, int dp, int m
     NNGP_CUDA_TRY(cudaGetLastError());
     const int grid = (int)std::min<int64_t>((n + kThreads / 32 - 1) / (kThreads / 32), (int64_t)kNumSMsB200 * 16);
     const SeedArgs sa{static_cast<const float *>(at(L.xs0)), static_cast<const float *>(at(L.xs1)), n, dp, m,
-                      order[0], order[1], p0of1, pos[1], seeds};
+                      order[0], order[1], p0of1, pos[1], combine, seeds};
     const bool ok = W == 128 ? dispatch_seed<8>(D, grid, sa, stream) : dispatch_seed<16>(D, grid, sa, stream);
     if (!ok) return fail(NNGP_ERR_UNSUPPORTED, "knn seeds: no kernel for D = " + std::to_string(D));
     NNGP_CUDA_TRY(cudaGetLastError());
     if (order0_out) *order0_out = order[0];
     if (pos0_out) *pos0_out = pos[0];
     if (keys0_out) *keys0_out = static_cast<const uint64_t *>(at(L.keys0));
+    return NNGP_OK;
+}
+
+// Refinement levels: prefixes n / 8, n / 64, ... (while at least kMinPoints), run in a second
+// workspace region sized for n / 8.
+size_t sub_bytes(int64_t n, int dp) { return n / 8 >= kMinPoints ? layout(n / 8, dp).total : 0; }
+
+}  // namespace
+
+size_t workspace(int64_t n, int dp) {
+    return n < kMinPoints ? 0 : align_up(layout(n, dp).total, 256) + sub_bytes(n, dp);
+}
+
+int window() {
+    const char *env = std::getenv("NNGP_KNN_SEED_W");
+    if (!env) return 128;
+    const int w = std::atoi(env);
+    return (w == 0 || w == 128 || w == 256) ? w : 128;
+}
+
+nngp_status prefix_seeds(const float *xs, int64_t n, int d, int D, int dp, int m, void *ws, size_t ws_bytes,
+                         float *seeds, cudaStream_t stream, const int32_t **order0_out, const int32_t **pos0_out,
+                         const uint64_t **keys0_out) {
+    const int W = window();
+    if (W == 0 || n < kMinPoints || m < 1 || d < 1 || d > 24 || D < d || dp % 4 != 0 || dp < D)
+        return fail(NNGP_ERR_UNSUPPORTED, "knn seeds: shape outside the seeded search");
+    const Layout L = layout(n, dp);
+    if (!ws || ws_bytes < workspace(n, dp)) return fail(NNGP_ERR_WORKSPACE, "knn seeds: workspace too small");
+    char *base = reinterpret_cast<char *>(align_up(reinterpret_cast<uintptr_t>(ws), 256));
+    nngp_status st = run_level(xs, n, d, D, dp, m, W, base, L, 0, seeds, stream, order0_out, pos0_out, keys0_out);
+    if (st != NNGP_OK) return st;
+    // rows i < n / 8 see few earlier points in the full windows: bound them again from the
+    // curves of the prefix alone (any m earlier points bound a row; the smaller bound is kept)
+    char *sub = base + align_up(L.total, 256);
+    for (int64_t p = n / 8; p >= kMinPoints; p /= 8) {
+        st = run_level(xs, p, d, D, dp, m, W, sub, layout(p, dp), 1, seeds, stream, nullptr, nullptr, nullptr);
+        if (st != NNGP_OK) return st;
+    }
     return NNGP_OK;
 }
 

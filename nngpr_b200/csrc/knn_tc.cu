@@ -276,7 +276,7 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
                                                          const int32_t *__restrict__ rows_perm,
                                                          const int32_t *__restrict__ row_off,
                                                          const int64_t *__restrict__ dev_sizes,
-                                                         const int32_t *__restrict__ item_order,
+                                                         const TcItems items,
                                                          const int32_t *__restrict__ ref_perm,
                                                          const int32_t *__restrict__ tile_off,
                                                          const int32_t *__restrict__ tile_list,
@@ -310,10 +310,10 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
     // themselves when rows_perm is null), from dev_sizes = {first_row, n_rows, n_items} on the
     // device or {0, n_query, ceil(n_query / ROWS)}; work item g is positions
     // [row_off[g], row_off[g + 1]) (at most ROWS) or ROWS consecutive positions.  Refs: with
-    // tile_list (pruned search), item g streams the tiles tile_list[tile_off[g] .. tile_off[g + 1])
+    // tile_list (pruned search), group g streams the tiles tile_list[tile_off[g] .. tile_off[g + 1])
     // of tiles_g, whose positions map to points through ref_perm, and j < limit(i) is checked per
-    // candidate; otherwise refs in index order up to the largest limit of the item's rows (the
-    // rows of an item ascend).  Items: item_order[k] or, for the prefix search, heaviest first.
+    // candidate; otherwise refs in index order up to the largest limit of the group's rows (the
+    // rows of a group ascend).  Items: see TcItems.
     const bool pruned = tile_list != nullptr;
     const int64_t first_row = dev_sizes ? dev_sizes[0] : 0;
     const int64_t n_rows = dev_sizes ? dev_sizes[1] : n_query;
@@ -362,7 +362,9 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
         const bool stop = (item >= n_items) || (*s_abort != 0);
         __syncthreads();
         if (stop) break;
-        const int64_t qtile = item_order ? (int64_t)item_order[item] : (has_cut ? (n_items - 1 - item) : item);
+        const int64_t desc = items.order ? (int64_t)items.order[item] : -1;  // the item's descriptor
+        const int64_t qtile = desc >= 0 ? (int64_t)items.group[desc] : (has_cut ? (n_items - 1 - item) : item);
+        const int32_t out_slot = desc >= 0 ? items.slot[desc] : -1;  // >= 0: partial lists for a merge
         int64_t q0, n_item_rows;  // the item's first row position and its row count
         if (row_off) {
             q0 = row_off[qtile];
@@ -372,14 +374,17 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
             n_item_rows = min((int64_t)C::ROWS, first_row + n_rows - q0);
         }
         auto point_of = [&](int64_t pos) -> int64_t { return rows_perm ? (int64_t)rows_perm[pos] : pos; };
-        const int32_t *tl = pruned ? tile_list + tile_off[qtile] : nullptr;  // this group's ref tiles
-        uint32_t ntiles;
-        if (pruned) {
+        uint32_t tfirst = 0, ntiles;  // the item's tiles: positions [tfirst, tfirst + ntiles) of the group's range
+        if (desc >= 0) {
+            tfirst = (uint32_t)items.t0[desc];
+            ntiles = (uint32_t)(items.t1[desc] - items.t0[desc]);
+        } else if (pruned) {
             ntiles = (uint32_t)(tile_off[qtile + 1] - tile_off[qtile]);
         } else {
             const int64_t block_limit = limit_of(point_of(q0 + n_item_rows - 1));
             ntiles = (uint32_t)((block_limit + RT - 1) / RT);
         }
+        const int32_t *tl = pruned ? tile_list + tile_off[qtile] + tfirst : nullptr;  // this item's ref tiles
 
         if (producer_warp) {
             if (lane == 0) {
@@ -391,7 +396,7 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
                 };
                 auto issue_tma = [&](uint32_t g) {
                     const uint32_t s = g % S;
-                    const int64_t t = pruned ? (int64_t)tl[g - G] : (int64_t)(g - G);
+                    const int64_t t = pruned ? (int64_t)tl[g - G] : (int64_t)(tfirst + (g - G));
                     mbar_arrive_expect_tx(&b_full[s], C::STAGE_BYTES);
                     tma_bulk_g2s(sB + s * C::STAGE_BYTES, tiles_g + t * C::STAGE_BYTES, C::STAGE_BYTES, &b_full[s]);
                     tma_issued = g + 1;
@@ -530,7 +535,7 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
                 }
                 tc_fence_after();
                 const float *exs = reinterpret_cast<const float *>(sB + s * C::STAGE_BYTES + C::OP_BYTES);
-                const int64_t j0 = (pruned ? (int64_t)tl[t] : (int64_t)t) * RT;  // first ref position of the tile
+                const int64_t j0 = (pruned ? (int64_t)tl[t] : (int64_t)(tfirst + t)) * RT;  // first ref position of the tile
                 const uint32_t taddr = tmem_base + ((uint32_t)(quad * 32) << 16) + b * C::BUF_COLS + qtw * RT;
                 // screen one 32-column chunk (scores in v): this row's candidate mask, 0 when no row
                 // of the warp has one (the common case, a handful of instructions)
@@ -654,7 +659,11 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
                         }
                     }
                     const int64_t rq = warp * 32 + rr;
-                    if (rq < n_item_rows && lane < m) out[point_of(q0 + rq) * m + lane] = (int32_t)(uint32_t)x;
+                    if (out_slot >= 0) {
+                        items.partial[((int64_t)out_slot * C::ROWS + rq) * 32 + lane] = x;
+                    } else if (rq < n_item_rows && lane < m) {
+                        out[point_of(q0 + rq) * m + lane] = (int32_t)(uint32_t)x;
+                    }
                 }
             }
         }

@@ -115,3 +115,20 @@ def test_pruned_ties_outlier_and_clusters(monkeypatch, capfd):
     c = search_mode(monkeypatch, z, 32, 0.8, True)
     assert np.array_equal(c, search_mode(monkeypatch, z, 32, 0.8, False))
     check_rows(z, c, 32, 0.8, rng, k=80)
+
+
+def test_split_work_items_merge_to_the_same_lists(monkeypatch, capfd):
+    """An outlier squeezes the other points into one Morton cell: seeds come from random windows
+    and groups need most tiles, so long tile ranges are split into several work items whose
+    partial lists are merged; the result equals the unpruned search and the oracle."""
+    import re
+    rng = np.random.default_rng(21)
+    y = rng.normal(size=(90000, 3))
+    y[777] = [3e7, 3e7, -3e7]
+    monkeypatch.setenv('NNGP_KNN_DEBUG', '1')
+    a = search_mode(monkeypatch, y, 32, 0.5, True)
+    err = capfd.readouterr().err
+    mt = re.search(r'groups=(\d+) items=(\d+)', err)
+    assert mt and int(mt.group(2)) > int(mt.group(1))  # some groups were split
+    assert np.array_equal(a, search_mode(monkeypatch, y, 32, 0.5, False))
+    check_rows(y, a, 32, 0.5, rng, k=100)
