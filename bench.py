@@ -64,7 +64,9 @@ WORKLOAD = ('nngp fit step, n=434874 d=3 m=32, isotropic RBF l=0.2, noise 1e-3; 
 # precision of the local systems: at this nugget nearly every FP32 system has a pivot below the
 # re-solve threshold, so FP64 systems are the faster exact choice (FP32 + re-solve: 51.9 ms/step)
 LOCAL = 'f64'
-ROOF = 'fp32'  # roofline of the search kernel: 'fp32' (the screen's issue) or 'tensor'
+# roofline kernel: 'local' (the FP64 local-systems kernel, the largest share of the d = 3 step once
+# the search is pruned), 'fp32' (the search kernel's screen issue) or 'tensor' (its TF32 MMAs)
+ROOF = 'local'
 DATA = 'synthetic (seeded stand-in for 3droad: shape 434874 x 3)'
 DTYPE = 'f32 search (tf32-split tensor screen) + f64 local'
 
@@ -79,7 +81,7 @@ WORKLOADS = {
         DTYPE='f32 search (tf32-split tensor screen) + f32 local (f64 re-solve) + f64 sums'),
 }
 WORKLOADS['differentiation'] = dict(
-    N_TRAIN=434_874, D=8, M=32, NOISE=4e-4, ALPHA=1e-10, LOCAL='f32',
+    N_TRAIN=434_874, D=8, M=32, NOISE=4e-4, ALPHA=1e-10, LOCAL='f32', ROOF='fp32',
     WORKLOAD=('nngp fit step, n=434874 d=8 m=32, x~U[0,1]^8, ARD RBF (8 length scales), noise 4e-4; '
               'fp32 exact neighbour search, fp32 local systems with fp64 re-solves, gradient w.r.t. 10 log '
               'hyperparameters; plus 50 device L-BFGS iterations through the autograd function'),
@@ -351,13 +353,13 @@ class ClockSampler:
 # ------------------------------------------------------------------------------------------
 # Our arm
 # ------------------------------------------------------------------------------------------
-PROFILE = {'fit3d': 'knn_tc_kernel_fit_n434874_d3_m32.md', 'precision': 'knn_tc_kernel_fit_n1000000_d16_m32.md',
+PROFILE = {'fit3d': 'local_warp_kernel_fit_fp64_n434874_d3_m32.md', 'precision': 'knn_tc_kernel_fit_n1000000_d16_m32.md',
            'differentiation': 'knn_tc_kernel_fit_n434874_d8_m32.md'}
 
 
 def read_profile_traffic():
-    """DRAM bytes per launch of the neighbour-search kernel of this workload from the committed
-    ncu summary (line 'traffic_bytes_per_launch: <int>'), or None."""
+    """DRAM bytes per launch of the roofline kernel of this workload from the committed ncu
+    summary (line 'traffic_bytes_per_launch: <int>'), or None."""
     if _WL not in PROFILE:
         return None
     path = os.path.join(ROOT, 'profiles', PROFILE[_WL])
@@ -398,6 +400,52 @@ def fp32_peak_tflops(torch, L, stream_ptr):
         flops = blocks * 256 * iters * 128
         best = max(best, flops / (s.elapsed_time(e) * 1e-3) / 1e12)
     return best
+
+
+def fp64_peak_tflops(torch, L, stream_ptr):
+    """FP64 FMA rate of this GPU measured with the library's probe kernel (TFLOP/s)."""
+    import ctypes
+    blocks = 148 * 8
+    out = torch.empty(blocks * 256, dtype=torch.float64, device='cuda')
+    iters = 1024
+    best = 0.0
+    for _ in range(4):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        st = L.nngp_fma_probe_f64(ctypes.c_void_p(out.data_ptr()), iters, blocks, stream_ptr)
+        e.record()
+        torch.cuda.synchronize()
+        assert st == 0
+        flops = blocks * 256 * iters * 128
+        best = max(best, flops / (s.elapsed_time(e) * 1e-3) / 1e12)
+    return best
+
+
+def local_flops_per_point(m, d, n_theta):
+    """FP64 flops of one local system of the fit step with its gradient: the Cholesky of the
+    augmented (m + 1) x (m + 1) matrix (2 k^3 / 3), its fill (k (k + 1) / 2 entries of 3d + 4
+    flops, the exponential counted once), the gradient terms (4 flops per entry and
+    hyperparameter) and the triangular solves (4 k^2)."""
+    k = m + 1
+    entries = k * (k + 1) // 2
+    return 2.0 * k ** 3 / 3.0 + entries * (3 * d + 4) + 4.0 * entries * n_theta + 4.0 * k * k
+
+
+def our_launches_per_step(n, d, m):
+    """Kernels of this library one fit step launches (CUB's sort and scan kernels not counted):
+    scale, centre sums and tile build; per seed level (the prefixes n, n/8, ... of at least
+    8,192 points) bounds, two x (Morton keys, inverse, coordinate gather), cross positions and
+    the seed kernel; the pruned search's planning (19), a second tile build, two search
+    launches and two merges, or one search launch; the local systems and the final sum."""
+    seeded = n >= 8192
+    levels = 0
+    p_ = n
+    while seeded and p_ >= 8192:
+        levels += 1
+        p_ //= 8
+    pruned = seeded and 65536 <= n <= 2_000_000 and d <= 4
+    search = (19 + 1 + 2 + 2) if pruned else 1
+    return 3 + 9 * levels + search + 2
 
 
 def run_plain(args, torch, x32, y64, xq32, p, flags, flush, lml_ours):
@@ -753,7 +801,23 @@ def run_ours(args):
         # work is cheap), the tensor pipe at d = 16 (the survey's roofline for that configuration)
         kp = (3 * (D + 1) + 7) // 8 * 8  # TF32 split width of the tensor-core operands
         issued = 2.0 * kp * pairs / (knn_avg_ms * 1e-3) / 1e12
-        if ROOF == 'tensor':
+        local_avg_ms = float(np.mean([a - b for a, b in zip(step_ms, knn_ms)]))
+        search = {'kernel': f'knn_tc_kernel<{D}> (prefix search: tcgen05 TF32-split screen, exact FP32 rescoring; '
+                            f'seeded rows, pruned tile lists for d <= 4)',
+                  'ms': knn_avg_ms,
+                  'brute_force_equivalent_tflops': achieved,
+                  'note': '2*d flops per (query, ref) pair over all n(n-1)/2 prefix pairs; the pruned search '
+                          'screens a small fraction of them, so this is a rate of the problem, not of a pipe'}
+        if ROOF == 'local':
+            fpk = fp64_peak_tflops(torch, L, ctypes.c_void_p(stream.cuda_stream))
+            lflops = local_flops_per_point(M, D, p.n_theta) * (r1 - r0)
+            lach = lflops / (local_avg_ms * 1e-3) / 1e12
+            roof = {'bound': 'fp64', 'achieved': lach, 'peak': fpk, 'unit': 'TFLOP/s', 'frac': lach / fpk,
+                    'peak_source': 'FP64 FMA probe measured in this run (MEASURED_PEAKS.json has no FP64 figure)',
+                    'kernel': 'local_warp_kernel<double, grad> (fused fill, Cholesky, solves, adjoint gradient)',
+                    'work': 'per point: 2k^3/3 + k(k+1)/2 (3d + 4 + 4 n_theta) + 4k^2 FP64 flops, k = m + 1',
+                    'local_ms': local_avg_ms, 'search': search}
+        elif ROOF == 'tensor':
             tpk, tsrc = tf32_peak_tflops()
             roof = {'bound': 'tensor', 'achieved': achieved, 'peak': tpk, 'unit': 'TFLOP/s', 'frac': achieved / tpk,
                     'peak_source': tsrc, 'issued_mma_tflops': issued, 'issued_frac': issued / tpk,
@@ -772,19 +836,21 @@ def run_ours(args):
                        'l2': 'flushed (256 MB write) before every timed step', 'lml': lml_val,
                        'lml_rel_err_vs_fp64_local': lml_err},
             'e2e': e2e,
-            'roofline': dict(roof, traffic=read_profile_traffic(),
-                             kernel=f'knn_tc_kernel<{D}> (prefix search: tcgen05 TF32-split screen, exact FP32 rescoring)',
-                             work='2*d flops per (query, ref) pair, n(n-1)/2 pairs, whichever pipe computes them; '
-                                  'issued_mma = 2*K\' per pair with the split width K\'',
-                             knn_ms=knn_avg_ms),
+            'roofline': dict(roof, traffic=read_profile_traffic()) if ROOF == 'local' else dict(
+                roof, traffic=read_profile_traffic(),
+                kernel=f'knn_tc_kernel<{D}> (prefix search: tcgen05 TF32-split screen, exact FP32 rescoring)',
+                work='2*d flops per (query, ref) pair, n(n-1)/2 pairs, whichever pipe computes them; '
+                     'issued_mma = 2*K\' per pair with the split width K\'',
+                knn_ms=knn_avg_ms),
             'cpu_baseline': cpu,
             'plain_gpu': plain,
             'lbfgs': lbfgs,
             'reused_lists_step': reuse,
             'predict': None if pred_ms is None else {'value': N_PRED / (pred_ms * 1e-3), 'unit': 'points/s',
                                                      'ms': pred_ms, 'n_query': N_PRED},
-            # per step: scale, centre sums, tile build, search, local systems, finalize
-            'gpu_launches': args.steps * 6,
+            'gpu_launches': args.steps * our_launches_per_step(r1 - r0 if world == 1 else 0, D, M),
+            'gpu_launches_note': 'kernels of libnngp_b200.so per step (see our_launches_per_step); CUB sort and '
+                                 'scan kernels the planning launches are not counted',
             'clocks': clocks.summary(),
         }
         print(json.dumps(line))

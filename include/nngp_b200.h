@@ -248,6 +248,9 @@ nngp_status nngp_predict_f64(const double *x_train, const double *y_train, int64
  * kernels above.
  * ------------------------------------------------------------------------------------- */
 nngp_status nngp_fma_probe(float *out, int64_t iters, int32_t blocks, void *stream);
+/* FP64 FMA-rate probe (measurement only): blocks x 256 threads, 8 FMA chains of 8 x iters
+ * steps each; out receives blocks x 256 doubles. */
+nngp_status nngp_fma_probe_f64(double *out, int64_t iters, int32_t blocks, void *stream);
 
 /* Plain FP32 GPU form of the neighbour search: the comparator the optimised search is measured
  * against (no counterpart in the reference's plugin interface; it restates the structure of the

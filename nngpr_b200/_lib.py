@@ -25,7 +25,7 @@ EXPORTED = (
     'nngp_knn_workspace_size_f32', 'nngp_knn_f32', 'nngp_knn_workspace_size_f64', 'nngp_knn_f64',
     'nngp_loglik_workspace_size', 'nngp_loglik_f32', 'nngp_loglik_f64',
     'nngp_loglik_rows_f32', 'nngp_loglik_rows_f64', 'nngp_loglik_f64_noalloc',
-    'nngp_predict_f32', 'nngp_predict_f64', 'nngp_fma_probe', 'nngp_tc_layout_selftest',
+    'nngp_predict_f32', 'nngp_predict_f64', 'nngp_fma_probe', 'nngp_fma_probe_f64', 'nngp_tc_layout_selftest',
     'nngp_plain_knn_f32', 'nngp_knn_reuse_prepare_f32', 'nngp_knn_reuse_rank_f32',
     'nngp_predict_full_workspace_size', 'nngp_predict_full_f64', 'nngp_sample_full_f64',
     'nngp_predict_cov_full_f64',
@@ -81,6 +81,7 @@ _SIGS = {
     'nngp_predict_f32': ([_vp, _vp, _i64, _vp, _i64, _i32, _i32, _vp, _i32, _kp, _f64, _vp, _vp, _vp, _vp], ctypes.c_int),
     'nngp_predict_f64': ([_vp, _vp, _i64, _vp, _i64, _i32, _i32, _vp, _i32, _kp, _f64, _vp, _vp, _vp, _vp], ctypes.c_int),
     'nngp_fma_probe': ([_vp, _i64, _i32, _vp], ctypes.c_int),
+    'nngp_fma_probe_f64': ([_vp, _i64, _i32, _vp], ctypes.c_int),
     'nngp_tc_layout_selftest': ([_vp, _vp, _i32, _vp, _vp, _vp], ctypes.c_int),
     'nngp_plain_knn_f32': ([_vp, _i64, _vp, _i64, _i32, _i32, _i32, _i64, _vp, _vp], ctypes.c_int),
     'nngp_predict_full_workspace_size': ([_i64, _i32], ctypes.c_size_t),

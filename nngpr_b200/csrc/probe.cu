@@ -1,6 +1,7 @@
-// FP32 FMA-rate probe: the denominator of the roofline fraction of the SIMT kernels here.
-// Each thread runs 8 independent FMA chains of `iters` steps (16 flops per step); the sum is
-// written out so nothing is eliminated.  The caller times the launch.
+// FMA-rate probes (FP32 and FP64): the denominators of the roofline fractions of the kernels
+// here that are bound by a SIMT pipe.  Each thread runs 8 independent FMA chains of `iters`
+// steps (16 flops per step); the sum is written out so nothing is eliminated.  The caller times
+// the launch.
 #include "common.cuh"
 
 namespace nngp {
@@ -18,6 +19,19 @@ __global__ void __launch_bounds__(256) fma_probe_kernel(float *out, int64_t iter
     out[blockIdx.x * blockDim.x + threadIdx.x] = v0 + v1 + v2 + v3 + v4 + v5 + v6 + v7;
 }
 
+__global__ void __launch_bounds__(256) fma_probe_f64_kernel(double *out, int64_t iters, double a, double b) {
+    double v0 = threadIdx.x * 1e-3, v1 = v0 + 1.0, v2 = v0 + 2.0, v3 = v0 + 3.0;
+    double v4 = v0 + 4.0, v5 = v0 + 5.0, v6 = v0 + 6.0, v7 = v0 + 7.0;
+    for (int64_t i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            v0 = fma(v0, a, b); v1 = fma(v1, a, b); v2 = fma(v2, a, b); v3 = fma(v3, a, b);
+            v4 = fma(v4, a, b); v5 = fma(v5, a, b); v6 = fma(v6, a, b); v7 = fma(v7, a, b);
+        }
+    }
+    out[blockIdx.x * blockDim.x + threadIdx.x] = v0 + v1 + v2 + v3 + v4 + v5 + v6 + v7;
+}
+
 }  // namespace nngp
 
 extern "C" nngp_status nngp_fma_probe(float *out, int64_t iters, int32_t blocks, void *stream) {
@@ -25,6 +39,15 @@ extern "C" nngp_status nngp_fma_probe(float *out, int64_t iters, int32_t blocks,
     set_error("");
     if (!out || iters <= 0 || blocks <= 0) return fail(NNGP_ERR_INVALID_ARGUMENT, "fma_probe: bad arguments");
     fma_probe_kernel<<<blocks, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(out, iters, 0.999999f, 1e-6f);
+    NNGP_CUDA_TRY(cudaGetLastError());
+    return NNGP_OK;
+}
+
+extern "C" nngp_status nngp_fma_probe_f64(double *out, int64_t iters, int32_t blocks, void *stream) {
+    using namespace nngp;
+    set_error("");
+    if (!out || iters <= 0 || blocks <= 0) return fail(NNGP_ERR_INVALID_ARGUMENT, "fma_probe_f64: bad arguments");
+    fma_probe_f64_kernel<<<blocks, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(out, iters, 0.999999, 1e-6);
     NNGP_CUDA_TRY(cudaGetLastError());
     return NNGP_OK;
 }
