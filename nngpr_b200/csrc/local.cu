@@ -93,23 +93,44 @@ template <bool MATERN, typename T> __device__ __forceinline__ T kern_g(int famil
 // ---------------------------------------------------------------------------------------
 // Warp kernel
 // ---------------------------------------------------------------------------------------
-// Shared memory per warp (bytes): xs (kWarpM + 1) x ds doubles | L kWarpM x (kWarpM + 1) doubles |
-// inverse diagonal kWarpM doubles | gradient accumulator n_theta doubles | the fill's kernel values
+// Shared memory per warp (bytes): two Cholesky column slots 2 x kWarpM doubles (16-byte
+// aligned, first) | xs (kWarpM + 1) x ds doubles | L kWarpM x (kWarpM + 1) doubles | inverse
+// diagonal kWarpM doubles | gradient accumulator n_theta doubles | the fill's kernel values
 // kWarpM x (kWarpM + 1) doubles (kept for the gradient, which would otherwise recompute them).
 struct WarpSmem {
     int ds;  // row stride of xs (d + 1)
-    size_t xs_bytes, l_bytes, idg_bytes, g_bytes, e_bytes, total;
+    size_t c_bytes, xs_bytes, l_bytes, idg_bytes, g_bytes, e_bytes, total;
+    size_t xs_off, l_off, idg_off, g_off, e_off;
     __host__ __device__ static WarpSmem make(int d, int n_theta) {
         WarpSmem s;
         s.ds = d + 1;
+        s.c_bytes = (size_t)2 * kWarpM * 8;
         s.xs_bytes = (size_t)(kWarpM + 1) * s.ds * 8;
         s.l_bytes = (size_t)kWarpM * (kWarpM + 1) * 8;
         s.idg_bytes = (size_t)kWarpM * 8;
         s.g_bytes = (size_t)(n_theta > 0 ? n_theta : 1) * 8;
         s.e_bytes = (size_t)kWarpM * (kWarpM + 1) * 8;
-        s.total = (s.xs_bytes + s.l_bytes + s.idg_bytes + s.g_bytes + s.e_bytes + 15) / 16 * 16;
+        s.xs_off = s.c_bytes;
+        s.l_off = s.xs_off + s.xs_bytes;
+        s.idg_off = s.l_off + s.l_bytes;
+        s.g_off = s.idg_off + s.idg_bytes;
+        s.e_off = s.g_off + s.g_bytes;
+        s.total = (s.e_off + s.e_bytes + 15) / 16 * 16;
         return s;
     }
+};
+
+// Vector of VW elements of TC read with one 16-byte shared-memory load.
+template <typename TC> struct Vec16;
+template <> struct Vec16<double> {
+    static constexpr int VW = 2;
+    using T = double2;
+    __device__ static double get(const double2 &v, int e) { return e == 0 ? v.x : v.y; }
+};
+template <> struct Vec16<float> {
+    static constexpr int VW = 4;
+    using T = float4;
+    __device__ static float get(const float4 &v, int e) { return e == 0 ? v.x : (e == 1 ? v.y : (e == 2 ? v.z : v.w)); }
 };
 
 // Solves point p's system in precision TC.  Returns false (and commits nothing) when TC is
@@ -123,11 +144,12 @@ __device__ __forceinline__ bool warp_system(const LocalArgs &a, int64_t p, int l
     constexpr int M = kWarpM;
     const unsigned FULL = 0xffffffffu;
     const WarpSmem lay = WarpSmem::make(a.d, a.n_theta);
-    TC *xs = reinterpret_cast<TC *>(wsm);
-    TC *Ls = reinterpret_cast<TC *>(wsm + lay.xs_bytes);
-    TC *idg = reinterpret_cast<TC *>(wsm + lay.xs_bytes + lay.l_bytes);
-    double *gacc = reinterpret_cast<double *>(wsm + lay.xs_bytes + lay.l_bytes + lay.idg_bytes);
-    TC *Es = reinterpret_cast<TC *>(wsm + lay.xs_bytes + lay.l_bytes + lay.idg_bytes + lay.g_bytes);
+    TC *colbuf = reinterpret_cast<TC *>(wsm);  // two column slots of kWarpM, 16-byte aligned
+    TC *xs = reinterpret_cast<TC *>(wsm + lay.xs_off);
+    TC *Ls = reinterpret_cast<TC *>(wsm + lay.l_off);
+    TC *idg = reinterpret_cast<TC *>(wsm + lay.idg_off);
+    double *gacc = reinterpret_cast<double *>(wsm + lay.g_off);
+    TC *Es = reinterpret_cast<TC *>(wsm + lay.e_off);
     constexpr bool STASH = GRAD && !MATERN;  // RBF gradient: reuse the fill's exponentials
     const int d = a.d, ds = lay.ds;
 
@@ -199,10 +221,24 @@ __device__ __forceinline__ bool warp_system(const LocalArgs &a, int64_t p, int l
         if (lane == k) l_own = lk;
         if (lane > k) kvec = fma(-r[k], lk, kvec);
         ss = fma(lk, lk, ss);
+        if (k + 1 < M) {
+            // column k of L to a shared slot (alternating slots: a lane that wrote column k has
+            // finished reading column k - 1), then every lane reads L[jj][k], jj > k, as
+            // broadcast 16-byte loads instead of one shuffle per element
+            TC *col = colbuf + (k & 1) * M;
+            col[lane] = r[k];
+            __syncwarp();
+            using V = Vec16<TC>;
+            const typename V::T *cv = reinterpret_cast<const typename V::T *>(col);
 #pragma unroll
-        for (int jj = k + 1; jj < M; ++jj) {
-            const TC ljk = __shfl_sync(FULL, r[k], jj);
-            r[jj] = fma(-r[k], ljk, r[jj]);
+            for (int q = (k + 1) / V::VW; q < M / V::VW; ++q) {
+                const typename V::T v = cv[q];
+#pragma unroll
+                for (int e = 0; e < V::VW; ++e) {
+                    const int jj = q * V::VW + e;
+                    if (jj > k) r[jj] = fma(-r[k], V::get(v, e), r[jj]);
+                }
+            }
         }
     }
     const TC s2 = kpp - ss;
@@ -355,7 +391,7 @@ __device__ __forceinline__ bool warp_system(const LocalArgs &a, int64_t p, int l
 }
 
 template <typename TIn, bool GRAD, bool PRED, bool MATERN>
-__global__ void __launch_bounds__(kLocWarps * 32) local_warp_kernel(
+__global__ void __launch_bounds__(kLocWarps * 32, 3) local_warp_kernel(
     const __grid_constant__ LocalArgs a, const TIn *__restrict__ x_ref, const TIn *__restrict__ y_ref,
     const TIn *__restrict__ x_pt, const TIn *__restrict__ y_pt, const int32_t *__restrict__ nbr,
     double *__restrict__ block_out, TIn *__restrict__ mean, TIn *__restrict__ var, int32_t *__restrict__ flags) {
@@ -363,7 +399,7 @@ __global__ void __launch_bounds__(kLocWarps * 32) local_warp_kernel(
     const WarpSmem lay = WarpSmem::make(a.d, a.n_theta);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned char *wsm = smem_raw + warp * lay.total;
-    double *gacc = reinterpret_cast<double *>(wsm + lay.xs_bytes + lay.l_bytes + lay.idg_bytes);
+    double *gacc = reinterpret_cast<double *>(wsm + lay.g_off);
     for (int t = lane; t < a.n_theta; t += 32) gacc[t] = 0.0;
     __syncwarp();
     double ll_acc = 0.0;
@@ -398,8 +434,7 @@ __global__ void __launch_bounds__(kLocWarps * 32) local_warp_kernel(
         for (int t = threadIdx.x; t < a.n_theta; t += blockDim.x) {
             double s = 0.0;
             for (int w = 0; w < kLocWarps; ++w)
-                s += reinterpret_cast<const double *>(smem_raw + w * lay.total + lay.xs_bytes + lay.l_bytes +
-                                                      lay.idg_bytes)[t];
+                s += reinterpret_cast<const double *>(smem_raw + w * lay.total + lay.g_off)[t];
             o[1 + t] = s;
         }
     }
