@@ -553,17 +553,25 @@ KnnPlan make_plan(int64_t n_ref, int64_t n_query, int d, int m, bool same) {
         off = align_up(off + 16, 256);
         p.off_ctr = off;
         off = align_up(off + 16, 256);
-        if (p.path == KnnPath::Tc && seed::workspace(n_ref, p.dp) > 0) {  // seeds of the prefix search
+        // seeds and pruned lists: of the prefix search (same) or, for other queries, of the query
+        // search (the size query plans with same = false and takes the larger of the two)
+        const size_t seed_ws = p.path != KnnPath::Tc ? 0
+                               : std::max(seed::workspace(n_ref, p.dp),
+                                          same ? (size_t)0 : seed::query_workspace_if(n_ref, n_query, p.dp));
+        if (seed_ws > 0) {
             p.off_seed = off;
-            off = align_up(off + (size_t)n_ref * sizeof(float), 256);
+            off = align_up(off + (size_t)std::max(n_ref, n_query) * sizeof(float), 256);
             p.off_seed_ws = off;
-            p.seed_ws_bytes = seed::workspace(n_ref, p.dp);
+            p.seed_ws_bytes = seed_ws;
             off = align_up(off + p.seed_ws_bytes, 256);
-            if (prune::workspace(n_ref, d, p.tv.rows_per_item) > 0) {  // pruned search: curve-order tiles + lists
+            const int G = p.tv.rows_per_item;
+            const size_t prune_ws = std::max(prune::workspace(n_ref, d, G),
+                                             same ? (size_t)0 : prune::workspace_query(n_ref, n_query, d, G));
+            if (prune_ws > 0) {  // pruned search: curve-order tiles + lists
                 p.off_tiles2 = align_up(off, 1024);
                 off = align_up(p.off_tiles2 + rec_bytes, 1024);
                 p.off_prune_ws = off;
-                p.prune_ws_bytes = prune::workspace(n_ref, d, p.tv.rows_per_item);
+                p.prune_ws_bytes = prune_ws;
                 off = align_up(off + p.prune_ws_bytes, 256);
             }
         }
@@ -651,11 +659,34 @@ nngp_status knn_impl(const T *ref, int64_t n_ref, const T *query, int64_t n_quer
                 if (sst != NNGP_OK) return sst;
                 seeds_c = sd;
             }
+            // queries against the set (predict): seeds from the refs' curve windows around each
+            // query, and (d <= 4) groups of queries in curve order with their tile lists
+            const int G = p.tv.rows_per_item;
+            const int32_t *qorder = nullptr;
+            const bool qseeded = !same && !has_cut && seed::window() > 0 && seed::query_workspace_if(n_ref, n_query, p.dp) > 0 &&
+                                 p.seed_ws_bytes >= seed::workspace_query(n_ref, n_query, p.dp);
+            if (qseeded) {
+                float *sd = reinterpret_cast<float *>(base + p.off_seed);
+                nngp_status sst = seed::query_seeds(refs, n_ref, qsc, n_query, d, round_d(d), p.dp, m,
+                                                    base + p.off_seed_ws, p.seed_ws_bytes, sd, stream, &order0, &qorder);
+                if (sst != NNGP_OK) return sst;
+                seeds_c = sd;
+            }
+            const size_t qprune_ws = qseeded ? prune::workspace_query(n_ref, n_query, d, G) : 0;
+            const bool qpruned = qseeded && qprune_ws > 0 && p.prune_ws_bytes >= qprune_ws && prune::enabled();
             // and, for large low-dimensional sets, visits per group of rows only the ref tiles its
             // seeds allow (rows and refs in curve order; loose and early rows stay in index order)
             const bool pruned = seeded && p.prune_ws_bytes > 0 && prune::enabled();
             prune::Lists lists;
             unsigned char *tiles_curve = reinterpret_cast<unsigned char *>(base + p.off_tiles2);
+            if (qpruned) {
+                nngp_status pst = prune::build_query(refs, n_ref, qsc, n_query, d, p.dp, G, seeds_c, order0, qorder,
+                                                     base + p.off_prune_ws, p.prune_ws_bytes, &lists, stream);
+                if (pst != NNGP_OK) return pst;
+                p.tv.build<<<grid_for(p.n_ref_pad), 256, 0, stream>>>(refs, n_ref, p.n_ref_pad, acc, order0, tiles_curve,
+                                                                      r2);
+                NNGP_CUDA_TRY(cudaGetLastError());
+            }
             if (pruned) {
                 nngp_status pst = prune::build(refs, n_ref, d, p.dp, p.tv.rows_per_item, seed::bits(d), seeds_c,
                                                order0, pos0, keys0, base + p.off_prune_ws, p.prune_ws_bytes, &lists,
@@ -699,7 +730,7 @@ nngp_status knn_impl(const T *ref, int64_t n_ref, const T *query, int64_t n_quer
                     std::fprintf(stderr,
                                  "nngp_knn: tensor-core path d=%d m=%d items<=%lld ctas/sm=%d grid=%d smem=%d seeded=%d "
                                  "pruned=%d\n",
-                                 d, m, (long long)items_bound, per_sm, grid, p.tv.smem, (int)seeded,
+                                 d, m, (long long)items_bound, per_sm, grid, p.tv.smem, (int)(seeded || qseeded),
                                  (int)(tile_list != nullptr));
                 void *args[] = {(void *)&tiles_c,  (void *)&q_c,      (void *)&acc_c,      (void *)&r2_c,
                                 (void *)&seeds_c,  (void *)&rows_perm, (void *)&row_off,   (void *)&dev_sizes,
@@ -721,6 +752,12 @@ nngp_status knn_impl(const T *ref, int64_t n_ref, const T *query, int64_t n_quer
                 lst = launch(tiles, lists.max_items[1], lists.rows, none, is, lists.index_items, none, none, none, ctr);
                 if (lst != NNGP_OK) return lst;
                 lst = prune::merge(lists, 1, p.tv.rows_per_item, m, out, stream);
+            } else if (qpruned) {
+                const int64_t *ps = reinterpret_cast<const int64_t *>(lists.pruned);
+                lst = launch(tiles_curve, lists.max_items[0], lists.rows, lists.row_off, ps, lists.pruned_items,
+                             lists.ref_order, lists.offsets, lists.tiles, ctr + 1);
+                if (lst != NNGP_OK) return lst;
+                lst = prune::merge(lists, 0, G, m, out, stream);
             } else {
                 const int64_t items = (n_query + p.tv.rows_per_item - 1) / p.tv.rows_per_item;
                 const tc::TcItems whole{};

@@ -246,9 +246,9 @@ __global__ void __launch_bounds__(kThreads) group_box_kernel(const float *__rest
                                                              const int32_t *__restrict__ rows,
                                                              const int32_t *__restrict__ row_off,
                                                              const DevSizes *__restrict__ pruned,
-                                                             const float *__restrict__ seeds, float *__restrict__ glo,
-                                                             float *__restrict__ ghi, float *__restrict__ gtau,
-                                                             int32_t *__restrict__ glim) {
+                                                             const float *__restrict__ seeds, int all_refs,
+                                                             float *__restrict__ glo, float *__restrict__ ghi,
+                                                             float *__restrict__ gtau, int32_t *__restrict__ glim) {
     const int lane = threadIdx.x & 31;
     const int64_t n_groups = pruned->n_groups;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -265,7 +265,7 @@ __global__ void __launch_bounds__(kThreads) group_box_kernel(const float *__rest
         for (int o = 16; o > 0; o >>= 1) tau = fmaxf(tau, __shfl_xor_sync(0xFFFFFFFFu, tau, o));
         if (lane == 0) {
             gtau[g] = tau;
-            glim[g] = lim;  // refs j < lim can serve some row of the group
+            glim[g] = all_refs ? INT32_MAX : lim;  // refs j < lim can serve some row of the group
         }
         for (int f = 0; f < d; ++f) {
             float lo = pos_inf<float>(), hi = neg_inf<float>();
@@ -469,6 +469,17 @@ __global__ void __launch_bounds__(kThreads) merge_kernel(const DevSizes *__restr
     }
 }
 
+// Groups of G consecutive rows of a search of n_rows queries (all pruned, no index order).
+__global__ void uniform_groups_kernel(int64_t n_rows, int G, int64_t n_groups, int32_t *__restrict__ row_off,
+                                      DevSizes *__restrict__ pruned, DevSizes *__restrict__ index_order) {
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g <= n_groups; g += (int64_t)gridDim.x * blockDim.x)
+        row_off[g] = (int32_t)min(g * (int64_t)G, n_rows);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *pruned = DevSizes{0, n_rows, n_groups, n_groups};
+        *index_order = DevSizes{n_rows, 0, 0, 0};
+    }
+}
+
 struct Layout {
     int64_t n_tiles, max_groups;
     size_t tlo, thi, tmin, stats, keys_a, keys_b, vals_a, vals_b, rvals_a, rvals_b, headpos, seg_start, gh, gid, row_off, sizes, glo,
@@ -537,6 +548,103 @@ Layout layout(int64_t n, int d, int G) {
 
 int grid_of(int64_t threads) {
     return (int)std::max<int64_t>(1, std::min<int64_t>((threads + kThreads - 1) / kThreads, (int64_t)kNumSMsB200 * 8));
+}
+
+// Work items of launch pl (0 pruned, 1 index order): per-group tile counts, the split, item
+// descriptors sorted by tile count (most first); fills out's item fields for pl.
+nngp_status plan_items(const Layout &L, char *base, int pl, DevSizes *sz, const int32_t *offsets, const int32_t *rows,
+                       int G, int64_t n, Lists *out, cudaStream_t stream) {
+    auto at = [&](size_t off) { return reinterpret_cast<void *>(base + off); };
+    nngp_status st = NNGP_OK;
+    const int64_t maxg = L.maxg[pl], g1 = maxg + 1, mi = L.max_items[pl];
+    int32_t *cnt = static_cast<int32_t *>(at(L.cnt[pl])), *cbase = static_cast<int32_t *>(at(L.cbase[pl]));
+    int32_t *K = static_cast<int32_t *>(at(L.K[pl])), *kbase = static_cast<int32_t *>(at(L.kbase[pl]));
+    int32_t *S = static_cast<int32_t *>(at(L.S[pl])), *sbase = static_cast<int32_t *>(at(L.sbase[pl]));
+    group_tiles_kernel<<<grid_of(g1), kThreads, 0, stream>>>(sz, maxg, offsets, rows, G, n, cnt);
+    NNGP_CUDA_TRY(cudaGetLastError());
+    auto scan = [&](int32_t *src, int32_t *dst) -> nngp_status {
+        size_t nb = 0;
+        NNGP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, nb, src, dst, (int)g1, stream));
+        if (nb > L.cub_bytes) return fail(NNGP_ERR_WORKSPACE, "knn pruning: scan scratch exceeds the budget");
+        nb = L.cub_bytes;
+        NNGP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(at(L.cub), nb, src, dst, (int)g1, stream));
+        return NNGP_OK;
+    };
+    if ((st = scan(cnt, cbase)) != NNGP_OK) return st;
+    split_kernel<<<grid_of(g1), kThreads, 0, stream>>>(sz, maxg, cnt, cbase, K, S);
+    NNGP_CUDA_TRY(cudaGetLastError());
+    if ((st = scan(K, kbase)) != NNGP_OK) return st;
+    if ((st = scan(S, sbase)) != NNGP_OK) return st;
+    int32_t *ig = static_cast<int32_t *>(at(L.igroup[pl])), *i0 = static_cast<int32_t *>(at(L.it0[pl]));
+    int32_t *i1 = static_cast<int32_t *>(at(L.it1[pl])), *is = static_cast<int32_t *>(at(L.islot[pl]));
+    cub::DoubleBuffer<uint32_t> okb(static_cast<uint32_t *>(at(L.okey_a[pl])), static_cast<uint32_t *>(at(L.okey_b[pl])));
+    cub::DoubleBuffer<int32_t> ovb(static_cast<int32_t *>(at(L.oval_a[pl])), static_cast<int32_t *>(at(L.oval_b[pl])));
+    item_fill_kernel<<<grid_of(mi), kThreads, 0, stream>>>(sz, maxg, mi, cnt, K, kbase, sbase, ig, i0, i1, is,
+                                                           okb.Current(), ovb.Current());
+    NNGP_CUDA_TRY(cudaGetLastError());
+    items_size_kernel<<<1, 1, 0, stream>>>(sz, maxg, kbase);
+    NNGP_CUDA_TRY(cudaGetLastError());
+    size_t need = 0;
+    NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, need, okb, ovb, (int)mi, 0, 32, stream));
+    if (need > L.cub_bytes) return fail(NNGP_ERR_WORKSPACE, "knn pruning: sort scratch exceeds the budget");
+    size_t have = L.cub_bytes;
+    NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(at(L.cub), have, okb, ovb, (int)mi, 0, 32, stream));
+    tc::TcItems &ti = pl == 0 ? out->pruned_items : out->index_items;
+    ti.group = ig;
+    ti.t0 = i0;
+    ti.t1 = i1;
+    ti.slot = is;
+    ti.order = ovb.Current();
+    ti.partial = static_cast<unsigned long long *>(at(L.partial[pl]));
+    out->split_k[pl] = K;
+    out->slot_base[pl] = sbase;
+    out->max_groups_of[pl] = maxg;
+    out->max_items[pl] = mi;
+    return NNGP_OK;
+}
+
+// Layout of a query search's plan: ref tiles of n_ref refs, uniform groups of the n_query rows,
+// the pruned launch's items only.
+Layout layout_query(int64_t n_ref, int64_t n_query, int d, int G) {
+    Layout L{};
+    L.n_tiles = (n_ref + kTileRefs - 1) / kTileRefs;
+    L.max_groups = (n_query + G - 1) / G;
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        const size_t o = off;
+        off = align_up(off + bytes, 256);
+        return o;
+    };
+    L.tlo = take((size_t)L.n_tiles * d * 4);
+    L.thi = take((size_t)L.n_tiles * d * 4);
+    L.tmin = take((size_t)L.n_tiles * 4);
+    L.row_off = take((size_t)(L.max_groups + 1) * 4);
+    L.sizes = take(2 * sizeof(DevSizes));
+    L.glo = take((size_t)L.max_groups * d * 4);
+    L.ghi = take((size_t)L.max_groups * d * 4);
+    L.gtau = take((size_t)L.max_groups * 4);
+    L.glim = take((size_t)L.max_groups * 4);
+    L.counts = take((size_t)(L.max_groups + 1) * 4);
+    L.offsets = take((size_t)(L.max_groups + 1) * 4);
+    L.maxg[0] = L.max_groups;
+    L.maxg[1] = 0;
+    const int64_t g1 = L.maxg[0] + 1;
+    L.max_items[0] = L.maxg[0] + kMaxSlots;
+    L.cnt[0] = take((size_t)g1 * 4);
+    L.cbase[0] = take((size_t)g1 * 4);
+    L.K[0] = take((size_t)g1 * 4);
+    L.kbase[0] = take((size_t)g1 * 4);
+    L.S[0] = take((size_t)g1 * 4);
+    L.sbase[0] = take((size_t)g1 * 4);
+    for (size_t *f : {&L.igroup[0], &L.it0[0], &L.it1[0], &L.islot[0], &L.okey_a[0], &L.okey_b[0], &L.oval_a[0],
+                      &L.oval_b[0]})
+        *f = take((size_t)L.max_items[0] * 4);
+    L.partial[0] = take((size_t)kMaxSlots * G * 32 * 8);
+    L.list = take((size_t)L.max_groups * L.n_tiles * 4);
+    L.cub_bytes = align_up((size_t)(4u << 20) + (size_t)(n_query + n_ref) / 2, 256);
+    L.cub = take(L.cub_bytes);
+    L.total = off + 256;
+    return L;
 }
 
 }  // namespace
@@ -638,8 +746,8 @@ nngp_status build(const float *xs, int64_t n, int d, int dp, int G, int bits, co
     NNGP_CUDA_TRY(cudaGetLastError());
 
     // tile lists, then the work order (longest list first)
-    group_box_kernel<<<grid_of(L.max_groups * 32), kThreads, 0, stream>>>(xs, d, dp, rows, row_off, sizes, seeds, glo,
-                                                                          ghi, gtau, glim);
+    group_box_kernel<<<grid_of(L.max_groups * 32), kThreads, 0, stream>>>(xs, d, dp, rows, row_off, sizes, seeds, 0,
+                                                                          glo, ghi, gtau, glim);
     NNGP_CUDA_TRY(cudaGetLastError());
     Boxes b{tlo, thi, glo, ghi, gtau, tmin, glim, d, (double)(d + 3) * 1.1920928955078125e-07};
     NNGP_CUDA_TRY(cudaMemsetAsync(counts + L.max_groups, 0, sizeof(int32_t), stream));
@@ -654,55 +762,9 @@ nngp_status build(const float *xs, int64_t n, int d, int dp, int G, int bits, co
     NNGP_CUDA_TRY(cudaGetLastError());
 
     // work items of both launches: long tile ranges split, most tiles first
-    for (int pl = 0; pl < 2; ++pl) {
-        const int64_t maxg = L.maxg[pl], g1 = maxg + 1, mi = L.max_items[pl];
-        int32_t *cnt = static_cast<int32_t *>(at(L.cnt[pl])), *cbase = static_cast<int32_t *>(at(L.cbase[pl]));
-        int32_t *K = static_cast<int32_t *>(at(L.K[pl])), *kbase = static_cast<int32_t *>(at(L.kbase[pl]));
-        int32_t *S = static_cast<int32_t *>(at(L.S[pl])), *sbase = static_cast<int32_t *>(at(L.sbase[pl]));
-        DevSizes *sz = sizes + pl;
-        group_tiles_kernel<<<grid_of(g1), kThreads, 0, stream>>>(sz, maxg, pl == 0 ? offsets : nullptr, rows, G, n,
-                                                                 cnt);
-        NNGP_CUDA_TRY(cudaGetLastError());
-        auto scan = [&](int32_t *src, int32_t *dst) -> nngp_status {
-            size_t nb = 0;
-            NNGP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, nb, src, dst, (int)g1, stream));
-            if (nb > L.cub_bytes) return fail(NNGP_ERR_WORKSPACE, "knn pruning: scan scratch exceeds the budget");
-            nb = L.cub_bytes;
-            NNGP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(at(L.cub), nb, src, dst, (int)g1, stream));
-            return NNGP_OK;
-        };
-        if ((st = scan(cnt, cbase)) != NNGP_OK) return st;
-        split_kernel<<<grid_of(g1), kThreads, 0, stream>>>(sz, maxg, cnt, cbase, K, S);
-        NNGP_CUDA_TRY(cudaGetLastError());
-        if ((st = scan(K, kbase)) != NNGP_OK) return st;
-        if ((st = scan(S, sbase)) != NNGP_OK) return st;
-        int32_t *ig = static_cast<int32_t *>(at(L.igroup[pl])), *i0 = static_cast<int32_t *>(at(L.it0[pl]));
-        int32_t *i1 = static_cast<int32_t *>(at(L.it1[pl])), *is = static_cast<int32_t *>(at(L.islot[pl]));
-        cub::DoubleBuffer<uint32_t> okb(static_cast<uint32_t *>(at(L.okey_a[pl])),
-                                        static_cast<uint32_t *>(at(L.okey_b[pl])));
-        cub::DoubleBuffer<int32_t> ovb(static_cast<int32_t *>(at(L.oval_a[pl])), static_cast<int32_t *>(at(L.oval_b[pl])));
-        item_fill_kernel<<<grid_of(mi), kThreads, 0, stream>>>(sz, maxg, mi, cnt, K, kbase, sbase, ig, i0, i1, is,
-                                                               okb.Current(), ovb.Current());
-        NNGP_CUDA_TRY(cudaGetLastError());
-        items_size_kernel<<<1, 1, 0, stream>>>(sz, maxg, kbase);
-        NNGP_CUDA_TRY(cudaGetLastError());
-        need = 0;
-        NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, need, okb, ovb, (int)mi, 0, 32, stream));
-        if ((st = cub_check(need)) != NNGP_OK) return st;
-        have = L.cub_bytes;
-        NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(at(L.cub), have, okb, ovb, (int)mi, 0, 32, stream));
-        tc::TcItems &ti = pl == 0 ? out->pruned_items : out->index_items;
-        ti.group = ig;
-        ti.t0 = i0;
-        ti.t1 = i1;
-        ti.slot = is;
-        ti.order = ovb.Current();
-        ti.partial = static_cast<unsigned long long *>(at(L.partial[pl]));
-        out->split_k[pl] = K;
-        out->slot_base[pl] = sbase;
-        out->max_groups_of[pl] = maxg;
-        out->max_items[pl] = mi;
-    }
+    for (int pl = 0; pl < 2; ++pl)
+        if ((st = plan_items(L, base, pl, sizes + pl, pl == 0 ? offsets : nullptr, rows, G, n, out, stream)) != NNGP_OK)
+            return st;
 
     out->rows = rows;
     out->ref_order = ref_order;
@@ -712,6 +774,66 @@ nngp_status build(const float *xs, int64_t n, int d, int dp, int G, int bits, co
     out->offsets = offsets;
     out->tiles = list;
     out->max_groups = L.max_groups;
+    return NNGP_OK;
+}
+
+size_t workspace_query(int64_t n_ref, int64_t n_query, int d, int rows_per_group) {
+    if (n_ref < kMinPoints || n_ref > kMaxPoints || n_query < 1 || d < 1 || d > kMaxDim || rows_per_group < 1) return 0;
+    return layout_query(n_ref, n_query, d, rows_per_group).total;
+}
+
+nngp_status build_query(const float *xs_ref, int64_t n_ref, const float *xq, int64_t n_query, int d, int dp, int G,
+                        const float *seeds, const int32_t *order0, const int32_t *qorder, void *ws, size_t ws_bytes,
+                        Lists *out, cudaStream_t stream) {
+    if (workspace_query(n_ref, n_query, d, G) == 0 || !xs_ref || !xq || !seeds || !order0 || !qorder || !out)
+        return fail(NNGP_ERR_UNSUPPORTED, "knn pruning: shape outside the pruned query search");
+    const Layout L = layout_query(n_ref, n_query, d, G);
+    if (!ws || ws_bytes < L.total) return fail(NNGP_ERR_WORKSPACE, "knn pruning: workspace too small");
+    char *base = reinterpret_cast<char *>(align_up(reinterpret_cast<uintptr_t>(ws), 256));
+    auto at = [&](size_t off) { return reinterpret_cast<void *>(base + off); };
+    float *tlo = static_cast<float *>(at(L.tlo)), *thi = static_cast<float *>(at(L.thi));
+    int32_t *tmin = static_cast<int32_t *>(at(L.tmin));
+    int32_t *row_off = static_cast<int32_t *>(at(L.row_off));
+    DevSizes *sizes = static_cast<DevSizes *>(at(L.sizes));
+    float *glo = static_cast<float *>(at(L.glo)), *ghi = static_cast<float *>(at(L.ghi));
+    float *gtau = static_cast<float *>(at(L.gtau));
+    int32_t *glim = static_cast<int32_t *>(at(L.glim));
+    int32_t *counts = static_cast<int32_t *>(at(L.counts)), *offsets = static_cast<int32_t *>(at(L.offsets));
+    int32_t *list = static_cast<int32_t *>(at(L.list));
+    nngp_status st = NNGP_OK;
+
+    tile_box_kernel<<<grid_of(L.n_tiles * 32), kThreads, 0, stream>>>(xs_ref, n_ref, d, dp, order0, L.n_tiles, tlo, thi,
+                                                                       tmin);
+    NNGP_CUDA_TRY(cudaGetLastError());
+    uniform_groups_kernel<<<grid_of(L.max_groups + 1), kThreads, 0, stream>>>(n_query, G, L.max_groups, row_off, sizes,
+                                                                              sizes + 1);
+    NNGP_CUDA_TRY(cudaGetLastError());
+    group_box_kernel<<<grid_of(L.max_groups * 32), kThreads, 0, stream>>>(xq, d, dp, qorder, row_off, sizes, seeds, 1,
+                                                                          glo, ghi, gtau, glim);
+    NNGP_CUDA_TRY(cudaGetLastError());
+    Boxes b{tlo, thi, glo, ghi, gtau, tmin, glim, d, (double)(d + 3) * 1.1920928955078125e-07};
+    NNGP_CUDA_TRY(cudaMemsetAsync(counts + L.max_groups, 0, sizeof(int32_t), stream));
+    count_kernel<<<grid_of(L.max_groups * 32), kThreads, 0, stream>>>(b, sizes, L.max_groups, L.n_tiles, counts);
+    NNGP_CUDA_TRY(cudaGetLastError());
+    size_t need = 0;
+    NNGP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, need, counts, offsets, (int)(L.max_groups + 1), stream));
+    if (need > L.cub_bytes) return fail(NNGP_ERR_WORKSPACE, "knn pruning: scan scratch exceeds the budget");
+    size_t have = L.cub_bytes;
+    NNGP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(at(L.cub), have, counts, offsets, (int)(L.max_groups + 1), stream));
+    fill_kernel<<<grid_of(L.max_groups * 32), kThreads, 0, stream>>>(b, sizes, L.n_tiles, offsets, list);
+    NNGP_CUDA_TRY(cudaGetLastError());
+    if ((st = plan_items(L, base, 0, sizes, offsets, qorder, G, n_ref, out, stream)) != NNGP_OK) return st;
+    out->rows = qorder;
+    out->ref_order = order0;
+    out->pruned = sizes;
+    out->index_order = sizes + 1;
+    out->row_off = row_off;
+    out->offsets = offsets;
+    out->tiles = list;
+    out->max_groups = L.max_groups;
+    out->index_items = tc::TcItems{};
+    out->split_k[1] = nullptr;
+    out->max_items[1] = 0;
     return NNGP_OK;
 }
 

@@ -75,6 +75,15 @@ nngp_status build(const float *xs, int64_t n, int d, int dp, int rows_per_group,
                   const float *seeds, const int32_t *order0, const int32_t *pos0, const uint64_t *keys0, void *ws,
                   size_t ws_bytes, Lists *out, cudaStream_t stream);
 
+// The same for a search of n_query queries against n_ref refs without a prefix rule (predict):
+// the queries in curve-0 order (qorder, from knn_seed's query_seeds) cut into groups of
+// rows_per_group, every ref tile (refs in their curve-0 order, order0) listed unless the box
+// distance rule excludes it.  All rows take the pruned launch (index_order is empty).
+size_t workspace_query(int64_t n_ref, int64_t n_query, int d, int rows_per_group);
+nngp_status build_query(const float *xs_ref, int64_t n_ref, const float *xq, int64_t n_query, int d, int dp,
+                        int rows_per_group, const float *seeds, const int32_t *order0, const int32_t *qorder, void *ws,
+                        size_t ws_bytes, Lists *out, cudaStream_t stream);
+
 // Combines the partial lists of the split groups of launch `which` (0 pruned, 1 index order)
 // into out (num_nn m).  Runs after that launch on the same stream.
 nngp_status merge(const Lists &lists, int which, int rows_per_group, int m, int32_t *out, cudaStream_t stream);

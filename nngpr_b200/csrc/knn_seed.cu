@@ -148,6 +148,36 @@ __device__ __forceinline__ uint32_t dist_bits(const float *__restrict__ row, con
     return __float_as_uint(d2);  // NaN bits lie above kInfBits and are never counted
 }
 
+// The m-th smallest of the warp's values (each lane holds N; 0xFFFFFFFF = none, NaN bits above
+// kInfBits never count): bisection on the bit patterns, stopped within kTolBits above it, so
+// at least m values are <= the result; kInfBits when fewer than m values are finite.
+template <int N>
+__device__ __forceinline__ uint32_t mth_smallest_bits(const uint32_t (&v)[N], int m) {
+    constexpr unsigned FULL = 0xFFFFFFFFu;
+    auto count_le = [&](uint32_t bound) -> int {
+        int c = 0;
+#pragma unroll
+        for (int e = 0; e < N; ++e) c += v[e] <= bound ? 1 : 0;
+        return (int)__reduce_add_sync(FULL, (unsigned)c);
+    };
+    if (count_le(kInfBits) < m) return kInfBits;
+    uint32_t mn = 0xFFFFFFFFu, mx = 0u;
+#pragma unroll
+    for (int e = 0; e < N; ++e) {
+        if (v[e] <= kInfBits) {
+            mn = min(mn, v[e]);
+            mx = max(mx, v[e]);
+        }
+    }
+    uint32_t lo = __reduce_min_sync(FULL, mn), hi = __reduce_max_sync(FULL, mx);  // count_le(hi) >= m
+    while (hi - lo > kTolBits) {  // invariant: count_le(hi) >= m; warp-uniform
+        const uint32_t mid = lo + ((hi - lo) >> 1);
+        if (count_le(mid) >= m) hi = mid;
+        else lo = mid + 1;
+    }
+    return hi;
+}
+
 // One warp per point (taken in curve-0 order).  Lane values: squared-distance bits of the refs
 // j < i in the window [p - W, p + W) of each curve (curve 1 skips refs inside curve 0's window,
 // so every ref counts once); 0xFFFFFFFF for the other slots.  The row's seed is the m-th
@@ -198,37 +228,71 @@ __global__ void __launch_bounds__(kThreads) seed_kernel(const float *__restrict_
             }
             v[VPL + t] = val;
         }
-        auto count_le = [&](uint32_t bound) -> int {
-            int c = 0;
-#pragma unroll
-            for (int e = 0; e < 2 * VPL; ++e) c += v[e] <= bound ? 1 : 0;
-            return (int)__reduce_add_sync(FULL, (unsigned)c);
-        };
-        uint32_t res = kInfBits;
-        if (count_le(kInfBits) >= m) {
-            uint32_t mn = 0xFFFFFFFFu, mx = 0u;
-#pragma unroll
-            for (int e = 0; e < 2 * VPL; ++e) {
-                if (v[e] <= kInfBits) {
-                    mn = min(mn, v[e]);
-                    mx = max(mx, v[e]);
-                }
-            }
-            uint32_t lo = __reduce_min_sync(FULL, mn), hi = __reduce_max_sync(FULL, mx);  // count_le(hi) >= m
-            while (hi - lo > kTolBits) {  // invariant: count_le(hi) >= m; warp-uniform
-                const uint32_t mid = lo + ((hi - lo) >> 1);
-                if (count_le(mid) >= m) hi = mid;
-                else lo = mid + 1;
-            }
-            res = hi;
-        }
+        const uint32_t res = mth_smallest_bits<2 * VPL>(v, m);
         if (lane == 0) seeds[i] = combine ? fminf(seeds[i], __uint_as_float(res)) : __uint_as_float(res);
     }
 }
 
+// First position in keys[0, n) whose key is >= key (keys ascending).
+__device__ __forceinline__ int64_t lower_bound_u64(const uint64_t *__restrict__ keys, int64_t n, uint64_t key) {
+    int64_t lo = 0, hi = n;
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (keys[mid] < key) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Seeds of queries against refs (no prefix rule: every ref counts).  One warp per query, taken
+// in curve-0 order (qorder) so that neighbouring warps read the same windows: the query's place
+// in each curve of the refs (binary search of its key among the refs' sorted keys), the refs
+// within W positions on either side (curve 1 skips refs inside curve 0's window), the m-th
+// smallest squared distance in the search's exact arithmetic.
+template <int D>
+__global__ void __launch_bounds__(kThreads) qseed_kernel(const float *__restrict__ xs0, const float *__restrict__ xs1,
+                                                         const uint64_t *__restrict__ keys0s,
+                                                         const uint64_t *__restrict__ keys1s, int64_t n_ref,
+                                                         const int32_t *__restrict__ p0_of1,
+                                                         const float *__restrict__ xq, int64_t n_query,
+                                                         const uint64_t *__restrict__ qkey0,
+                                                         const uint64_t *__restrict__ qkey1,
+                                                         const int32_t *__restrict__ qorder, int dp, int m,
+                                                         float *__restrict__ seeds) {
+    constexpr int VPL = 8, W = VPL * 16;
+    const int lane = threadIdx.x & 31;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t k = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; k < n_query; k += nwarps) {
+        const int64_t q = qorder[k];
+        float qv[D];
+#pragma unroll
+        for (int f = 0; f < D; ++f) qv[f] = xq[q * dp + f];
+        const int64_t c0 = lower_bound_u64(keys0s, n_ref, qkey0[q]);
+        const int64_t c1 = lower_bound_u64(keys1s, n_ref, qkey1[q]);
+        uint32_t v[2 * VPL];
+#pragma unroll
+        for (int t = 0; t < VPL; ++t) {
+            const int64_t pk = c0 - W + lane + 32 * t;
+            v[t] = (pk >= 0 && pk < n_ref) ? dist_bits<D>(xs0 + pk * dp, qv) : 0xFFFFFFFFu;
+        }
+#pragma unroll
+        for (int t = 0; t < VPL; ++t) {
+            const int64_t pk = c1 - W + lane + 32 * t;
+            uint32_t val = 0xFFFFFFFFu;
+            if (pk >= 0 && pk < n_ref) {
+                const int64_t pj = p0_of1[pk];
+                if (pj < c0 - W || pj >= c0 + W) val = dist_bits<D>(xs1 + pk * dp, qv);
+            }
+            v[VPL + t] = val;
+        }
+        const uint32_t res = mth_smallest_bits<2 * VPL>(v, m);
+        if (lane == 0) seeds[q] = __uint_as_float(res);
+    }
+}
+
 struct Layout {
-    size_t keys_a, keys_b, keys0, idx0_a, idx0_b, idx1_a, idx1_b, pos0, pos1, p0of1, xs0, xs1, bounds, cub, cub_bytes,
-        total;
+    size_t keys_a, keys_b, keys0, keys1, idx0_a, idx0_b, idx1_a, idx1_b, pos0, pos1, p0of1, xs0, xs1, bounds, cub,
+        cub_bytes, total;
 };
 
 Layout layout(int64_t n, int dp) {
@@ -242,6 +306,7 @@ Layout layout(int64_t n, int dp) {
     L.keys_a = take((size_t)n * 8);
     L.keys_b = take((size_t)n * 8);
     L.keys0 = take((size_t)n * 8);
+    L.keys1 = take((size_t)n * 8);
     L.idx0_a = take((size_t)n * 4);
     L.idx0_b = take((size_t)n * 4);
     L.idx1_a = take((size_t)n * 4);
@@ -299,6 +364,8 @@ int grid_of(int64_t work) {
 
 // One level: seeds of the points [0, n) from the windows of the curves of those points only
 // (combine: keep the smaller of the old and the new bound).
+// seeds == nullptr: only the curves (orders, inverse, sorted keys of both curves, coordinates in
+// curve order), for the query seeds.
 nngp_status run_level(const float *xs, int64_t n, int d, int D, int dp, int m, int W, char *base, const Layout &L,
                       int combine, float *seeds, cudaStream_t stream, const int32_t **order0_out,
                       const int32_t **pos0_out, const uint64_t **keys0_out) {
@@ -328,8 +395,9 @@ nngp_status run_level(const float *xs, int64_t n, int d, int D, int dp, int m, i
         size_t have = L.cub_bytes;
         NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(at(L.cub), have, dk, dv, (int)n, 0, bits * d, stream));
         order[c] = dv.Current();
-        if (c == 0 && keys0_out) {  // the curve-0 keys in curve order, for callers that cut the curve into cells
-            NNGP_CUDA_TRY(cudaMemcpyAsync(at(L.keys0), dk.Current(), (size_t)n * 8, cudaMemcpyDeviceToDevice, stream));
+        if ((c == 0 && keys0_out) || !seeds) {  // sorted keys, for cells along the curve or query positions
+            NNGP_CUDA_TRY(cudaMemcpyAsync(at(c ? L.keys1 : L.keys0), dk.Current(), (size_t)n * 8,
+                                          cudaMemcpyDeviceToDevice, stream));
         }
         inverse_kernel<<<grid_of(n), kThreads, 0, stream>>>(order[c], n, pos[c]);
         NNGP_CUDA_TRY(cudaGetLastError());
@@ -340,16 +408,49 @@ nngp_status run_level(const float *xs, int64_t n, int d, int D, int dp, int m, i
     int32_t *p0of1 = static_cast<int32_t *>(at(L.p0of1));
     cross_pos_kernel<<<grid_of(n), kThreads, 0, stream>>>(order[1], pos[0], n, p0of1);
     NNGP_CUDA_TRY(cudaGetLastError());
+    if (order0_out) *order0_out = order[0];
+    if (pos0_out) *pos0_out = pos[0];
+    if (keys0_out) *keys0_out = static_cast<const uint64_t *>(at(L.keys0));
+    if (!seeds) return NNGP_OK;
     const int grid = (int)std::min<int64_t>((n + kThreads / 32 - 1) / (kThreads / 32), (int64_t)kNumSMsB200 * 16);
     const SeedArgs sa{static_cast<const float *>(at(L.xs0)), static_cast<const float *>(at(L.xs1)), n, dp, m,
                       order[0], order[1], p0of1, pos[1], combine, seeds};
     const bool ok = W == 128 ? dispatch_seed<8>(D, grid, sa, stream) : dispatch_seed<16>(D, grid, sa, stream);
     if (!ok) return fail(NNGP_ERR_UNSUPPORTED, "knn seeds: no kernel for D = " + std::to_string(D));
     NNGP_CUDA_TRY(cudaGetLastError());
-    if (order0_out) *order0_out = order[0];
-    if (pos0_out) *pos0_out = pos[0];
-    if (keys0_out) *keys0_out = static_cast<const uint64_t *>(at(L.keys0));
     return NNGP_OK;
+}
+
+// Query region of the query-seed workspace.
+struct QLayout {
+    size_t k0, k1, kb, kb2, ia, ib, cub, cub_bytes, total;
+};
+QLayout qlayout(int64_t nq) {
+    QLayout Q{};
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        const size_t o = off;
+        off = align_up(off + bytes, 256);
+        return o;
+    };
+    Q.k0 = take((size_t)nq * 8);
+    Q.k1 = take((size_t)nq * 8);
+    Q.kb = take((size_t)nq * 8);
+    Q.kb2 = take((size_t)nq * 8);
+    Q.ia = take((size_t)nq * 4);
+    Q.ib = take((size_t)nq * 4);
+    Q.cub_bytes = align_up((size_t)(4u << 20) + (size_t)nq / 2, 256);
+    Q.cub = take(Q.cub_bytes);
+    Q.total = off + 256;
+    return Q;
+}
+
+template <int D>
+void launch_qseed(int grid, const float *xs0, const float *xs1, const uint64_t *k0s, const uint64_t *k1s, int64_t n_ref,
+                  const int32_t *p0of1, const float *xq, int64_t nq, const uint64_t *qk0, const uint64_t *qk1,
+                  const int32_t *qorder, int dp, int m, float *seeds, cudaStream_t stream) {
+    qseed_kernel<D><<<grid, kThreads, 0, stream>>>(xs0, xs1, k0s, k1s, n_ref, p0of1, xq, nq, qk0, qk1, qorder, dp, m,
+                                                   seeds);
 }
 
 // Refinement levels: prefixes n / 8, n / 64, ... (while at least kMinPoints), run in a second
@@ -357,6 +458,64 @@ nngp_status run_level(const float *xs, int64_t n, int d, int D, int dp, int m, i
 size_t sub_bytes(int64_t n, int dp) { return n / 8 >= kMinPoints ? layout(n / 8, dp).total : 0; }
 
 }  // namespace
+
+size_t workspace_query(int64_t n_ref, int64_t n_query, int dp) {
+    if (n_ref < kMinPoints || n_query < 1) return 0;
+    return align_up(layout(n_ref, dp).total, 256) + qlayout(n_query).total;
+}
+
+nngp_status query_seeds(const float *xs_ref, int64_t n_ref, const float *xq, int64_t n_query, int d, int D, int dp,
+                        int m, void *ws, size_t ws_bytes, float *seeds, cudaStream_t stream, const int32_t **order0_out,
+                        const int32_t **qorder_out) {
+    if (n_ref < kMinPoints || n_query < 1 || m < 1 || d < 1 || d > 24 || D < d || dp % 4 != 0 || dp < D)
+        return fail(NNGP_ERR_UNSUPPORTED, "knn query seeds: shape outside the seeded search");
+    const Layout L = layout(n_ref, dp);
+    if (!ws || ws_bytes < workspace_query(n_ref, n_query, dp))
+        return fail(NNGP_ERR_WORKSPACE, "knn query seeds: workspace too small");
+    char *base = reinterpret_cast<char *>(align_up(reinterpret_cast<uintptr_t>(ws), 256));
+    const int32_t *order0 = nullptr;
+    nngp_status st = run_level(xs_ref, n_ref, d, D, dp, m, 128, base, L, 0, nullptr, stream, &order0, nullptr, nullptr);
+    if (st != NNGP_OK) return st;
+    char *qb = base + align_up(L.total, 256);
+    const QLayout Q = qlayout(n_query);
+    auto qat = [&](size_t off) { return reinterpret_cast<void *>(qb + off); };
+    auto at = [&](size_t off) { return reinterpret_cast<void *>(base + off); };
+    const uint32_t *lo = static_cast<const uint32_t *>(at(L.bounds)), *hi = lo + 256;
+    const int bits = seed::bits(d);
+    uint64_t *qk0 = static_cast<uint64_t *>(qat(Q.k0)), *qk1 = static_cast<uint64_t *>(qat(Q.k1));
+    int32_t *ia = static_cast<int32_t *>(qat(Q.ia));
+    // the queries' keys on the refs' grids (their bounds: queries outside them clamp to the edge)
+    keys_kernel<<<grid_of(n_query), kThreads, 0, stream>>>(xq, n_query, d, dp, lo, hi, bits, 1, qk1, ia);
+    NNGP_CUDA_TRY(cudaGetLastError());
+    keys_kernel<<<grid_of(n_query), kThreads, 0, stream>>>(xq, n_query, d, dp, lo, hi, bits, 0, qk0, ia);
+    NNGP_CUDA_TRY(cudaGetLastError());
+    // query order along curve 0 (sorts a copy of the keys; qk0 stays indexed by query)
+    NNGP_CUDA_TRY(cudaMemcpyAsync(qat(Q.kb), qk0, (size_t)n_query * 8, cudaMemcpyDeviceToDevice, stream));
+    cub::DoubleBuffer<uint64_t> dk(static_cast<uint64_t *>(qat(Q.kb)), static_cast<uint64_t *>(qat(Q.kb2)));
+    cub::DoubleBuffer<int32_t> dv(ia, static_cast<int32_t *>(qat(Q.ib)));
+    size_t need = 0;
+    NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, need, dk, dv, (int)n_query, 0, bits * d, stream));
+    if (need > Q.cub_bytes) return fail(NNGP_ERR_WORKSPACE, "knn query seeds: sort scratch exceeds the budget");
+    size_t have = Q.cub_bytes;
+    NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(qat(Q.cub), have, dk, dv, (int)n_query, 0, bits * d, stream));
+    const int32_t *qorder = dv.Current();
+    const int grid = (int)std::min<int64_t>((n_query + kThreads / 32 - 1) / (kThreads / 32), (int64_t)kNumSMsB200 * 16);
+    const float *xs0 = static_cast<const float *>(at(L.xs0)), *xs1 = static_cast<const float *>(at(L.xs1));
+    const uint64_t *k0s = static_cast<const uint64_t *>(at(L.keys0)), *k1s = static_cast<const uint64_t *>(at(L.keys1));
+    const int32_t *p0of1 = static_cast<const int32_t *>(at(L.p0of1));
+    switch (D) {
+#define NNGP_QS(DD) \
+    case DD: launch_qseed<DD>(grid, xs0, xs1, k0s, k1s, n_ref, p0of1, xq, n_query, qk0, qk1, qorder, dp, m, seeds, stream); break;
+        NNGP_QS(1) NNGP_QS(2) NNGP_QS(3) NNGP_QS(4) NNGP_QS(5) NNGP_QS(6) NNGP_QS(7) NNGP_QS(8) NNGP_QS(12) NNGP_QS(16)
+        NNGP_QS(20) NNGP_QS(24)
+#undef NNGP_QS
+        default: return fail(NNGP_ERR_UNSUPPORTED, "knn query seeds: no kernel for D = " + std::to_string(D));
+    }
+    NNGP_CUDA_TRY(cudaGetLastError());
+    if (order0_out) *order0_out = order0;
+    if (qorder_out) *qorder_out = qorder;
+    return NNGP_OK;
+}
 
 size_t workspace(int64_t n, int dp) {
     return n < kMinPoints ? 0 : align_up(layout(n, dp).total, 256) + sub_bytes(n, dp);

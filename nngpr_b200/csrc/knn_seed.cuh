@@ -30,6 +30,22 @@ nngp_status prefix_seeds(const float *xs, int64_t n, int d, int D, int dp, int m
                          float *seeds, cudaStream_t stream, const int32_t **order0 = nullptr,
                          const int32_t **pos0 = nullptr, const uint64_t **keys0 = nullptr);
 
+// Seeds of a search of n_query queries against n_ref refs (no prefix rule): seeds[q] >= the m-th
+// smallest squared distance from query q to the refs, in the search's FP32 arithmetic, from the
+// refs' curve windows around the query's place in each curve.  xs_ref / xq: scaled points, row
+// stride dp.  order0: the refs' curve-0 order (ref tiles of a pruned search use it); qorder: the
+// queries in curve-0 order.  Runs on `stream`.
+size_t workspace_query(int64_t n_ref, int64_t n_query, int dp);
+// The query-search seeds are used (and budgeted) from this many queries on: below it the refs'
+// sorts cost more than the seeds save.
+constexpr int64_t kMinQueries = 16384;
+inline size_t query_workspace_if(int64_t n_ref, int64_t n_query, int dp) {
+    return n_query >= kMinQueries ? workspace_query(n_ref, n_query, dp) : 0;
+}
+nngp_status query_seeds(const float *xs_ref, int64_t n_ref, const float *xq, int64_t n_query, int d, int D, int dp,
+                        int m, void *ws, size_t ws_bytes, float *seeds, cudaStream_t stream, const int32_t **order0,
+                        const int32_t **qorder);
+
 // Bits per dimension of the Morton keys for d features.
 inline int bits(int d) { return d < 7 ? 10 : 64 / d; }
 

@@ -58,7 +58,8 @@ constexpr int THREADS = 5 * 32;   // layout self-test: 4 epilogue warps + the MM
 constexpr int LIST = 32;       // largest num_nn
 constexpr int HS = 33;         // heap row stride in 64-bit keys (odd: rows of a warp hit distinct banks)
 constexpr int DRAIN_AT = 32;   // queued entries that trigger a drain at the end of a tile (8: +2%, 128: +7% at d = 3)
-constexpr int QCAP = 256;      // candidate queue entries per epilogue warp
+constexpr int QCAP = 64;       // candidate queue entries per epilogue warp (a drain runs before an
+                               // iteration that could overflow it; 64 leaves room for a third stage)
 constexpr uint32_t kSelftestCols = 2 * RT;  // TMEM columns of the layout self-test
 constexpr float kEpsTc = 1.52587890625e-05f;       // 2^-16
 constexpr float kPadNorm = 1.7014118346046923e38f;  // 2^127: padded refs never pass a finite screen
@@ -85,7 +86,7 @@ struct Cfg {
     static constexpr int LIST_BYTES = ROWS * HS * 8;  // one heap of keys per query
     static constexpr int QUEUE_BYTES = EPI_WARPS * QCAP * (8 + 1);  // key + row
     static constexpr int BAR_BYTES = 256;
-    static constexpr int FIXED = 1024 + A_BYTES + LIST_BYTES + QUEUE_BYTES + BAR_BYTES;
+    static constexpr int FIXED = 128 + A_BYTES + LIST_BYTES + QUEUE_BYTES + BAR_BYTES;  // 128: base alignment slack
     // as many CTAs per SM (up to 3) as hold at least 2 stages each: more epilogue warps per
     // scheduler.  Three CTAs share TMEM with one accumulator buffer each (the epilogue frees it
     // as soon as a tile's scores are in registers); one or two CTAs double-buffer it.
@@ -287,9 +288,10 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
     constexpr int S = C::STAGES;
     constexpr int EPI_WARPS = C::EPI_WARPS;
     constexpr unsigned FULL = 0xffffffffu;
-    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    // 128-byte base: the no-swizzle UMMA operands and the bulk copies need 16-byte alignment
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     unsigned char *sm =
-        reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+        reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
     unsigned char *sA = sm;
     unsigned char *sB = sA + C::A_BYTES;
     uint64_t *H = reinterpret_cast<uint64_t *>(sB + S * C::STAGE_BYTES);  // [ROWS][HS] heaps

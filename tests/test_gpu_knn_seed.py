@@ -132,3 +132,46 @@ def test_split_work_items_merge_to_the_same_lists(monkeypatch, capfd):
     assert mt and int(mt.group(2)) > int(mt.group(1))  # some groups were split
     assert np.array_equal(a, search_mode(monkeypatch, y, 32, 0.5, False))
     check_rows(y, a, 32, 0.5, rng, k=100)
+
+
+def query_search(monkeypatch, ref, q, m, ls, window, prune=True):
+    monkeypatch.setenv('NNGP_KNN_SEED_W', str(window))
+    monkeypatch.setenv('NNGP_KNN_PRUNE', '1' if prune else '0')
+    r = torch.from_numpy(np.ascontiguousarray(ref, dtype=np.float32)).cuda()
+    qq = torch.from_numpy(np.ascontiguousarray(q, dtype=np.float32)).cuda()
+    flags = ops.new_flags(r.device)
+    out = ops.knn(r, qq, m, None, ls, flags=flags)
+    assert int(flags.item()) == 0
+    return out.cpu().numpy()
+
+
+@pytest.mark.parametrize('d,n_ref,n_query', [(2, 70000, 20000), (3, 70000, 100000), (4, 30000, 40000),
+                                             (5, 30000, 20000), (16, 20000, 30000)])
+def test_query_search_seeded_and_pruned_equal_plain_and_oracle(monkeypatch, d, n_ref, n_query):
+    """Queries against a set (the predict search): seeds from the refs' curve windows around each
+    query and, for d <= 4, curve-ordered query groups with tile lists; the same lists."""
+    rng = np.random.default_rng(7 * d + n_query)
+    ref = rng.uniform(-1, 1, (n_ref, d))
+    q = rng.uniform(-1.2, 1.2, (n_query, d))  # some queries outside the refs' box
+    ls = rng.uniform(0.3, 2.0, d) if d % 2 else 0.35
+    plain = query_search(monkeypatch, ref, q, 32, ls, 0)
+    assert np.array_equal(query_search(monkeypatch, ref, q, 32, ls, 128), plain)
+    assert np.array_equal(query_search(monkeypatch, ref, q, 32, ls, 128, prune=False), plain)
+    rows = np.sort(rng.choice(n_query, 150, replace=False))
+    assert np.array_equal(plain[rows], O.knn(ref, q[rows], 32, None, ls))
+
+
+def test_query_search_engages_and_handles_duplicates_and_outliers(monkeypatch, capfd):
+    rng = np.random.default_rng(5)
+    ref = rng.integers(0, 10, (70000, 3)).astype(np.float64)  # many exact ties
+    ref[123] = [5e6, 5e6, 5e6]
+    q = rng.integers(0, 10, (30000, 3)).astype(np.float64)
+    q[77] = [-4e6, 0, 0]
+    monkeypatch.setenv('NNGP_KNN_DEBUG', '1')
+    a = query_search(monkeypatch, ref, q, 16, None, 128)
+    err = capfd.readouterr().err
+    assert 'seeded=1 pruned=1' in err
+    b = query_search(monkeypatch, ref, q, 16, None, 0)
+    assert np.array_equal(a, b)
+    rows = np.sort(np.r_[77, rng.choice(30000, 100, replace=False)])
+    assert np.array_equal(a[rows], O.knn(ref, q[rows], 16, None, None))
