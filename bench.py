@@ -633,7 +633,7 @@ def run_ours(args):
 
     from nngpr_b200 import B200Nngpr, _lib, ops
     from nngpr_b200.kernel_params import extract
-    from nngpr_b200.sharding import fit_step_rows, row_partition
+    from nngpr_b200.sharding import fit_step_rows, row_partition, search_is_pruned
 
     L = _lib.lib()
     _lib.check(L.nngp_check_device(), 'nngp_check_device')
@@ -644,7 +644,7 @@ def run_ours(args):
     x32 = x64.to(torch.float32)
     # the local systems' copies (FP64, or FP32 with FP64 re-solves for the precision workload)
     xl, yl = (x64, y64) if LOCAL == 'f64' else (x32, y64.to(torch.float32))
-    bounds = row_partition(n, world)
+    bounds = row_partition(n, world, equal_rows=search_is_pruned(n, D))
     r0, r1 = bounds[rank], bounds[rank + 1]
     q_rows = x32[r0:r1]
     flags = ops.new_flags(dev)
@@ -848,7 +848,7 @@ def run_ours(args):
             'reused_lists_step': reuse,
             'predict': None if pred_ms is None else {'value': N_PRED / (pred_ms * 1e-3), 'unit': 'points/s',
                                                      'ms': pred_ms, 'n_query': N_PRED},
-            'gpu_launches': args.steps * our_launches_per_step(r1 - r0 if world == 1 else 0, D, M),
+            'gpu_launches': args.steps * our_launches_per_step(n, D, M),  # row shards take the same path
             'gpu_launches_note': 'kernels of libnngp_b200.so per step (see our_launches_per_step); CUB sort and '
                                  'scan kernels the planning launches are not counted',
             'clocks': clocks.summary(),

@@ -647,8 +647,14 @@ nngp_status knn_impl(const T *ref, int64_t n_ref, const T *query, int64_t n_quer
             NNGP_CUDA_TRY(cudaGetLastError());
             NNGP_CUDA_TRY(ensure_smem_limit(reinterpret_cast<const void *>(p.tv.fn), p.tv.smem, 100));
             // the prefix search of a point set over itself (the fit step) starts every row from a
-            // proven bound of its m-th distance: the same lists, far fewer candidates
-            const bool seeded = same && has_cut && cut == 0 && p.seed_ws_bytes > 0 && seed::window() > 0;
+            // proven bound of its m-th distance: the same lists, far fewer candidates.  A row shard
+            // of it (query = rows [cut, cut + n_query) of ref, as a view: the multi-GPU fit step)
+            // takes the same path for its rows.
+            const bool shard = !same && has_cut && cut >= 0 && cut + n_query <= n_ref &&
+                               query == ref + (size_t)cut * (size_t)d;
+            const int64_t row_lo = shard ? cut : 0;  // the searched rows are the points [row_lo, row_lo + n_query)
+            const bool seeded = ((same && has_cut && cut == 0) || shard) && seed::workspace(n_ref, p.dp) > 0 &&
+                                p.seed_ws_bytes >= seed::workspace(n_ref, p.dp) && seed::window() > 0;
             const float *seeds_c = nullptr;
             const int32_t *order0 = nullptr, *pos0 = nullptr;
             const uint64_t *keys0 = nullptr;
@@ -676,7 +682,8 @@ nngp_status knn_impl(const T *ref, int64_t n_ref, const T *query, int64_t n_quer
             const bool qpruned = qseeded && qprune_ws > 0 && p.prune_ws_bytes >= qprune_ws && prune::enabled();
             // and, for large low-dimensional sets, visits per group of rows only the ref tiles its
             // seeds allow (rows and refs in curve order; loose and early rows stay in index order)
-            const bool pruned = seeded && p.prune_ws_bytes > 0 && prune::enabled();
+            const bool pruned = seeded && prune::workspace(n_ref, d, G) > 0 &&
+                                p.prune_ws_bytes >= prune::workspace(n_ref, d, G) && prune::enabled();
             prune::Lists lists;
             unsigned char *tiles_curve = reinterpret_cast<unsigned char *>(base + p.off_tiles2);
             if (qpruned) {
@@ -688,9 +695,9 @@ nngp_status knn_impl(const T *ref, int64_t n_ref, const T *query, int64_t n_quer
                 NNGP_CUDA_TRY(cudaGetLastError());
             }
             if (pruned) {
-                nngp_status pst = prune::build(refs, n_ref, d, p.dp, p.tv.rows_per_item, seed::bits(d), seeds_c,
-                                               order0, pos0, keys0, base + p.off_prune_ws, p.prune_ws_bytes, &lists,
-                                               stream);
+                nngp_status pst = prune::build(refs, n_ref, row_lo, row_lo + n_query, d, p.dp, p.tv.rows_per_item,
+                                               seed::bits(d), seeds_c, order0, pos0, keys0, base + p.off_prune_ws,
+                                               p.prune_ws_bytes, &lists, stream);
                 if (pst != NNGP_OK) return pst;
                 p.tv.build<<<grid_for(p.n_ref_pad), 256, 0, stream>>>(refs, n_ref, p.n_ref_pad, acc, lists.ref_order,
                                                                       tiles_curve, r2);
@@ -720,10 +727,13 @@ nngp_status knn_impl(const T *ref, int64_t n_ref, const T *query, int64_t n_quer
             const unsigned int *r2_c = r2;
             const int32_t *none = nullptr;
             const int64_t *no_sizes = nullptr;
+            // cut_arg / out_base: rows of point indices use cut 0 (limit = the point's index) and
+            // write the row of point i at out[(i - out_base) * m]
             auto launch = [&](const unsigned char *tiles_c, int64_t items_bound, const int32_t *rows_perm,
                               const int32_t *row_off, const int64_t *dev_sizes, const tc::TcItems &items,
                               const int32_t *ref_perm, const int32_t *tile_off, const int32_t *tile_list,
-                              int *counter) -> nngp_status {
+                              int *counter, const float *seeds_arg, int64_t cut_arg, int64_t out_base,
+                              const float *q_arg) -> nngp_status {
                 if (items_bound == 0) return NNGP_OK;
                 const int grid = (int)std::min<int64_t>(items_bound, (int64_t)num_sms_knn() * per_sm);
                 if (const char *dbg = std::getenv("NNGP_KNN_DEBUG"); dbg && dbg[0] == '1')
@@ -732,11 +742,12 @@ nngp_status knn_impl(const T *ref, int64_t n_ref, const T *query, int64_t n_quer
                                  "pruned=%d\n",
                                  d, m, (long long)items_bound, per_sm, grid, p.tv.smem, (int)(seeded || qseeded),
                                  (int)(tile_list != nullptr));
-                void *args[] = {(void *)&tiles_c,  (void *)&q_c,      (void *)&acc_c,      (void *)&r2_c,
-                                (void *)&seeds_c,  (void *)&rows_perm, (void *)&row_off,   (void *)&dev_sizes,
+                void *args[] = {(void *)&tiles_c,  (void *)&q_arg,     (void *)&acc_c,      (void *)&r2_c,
+                                (void *)&seeds_arg, (void *)&rows_perm, (void *)&row_off,  (void *)&dev_sizes,
                                 (void *)&items,    (void *)&ref_perm, (void *)&tile_off, (void *)&tile_list,
                                 (void *)&counter,  (void *)&n_query,  (void *)&n_ref,      (void *)&has_cut,
-                                (void *)&cut,      (void *)&m,        (void *)&out,        (void *)&flags};
+                                (void *)&cut_arg,  (void *)&m,        (void *)&out_base,   (void *)&out,
+                                (void *)&flags};
                 NNGP_CUDA_TRY(cudaLaunchKernel(reinterpret_cast<const void *>(p.tv.fn), dim3(grid), dim3(p.tv.threads),
                                                args, (size_t)p.tv.smem, stream));
                 return NNGP_OK;
@@ -745,23 +756,28 @@ nngp_status knn_impl(const T *ref, int64_t n_ref, const T *query, int64_t n_quer
             if (pruned) {
                 const int64_t *ps = reinterpret_cast<const int64_t *>(lists.pruned);
                 const int64_t *is = reinterpret_cast<const int64_t *>(lists.index_order);
+                // rows are point indices (the refs' scaled copy holds them), cut 0, shard offset
+                const float *pts = refs;
                 lst = launch(tiles_curve, lists.max_items[0], lists.rows, lists.row_off, ps, lists.pruned_items,
-                             lists.ref_order, lists.offsets, lists.tiles, ctr + 1);
+                             lists.ref_order, lists.offsets, lists.tiles, ctr + 1, seeds_c, 0, row_lo, pts);
                 if (lst != NNGP_OK) return lst;
-                if ((lst = prune::merge(lists, 0, p.tv.rows_per_item, m, out, stream)) != NNGP_OK) return lst;
-                lst = launch(tiles, lists.max_items[1], lists.rows, none, is, lists.index_items, none, none, none, ctr);
+                if ((lst = prune::merge(lists, 0, p.tv.rows_per_item, m, row_lo, out, stream)) != NNGP_OK) return lst;
+                lst = launch(tiles, lists.max_items[1], lists.rows, none, is, lists.index_items, none, none, none, ctr,
+                             seeds_c, 0, row_lo, pts);
                 if (lst != NNGP_OK) return lst;
-                lst = prune::merge(lists, 1, p.tv.rows_per_item, m, out, stream);
+                lst = prune::merge(lists, 1, p.tv.rows_per_item, m, row_lo, out, stream);
             } else if (qpruned) {
                 const int64_t *ps = reinterpret_cast<const int64_t *>(lists.pruned);
                 lst = launch(tiles_curve, lists.max_items[0], lists.rows, lists.row_off, ps, lists.pruned_items,
-                             lists.ref_order, lists.offsets, lists.tiles, ctr + 1);
+                             lists.ref_order, lists.offsets, lists.tiles, ctr + 1, seeds_c, cut, 0, q_c);
                 if (lst != NNGP_OK) return lst;
-                lst = prune::merge(lists, 0, G, m, out, stream);
+                lst = prune::merge(lists, 0, G, m, 0, out, stream);
             } else {
+                // rows are query rows (limit = row + cut); a seeded shard's seeds are indexed by point
                 const int64_t items = (n_query + p.tv.rows_per_item - 1) / p.tv.rows_per_item;
                 const tc::TcItems whole{};
-                lst = launch(tiles, items, none, none, no_sizes, whole, none, none, none, ctr);
+                const float *seeds_rows = seeds_c ? seeds_c + row_lo : nullptr;
+                lst = launch(tiles, items, none, none, no_sizes, whole, none, none, none, ctr, seeds_rows, cut, 0, q_c);
             }
             if (lst != NNGP_OK) return lst;
         }

@@ -42,6 +42,7 @@ constexpr int kEarlyShift = 3;       // rows below n / 8 take the index-order se
 constexpr int kBands = kEarlyShift + 1;  // band b: rows [n / 2^(b + 1), n / 2^b) (the last only at rounding edges)
 constexpr int kLooseLog2Q = 4 * 256;  // seed > 16 x band geometric mean (log2 in 1/256 units)
 constexpr uint64_t kIndexOrderTag = 1ull << 36;  // above (band << 32 | curve position) for bands < 16
+constexpr uint64_t kOutsideTag = 1ull << 37;     // rows outside the searched range: sorted last, not searched
 
 __device__ __forceinline__ int band_of(int64_t i, int64_t n) {
     int b = 0;
@@ -137,16 +138,25 @@ __global__ void __launch_bounds__(kThreads) band_stats_kernel(int64_t n, int64_t
     }
 }
 
-// Sort keys: pruned rows (band << 32 | curve position), the others (2^36 | index); counts
-// of pruned rows per band and in total.
-__global__ void __launch_bounds__(kThreads) classify_kernel(int64_t n, int64_t early, const float *__restrict__ seeds,
+// Sort keys of the rows [row_lo, row_hi): pruned rows (band << 32 | curve position), the others
+// (2^36 | index); rows outside the range (2^37 | index).  Counts of pruned rows per band and of
+// the index-order rows.
+__global__ void __launch_bounds__(kThreads) classify_kernel(int64_t n, int64_t early, int64_t row_lo, int64_t row_hi,
+                                                            const float *__restrict__ seeds,
                                                             const int32_t *__restrict__ pos0,
                                                             const unsigned long long *__restrict__ sum,
                                                             const unsigned long long *__restrict__ cnt,
                                                             uint64_t *__restrict__ keys, int32_t *__restrict__ vals,
-                                                            unsigned long long *__restrict__ pruned_cnt) {
+                                                            unsigned long long *__restrict__ pruned_cnt,
+                                                            unsigned long long *__restrict__ index_cnt) {
     unsigned long long c[kBands] = {};
+    unsigned long long ci = 0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        vals[i] = (int32_t)i;
+        if (i < row_lo || i >= row_hi) {
+            keys[i] = kOutsideTag | (uint64_t)i;
+            continue;
+        }
         bool pruned = false;
         int b = 0;
         if (i >= early) {
@@ -158,8 +168,8 @@ __global__ void __launch_bounds__(kThreads) classify_kernel(int64_t n, int64_t e
             }
         }
         keys[i] = pruned ? ((uint64_t)b << 32 | (uint32_t)pos0[i]) : (kIndexOrderTag | (uint64_t)i);
-        vals[i] = (int32_t)i;
         if (pruned) c[b] += 1;
+        else ci += 1;
     }
 #pragma unroll
     for (int b = 0; b < kBands; ++b) {
@@ -167,6 +177,8 @@ __global__ void __launch_bounds__(kThreads) classify_kernel(int64_t n, int64_t e
         for (int o = 16; o > 0; o >>= 1) cv += __shfl_xor_sync(0xFFFFFFFFu, cv, o);
         if ((threadIdx.x & 31) == 0 && cv > 0) atomicAdd(pruned_cnt + b, cv);
     }
+    for (int o = 16; o > 0; o >>= 1) ci += __shfl_xor_sync(0xFFFFFFFFu, ci, o);
+    if ((threadIdx.x & 31) == 0 && ci > 0) atomicAdd(index_cnt, ci);
 }
 
 // Octree cell level of band b: cells of 2^(d L) per level hold about 256 of the band's pruned
@@ -225,7 +237,8 @@ __global__ void __launch_bounds__(kThreads) row_off_kernel(int64_t n, const int3
 }
 
 __global__ void sizes_kernel(int64_t n, int G, const int32_t *__restrict__ gh, const int32_t *__restrict__ gid,
-                             const unsigned long long *__restrict__ pruned_cnt, int32_t *__restrict__ row_off,
+                             const unsigned long long *__restrict__ pruned_cnt,
+                             const unsigned long long *__restrict__ index_cnt, int32_t *__restrict__ row_off,
                              DevSizes *__restrict__ pruned, DevSizes *__restrict__ index_order) {
     unsigned long long total = 0;
     for (int b = 0; b < kBands; ++b) total += pruned_cnt[b];
@@ -236,8 +249,8 @@ __global__ void sizes_kernel(int64_t n, int G, const int32_t *__restrict__ gh, c
     pruned->n_items = n_groups;
     pruned->n_groups = n_groups;
     index_order->first_row = (int64_t)total;
-    index_order->n_rows = n - (int64_t)total;
-    index_order->n_groups = (n - (int64_t)total + G - 1) / G;
+    index_order->n_rows = (int64_t)*index_cnt;
+    index_order->n_groups = ((int64_t)*index_cnt + G - 1) / G;
     index_order->n_items = index_order->n_groups;
 }
 
@@ -437,7 +450,7 @@ __global__ void __launch_bounds__(kThreads) merge_kernel(const DevSizes *__restr
                                                          const int32_t *__restrict__ row_off,
                                                          const int32_t *__restrict__ rows,
                                                          const unsigned long long *__restrict__ partial, int m,
-                                                         int32_t *__restrict__ out) {
+                                                         int64_t out_base, int32_t *__restrict__ out) {
     const unsigned FULL = 0xFFFFFFFFu;
     const int lane = threadIdx.x & 31;
     const int64_t ng = sz->n_groups;
@@ -465,7 +478,7 @@ __global__ void __launch_bounds__(kThreads) merge_kernel(const DevSizes *__restr
                 cur = ((lane & j) == 0) ? (o < cur ? o : cur) : (o > cur ? o : cur);
             }
         }
-        if (lane < m) out[(int64_t)rows[r0 + r] * m + lane] = (int32_t)(uint32_t)cur;
+        if (lane < m) out[((int64_t)rows[r0 + r] - out_base) * m + lane] = (int32_t)(uint32_t)cur;
     }
 }
 
@@ -504,7 +517,7 @@ Layout layout(int64_t n, int d, int G) {
     L.tlo = take((size_t)L.n_tiles * d * 4);
     L.thi = take((size_t)L.n_tiles * d * 4);
     L.tmin = take((size_t)L.n_tiles * 4);
-    L.stats = take(3 * kBands * 8);
+    L.stats = take((3 * kBands + 1) * 8);
     L.keys_a = take((size_t)n * 8);
     L.keys_b = take((size_t)n * 8);
     L.vals_a = take((size_t)n * 4);
@@ -661,9 +674,9 @@ size_t workspace(int64_t n, int d, int rows_per_group) {
     return layout(n, d, rows_per_group).total;
 }
 
-nngp_status build(const float *xs, int64_t n, int d, int dp, int G, int bits, const float *seeds,
-                  const int32_t *order0, const int32_t *pos0, const uint64_t *keys0, void *ws, size_t ws_bytes,
-                  Lists *out, cudaStream_t stream) {
+nngp_status build(const float *xs, int64_t n, int64_t row_lo, int64_t row_hi, int d, int dp, int G, int bits,
+                  const float *seeds, const int32_t *order0, const int32_t *pos0, const uint64_t *keys0, void *ws,
+                  size_t ws_bytes, Lists *out, cudaStream_t stream) {
     if (n < kMinPoints || n > kMaxPoints || d < 1 || d > kMaxDim || G < 1 || bits < 1 || d * bits > 60 || !xs ||
         !seeds || !order0 || !pos0 || !keys0 || !out)
         return fail(NNGP_ERR_UNSUPPORTED, "knn pruning: shape outside the pruned search");
@@ -674,7 +687,9 @@ nngp_status build(const float *xs, int64_t n, int d, int dp, int G, int bits, co
     float *tlo = static_cast<float *>(at(L.tlo)), *thi = static_cast<float *>(at(L.thi));
     int32_t *tmin = static_cast<int32_t *>(at(L.tmin));
     unsigned long long *sum = static_cast<unsigned long long *>(at(L.stats)), *cnt = sum + kBands,
-                       *pcnt = sum + 2 * kBands;
+                       *pcnt = sum + 2 * kBands, *icnt = sum + 3 * kBands;
+    if (row_lo < 0 || row_hi > n || row_lo > row_hi)
+        return fail(NNGP_ERR_INVALID_ARGUMENT, "knn pruning: row range outside [0, n)");
     int32_t *headpos = static_cast<int32_t *>(at(L.headpos)), *seg_start = static_cast<int32_t *>(at(L.seg_start));
     int32_t *gh = static_cast<int32_t *>(at(L.gh)), *gid = static_cast<int32_t *>(at(L.gid));
     int32_t *row_off = static_cast<int32_t *>(at(L.row_off));
@@ -706,23 +721,23 @@ nngp_status build(const float *xs, int64_t n, int d, int dp, int G, int bits, co
     tile_box_kernel<<<grid_of(L.n_tiles * 32), kThreads, 0, stream>>>(xs, n, d, dp, ref_order, L.n_tiles, tlo, thi,
                                                                        tmin);
     NNGP_CUDA_TRY(cudaGetLastError());
-    NNGP_CUDA_TRY(cudaMemsetAsync(sum, 0, 3 * kBands * 8, stream));
+    NNGP_CUDA_TRY(cudaMemsetAsync(sum, 0, (3 * kBands + 1) * 8, stream));
     band_stats_kernel<<<grid_of(n - early), kThreads, 0, stream>>>(n, early, seeds, sum, cnt);
     NNGP_CUDA_TRY(cudaGetLastError());
-    classify_kernel<<<grid_of(n), kThreads, 0, stream>>>(n, early, seeds, pos0, sum, cnt,
+    classify_kernel<<<grid_of(n), kThreads, 0, stream>>>(n, early, row_lo, row_hi, seeds, pos0, sum, cnt,
                                                          static_cast<uint64_t *>(at(L.keys_a)),
-                                                         static_cast<int32_t *>(at(L.vals_a)), pcnt);
+                                                         static_cast<int32_t *>(at(L.vals_a)), pcnt, icnt);
     NNGP_CUDA_TRY(cudaGetLastError());
 
     // rows: pruned (band, curve position) first, then the index-order rows ascending
     cub::DoubleBuffer<uint64_t> dk(static_cast<uint64_t *>(at(L.keys_a)), static_cast<uint64_t *>(at(L.keys_b)));
     cub::DoubleBuffer<int32_t> dv(static_cast<int32_t *>(at(L.vals_a)), static_cast<int32_t *>(at(L.vals_b)));
     size_t need = 0;
-    NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, need, dk, dv, (int)n, 0, 37, stream));
+    NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, need, dk, dv, (int)n, 0, 38, stream));
     nngp_status st = cub_check(need);
     if (st != NNGP_OK) return st;
     size_t have = L.cub_bytes;
-    NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(at(L.cub), have, dk, dv, (int)n, 0, 37, stream));
+    NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(at(L.cub), have, dk, dv, (int)n, 0, 38, stream));
     const int32_t *rows = dv.Current();
 
     // groups: segments of one band and one octree cell, cut every G rows
@@ -742,7 +757,7 @@ nngp_status build(const float *xs, int64_t n, int d, int dp, int G, int bits, co
     NNGP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(at(L.cub), have, gh, gid, (int)n, stream));
     row_off_kernel<<<grid_of(n), kThreads, 0, stream>>>(n, gh, gid, row_off);
     NNGP_CUDA_TRY(cudaGetLastError());
-    sizes_kernel<<<1, 1, 0, stream>>>(n, G, gh, gid, pcnt, row_off, sizes, sizes + 1);
+    sizes_kernel<<<1, 1, 0, stream>>>(n, G, gh, gid, pcnt, icnt, row_off, sizes, sizes + 1);
     NNGP_CUDA_TRY(cudaGetLastError());
 
     // tile lists, then the work order (longest list first)
@@ -837,7 +852,7 @@ nngp_status build_query(const float *xs_ref, int64_t n_ref, const float *xq, int
     return NNGP_OK;
 }
 
-nngp_status merge(const Lists &lists, int which, int G, int m, int32_t *out, cudaStream_t stream) {
+nngp_status merge(const Lists &lists, int which, int G, int m, int64_t out_base, int32_t *out, cudaStream_t stream) {
     if (which < 0 || which > 1 || !lists.split_k[which]) return fail(NNGP_ERR_INVALID_ARGUMENT, "knn merge: no plan");
     const DevSizes *sz = which == 0 ? lists.pruned : lists.index_order;
     const tc::TcItems &ti = which == 0 ? lists.pruned_items : lists.index_items;
@@ -845,7 +860,7 @@ nngp_status merge(const Lists &lists, int which, int G, int m, int32_t *out, cud
     merge_kernel<<<grid_of(maxg * G * 32), kThreads, 0, stream>>>(sz, maxg, G, lists.split_k[which],
                                                                   lists.slot_base[which],
                                                                   which == 0 ? lists.row_off : nullptr, lists.rows,
-                                                                  ti.partial, m, out);
+                                                                  ti.partial, m, out_base, out);
     NNGP_CUDA_TRY(cudaGetLastError());
     return NNGP_OK;
 }

@@ -71,9 +71,11 @@ size_t workspace(int64_t n, int d, int rows_per_group);
 // shrunk by the FP32 rounding bound, exceeds the largest seed of the group; tiles whose box meets
 // the group's come first.  Neither rule excludes a neighbour of any row, so the search returns
 // the same lists.  No host synchronisation: sizes stay on the device.
-nngp_status build(const float *xs, int64_t n, int d, int dp, int rows_per_group, int bits_per_dim,
-                  const float *seeds, const int32_t *order0, const int32_t *pos0, const uint64_t *keys0, void *ws,
-                  size_t ws_bytes, Lists *out, cudaStream_t stream);
+// Only the rows [row_lo, row_hi) are planned (a row shard of the multi-GPU fit step; [0, n) for
+// the whole search); the refs are all n points.
+nngp_status build(const float *xs, int64_t n, int64_t row_lo, int64_t row_hi, int d, int dp, int rows_per_group,
+                  int bits_per_dim, const float *seeds, const int32_t *order0, const int32_t *pos0,
+                  const uint64_t *keys0, void *ws, size_t ws_bytes, Lists *out, cudaStream_t stream);
 
 // The same for a search of n_query queries against n_ref refs without a prefix rule (predict):
 // the queries in curve-0 order (qorder, from knn_seed's query_seeds) cut into groups of
@@ -85,8 +87,10 @@ nngp_status build_query(const float *xs_ref, int64_t n_ref, const float *xq, int
                         size_t ws_bytes, Lists *out, cudaStream_t stream);
 
 // Combines the partial lists of the split groups of launch `which` (0 pruned, 1 index order)
-// into out (num_nn m).  Runs after that launch on the same stream.
-nngp_status merge(const Lists &lists, int which, int rows_per_group, int m, int32_t *out, cudaStream_t stream);
+// into out (num_nn m; row of point i at out[(i - out_base) * m]).  Runs after that launch on the
+// same stream.
+nngp_status merge(const Lists &lists, int which, int rows_per_group, int m, int64_t out_base, int32_t *out,
+                  cudaStream_t stream);
 
 }  // namespace prune
 }  // namespace nngp

@@ -283,7 +283,8 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
                                                          const int32_t *__restrict__ tile_list,
                                                          int *__restrict__ work_counter, int64_t n_query,
                                                          int64_t n_ref, int has_cut, int64_t cut, int m,
-                                                         int32_t *__restrict__ out, int32_t *__restrict__ flags) {
+                                                         int64_t out_base, int32_t *__restrict__ out,
+                                                         int32_t *__restrict__ flags) {
     using C = Cfg<D, QTILES>;
     constexpr int S = C::STAGES;
     constexpr int EPI_WARPS = C::EPI_WARPS;
@@ -664,7 +665,7 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
                     if (out_slot >= 0) {
                         items.partial[((int64_t)out_slot * C::ROWS + rq) * 32 + lane] = x;
                     } else if (rq < n_item_rows && lane < m) {
-                        out[point_of(q0 + rq) * m + lane] = (int32_t)(uint32_t)x;
+                        out[(point_of(q0 + rq) - out_base) * m + lane] = (int32_t)(uint32_t)x;  // out_base: shard's first row
                     }
                 }
             }

@@ -8,7 +8,11 @@ the reference's own batching rule, ``base_nngpr.py:530-535``), solves their loca
 gives every rank the full value and gradient.  X and y are replicated.
 
 Rows are split so that the prefix-search pair counts (row i scans i refs) are equal:
-rank r owns ``[n sqrt(r / R), n sqrt((r + 1) / R))``.
+rank r owns ``[n sqrt(r / R), n sqrt((r + 1) / R))`` (``row_partition``), the right split when
+the search cost grows with the prefix.  When the library prunes the search (FP32, d <= 4,
+65,536 <= n <= 2,000,000, see ``search_is_pruned``) a row costs about the same wherever it is
+(its tile list covers its neighbourhood, not its prefix), and so do the local systems: equal row
+counts balance the ranks (``row_partition(..., equal_rows=True)``).
 """
 
 from __future__ import annotations
@@ -16,10 +20,18 @@ from __future__ import annotations
 import math
 
 
-def row_partition(n: int, world: int) -> list[int]:
-    """Boundaries ``b[0] = 0 <= b[1] <= ... <= b[world] = n`` with equal pair counts."""
+def search_is_pruned(n: int, d: int, float32: bool = True) -> bool:
+    """Whether the library's fit-step search of n points in d dimensions is pruned."""
+    return float32 and d <= 4 and 65536 <= n <= 2_000_000
+
+
+def row_partition(n: int, world: int, equal_rows: bool = False) -> list[int]:
+    """Boundaries ``b[0] = 0 <= b[1] <= ... <= b[world] = n`` with equal pair counts (or, with
+    ``equal_rows``, equal row counts)."""
     if world < 1:
         raise ValueError('world must be >= 1')
+    if equal_rows:
+        return [n * r // world for r in range(world + 1)]
     b = [int(round(n * math.sqrt(r / world))) for r in range(world + 1)]
     b[0], b[-1] = 0, n
     for r in range(1, world + 1):

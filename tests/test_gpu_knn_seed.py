@@ -175,3 +175,26 @@ def test_query_search_engages_and_handles_duplicates_and_outliers(monkeypatch, c
     assert np.array_equal(a, b)
     rows = np.sort(np.r_[77, rng.choice(30000, 100, replace=False)])
     assert np.array_equal(a[rows], O.knn(ref, q[rows], 16, None, None))
+
+
+@pytest.mark.parametrize('d', [3, 8])
+def test_row_shards_of_the_prefix_search(monkeypatch, capfd, d):
+    """The multi-GPU fit step searches row shards: query = rows [r0, r1) of the set as a view,
+    ref_cut_index = r0.  Shards are seeded (and pruned for d <= 4) over their own rows and
+    equal the corresponding rows of the whole search."""
+    rng = np.random.default_rng(40 + d)
+    n = 100000
+    x = rng.uniform(-1, 1, (n, d))
+    ls = 0.3
+    monkeypatch.setenv('NNGP_KNN_SEED_W', '128')
+    monkeypatch.setenv('NNGP_KNN_PRUNE', '1')
+    t = torch.from_numpy(x.astype(np.float32)).cuda()
+    full = ops.knn(t, t, 32, 0, ls).cpu().numpy()
+    monkeypatch.setenv('NNGP_KNN_DEBUG', '1')
+    for r0, r1 in [(0, 30000), (30000, 71000), (71000, n)]:
+        got = ops.knn(t, t[r0:r1], 32, r0, ls).cpu().numpy()
+        err = capfd.readouterr().err
+        assert 'seeded=1' in err and (('pruned=1' in err) == (d <= 4))
+        assert np.array_equal(got, full[r0:r1])
+    monkeypatch.setenv('NNGP_KNN_SEED_W', '0')
+    np.testing.assert_array_equal(ops.knn(t, t[50000:60000], 32, 50000, ls).cpu().numpy(), full[50000:60000])

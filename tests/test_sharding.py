@@ -17,6 +17,15 @@ import torch.multiprocessing as mp
 from nngpr_b200.sharding import prefix_pairs, row_partition
 
 
+def test_row_partition_equal_rows_for_the_pruned_search():
+    from nngpr_b200.sharding import search_is_pruned
+    assert search_is_pruned(434874, 3) and not search_is_pruned(434874, 8) and not search_is_pruned(30000, 3)
+    for n, world in [(434874, 8), (10, 3), (1, 4)]:
+        b = row_partition(n, world, equal_rows=True)
+        assert b[0] == 0 and b[-1] == n and all(b[i] <= b[i + 1] for i in range(world))
+        assert max(b[i + 1] - b[i] for i in range(world)) - min(b[i + 1] - b[i] for i in range(world)) <= 1
+
+
 def test_row_partition_balances_prefix_pairs():
     for n, world in [(434874, 2), (434874, 8), (1000, 3), (7, 4), (1, 2)]:
         b = row_partition(n, world)
