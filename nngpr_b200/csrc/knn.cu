@@ -661,7 +661,8 @@ nngp_status knn_impl(const T *ref, int64_t n_ref, const T *query, int64_t n_quer
             if (seeded) {
                 float *sd = reinterpret_cast<float *>(base + p.off_seed);
                 nngp_status sst = seed::prefix_seeds(refs, n_ref, d, round_d(d), p.dp, m, base + p.off_seed_ws,
-                                                     p.seed_ws_bytes, sd, stream, &order0, &pos0, &keys0);
+                                                     p.seed_ws_bytes, sd, stream, &order0, &pos0, &keys0, row_lo,
+                                                     row_lo + n_query);
                 if (sst != NNGP_OK) return sst;
                 seeds_c = sd;
             }

@@ -107,14 +107,16 @@ __global__ void __launch_bounds__(kThreads) ref_keys_kernel(int64_t n, const int
     }
 }
 
-// Per band: sum of log2q(seed) over the finite seeds of rows >= early, and their count
-// (integer sums: the result does not depend on the order of the atomics).
-__global__ void __launch_bounds__(kThreads) band_stats_kernel(int64_t n, int64_t early, const float *__restrict__ seeds,
+// Per band: sum of log2q(seed) over the finite seeds of the rows [early, row_hi) (early already
+// raised to the shard's first row), and their count (integer sums: the result does not depend on
+// the order of the atomics).
+__global__ void __launch_bounds__(kThreads) band_stats_kernel(int64_t n, int64_t early, int64_t row_hi,
+                                                              const float *__restrict__ seeds,
                                                               unsigned long long *__restrict__ sum,
                                                               unsigned long long *__restrict__ cnt) {
     long long s[kBands] = {};
     unsigned long long c[kBands] = {};
-    for (int64_t i = early + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+    for (int64_t i = early + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < row_hi;
          i += (int64_t)gridDim.x * blockDim.x) {
         const float tau = seeds[i];
         if (!isinf(tau)) {
@@ -722,7 +724,8 @@ nngp_status build(const float *xs, int64_t n, int64_t row_lo, int64_t row_hi, in
                                                                        tmin);
     NNGP_CUDA_TRY(cudaGetLastError());
     NNGP_CUDA_TRY(cudaMemsetAsync(sum, 0, (3 * kBands + 1) * 8, stream));
-    band_stats_kernel<<<grid_of(n - early), kThreads, 0, stream>>>(n, early, seeds, sum, cnt);
+    band_stats_kernel<<<grid_of(n - early), kThreads, 0, stream>>>(n, std::max(early, row_lo), row_hi, seeds, sum,
+                                                                   cnt);
     NNGP_CUDA_TRY(cudaGetLastError());
     classify_kernel<<<grid_of(n), kThreads, 0, stream>>>(n, early, row_lo, row_hi, seeds, pos0, sum, cnt,
                                                          static_cast<uint64_t *>(at(L.keys_a)),

@@ -23,6 +23,7 @@
 #include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
+#include <climits>
 #include <cstdlib>
 #include <string>
 
@@ -189,13 +190,14 @@ __global__ void __launch_bounds__(kThreads) seed_kernel(const float *__restrict_
                                                         const int32_t *__restrict__ order1,
                                                         const int32_t *__restrict__ p0_of1,
                                                         const int32_t *__restrict__ pos1, int combine,
-                                                        float *__restrict__ seeds) {
+                                                        int64_t row_lo, int64_t row_hi, float *__restrict__ seeds) {
     constexpr int W = VPL * 16;
     constexpr unsigned FULL = 0xFFFFFFFFu;
     const int lane = threadIdx.x & 31;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t k = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; k < n; k += nwarps) {
         const int64_t i = order0[k];
+        if (i < row_lo || i >= row_hi) continue;  // another rank's rows (left unset)
         if (i < m) {  // fewer than m earlier points: no bound
             if (lane == 0 && !combine) seeds[i] = __uint_as_float(kInfBits);
             continue;
@@ -329,13 +331,14 @@ struct SeedArgs {
     int dp, m;
     const int32_t *o0, *o1, *p0of1, *p1;
     int combine;
+    int64_t row_lo, row_hi;
     float *seeds;
 };
 
 template <int D, int VPL>
 void launch_seed(int grid, const SeedArgs &a, cudaStream_t stream) {
     seed_kernel<D, VPL><<<grid, kThreads, 0, stream>>>(a.xs0, a.xs1, a.n, a.dp, a.m, a.o0, a.o1, a.p0of1, a.p1,
-                                                       a.combine, a.seeds);
+                                                       a.combine, a.row_lo, a.row_hi, a.seeds);
 }
 
 template <int VPL>
@@ -366,9 +369,11 @@ int grid_of(int64_t work) {
 // (combine: keep the smaller of the old and the new bound).
 // seeds == nullptr: only the curves (orders, inverse, sorted keys of both curves, coordinates in
 // curve order), for the query seeds.
+// Only the rows [row_lo, row_hi) get seeds (the others are left as they were).
 nngp_status run_level(const float *xs, int64_t n, int d, int D, int dp, int m, int W, char *base, const Layout &L,
                       int combine, float *seeds, cudaStream_t stream, const int32_t **order0_out,
-                      const int32_t **pos0_out, const uint64_t **keys0_out) {
+                      const int32_t **pos0_out, const uint64_t **keys0_out, int64_t row_lo = 0,
+                      int64_t row_hi = INT64_MAX) {
     auto at = [&](size_t off) { return reinterpret_cast<void *>(base + off); };
     uint64_t *keys_a = static_cast<uint64_t *>(at(L.keys_a)), *keys_b = static_cast<uint64_t *>(at(L.keys_b));
     int32_t *idx[2][2] = {{static_cast<int32_t *>(at(L.idx0_a)), static_cast<int32_t *>(at(L.idx0_b))},
@@ -414,7 +419,7 @@ nngp_status run_level(const float *xs, int64_t n, int d, int D, int dp, int m, i
     if (!seeds) return NNGP_OK;
     const int grid = (int)std::min<int64_t>((n + kThreads / 32 - 1) / (kThreads / 32), (int64_t)kNumSMsB200 * 16);
     const SeedArgs sa{static_cast<const float *>(at(L.xs0)), static_cast<const float *>(at(L.xs1)), n, dp, m,
-                      order[0], order[1], p0of1, pos[1], combine, seeds};
+                      order[0], order[1], p0of1, pos[1], combine, row_lo, row_hi, seeds};
     const bool ok = W == 128 ? dispatch_seed<8>(D, grid, sa, stream) : dispatch_seed<16>(D, grid, sa, stream);
     if (!ok) return fail(NNGP_ERR_UNSUPPORTED, "knn seeds: no kernel for D = " + std::to_string(D));
     NNGP_CUDA_TRY(cudaGetLastError());
@@ -530,20 +535,23 @@ int window() {
 
 nngp_status prefix_seeds(const float *xs, int64_t n, int d, int D, int dp, int m, void *ws, size_t ws_bytes,
                          float *seeds, cudaStream_t stream, const int32_t **order0_out, const int32_t **pos0_out,
-                         const uint64_t **keys0_out) {
+                         const uint64_t **keys0_out, int64_t row_lo, int64_t row_hi) {
     const int W = window();
+    if (row_hi < 0 || row_hi > n) row_hi = n;
     if (W == 0 || n < kMinPoints || m < 1 || d < 1 || d > 24 || D < d || dp % 4 != 0 || dp < D)
         return fail(NNGP_ERR_UNSUPPORTED, "knn seeds: shape outside the seeded search");
     const Layout L = layout(n, dp);
     if (!ws || ws_bytes < workspace(n, dp)) return fail(NNGP_ERR_WORKSPACE, "knn seeds: workspace too small");
     char *base = reinterpret_cast<char *>(align_up(reinterpret_cast<uintptr_t>(ws), 256));
-    nngp_status st = run_level(xs, n, d, D, dp, m, W, base, L, 0, seeds, stream, order0_out, pos0_out, keys0_out);
+    nngp_status st = run_level(xs, n, d, D, dp, m, W, base, L, 0, seeds, stream, order0_out, pos0_out, keys0_out,
+                               row_lo, row_hi);
     if (st != NNGP_OK) return st;
     // rows i < n / 8 see few earlier points in the full windows: bound them again from the
     // curves of the prefix alone (any m earlier points bound a row; the smaller bound is kept)
     char *sub = base + align_up(L.total, 256);
-    for (int64_t p = n / 8; p >= kMinPoints; p /= 8) {
-        st = run_level(xs, p, d, D, dp, m, W, sub, layout(p, dp), 1, seeds, stream, nullptr, nullptr, nullptr);
+    for (int64_t p = n / 8; p >= kMinPoints && p > row_lo; p /= 8) {
+        st = run_level(xs, p, d, D, dp, m, W, sub, layout(p, dp), 1, seeds, stream, nullptr, nullptr, nullptr, row_lo,
+                       row_hi);
         if (st != NNGP_OK) return st;
     }
     return NNGP_OK;

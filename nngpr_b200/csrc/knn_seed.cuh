@@ -26,9 +26,11 @@ int window();
 // order0 / pos0 / keys0 (optional): the curve-0 order of the points (a permutation of 0..n-1),
 // its inverse and the curve-0 Morton keys in that order (key of point i = keys0[pos0[i]];
 // bits() bits per dimension, interleaved), left in ws for the caller.
+// row_lo / row_hi: only the rows [row_lo, row_hi) get seeds (a row shard; -1: up to n).
 nngp_status prefix_seeds(const float *xs, int64_t n, int d, int D, int dp, int m, void *ws, size_t ws_bytes,
                          float *seeds, cudaStream_t stream, const int32_t **order0 = nullptr,
-                         const int32_t **pos0 = nullptr, const uint64_t **keys0 = nullptr);
+                         const int32_t **pos0 = nullptr, const uint64_t **keys0 = nullptr, int64_t row_lo = 0,
+                         int64_t row_hi = -1);
 
 // Seeds of a search of n_query queries against n_ref refs (no prefix rule): seeds[q] >= the m-th
 // smallest squared distance from query q to the refs, in the search's FP32 arithmetic, from the
