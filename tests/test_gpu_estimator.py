@@ -125,3 +125,17 @@ def test_pickle_round_trip():
     np.testing.assert_array_equal(mean, m2)
     np.testing.assert_array_equal(std, s2)
     assert back.log_marginal_likelihood(back.kernel_.theta) == gpr.log_marginal_likelihood(gpr.kernel_.theta)
+
+
+@pytest.mark.parametrize('mode', ['only-nn', 'yes', 'no'])
+def test_keep_resident_false_uploads_each_call_with_identical_results(mode):
+    """keep_resident=False uploads X and y on every call (the reference's behaviour): the
+    results equal the resident path's bit for bit, call after call."""
+    g = load('cpu_n2000_d3_m16')
+    kw = dict(kernel=KERNELS['cpu_n2000_d3_m16'](), num_nn=16, optimizer=None, allow_downcast_f32=mode)
+    a = B200Nngpr(**kw).fit(g['x'], g['y'])
+    b = B200Nngpr(keep_resident=False, **kw).fit(g['x'], g['y'])
+    for theta in (g['theta'], g['theta'] + 0.1, g['theta']):
+        la, ga = a.log_marginal_likelihood(theta, eval_gradient=True)
+        lb, gb = b.log_marginal_likelihood(theta, eval_gradient=True)
+        assert la == lb and np.array_equal(ga, gb)
