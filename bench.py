@@ -443,7 +443,8 @@ def our_launches_per_step(n, d, m):
     while seeded and p_ >= 8192:
         levels += 1
         p_ //= 8
-    pruned = seeded and 65536 <= n <= 2_000_000 and d <= 4
+    from nngpr_b200.sharding import search_is_pruned
+    pruned = seeded and search_is_pruned(n, d)
     search = (19 + 1 + 2 + 2) if pruned else 1
     return 3 + 9 * levels + search + 2
 
@@ -803,7 +804,7 @@ def run_ours(args):
         issued = 2.0 * kp * pairs / (knn_avg_ms * 1e-3) / 1e12
         local_avg_ms = float(np.mean([a - b for a, b in zip(step_ms, knn_ms)]))
         search = {'kernel': f'knn_tc_kernel<{D}> (prefix search: tcgen05 TF32-split screen, exact FP32 rescoring; '
-                            f'seeded rows, pruned tile lists for d <= 4)',
+                            f'seeded rows, pruned tile lists)',
                   'ms': knn_avg_ms,
                   'brute_force_equivalent_tflops': achieved,
                   'note': '2*d flops per (query, ref) pair over all n(n-1)/2 prefix pairs; the pruned search '

@@ -43,6 +43,14 @@ constexpr int kBands = kEarlyShift + 1;  // band b: rows [n / 2^(b + 1), n / 2^b
 constexpr int kLooseLog2Q = 4 * 256;  // seed > 16 x band geometric mean (log2 in 1/256 units)
 constexpr uint64_t kIndexOrderTag = 1ull << 36;  // above (band << 32 | curve position) for bands < 16
 constexpr uint64_t kOutsideTag = 1ull << 37;     // rows outside the searched range: sorted last, not searched
+// The pruned rows go back to index order when their tile lists hold more tiles than their
+// index-order groups would stream.  Lists that exclude nothing hold about 4/3 of those tiles
+// (a group in curve order needs the tiles up to its largest index, an index-order group up to
+// about its mean); measured on B200 the pruned search wins up to a ratio of about 0.8 and loses
+// from about 1.3 on.
+constexpr double kFallbackFrac = 1.0;
+constexpr int kStats = 3 * kBands + 3;  // per band: seed log sums, counts, pruned counts; index-order
+                                        // count; sum of the pruned rows' indices; fallback flag
 
 __device__ __forceinline__ int band_of(int64_t i, int64_t n) {
     int b = 0;
@@ -150,9 +158,10 @@ __global__ void __launch_bounds__(kThreads) classify_kernel(int64_t n, int64_t e
                                                             const unsigned long long *__restrict__ cnt,
                                                             uint64_t *__restrict__ keys, int32_t *__restrict__ vals,
                                                             unsigned long long *__restrict__ pruned_cnt,
-                                                            unsigned long long *__restrict__ index_cnt) {
+                                                            unsigned long long *__restrict__ index_cnt,
+                                                            unsigned long long *__restrict__ pruned_isum) {
     unsigned long long c[kBands] = {};
-    unsigned long long ci = 0;
+    unsigned long long ci = 0, si = 0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         vals[i] = (int32_t)i;
         if (i < row_lo || i >= row_hi) {
@@ -170,8 +179,12 @@ __global__ void __launch_bounds__(kThreads) classify_kernel(int64_t n, int64_t e
             }
         }
         keys[i] = pruned ? ((uint64_t)b << 32 | (uint32_t)pos0[i]) : (kIndexOrderTag | (uint64_t)i);
-        if (pruned) c[b] += 1;
-        else ci += 1;
+        if (pruned) {
+            c[b] += 1;
+            si += (unsigned long long)i;
+        } else {
+            ci += 1;
+        }
     }
 #pragma unroll
     for (int b = 0; b < kBands; ++b) {
@@ -179,8 +192,12 @@ __global__ void __launch_bounds__(kThreads) classify_kernel(int64_t n, int64_t e
         for (int o = 16; o > 0; o >>= 1) cv += __shfl_xor_sync(0xFFFFFFFFu, cv, o);
         if ((threadIdx.x & 31) == 0 && cv > 0) atomicAdd(pruned_cnt + b, cv);
     }
-    for (int o = 16; o > 0; o >>= 1) ci += __shfl_xor_sync(0xFFFFFFFFu, ci, o);
+    for (int o = 16; o > 0; o >>= 1) {
+        ci += __shfl_xor_sync(0xFFFFFFFFu, ci, o);
+        si += __shfl_xor_sync(0xFFFFFFFFu, si, o);
+    }
     if ((threadIdx.x & 31) == 0 && ci > 0) atomicAdd(index_cnt, ci);
+    if ((threadIdx.x & 31) == 0 && si > 0) atomicAdd(pruned_isum, si);
 }
 
 // Octree cell level of band b: cells of 2^(d L) per level hold about 256 of the band's pruned
@@ -254,6 +271,33 @@ __global__ void sizes_kernel(int64_t n, int G, const int32_t *__restrict__ gh, c
     index_order->n_rows = (int64_t)*index_cnt;
     index_order->n_groups = ((int64_t)*index_cnt + G - 1) / G;
     index_order->n_items = index_order->n_groups;
+}
+
+// Index-order fallback: when the listed tiles (offsets[max_groups]) exceed kFallbackFrac x the
+// tiles the pruned rows' index-order groups would stream (sum of their indices / (tile x G)),
+// every row of [row_lo, row_hi) takes the index-order launch and the pruned launch is empty.
+__global__ void fallback_kernel(const int32_t *__restrict__ offsets, int64_t max_groups, int G, int64_t row_lo,
+                                int64_t row_hi, const unsigned long long *__restrict__ pruned_isum,
+                                DevSizes *__restrict__ pruned, DevSizes *__restrict__ index_order,
+                                unsigned long long *__restrict__ flag) {
+    const double listed = (double)offsets[max_groups];
+    const double index_tiles = (double)*pruned_isum / ((double)kTileRefs * (double)G);
+    const bool back = pruned->n_groups > 0 && listed > kFallbackFrac * index_tiles;
+    *flag = back ? 1ull : 0ull;
+    if (!back) return;
+    const int64_t nr = row_hi - row_lo;
+    *pruned = DevSizes{0, 0, 0, 0};
+    *index_order = DevSizes{0, nr, (nr + G - 1) / G, (nr + G - 1) / G};
+}
+
+// Under the fallback the row order becomes the searched range ascending.
+__global__ void __launch_bounds__(kThreads) fallback_rows_kernel(int64_t row_lo, int64_t row_hi,
+                                                                 const unsigned long long *__restrict__ flag,
+                                                                 int32_t *__restrict__ rows) {
+    if (*flag == 0) return;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < row_hi - row_lo;
+         k += (int64_t)gridDim.x * blockDim.x)
+        rows[k] = (int32_t)(row_lo + k);
 }
 
 // Box, largest seed and largest index of every pruned group; one warp per group.
@@ -519,7 +563,7 @@ Layout layout(int64_t n, int d, int G) {
     L.tlo = take((size_t)L.n_tiles * d * 4);
     L.thi = take((size_t)L.n_tiles * d * 4);
     L.tmin = take((size_t)L.n_tiles * 4);
-    L.stats = take((3 * kBands + 1) * 8);
+    L.stats = take(kStats * 8);
     L.keys_a = take((size_t)n * 8);
     L.keys_b = take((size_t)n * 8);
     L.vals_a = take((size_t)n * 4);
@@ -679,7 +723,7 @@ size_t workspace(int64_t n, int d, int rows_per_group) {
 nngp_status build(const float *xs, int64_t n, int64_t row_lo, int64_t row_hi, int d, int dp, int G, int bits,
                   const float *seeds, const int32_t *order0, const int32_t *pos0, const uint64_t *keys0, void *ws,
                   size_t ws_bytes, Lists *out, cudaStream_t stream) {
-    if (n < kMinPoints || n > kMaxPoints || d < 1 || d > kMaxDim || G < 1 || bits < 1 || d * bits > 60 || !xs ||
+    if (n < kMinPoints || n > kMaxPoints || d < 1 || d > kMaxDim || G < 1 || bits < 1 || d * bits > 64 || !xs ||
         !seeds || !order0 || !pos0 || !keys0 || !out)
         return fail(NNGP_ERR_UNSUPPORTED, "knn pruning: shape outside the pruned search");
     const Layout L = layout(n, d, G);
@@ -689,7 +733,8 @@ nngp_status build(const float *xs, int64_t n, int64_t row_lo, int64_t row_hi, in
     float *tlo = static_cast<float *>(at(L.tlo)), *thi = static_cast<float *>(at(L.thi));
     int32_t *tmin = static_cast<int32_t *>(at(L.tmin));
     unsigned long long *sum = static_cast<unsigned long long *>(at(L.stats)), *cnt = sum + kBands,
-                       *pcnt = sum + 2 * kBands, *icnt = sum + 3 * kBands;
+                       *pcnt = sum + 2 * kBands, *icnt = sum + 3 * kBands, *isum = sum + 3 * kBands + 1,
+                       *fallback = sum + 3 * kBands + 2;
     if (row_lo < 0 || row_hi > n || row_lo > row_hi)
         return fail(NNGP_ERR_INVALID_ARGUMENT, "knn pruning: row range outside [0, n)");
     int32_t *headpos = static_cast<int32_t *>(at(L.headpos)), *seg_start = static_cast<int32_t *>(at(L.seg_start));
@@ -723,13 +768,13 @@ nngp_status build(const float *xs, int64_t n, int64_t row_lo, int64_t row_hi, in
     tile_box_kernel<<<grid_of(L.n_tiles * 32), kThreads, 0, stream>>>(xs, n, d, dp, ref_order, L.n_tiles, tlo, thi,
                                                                        tmin);
     NNGP_CUDA_TRY(cudaGetLastError());
-    NNGP_CUDA_TRY(cudaMemsetAsync(sum, 0, (3 * kBands + 1) * 8, stream));
+    NNGP_CUDA_TRY(cudaMemsetAsync(sum, 0, kStats * 8, stream));
     band_stats_kernel<<<grid_of(n - early), kThreads, 0, stream>>>(n, std::max(early, row_lo), row_hi, seeds, sum,
                                                                    cnt);
     NNGP_CUDA_TRY(cudaGetLastError());
     classify_kernel<<<grid_of(n), kThreads, 0, stream>>>(n, early, row_lo, row_hi, seeds, pos0, sum, cnt,
                                                          static_cast<uint64_t *>(at(L.keys_a)),
-                                                         static_cast<int32_t *>(at(L.vals_a)), pcnt, icnt);
+                                                         static_cast<int32_t *>(at(L.vals_a)), pcnt, icnt, isum);
     NNGP_CUDA_TRY(cudaGetLastError());
 
     // rows: pruned (band, curve position) first, then the index-order rows ascending
@@ -741,7 +786,7 @@ nngp_status build(const float *xs, int64_t n, int64_t row_lo, int64_t row_hi, in
     if (st != NNGP_OK) return st;
     size_t have = L.cub_bytes;
     NNGP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(at(L.cub), have, dk, dv, (int)n, 0, 38, stream));
-    const int32_t *rows = dv.Current();
+    int32_t *rows = dv.Current();
 
     // groups: segments of one band and one octree cell, cut every G rows
     segment_kernel<<<grid_of(n), kThreads, 0, stream>>>(n, dk.Current(), rows, pos0, keys0, pcnt, d, bits, headpos);
@@ -776,6 +821,10 @@ nngp_status build(const float *xs, int64_t n, int64_t row_lo, int64_t row_hi, in
     if ((st = cub_check(need)) != NNGP_OK) return st;
     have = L.cub_bytes;
     NNGP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(at(L.cub), have, counts, offsets, (int)(L.max_groups + 1), stream));
+    fallback_kernel<<<1, 1, 0, stream>>>(offsets, L.max_groups, G, row_lo, row_hi, isum, sizes, sizes + 1, fallback);
+    NNGP_CUDA_TRY(cudaGetLastError());
+    fallback_rows_kernel<<<grid_of(row_hi - row_lo), kThreads, 0, stream>>>(row_lo, row_hi, fallback, rows);
+    NNGP_CUDA_TRY(cudaGetLastError());
     fill_kernel<<<grid_of(L.max_groups * 32), kThreads, 0, stream>>>(b, sizes, L.n_tiles, offsets, list);
     NNGP_CUDA_TRY(cudaGetLastError());
 

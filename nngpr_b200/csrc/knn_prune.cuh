@@ -14,7 +14,7 @@ namespace prune {
 
 constexpr int64_t kMinPoints = 65536;  // below this the index-order search is short enough
 constexpr int64_t kMaxPoints = 2000000;  // the tile lists' worst-case bound (groups x tiles) grows as n^2
-constexpr int kMaxDim = 4;             // bounding boxes stop pruning in more dimensions
+constexpr int kMaxDim = 24;            // every shape of the tensor-core search (d <= 24)
 constexpr int kTileRefs = 128;         // refs per tile (the tensor-core search's ref tile)
 
 // Rows [0, early_rows(n)) = [0, n / 8) always take the index-order search: their prefixes are

@@ -9,7 +9,7 @@ gives every rank the full value and gradient.  X and y are replicated.
 
 Rows are split so that the prefix-search pair counts (row i scans i refs) are equal:
 rank r owns ``[n sqrt(r / R), n sqrt((r + 1) / R))`` (``row_partition``), the right split when
-the search cost grows with the prefix.  When the library prunes the search (FP32, d <= 4,
+the search cost grows with the prefix.  When the library prunes the search (FP32, d <= 24,
 65,536 <= n <= 2,000,000, see ``search_is_pruned``) a row costs about the same wherever it is
 (its tile list covers its neighbourhood, not its prefix), and so do the local systems: equal row
 counts balance the ranks (``row_partition(..., equal_rows=True)``).
@@ -22,7 +22,7 @@ import math
 
 def search_is_pruned(n: int, d: int, float32: bool = True) -> bool:
     """Whether the library's fit-step search of n points in d dimensions is pruned."""
-    return float32 and d <= 4 and 65536 <= n <= 2_000_000
+    return float32 and d <= 24 and 65536 <= n <= 2_000_000
 
 
 def row_partition(n: int, world: int, equal_rows: bool = False) -> list[int]:

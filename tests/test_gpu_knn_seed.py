@@ -120,7 +120,8 @@ def test_pruned_ties_outlier_and_clusters(monkeypatch, capfd):
 def test_split_work_items_merge_to_the_same_lists(monkeypatch, capfd):
     """An outlier squeezes the other points into one Morton cell: seeds come from random windows
     and groups need most tiles, so long tile ranges are split into several work items whose
-    partial lists are merged; the result equals the unpruned search and the oracle."""
+    partial lists are merged (in whichever launch takes the rows); the result equals the
+    unpruned search and the oracle."""
     import re
     rng = np.random.default_rng(21)
     y = rng.normal(size=(90000, 3))
@@ -128,8 +129,12 @@ def test_split_work_items_merge_to_the_same_lists(monkeypatch, capfd):
     monkeypatch.setenv('NNGP_KNN_DEBUG', '1')
     a = search_mode(monkeypatch, y, 32, 0.5, True)
     err = capfd.readouterr().err
-    mt = re.search(r'groups=(\d+) items=(\d+)', err)
-    assert mt and int(mt.group(2)) > int(mt.group(1))  # some groups were split
+    mt = re.search(r'pruned rows=(\d+) groups=(\d+) items=(\d+) .* index-order rows=(\d+) items=(\d+)', err)
+    assert mt
+    _, pg, pi, ir, ii = map(int, mt.groups())
+    # some groups were split: in the pruned launch, or in the index-order launch (128-row groups)
+    # when the lists fall back to index order
+    assert pi > pg or ii > -(-ir // 128)
     assert np.array_equal(a, search_mode(monkeypatch, y, 32, 0.5, False))
     check_rows(y, a, 32, 0.5, rng, k=100)
 
@@ -180,7 +185,7 @@ def test_query_search_engages_and_handles_duplicates_and_outliers(monkeypatch, c
 @pytest.mark.parametrize('d', [3, 8])
 def test_row_shards_of_the_prefix_search(monkeypatch, capfd, d):
     """The multi-GPU fit step searches row shards: query = rows [r0, r1) of the set as a view,
-    ref_cut_index = r0.  Shards are seeded (and pruned for d <= 4) over their own rows and
+    ref_cut_index = r0.  Shards are seeded and pruned over their own rows and
     equal the corresponding rows of the whole search."""
     rng = np.random.default_rng(40 + d)
     n = 100000
@@ -194,7 +199,32 @@ def test_row_shards_of_the_prefix_search(monkeypatch, capfd, d):
     for r0, r1 in [(0, 30000), (30000, 71000), (71000, n)]:
         got = ops.knn(t, t[r0:r1], 32, r0, ls).cpu().numpy()
         err = capfd.readouterr().err
-        assert 'seeded=1' in err and (('pruned=1' in err) == (d <= 4))
+        assert 'seeded=1' in err and 'pruned=1' in err
         assert np.array_equal(got, full[r0:r1])
     monkeypatch.setenv('NNGP_KNN_SEED_W', '0')
     np.testing.assert_array_equal(ops.knn(t, t[50000:60000], 32, 50000, ls).cpu().numpy(), full[50000:60000])
+
+
+def test_index_order_fallback_when_boxes_do_not_prune(monkeypatch, capfd):
+    """Uniform points in 24 dimensions: every group's box meets nearly every tile's, so the tile
+    lists would stream more tiles than index order; the search puts every row back in index order
+    (the pruned launch is empty).  Whole set and row shards equal the unpruned search; 3-d points
+    keep their pruned rows."""
+    rng = np.random.default_rng(77)
+    n = 100000
+    x = rng.uniform(-1, 1, (n, 24))
+    monkeypatch.setenv('NNGP_KNN_DEBUG', '1')
+    a = search_mode(monkeypatch, x, 32, 0.5, True)
+    assert 'pruned rows=0 ' in capfd.readouterr().err
+    assert np.array_equal(a, search_mode(monkeypatch, x, 32, 0.5, False))
+    check_rows(x, a, 32, 0.5, rng, k=60)
+    monkeypatch.setenv('NNGP_KNN_PRUNE', '1')
+    t = torch.from_numpy(x.astype(np.float32)).cuda()
+    for r0, r1 in [(0, 40000), (40000, n)]:
+        got = ops.knn(t, t[r0:r1], 32, r0, 0.5).cpu().numpy()
+        assert 'pruned rows=0 ' in capfd.readouterr().err
+        assert np.array_equal(got, a[r0:r1])
+    y = rng.uniform(-1, 1, (n, 3))
+    search_mode(monkeypatch, y, 32, 0.3, True)
+    err = capfd.readouterr().err
+    assert 'pruned rows=' in err and 'pruned rows=0 ' not in err

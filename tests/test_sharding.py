@@ -19,7 +19,8 @@ from nngpr_b200.sharding import prefix_pairs, row_partition
 
 def test_row_partition_equal_rows_for_the_pruned_search():
     from nngpr_b200.sharding import search_is_pruned
-    assert search_is_pruned(434874, 3) and not search_is_pruned(434874, 8) and not search_is_pruned(30000, 3)
+    assert search_is_pruned(434874, 3) and search_is_pruned(434874, 8) and not search_is_pruned(434874, 33)
+    assert not search_is_pruned(30000, 3)
     for n, world in [(434874, 8), (10, 3), (1, 4)]:
         b = row_partition(n, world, equal_rows=True)
         assert b[0] == 0 and b[-1] == n and all(b[i] <= b[i + 1] for i in range(world))
