@@ -435,7 +435,8 @@ def our_launches_per_step(n, d, m):
     """Kernels of this library one fit step launches (CUB's sort and scan kernels not counted):
     scale, centre sums and tile build; per seed level (the prefixes n, n/8, ... of at least
     8,192 points) bounds, two x (Morton keys, inverse, coordinate gather), cross positions and
-    the seed kernel; the pruned search's planning (19), a second tile build, two search
+    the seed kernel; the pruned search's planning (21, the index-order fallback's two
+    included), a second tile build, two search
     launches and two merges, or one search launch; the local systems and the final sum."""
     seeded = n >= 8192
     levels = 0
@@ -445,7 +446,7 @@ def our_launches_per_step(n, d, m):
         p_ //= 8
     from nngpr_b200.sharding import search_is_pruned
     pruned = seeded and search_is_pruned(n, d)
-    search = (19 + 1 + 2 + 2) if pruned else 1
+    search = (21 + 1 + 2 + 2) if pruned else 1
     return 3 + 9 * levels + search + 2
 
 
@@ -842,6 +843,9 @@ def run_ours(args):
                 kernel=f'knn_tc_kernel<{D}> (prefix search: tcgen05 TF32-split screen, exact FP32 rescoring)',
                 work='2*d flops per (query, ref) pair, n(n-1)/2 pairs, whichever pipe computes them; '
                      'issued_mma = 2*K\' per pair with the split width K\'',
+                pruned=search_is_pruned(n, D),
+                pruned_note='when pruned, the search screens only the pairs its tile lists keep, so achieved (and '
+                            'frac) is the brute-force rate of the problem and can exceed the pipe\'s peak',
                 knn_ms=knn_avg_ms),
             'cpu_baseline': cpu,
             'plain_gpu': plain,

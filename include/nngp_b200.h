@@ -122,10 +122,10 @@ nngp_status nngp_check_device(void);
  *
  * The fit step's search of a set over itself (ref == query, n_ref == n_query, has_ref_cut with
  * ref_cut_index 0, FP32, n >= 8,192) starts every row from a proven bound of its num_nn-th
- * distance (Morton-window seeds) and, for d <= 4 and 65,536 <= n <= 2,000,000, visits per group
+ * distance (Morton-window seeds) and, for d <= 24 and 65,536 <= n <= 2,000,000, visits per group
  * of rows only the ref tiles bounding boxes cannot exclude; the lists are the same.
  * A search of other queries without a cut (predict: n_ref >= 8,192, n_query >= 16,384) seeds
- * every query from the refs' curve windows around it and, for d <= 4, prunes the same way.
+ * every query from the refs' curve windows around it and, for d <= 24, prunes the same way.
  * NNGP_KNN_SEED_W=0 / NNGP_KNN_PRUNE=0 switch these off (testing).  The workspace covers them.
  * ------------------------------------------------------------------------------------- */
 size_t nngp_knn_workspace_size_f32(int64_t n_ref, int64_t n_query, int32_t d, int32_t num_nn);

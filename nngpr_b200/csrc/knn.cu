@@ -667,7 +667,7 @@ nngp_status knn_impl(const T *ref, int64_t n_ref, const T *query, int64_t n_quer
                 seeds_c = sd;
             }
             // queries against the set (predict): seeds from the refs' curve windows around each
-            // query, and (d <= 4) groups of queries in curve order with their tile lists
+            // query, and (d <= 24) groups of queries in curve order with their tile lists
             const int G = p.tv.rows_per_item;
             const int32_t *qorder = nullptr;
             const bool qseeded = !same && !has_cut && seed::window() > 0 && seed::query_workspace_if(n_ref, n_query, p.dp) > 0 &&
@@ -681,8 +681,9 @@ nngp_status knn_impl(const T *ref, int64_t n_ref, const T *query, int64_t n_quer
             }
             const size_t qprune_ws = qseeded ? prune::workspace_query(n_ref, n_query, d, G) : 0;
             const bool qpruned = qseeded && qprune_ws > 0 && p.prune_ws_bytes >= qprune_ws && prune::enabled();
-            // and, for large low-dimensional sets, visits per group of rows only the ref tiles its
-            // seeds allow (rows and refs in curve order; loose and early rows stay in index order)
+            // and, for large sets (d <= 24), visits per group of rows only the ref tiles its seeds
+            // allow (rows and refs in curve order; loose and early rows stay in index order, and all
+            // rows go back to it on the device when the lists exclude too little)
             const bool pruned = seeded && prune::workspace(n_ref, d, G) > 0 &&
                                 p.prune_ws_bytes >= prune::workspace(n_ref, d, G) && prune::enabled();
             prune::Lists lists;
