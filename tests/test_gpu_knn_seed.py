@@ -154,7 +154,7 @@ def query_search(monkeypatch, ref, q, m, ls, window, prune=True):
                                              (5, 30000, 20000), (16, 20000, 30000)])
 def test_query_search_seeded_and_pruned_equal_plain_and_oracle(monkeypatch, d, n_ref, n_query):
     """Queries against a set (the predict search): seeds from the refs' curve windows around each
-    query and, for d <= 4, curve-ordered query groups with tile lists; the same lists."""
+    query and curve-ordered query groups with tile lists; the same lists."""
     rng = np.random.default_rng(7 * d + n_query)
     ref = rng.uniform(-1, 1, (n_ref, d))
     q = rng.uniform(-1.2, 1.2, (n_query, d))  # some queries outside the refs' box
