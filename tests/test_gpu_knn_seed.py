@@ -151,7 +151,8 @@ def query_search(monkeypatch, ref, q, m, ls, window, prune=True):
 
 
 @pytest.mark.parametrize('d,n_ref,n_query', [(2, 70000, 20000), (3, 70000, 100000), (4, 30000, 40000),
-                                             (5, 30000, 20000), (16, 20000, 30000)])
+                                             (5, 30000, 20000), (16, 20000, 30000), (8, 70000, 30000),
+                                             (16, 70000, 20000)])
 def test_query_search_seeded_and_pruned_equal_plain_and_oracle(monkeypatch, d, n_ref, n_query):
     """Queries against a set (the predict search): seeds from the refs' curve windows around each
     query and curve-ordered query groups with tile lists; the same lists."""
