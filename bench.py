@@ -1,36 +1,40 @@
 """Benchmark of the NNGP fit step (log-likelihood + gradient) on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload W]
 
-Workload (the reference's FP32 GPU configuration, synthetic data of its shape; seed 0):
-n = 434,874 training points, d = 3, x ~ U[-1, 1]^3 scaled per axis by (1, 0.7, 0.4),
-y = sum_k sin(3 x_k) + N(0, 0.05^2), m = 32 neighbours, ConstantKernel(1) * RBF(0.2) +
-WhiteKernel(1e-3), alpha = 1e-10.  One step = one full fit step over all n points: the
-prefix neighbour search (point i among points [0, i)), the fused local systems with the
-adjoint gradient (FP64 systems, the default allow_downcast_f32='only-nn': at this nugget
-almost every FP32 system would need the FP64 re-solve) and the FP64 reduction.  Predict
-throughput at 100,000 test points is reported beside it.
+Default workload (the mixed-precision configuration the target is quoted on; synthetic data of
+its shape, seed 0): n = 1,000,000 training points, d = 16, x from a 64-component Gaussian
+mixture with means ~ U[-3, 3]^16 and std 0.5, y = 256 random Fourier features
+(omega ~ N(0, 1/0.8^2), phases ~ U[0, 2 pi], weights N(0, 1) sqrt(2/256)) + N(0, 0.01^2),
+m = 32, ConstantKernel(1) * RBF(0.8) + WhiteKernel(1e-4), alpha = 1e-10.  One step = one full
+fit step over all n points: the prefix neighbour search (point i among points [0, i), FP32,
+tensor-core screen, exact FP32 rescoring), the fused FP32 local systems with the adjoint
+gradient (systems whose pivot falls below the threshold re-solved in FP64) and the FP64
+reduction.  The line adds the log-likelihood error against FP64 local systems on the same
+lists, the fraction of systems re-solved in FP64, the error against the reference's own FP64
+NumpyNngpr on a 20,000-point subset, predict throughput at 100,000 test points and a short
+served-predict stream.
 
---workload precision: the mixed-precision configuration instead (n = 1,000,000, d = 16, x from
-a 64-component Gaussian mixture with means ~ U[-3, 3]^16 and std 0.5, y = 256 random Fourier
-features (omega ~ N(0, 1/0.8^2), phases ~ U[0, 2 pi], weights N(0, 1) sqrt(2/256)) +
-N(0, 0.01^2), m = 32, ConstantKernel(1) * RBF(0.8) + WhiteKernel(1e-4)): FP32 search on the
-tensor cores, FP32 local systems with an FP64 re-solve of small pivots, FP64 reductions; the
-line adds the log-likelihood error against FP64 local systems on the same neighbour lists.
+--workload fit3d: the reference's FP32 GPU configuration (n = 434,874, d = 3,
+x ~ U[-1, 1]^3 scaled per axis by (1, 0.7, 0.4), y = sum_k sin(3 x_k) + N(0, 0.05^2),
+ConstantKernel(1) * RBF(0.2) + WhiteKernel(1e-3), FP64 local systems).  --workload
+differentiation / serving: the other configurations (see WORKLOADS).
 
 Our arm prints one JSON line (rank 0) with value = fit steps per second with the inputs
 resident in HBM, e2e = the same through the public estimator API uploading X, y from pinned
-host memory on every call, the roofline of the dominant kernel (the neighbour search),
-a cpu_baseline (the reference's NumpyNngpr on the host cores, on a bounded sample of the
-same fit step, extrapolated by row count) and the SM clocks sampled during the timed steps.
+host memory on every call, the roofline of the dominant kernel (the neighbour search for
+d = 16 and d = 8, the FP64 local-systems kernel for d = 3), a cpu_baseline (the reference's
+NumpyNngpr on the host cores: a row-sampled estimate of the full step, calibrated against a
+full reference step on the first 20,000 points timed in the same run) and the SM clocks
+sampled during the timed steps.
 
 --impl reference runs the reference's own CPU implementation (NumpyNngpr from
-baseline/_ref, its _log_likelihood_worker on a bounded sample of rows spread over the same
-fit step, all host cores) and prints the same metric.
+baseline/_ref: its _log_likelihood_worker on a bounded sample of rows spread over the same
+fit step, all host cores, with the same calibration) and prints the same metric.
 
-With N > 1 GPUs (torchrun) the fit step is split into N row ranges with equal neighbour-search
-pair counts; each rank searches and solves its rows and the (1 + n_theta) partial sums are
-all-reduced over NCCL (strong scaling: the total work is fixed).
+With N > 1 GPUs (torchrun) the fit step is split into N row ranges; each rank searches and
+solves its rows and the (1 + n_theta) partial sums are all-reduced over NCCL (strong scaling:
+the total work is fixed).
 """
 
 from __future__ import annotations
@@ -67,6 +71,9 @@ LOCAL = 'f64'
 # roofline kernel: 'local' (the FP64 local-systems kernel, the largest share of the d = 3 step once
 # the search is pruned), 'fp32' (the search kernel's screen issue) or 'tensor' (its TF32 MMAs)
 ROOF = 'local'
+# FP32 local systems: re-solve in FP64 when a pivot falls below this fraction of the kernel
+# diagonal (None: the library default, nngpr_b200.ops.DEFAULT_PIVOT_TOL)
+PIVOT = None
 DATA = 'synthetic (seeded stand-in for 3droad: shape 434874 x 3)'
 DTYPE = 'f32 search (tf32-split tensor screen) + f64 local'
 
@@ -187,7 +194,12 @@ def default_cpu_workers(gb_per_worker=4.0, cap=32):
 class CpuBaseline:
     """Times the reference's FP64 worker (``_log_likelihood_worker``, default ``only-nn``
     search) on ``cores`` processes, each processing one batch of ``rows`` points placed at
-    stratified positions of the full fit step, and extrapolates to all n points."""
+    stratified positions of the full fit step, and extrapolates to all n points.
+
+    ``calibrate`` checks that model against a full step: the reference's own
+    ``log_marginal_likelihood(theta, eval_gradient=True)`` on the first ``subset`` points (its
+    multiprocessing pool over the same cores), beside the row-sampled estimate of that same
+    subset step; the ratio scales the full-size estimate."""
 
     def __init__(self, x, y, rows_per_task=200, cores=None, seed=1):
         NumpyNngpr, bk, kind = _import_reference()
@@ -196,7 +208,11 @@ class CpuBaseline:
         self.rows = rows_per_task
         self.n = x.shape[0]
         self.rng = np.random.default_rng(seed)
+        self.ratio = 1.0
+        self.calibration = None
+        self.x, self.y = x, y
         if kind == 'reference':
+            self.NumpyNngpr, self.bk = NumpyNngpr, bk
             kernel = bk.ConstantKernel(1.0) * bk.RBF(LS) + bk.WhiteKernel(NOISE)
             gpr = NumpyNngpr(kernel=kernel, num_nn=M, alpha=ALPHA, optimizer=None, batch_size=rows_per_task,
                              num_workers=1, distribute_method='sequential')
@@ -208,13 +224,70 @@ class CpuBaseline:
                         y=gpr.y_train_[:, None])
         self.n_tasks = (self.n + rows_per_task - 1) // rows_per_task
 
-    def sample(self):
-        """One bounded sample: ``cores`` tasks at stratified positions, run in parallel on the
-        host cores.  Returns the summed per-task seconds (each task timed inside its worker
-        process) and the rows processed."""
-        edges = np.linspace(0, self.n_tasks, self.cores + 1)
+    def _reference_gpr(self, n, **kw):
+        """The reference estimator in its fitted state on the first n points, its own pool over
+        ``self.cores`` processes (``distribute_method`` left at the reference's default)."""
+        kernel = self.bk.ConstantKernel(1.0) * self.bk.RBF(LS) + self.bk.WhiteKernel(NOISE)
+        g = self.NumpyNngpr(kernel=kernel, num_nn=M, alpha=ALPHA, optimizer=None, num_workers=self.cores, **kw)
+        g.X_train_, g.y_train_, g.kernel_ = (np.asarray(self.x[:n], np.float64), np.asarray(self.y[:n], np.float64),
+                                             kernel)
+        return g
+
+    def full_subset_step(self, n, repeats=2, **kw):
+        """Seconds of the reference's full log_marginal_likelihood(theta, eval_gradient=True) on
+        the first n points (best of ``repeats``), with its lml and gradient."""
+        g = self._reference_gpr(n, **kw)
+        best, out = None, None
+        for _ in range(repeats):
+            t0 = time.perf_counter()
+            lml, grad = g.log_marginal_likelihood(g.kernel_.theta, eval_gradient=True)
+            dt = time.perf_counter() - t0
+            best = dt if best is None else min(best, dt)
+            out = (float(lml), np.asarray(grad, np.float64))
+        return best, out
+
+    def calibrate(self, subset=20000, repeats=3):
+        """Row-sampled estimate vs a full reference step on the first ``subset`` points (the
+        estimator's task size, and the reference's default batch size beside it); sets
+        ``self.ratio`` = full / estimate."""
+        if self.kind != 'reference' or self.n < 2 * subset:
+            return None
+        full_s, _ = self.full_subset_step(subset, batch_size=self.rows)
+        default_s, _ = self.full_subset_step(subset, repeats=1)
+        sub_tasks = (subset + self.rows - 1) // self.rows
+        est = []
+        for _ in range(repeats):
+            dt, rows = self.sample(n_tasks=sub_tasks)
+            est.append(dt * subset / rows / self.cores)
+        est_s = float(np.median(est))
+        self.ratio = full_s / est_s
+        self.calibration = {
+            'subset_n': subset, 'subset_full_step_s': full_s, 'subset_sampled_estimate_s': est_s,
+            'ratio_full_over_estimate': self.ratio, 'subset_full_step_default_batch_s': default_s,
+            'note': (f'full reference log_marginal_likelihood(theta, eval_gradient=True) on the first {subset} points '
+                     f'with its multiprocessing pool over {self.cores} processes (batch_size {self.rows}, the '
+                     f'estimator\'s task size; with the reference\'s default batch size beside it), against the '
+                     f'row-sampled estimate of the same subset step; the full-size estimate is multiplied by the '
+                     f'ratio')}
+        return self.calibration
+
+    def reference_fp64(self, subset=20000):
+        """The reference's own FP64 result (allow_downcast_f32='no': FP64 search and systems) of
+        the fit step on the first ``subset`` points: (lml, gradient), or None without it."""
+        if self.kind != 'reference':
+            return None
+        _, out = self.full_subset_step(min(subset, self.n), repeats=1, batch_size=self.rows,
+                                       allow_downcast_f32='no')
+        return out
+
+    def sample(self, n_tasks=None):
+        """One bounded sample: ``cores`` tasks at stratified positions of the first ``n_tasks``
+        tasks (default: the whole step), run in parallel on the host cores.  Returns the summed
+        per-task seconds (each task timed inside its worker process) and the rows processed."""
+        n_tasks = self.n_tasks if n_tasks is None else n_tasks
+        edges = np.linspace(0, n_tasks, self.cores + 1)
         tasks = [int(self.rng.integers(int(a), max(int(a) + 1, int(b)))) for a, b in zip(edges[:-1], edges[1:])]
-        tasks = sorted(set(min(t, self.n_tasks - 1) for t in tasks))
+        tasks = sorted(set(min(t, n_tasks - 1) for t in tasks))
         rows = sum(min(self.n, (t + 1) * self.rows) - t * self.rows for t in tasks)
         env_keys = ('OPENBLAS_NUM_THREADS', 'MKL_NUM_THREADS', 'OMP_NUM_THREADS')
         bak = {k: os.environ.get(k) for k in env_keys}
@@ -249,15 +322,36 @@ _CPU_PORT = {}
 
 def cpu_steps_per_s(cb: CpuBaseline, steps: int):
     """Fit steps per second of the CPU implementation: core-seconds per row measured on the
-    samples, times n rows, divided by the cores (perfect scaling over the cores assumed, which
-    favours the CPU: the reference's pool adds fork and pickling costs on top)."""
+    samples, times n rows, divided by the cores, times the calibration ratio (a full reference
+    step against the same estimate on a subset, ``CpuBaseline.calibrate``; 1 without it).
+    Returns (steps/s, calibrated step seconds, rows sampled, core-seconds, uncalibrated step s)."""
     tot_t, tot_rows = 0.0, 0
     for _ in range(steps):
         dt, rows = cb.sample()
         tot_t += dt
         tot_rows += rows
-    full_step_s = tot_t * cb.n / tot_rows / cb.cores
-    return 1.0 / full_step_s, full_step_s, tot_rows, tot_t
+    raw_s = tot_t * cb.n / tot_rows / cb.cores
+    full_step_s = raw_s * cb.ratio
+    return 1.0 / full_step_s, full_step_s, tot_rows, tot_t, raw_s
+
+
+L2_NOTE = 'GPU arm: 256 MB written before every timed step (L2 flushed); CPU arm: inputs larger than its caches'
+SUBSET = 20000  # points of the full reference step that calibrates the CPU estimate (and the FP64 check)
+
+
+def cpu_baseline_obj(cb, sps, full_s, rows, t, raw_s, steps):
+    """The line's cpu_baseline object (what was timed, how it was scaled)."""
+    o = {'value': sps, 'unit': UNIT, 'cores': cb.cores, 'kind': cb.kind,
+         'sample': (f'{rows} rows in batches of {cb.rows} at stratified positions of the n={cb.n} fit step over '
+                    f'{steps} samples ({t:.1f} core-s); full step = core-s per row x n / {cb.cores} cores = '
+                    f'{raw_s:.1f} s, x {cb.ratio:.3f} (full {SUBSET}-point reference step / its row-sampled '
+                    f'estimate) = {full_s:.1f} s'),
+         'full_step_s': full_s, 'sampled_estimate_s': raw_s}
+    if cb.calibration is not None:
+        o['calibration'] = cb.calibration
+        o['subset_full_step_s'] = cb.calibration['subset_full_step_s']
+        o['subset_sampled_estimate_s'] = cb.calibration['subset_sampled_estimate_s']
+    return o
 
 
 def prepare_cpu_baseline(x, y):
@@ -607,6 +701,26 @@ def run_serving(args):
     print(json.dumps(line))
 
 
+def serving_summary(args):
+    """The served-predict configuration (n = 16,599, d = 18: PredictServer under a Poisson stream),
+    run as a child process of this benchmark after its own timed steps, condensed for this line."""
+    cmd = [sys.executable, os.path.abspath(__file__), '--workload', 'serving', '--requests', str(args.serve_requests),
+           '--rate', str(args.rate), '--plain-requests', str(args.serve_plain_requests), '--warmup', '3']
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+        line = next(ln for ln in reversed(r.stdout.splitlines()) if ln.startswith('{'))
+        d = json.loads(line)
+    except Exception as e:  # reported, never fatal to the fit-step line
+        return {'error': f'{type(e).__name__}: {e}'[:300]}
+    lat = d['latency']
+    return {'metric': 'served predict', 'config': d['config'], 'points_per_s': d['value'],
+            'p50_ms': lat['p50_ms'], 'p99_ms': lat['p99_ms'], 'p99_ms_le_1k_points': lat['p99_ms_le_1k_points'],
+            'one_k_alone': d['one_k_alone'], 'saturated_points_per_s': d['saturated']['points_per_s'],
+            'plain_gpu': {k: d['plain_gpu'][k] for k in ('points_per_s', 'p50_ms', 'p99_ms', 'requests')},
+            'speedup_points_per_s': d['speedup_points_per_s'], 'clocks': d['clocks'],
+            'note': 'latency = host completion - scheduled arrival (H2D, queueing and D2H included)'}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -618,14 +732,15 @@ def run_ours(args):
     n = x.shape[0]
 
     cpu = None
+    ref_np64 = None  # the reference's own FP64 (lml, grad) on the first SUBSET points
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         # before any CUDA call: the reference's worker pool forks
         cb = prepare_cpu_baseline(x, y)
-        sps, full_s, rows, t = cpu_steps_per_s(cb, args.cpu_samples)
-        cpu = {'value': sps, 'unit': UNIT, 'cores': cb.cores, 'kind': cb.kind,
-               'sample': f'{rows} rows in batches of {cb.rows} at stratified positions of the n={n} fit step '
-                         f'({t:.1f} core-s; full step extrapolated by row count over {cb.cores} cores: '
-                         f'{full_s:.0f} s)'}
+        cb.calibrate(SUBSET)
+        sps, full_s, rows, t, raw_s = cpu_steps_per_s(cb, args.cpu_samples)
+        cpu = cpu_baseline_obj(cb, sps, full_s, rows, t, raw_s, args.cpu_samples)
+        if not args.no_accuracy:
+            ref_np64 = cb.reference_fp64(SUBSET)
 
     torch.cuda.set_device(local_rank)
     dev = torch.device('cuda', local_rank)
@@ -656,11 +771,11 @@ def run_ours(args):
 
     def step(ev=None):
         if ev is None:
-            fit_step_rows(x32, xl, yl, p, ALPHA, M, r0, r1, LS, flags=flags, out=out)
+            fit_step_rows(x32, xl, yl, p, ALPHA, M, r0, r1, LS, pivot_tol=PIVOT, flags=flags, out=out)
         else:  # the same two calls, with an event between them to time the search alone
             nbr = ops.knn(x32, q_rows, M, r0, LS, flags=flags)  # rows [r0, r1) among points [0, i)
             ev.record()
-            ops.loglik(xl, yl, nbr, p, ALPHA, True, flags=flags, out=out, row_begin=r0)
+            ops.loglik(xl, yl, nbr, p, ALPHA, True, pivot_tol=PIVOT, flags=flags, out=out, row_begin=r0)
         if world > 1:
             dist.all_reduce(out)
         return out
@@ -699,10 +814,37 @@ def run_ours(args):
         tot_ms = float(t.item())
     lml_val = float(out[0].item())
     lml_err = None
-    if LOCAL != 'f64' and world == 1:  # error of the mixed-precision result against FP64 systems
+    accuracy = None
+    if LOCAL != 'f64' and world == 1:
+        # the mixed-precision result against FP64 local systems on the same lists, and how many
+        # systems the FP32 pass handed to the FP64 re-solve
         nbr_all = ops.knn(x32, x32, M, 0, LS, flags=flags)
-        ref64 = ops.loglik(x64, y64, nbr_all, p, ALPHA, True, flags=flags)
-        lml_err = abs(lml_val - float(ref64[0].item())) / abs(float(ref64[0].item()))
+        g64 = ops.loglik(x64, y64, nbr_all, p, ALPHA, True, flags=flags).cpu().numpy()
+        st = {}
+        g32 = ops.loglik(xl, yl, nbr_all, p, ALPHA, True, pivot_tol=PIVOT, flags=flags, stats=st).cpu().numpy()
+        n_fp64 = int(st['fp64_systems'].item())
+        lml_err = abs(lml_val - g64[0]) / abs(g64[0])
+        accuracy = {'lml_rel_err_vs_fp64_local': float(lml_err),
+                    'grad_rel_err_vs_fp64_local': float(np.max(np.abs(g32[1:] - g64[1:])) / np.max(np.abs(g64[1:]))),
+                    'fp64_resolved_systems': n_fp64, 'fp64_resolved_frac': n_fp64 / n, 'pivot_tol': PIVOT,
+                    'note': 'FP64 local systems computed by the FP64 kernel on the same lists (that kernel equals '
+                            'the reference FP64 worker to 1e-10 on the golden cases); pivot_tol is relative to the '
+                            'kernel diagonal'}
+    if ref_np64 is not None and world == 1:
+        # the reference's own FP64 NumpyNngpr (FP64 search and systems) on the first SUBSET points,
+        # against this library's fit step on the same points (FP32 search, mixed-precision systems)
+        sub = min(SUBSET, n)
+        nb_s = ops.knn(x32[:sub], x32[:sub], M, 0, LS, flags=flags)
+        o_s = ops.loglik(xl[:sub].contiguous(), yl[:sub].contiguous(), nb_s, p, ALPHA, True, pivot_tol=PIVOT,
+                         flags=flags).cpu().numpy()
+        r_lml, r_grad = ref_np64
+        accuracy = dict(accuracy or {})
+        accuracy['vs_reference_numpy_fp64'] = {
+            'n': sub, 'lml': float(o_s[0]), 'reference_lml': r_lml,
+            'lml_rel_err': abs(float(o_s[0]) - r_lml) / abs(r_lml),
+            'grad_rel_err': float(np.max(np.abs(o_s[1:] - r_grad)) / np.max(np.abs(r_grad))),
+            'note': f'reference NumpyNngpr(allow_downcast_f32="no") log_marginal_likelihood on the first {sub} points '
+                    f'(its own FP64 search), timed in the CPU-baseline phase of this run'}
 
     # ---- reused neighbour lists (isotropic length scale): what later L-BFGS steps cost -------
     reuse = None
@@ -792,6 +934,10 @@ def run_ours(args):
                                               abs(plain['lml'] - lml_val) / abs(lml_val))
         plain['speedup'] = (1e3 / (tot_ms / args.steps)) / plain['value']
 
+    serving = None
+    if rank == 0 and world == 1 and not args.no_serving and _WL != 'serving':
+        serving = serving_summary(args)
+
     if rank == 0:
         import ctypes
         peak = fp32_peak_tflops(torch, L, ctypes.c_void_p(stream.cuda_stream))
@@ -834,9 +980,8 @@ def run_ours(args):
             'warmup': args.warmup, 'ms_per_step': ms_per_step, 'higher_is_better': True,
             'scaling': 'strong' if world > 1 else 'weak', 'vs_baseline': None, 'dtype': DTYPE,
             'data': DATA,
-            'config': {'workload': WORKLOAD, 'n': n, 'd': D, 'm': M, 'parallelism': f'rows{world}',
-                       'l2': 'flushed (256 MB write) before every timed step', 'lml': lml_val,
-                       'lml_rel_err_vs_fp64_local': lml_err},
+            'config': {'workload': WORKLOAD, 'n': n, 'd': D, 'm': M, 'l2': L2_NOTE},
+            'parallelism': f'rows{world}', 'lml': lml_val, 'lml_rel_err_vs_fp64_local': lml_err,
             'e2e': e2e,
             'roofline': dict(roof, traffic=read_profile_traffic()) if ROOF == 'local' else dict(
                 roof, traffic=read_profile_traffic(),
@@ -848,9 +993,11 @@ def run_ours(args):
                             'frac) is the brute-force rate of the problem and can exceed the pipe\'s peak',
                 knn_ms=knn_avg_ms),
             'cpu_baseline': cpu,
+            'accuracy': accuracy,
             'plain_gpu': plain,
             'lbfgs': lbfgs,
             'reused_lists_step': reuse,
+            'serving': serving,
             'predict': None if pred_ms is None else {'value': N_PRED / (pred_ms * 1e-3), 'unit': 'points/s',
                                                      'ms': pred_ms, 'n_query': N_PRED},
             'gpu_launches': args.steps * our_launches_per_step(n, D, M),  # row shards take the same path
@@ -874,19 +1021,18 @@ def run_reference(args):
         return
     x, y, _ = make_data()
     cb = prepare_cpu_baseline(x, y)
+    cb.calibrate(SUBSET)
     for _ in range(args.warmup):
         cb.sample()
-    sps, full_s, rows, t = cpu_steps_per_s(cb, args.steps)
+    sps, full_s, rows, t, raw_s = cpu_steps_per_s(cb, args.steps)
+    cpu = cpu_baseline_obj(cb, sps, full_s, rows, t, raw_s, args.steps)
     line = {
         'metric': METRIC, 'value': sps, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
         'ms_per_step': full_s * 1e3, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
-        'dtype': 'f64', 'data': 'synthetic (seeded stand-in for 3droad: shape 434874 x 3)',
-        'config': {'workload': WORKLOAD, 'n': N_TRAIN, 'd': D, 'm': M, 'parallelism': 'host processes'},
-        'impl': 'reference',
-        'cpu_baseline': {'value': sps, 'unit': UNIT, 'cores': cb.cores, 'kind': cb.kind,
-                         'sample': f'{rows} rows in batches of {cb.rows} at stratified positions of the fit step '
-                                   f'({t:.1f} core-s over {args.steps} steps; full step extrapolated by row '
-                                   f'count over {cb.cores} cores)'},
+        'dtype': 'f64 systems (the reference default allow_downcast_f32=only-nn: f32 search)', 'data': DATA,
+        'config': {'workload': WORKLOAD, 'n': N_TRAIN, 'd': D, 'm': M, 'l2': L2_NOTE},
+        'parallelism': 'host processes', 'impl': 'reference',
+        'cpu_baseline': cpu,
         'e2e': {'value': sps, 'unit': UNIT, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
     }
     print(json.dumps(line))
@@ -904,20 +1050,32 @@ def main():
     ap.add_argument('--no-predict', action='store_true', help='skip the predict timing')
     ap.add_argument('--no-plain', action='store_true', help='skip the plain FP32 GPU comparator')
     ap.add_argument('--no-reuse', action='store_true', help='skip the reused-neighbour-list step timing')
-    ap.add_argument('--plain-steps', type=int, default=3, help='timed steps of the plain comparator (best reported)')
+    ap.add_argument('--plain-steps', type=int, default=2, help='timed steps of the plain comparator (best reported)')
     ap.add_argument('--requests', type=int, default=400, help='serving workload: requests in the stream')
     ap.add_argument('--rate', type=float, default=200.0, help='serving workload: mean arrivals per second')
     ap.add_argument('--plain-requests', type=int, default=100, help='serving workload: requests the plain form runs')
-    ap.add_argument('--workload', choices=sorted(WORKLOADS), default='fit3d',
-                    help='fit3d: n=434,874 d=3 (default); precision: n=1,000,000 d=16 mixed precision')
+    ap.add_argument('--serve-requests', type=int, default=300, help='requests of the served stream in the fit-step line')
+    ap.add_argument('--serve-plain-requests', type=int, default=10,
+                    help='requests the plain form runs for the served stream in the fit-step line')
+    ap.add_argument('--no-accuracy', action='store_true',
+                    help='skip the reference FP64 run on the first 20,000 points (the line\'s accuracy object)')
+    ap.add_argument('--no-serving', action='store_true', help='skip the short served-predict stream')
+    ap.add_argument('--workload', choices=sorted(WORKLOADS), default='precision',
+                    help='precision: n=1,000,000 d=16 mixed precision (default); fit3d: n=434,874 d=3; '
+                         'differentiation: n=434,874 d=8 ARD; serving: the served-predict stream alone')
     ap.add_argument('--n', type=int, default=None,
-                    help='training points (smaller cases are for profiling; the metric is quoted at 434874)')
+                    help='training points (smaller cases are for profiling; the metric is quoted at the '
+                         'workload\'s own n)')
+    ap.add_argument('--pivot-tol', type=float, default=None,
+                    help='FP64 re-solve threshold of the FP32 local systems (relative to the kernel diagonal)')
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    global _WL
+    global _WL, PIVOT
     _WL = args.workload
     globals().update(WORKLOADS[args.workload])
+    if args.pivot_tol is not None:
+        PIVOT = args.pivot_tol
     if args.impl == 'reference':
         run_reference(args)
     elif args.workload == 'serving':

@@ -105,6 +105,14 @@ const char *nngp_status_string(nngp_status status);
 /* NNGP_OK if the current device is an sm_100 part this build runs on. */
 nngp_status nngp_check_device(void);
 
+/* Failure-path testing (no counterpart in the reference): the time limit, in nanoseconds of the
+ * GPU's global timer, of the bounded waits in the tensor-core search's main loop (default 2 s;
+ * 0 restores the default).  A wait that runs out raises NNGP_FLAG_TIMEOUT and the kernel returns
+ * after draining the copies and MMAs it issued (those drains always use the 2 s default), so a
+ * tiny limit turns a search into a clean, flagged failure whose results are invalid, and the next
+ * call with the default limit runs normally.  Process-wide; returns the previous limit. */
+uint64_t nngp_set_wait_limit_ns(uint64_t ns);
+
 /* ---------------------------------------------------------------------------------------
  * Nearest-neighbour search
  *
@@ -190,6 +198,15 @@ nngp_status nngp_loglik_f64(const double *x, const double *y, int64_t n, int32_t
                             void *stream);
 
 /*
+ * How many local systems the last nngp_loglik_f32 / nngp_loglik_rows_f32 call given `workspace`
+ * re-solved in FP64 (the count behind NNGP_FLAG_FP64_FALLBACK; 0 after an f64 call): the DEVICE
+ * address of an unsigned 64-bit counter inside the workspace, valid once the stream has reached
+ * the end of that call and until the workspace is used again.  No counterpart in the reference
+ * (its FP32 mode has no FP64 re-solve); a host-only function, no GPU work.
+ */
+const uint64_t *nngp_loglik_fp64_count(const void *workspace);
+
+/*
  * Same as nngp_loglik_f32/_f64 restricted to the points [row_begin, row_begin + row_count)
  * (nbr then has row_count rows; neighbour indices still refer to all n rows of x, y).
  * Replaces one task of the reference's row-batched worker loop (base_nngpr.py:440-449,
@@ -217,7 +234,8 @@ nngp_status nngp_loglik_rows_f64(const double *x, const double *y, int64_t n, in
  * Same inputs, outputs and results as nngp_loglik_f64 (which it matches bit for bit on a
  * 148-SM B200); it rejects more than 35 hyperparameters (n_theta > 35 with eval_gradient)
  * with NNGP_ERR_UNSUPPORTED.  The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress); make that first call before any stream capture.  All calls share
+ * (cudaGetSymbolAddress) and keeps it for the life of the process; make that first call before
+ * any stream capture, and do not use the library across a cudaDeviceReset.  All calls share
  * the array: calls that overlap on the GPU (other streams or host threads on the same device)
  * race on it and must be serialised by the caller.
  */
@@ -321,6 +339,11 @@ nngp_status nngp_sample_full_f64(const double *x_full, const double *y_train, in
  * descriptors, tcgen05.mma and TMEM reads as the search kernel.  One CTA. */
 nngp_status nngp_tc_layout_selftest(const float *a, const float *b, int32_t kp, float *d, int32_t *status_flags,
                                     void *stream);
+/* The same for the BF16 operands of the search at d >= 12 (tcgen05.mma kind::f16, K = 16 per
+ * instruction): a and b hold values exactly representable in BF16 (converted with round to
+ * nearest on staging), kp = 16, 32 or 64. */
+nngp_status nngp_tc_layout_selftest_bf16(const float *a, const float *b, int32_t kp, float *d,
+                                         int32_t *status_flags, void *stream);
 
 #ifdef __cplusplus
 }

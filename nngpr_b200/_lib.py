@@ -21,11 +21,12 @@ NNGP_FLAG_FP64_FALLBACK = 8
 
 # every symbol include/nngp_b200.h declares
 EXPORTED = (
-    'nngp_abi_version', 'nngp_last_error', 'nngp_status_string', 'nngp_check_device',
+    'nngp_abi_version', 'nngp_last_error', 'nngp_status_string', 'nngp_check_device', 'nngp_set_wait_limit_ns',
     'nngp_knn_workspace_size_f32', 'nngp_knn_f32', 'nngp_knn_workspace_size_f64', 'nngp_knn_f64',
-    'nngp_loglik_workspace_size', 'nngp_loglik_f32', 'nngp_loglik_f64',
+    'nngp_loglik_workspace_size', 'nngp_loglik_f32', 'nngp_loglik_f64', 'nngp_loglik_fp64_count',
     'nngp_loglik_rows_f32', 'nngp_loglik_rows_f64', 'nngp_loglik_f64_noalloc',
     'nngp_predict_f32', 'nngp_predict_f64', 'nngp_fma_probe', 'nngp_fma_probe_f64', 'nngp_tc_layout_selftest',
+    'nngp_tc_layout_selftest_bf16',
     'nngp_plain_knn_f32', 'nngp_knn_reuse_prepare_f32', 'nngp_knn_reuse_rank_f32',
     'nngp_predict_full_workspace_size', 'nngp_predict_full_f64', 'nngp_sample_full_f64',
     'nngp_predict_cov_full_f64',
@@ -71,6 +72,8 @@ _SIGS = {
     'nngp_knn_f32': ([_vp, _i64, _vp, _i64, _i32, _dp, _i32, _i32, _i32, _i64, _vp, _vp, _vp, _sz, _vp], ctypes.c_int),
     'nngp_knn_f64': ([_vp, _i64, _vp, _i64, _i32, _dp, _i32, _i32, _i32, _i64, _vp, _vp, _vp, _sz, _vp], ctypes.c_int),
     'nngp_loglik_workspace_size': ([_i64, _i32, _i32, _i32, _i32], _sz),
+    'nngp_loglik_fp64_count': ([_vp], _vp),
+    'nngp_set_wait_limit_ns': ([ctypes.c_uint64], ctypes.c_uint64),
     'nngp_loglik_f32': ([_vp, _vp, _i64, _i32, _i32, _vp, _i32, _kp, _i32, _f64, _vp, _vp, _vp, _sz, _vp], ctypes.c_int),
     'nngp_loglik_f64': ([_vp, _vp, _i64, _i32, _i32, _vp, _i32, _kp, _i32, _f64, _vp, _vp, _vp, _sz, _vp], ctypes.c_int),
     'nngp_loglik_rows_f32': ([_vp, _vp, _i64, _i32, _i32, _i64, _i64, _vp, _i32, _kp, _i32, _f64, _vp, _vp, _vp, _sz, _vp],
@@ -83,6 +86,7 @@ _SIGS = {
     'nngp_fma_probe': ([_vp, _i64, _i32, _vp], ctypes.c_int),
     'nngp_fma_probe_f64': ([_vp, _i64, _i32, _vp], ctypes.c_int),
     'nngp_tc_layout_selftest': ([_vp, _vp, _i32, _vp, _vp, _vp], ctypes.c_int),
+    'nngp_tc_layout_selftest_bf16': ([_vp, _vp, _i32, _vp, _vp, _vp], ctypes.c_int),
     'nngp_plain_knn_f32': ([_vp, _i64, _vp, _i64, _i32, _i32, _i32, _i64, _vp, _vp], ctypes.c_int),
     'nngp_predict_full_workspace_size': ([_i64, _i32], ctypes.c_size_t),
     'nngp_predict_full_f64': ([_vp, _vp, _i64, _i64, _i32, _i32, _vp, _i32, ctypes.POINTER(NngpKernel), _i32, _vp,

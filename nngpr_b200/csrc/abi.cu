@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <exception>
 #include <map>
 #include <mutex>
@@ -67,6 +68,13 @@ nngp_status cuda_fail(cudaError_t e, const char *what) {
 
 const char *last_error_cstr() { return g_last_error.c_str(); }
 
+namespace {
+std::atomic<uint64_t> g_wait_limit{kWaitLimitNs};
+}
+
+uint64_t wait_limit_ns() { return g_wait_limit.load(std::memory_order_relaxed); }
+uint64_t set_wait_limit_ns(uint64_t ns) { return g_wait_limit.exchange(ns == 0 ? kWaitLimitNs : ns); }
+
 cudaError_t ensure_smem_limit(const void *fn, int bytes, int carveout) {
     static std::mutex mu;
     static std::map<std::pair<const void *, int>, std::pair<int, int>> done;  // (fn, device) -> (bytes, carveout)
@@ -112,6 +120,8 @@ template <typename F> nngp_status guarded(F &&f) {
 extern "C" {
 
 int32_t nngp_abi_version(void) { return NNGP_ABI_VERSION; }
+
+uint64_t nngp_set_wait_limit_ns(uint64_t ns) { return set_wait_limit_ns(ns); }
 
 const char *nngp_last_error(void) { return last_error_cstr(); }
 
@@ -231,6 +241,11 @@ nngp_status nngp_knn_reuse_rank_f32(const float *x, int64_t n, int32_t d, double
 
 size_t nngp_loglik_workspace_size(int64_t n, int32_t d, int32_t ydim, int32_t m, int32_t n_theta) {
     return loglik_workspace(n, d, ydim, m, n_theta);
+}
+
+const uint64_t *nngp_loglik_fp64_count(const void *workspace) {
+    if (!workspace) return nullptr;
+    return reinterpret_cast<const uint64_t *>(align_up(reinterpret_cast<uintptr_t>(workspace), 256));
 }
 
 nngp_status nngp_loglik_f32(const float *x, const float *y, int64_t n, int32_t d, int32_t ydim, const int32_t *nbr,

@@ -102,15 +102,20 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Bounded wait on an mbarrier phase: false after kWaitLimitNs without completion.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+// Bounded wait on an mbarrier phase: false after limit_ns without completion.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, uint64_t limit_ns = kWaitLimitNs) {
     if (mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = global_timer_ns();
     while (true) {
         if (mbar_try_wait(bar, parity)) return true;
-        if (global_timer_ns() - t0 > kWaitLimitNs) return false;
+        if (global_timer_ns() - t0 > limit_ns) return false;
     }
 }
+
+// Limit of the bounded waits in the search's main loop (a kernel argument; kWaitLimitNs unless
+// nngp_set_wait_limit_ns changed it to exercise the failure path).  The waits that drain a
+// CTA's own copies and MMAs before it frees TMEM always use kWaitLimitNs.  Defined in abi.cu.
+uint64_t wait_limit_ns();
 
 // Global -> shared bulk copy completing on `bar` (16-byte aligned addresses, bytes % 16 == 0).
 __device__ __forceinline__ void tma_bulk_g2s(void *dst_smem, const void *src_gmem, uint32_t bytes, uint64_t *bar) {

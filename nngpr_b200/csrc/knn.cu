@@ -729,6 +729,7 @@ nngp_status knn_impl(const T *ref, int64_t n_ref, const T *query, int64_t n_quer
             const unsigned int *r2_c = r2;
             const int32_t *none = nullptr;
             const int64_t *no_sizes = nullptr;
+            const uint64_t wait_ns = wait_limit_ns();
             // cut_arg / out_base: rows of point indices use cut 0 (limit = the point's index) and
             // write the row of point i at out[(i - out_base) * m]
             auto launch = [&](const unsigned char *tiles_c, int64_t items_bound, const int32_t *rows_perm,
@@ -749,7 +750,7 @@ nngp_status knn_impl(const T *ref, int64_t n_ref, const T *query, int64_t n_quer
                                 (void *)&items,    (void *)&ref_perm, (void *)&tile_off, (void *)&tile_list,
                                 (void *)&counter,  (void *)&n_query,  (void *)&n_ref,      (void *)&has_cut,
                                 (void *)&cut_arg,  (void *)&m,        (void *)&out_base,   (void *)&out,
-                                (void *)&flags};
+                                (void *)&flags,    (void *)&wait_ns};
                 NNGP_CUDA_TRY(cudaLaunchKernel(reinterpret_cast<const void *>(p.tv.fn), dim3(grid), dim3(p.tv.threads),
                                                args, (size_t)p.tv.smem, stream));
                 return NNGP_OK;

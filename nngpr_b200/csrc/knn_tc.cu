@@ -61,27 +61,41 @@ constexpr int DRAIN_AT = 32;   // queued entries that trigger a drain at the end
 constexpr int QCAP = 64;       // candidate queue entries per epilogue warp (a drain runs before an
                                // iteration that could overflow it; 64 leaves room for a third stage)
 constexpr uint32_t kSelftestCols = 2 * RT;  // TMEM columns of the layout self-test
-constexpr float kEpsTc = 1.52587890625e-05f;       // 2^-16
+constexpr float kEpsTc = 1.52587890625e-05f;       // 2^-16: TF32 x3 split
+constexpr float kEpsBf = 6.103515625e-05f;         // 2^-14: BF16 x3 split
 constexpr float kPadNorm = 1.7014118346046923e38f;  // 2^127: padded refs never pass a finite screen
 // list key: FP32 distance bits (non-negative, so integer order = float order) << 32 | index;
 // an empty slot is (+inf, 0xffffffff), larger than every real entry, read back as index -1
 constexpr uint64_t kEmptyKey = (uint64_t)0x7F800000u << 32 | 0xFFFFFFFFu;
 
 // D: padded dimension; QTILES: 128-query tiles per work item (their MMAs share each staged ref
-// tile; 4 epilogue warps per query tile, one per TMEM lane quadrant)
+// tile; 4 epilogue warps per query tile, one per TMEM lane quadrant).
+// Operands: D <= 8 a TF32 x3 split (kind::tf32, K = 8 per MMA, 4-byte elements); D >= 12 a BF16 x3
+// split (kind::f16, K = 16 per MMA, 2-byte elements): half the bytes per ref tile and, at the
+// tensor pipe's doubled BF16 rate, 4 instead of 7 MMA steps per tile at D = 16.
 template <int D, int QTILES>
 struct Cfg {
+    static constexpr bool BF16 = false && D >= 12;
+    static constexpr int ESZ = BF16 ? 2 : 4;        // operand element bytes
+    static constexpr int EPC = 16 / ESZ;            // elements per 16-byte core-matrix row
+    static constexpr int KMMA = BF16 ? 16 : 8;      // UMMA K of one instruction
+    static constexpr float EPS = BF16 ? kEpsBf : kEpsTc;
     static constexpr int EPI_WARPS = 4 * QTILES;
     static constexpr int THREADS = (EPI_WARPS + 1) * 32;
     static constexpr int ROWS = QT * QTILES;        // queries per work item
     static constexpr int U = D + 1;                 // coordinates + the norm column
-    static constexpr int KP = (3 * U + 7) / 8 * 8;  // split operand width (tf32), multiple of 8
-    static constexpr int NMMA = KP / 8;             // UMMA K = 8 for tf32
+    static constexpr int KP = (3 * U + KMMA - 1) / KMMA * KMMA;  // split operand width
+    static constexpr int NMMA = KP / KMMA;
     static constexpr int DP = (D + 3) / 4 * 4;      // exact-coordinate row length
-    static constexpr int OP_BYTES = RT * KP * 4;    // B operand block of a ref tile
+    static constexpr int OP_BYTES = RT * KP * ESZ;  // B operand block of a ref tile
     static constexpr int EX_BYTES = RT * DP * 4;    // exact coordinates of a ref tile
-    static constexpr int STAGE_BYTES = OP_BYTES + EX_BYTES;
-    static constexpr int A_TILE = QT * KP * 4;      // query operand of one query tile
+    // where a staged tile keeps its refs' point indices: the spare last slot of each exact-coordinate
+    // row when DP > D (1), a block after the coordinates for the BF16 shapes (2); D = 4 and 8 read
+    // them from global memory (0: a block would cost those shapes a pipeline stage)
+    static constexpr int IX_MODE = DP > D ? 1 : (BF16 ? 2 : 0);
+    static constexpr int IX_BYTES = IX_MODE == 2 ? RT * 4 : 0;
+    static constexpr int STAGE_BYTES = OP_BYTES + EX_BYTES + IX_BYTES;
+    static constexpr int A_TILE = QT * KP * ESZ;    // query operand of one query tile
     static constexpr int A_BYTES = A_TILE * QTILES;
     static constexpr int LIST_BYTES = ROWS * HS * 8;  // one heap of keys per query
     static constexpr int QUEUE_BYTES = EPI_WARPS * QCAP * (8 + 1);  // key + row
@@ -109,15 +123,50 @@ struct Cfg {
     static constexpr uint32_t B_LBO = (RT / 8) * 128;
 };
 
-// byte offset of element (row, k) of a K-major, no-swizzle UMMA operand with `rows` rows
+// byte offset of element (row, k) of a K-major, no-swizzle UMMA operand with `rows` rows and
+// ESZ-byte elements (core matrices of 8 rows x 16 bytes)
+template <int ESZ = 4>
 __host__ __device__ __forceinline__ uint32_t op_offset(int row, int k, int rows) {
-    return (uint32_t)((k >> 2) * (rows / 8) * 128 + (row >> 3) * 128 + (row & 7) * 16 + (k & 3) * 4);
+    constexpr int EPC = 16 / ESZ;
+    return (uint32_t)((k / EPC) * (rows / 8) * 128 + (row >> 3) * 128 + (row & 7) * 16 + (k % EPC) * ESZ);
 }
 
 __device__ __forceinline__ float tf32_round(float x) {
     uint32_t r;
     asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
     return __uint_as_float(r);
+}
+
+// x rounded to the nearest BF16 (ties to even), as its 16-bit pattern and as a float
+__device__ __forceinline__ uint16_t bf16_bits(float x) {
+    uint16_t r;
+    asm("cvt.rn.bf16.f32 %0, %1;" : "=h"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float bf16_value(uint16_t b) { return __uint_as_float((uint32_t)b << 16); }
+
+// Element k of one row of a split operand: blocks [hi | hi | lo] (query side, lo_block = 2) or
+// [hi | lo | hi] (ref side, lo_block = 1) of the U values v, then zeros; the products
+// A' B'^T = a_hi b_hi + a_hi b_lo + a_lo b_hi.  Stored at `dst` as TF32 (float) or BF16.
+template <bool BF16, int U>
+__device__ __forceinline__ void put_split(unsigned char *dst_row_base, int row, int rows, int k, int lo_block,
+                                          const float (&v)[U]) {
+    float val = 0.f;
+    const int blk = k / U, f = k - blk * U;
+    if constexpr (BF16) {
+        uint16_t bits = 0;
+        if (blk < 3) {
+            const uint16_t hi = bf16_bits(v[f]);
+            bits = (blk == lo_block) ? bf16_bits(v[f] - bf16_value(hi)) : hi;
+        }
+        *reinterpret_cast<uint16_t *>(dst_row_base + op_offset<2>(row, k, rows)) = bits;
+    } else {
+        if (blk < 3) {
+            const float hi = tf32_round(v[f]);
+            val = (blk == lo_block) ? (v[f] - hi) : hi;
+        }
+        *reinterpret_cast<float *>(dst_row_base + op_offset<4>(row, k, rows)) = val;
+    }
 }
 
 __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
@@ -129,9 +178,12 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint3
     return d;                // base offset 0, lbo mode 0, layout SWIZZLE_NONE
 }
 
-// instruction descriptor: F32 accumulate, TF32 A and B, both K-major, N = RT, M = QT
+// instruction descriptors: F32 accumulate, both operands K-major, N = RT, M = QT; A and B TF32
+// (kind::tf32, format 2) or BF16 (kind::f16, format 1) -- A and B of one type
 constexpr uint32_t kIdesc =
     (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(RT >> 3) << 17) | ((uint32_t)(QT >> 4) << 24);
+constexpr uint32_t kIdescBf16 =
+    (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(RT >> 3) << 17) | ((uint32_t)(QT >> 4) << 24);
 
 __device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
     asm volatile(
@@ -140,6 +192,21 @@ __device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t adesc, uint64
         "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
         "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0)
         : "memory");
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(kIdescBf16), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0)
+        : "memory");
+}
+
+template <bool BF16>
+__device__ __forceinline__ void mma_op(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+    if constexpr (BF16) mma_bf16(tmem_d, adesc, bdesc, accumulate);
+    else mma_tf32(tmem_d, adesc, bdesc, accumulate);
 }
 
 __device__ __forceinline__ void mma_commit(uint64_t *bar) {
@@ -209,8 +276,9 @@ __device__ __forceinline__ float min3f(float a, float b, float c) {
     return r;
 }
 
-// Ref tiles in global memory: per tile [B' operand block (UMMA layout) | exact coordinates (RT x DP)].
-// xs: scaled refs (n_pad x DP, zero padded); acc: per-feature sums for the centre.
+// Ref tiles in global memory: per tile [B' operand block (UMMA layout) | exact coordinates (RT x DP)
+// | point indices (RT int32, -1 for padding)].  xs: scaled refs (n_pad x DP, zero padded); acc:
+// per-feature sums for the centre.
 template <int D>
 __global__ void build_tc_tiles_kernel(const float *__restrict__ xs, int64_t n, int64_t n_pad,
                                       const double *__restrict__ acc, const int32_t *__restrict__ perm,
@@ -245,19 +313,13 @@ __global__ void build_tc_tiles_kernel(const float *__restrict__ xs, int64_t n, i
             for (int f = 0; f < D; ++f) b[f] = 0.f;
             b[D] = kPadNorm;
         }
-        float *op = reinterpret_cast<float *>(base);
-        for (int k = 0; k < C::KP; ++k) {
-            float v = 0.f;
-            const int blk = k / C::U, f = k - blk * C::U;
-            if (blk < 3) {
-                const float hi = tf32_round(b[f]);
-                v = (blk == 1) ? (b[f] - hi) : hi;  // [b_hi | b_lo | b_hi]
-            }
-            op[op_offset(row, k, RT) / 4] = v;
-        }
+        for (int k = 0; k < C::KP; ++k) put_split<C::BF16, C::U>(base, row, RT, k, 1, b);  // [b_hi | b_lo | b_hi]
+        const int32_t pidx = i < n ? (int32_t)(perm ? (int64_t)perm[i] : i) : -1;
+        if (C::IX_MODE == 1) ex[C::DP - 1] = __int_as_float(pidx);
         float *exo = reinterpret_cast<float *>(base + C::OP_BYTES) + row * C::DP;
 #pragma unroll
         for (int k = 0; k < C::DP; ++k) exo[k] = ex[k];
+        if (C::IX_MODE == 2) reinterpret_cast<int32_t *>(base + C::OP_BYTES + C::EX_BYTES)[row] = pidx;
     }
     mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, 16));
     mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, 8));
@@ -284,7 +346,7 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
                                                          int *__restrict__ work_counter, int64_t n_query,
                                                          int64_t n_ref, int has_cut, int64_t cut, int m,
                                                          int64_t out_base, int32_t *__restrict__ out,
-                                                         int32_t *__restrict__ flags) {
+                                                         int32_t *__restrict__ flags, uint64_t wait_ns) {
     using C = Cfg<D, QTILES>;
     constexpr int S = C::STAGES;
     constexpr int EPI_WARPS = C::EPI_WARPS;
@@ -314,7 +376,8 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
     // device or {0, n_query, ceil(n_query / ROWS)}; work item g is positions
     // [row_off[g], row_off[g + 1]) (at most ROWS) or ROWS consecutive positions.  Refs: with
     // tile_list (pruned search), group g streams the tiles tile_list[tile_off[g] .. tile_off[g + 1])
-    // of tiles_g, whose positions map to points through ref_perm, and j < limit(i) is checked per
+    // of tiles_g (each staged tile carries its refs' point indices; ref_perm is the same map in
+    // global memory, kept for the host's bookkeeping), and j < limit(i) is checked per
     // candidate; otherwise refs in index order up to the largest limit of the group's rows (the
     // rows of a group ascend).  Items: see TcItems.
     const bool pruned = tile_list != nullptr;
@@ -351,6 +414,7 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
     uint32_t it = 0;      // work items this CTA has processed (phase of a_ready)
     bool aborted = false;
     uint32_t tma_issued = 0, tma_landed = 0;  // producer lane: copies issued / waited for (drain on abort)
+    uint32_t mma_issued = 0;                  // producer lane: tiles whose MMAs were issued and committed
 
     auto limit_of = [&](int64_t qq) -> int64_t {
         if (!has_cut) return n_ref;
@@ -391,11 +455,11 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
 
         if (producer_warp) {
             if (lane == 0) {
-                if (!mbar_wait_bounded(a_ready, it & 1)) aborted = true;  // query operand of this item
+                if (!mbar_wait_bounded(a_ready, it & 1, wait_ns)) aborted = true;  // query operand of this item
                 const uint32_t G = g_tile;
                 auto wait_empty = [&](uint32_t g) -> bool {
                     const uint32_t k = g / S;
-                    return mbar_wait_bounded(&b_empty[g % S], (k & 1) ^ 1);
+                    return mbar_wait_bounded(&b_empty[g % S], (k & 1) ^ 1, wait_ns);
                 };
                 auto issue_tma = [&](uint32_t g) {
                     const uint32_t s = g % S;
@@ -415,12 +479,12 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
                 for (uint32_t t = 0; t < ntiles && !aborted; ++t) {
                     const uint32_t g = G + t;
                     const uint32_t s = g % S, b = g % C::NBUF, use = g / C::NBUF;
-                    if (!mbar_wait_bounded(&b_full[s], (g / S) & 1)) {
+                    if (!mbar_wait_bounded(&b_full[s], (g / S) & 1, wait_ns)) {
                         aborted = true;
                         break;
                     }
                     tma_landed = g + 1;
-                    if (!mbar_wait_bounded(&t_empty[b], (use & 1) ^ 1)) {
+                    if (!mbar_wait_bounded(&t_empty[b], (use & 1) ^ 1, wait_ns)) {
                         aborted = true;
                         break;
                     }
@@ -431,14 +495,15 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
                         const uint32_t d_tmem = tmem_base + b * C::BUF_COLS + qt * RT;
                         const uint32_t aq = a_addr + qt * C::A_TILE;
 #pragma unroll
-                        for (int i = 0; i < C::NMMA; ++i) {
+                        for (int i = 0; i < C::NMMA; ++i) {  // one MMA spans two 16-byte K chunks
                             const uint64_t ad = smem_desc(aq + i * 2 * C::A_LBO, C::A_LBO, 128);
                             const uint64_t bd = smem_desc(b_addr + i * 2 * C::B_LBO, C::B_LBO, 128);
-                            mma_tf32(d_tmem, ad, bd, i > 0 ? 1u : 0u);
+                            mma_op<C::BF16>(d_tmem, ad, bd, i > 0 ? 1u : 0u);
                         }
                     }
                     mma_commit(&t_full[b]);
                     mma_commit(&b_empty[s]);
+                    mma_issued = g + 1;
                     const uint32_t gr = g - 1 + S;  // refill the stage that MMA g-1 used
                     if (t > 0 && gr < G + ntiles) {
                         if (!wait_empty(gr)) {
@@ -469,21 +534,13 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
                 nq = fmaf(qc[f], qc[f], nq);
             }
             const float span = sqrtf(nq) * 1.0001f + rmax;
-            const float eps = kEpsTc * span * span;
+            const float eps = C::EPS * span * span;
             {  // query operand row: A' = [a_hi | a_hi | a_lo], a = [qc, 1]
                 float a[C::U];
 #pragma unroll
                 for (int f = 0; f < D; ++f) a[f] = active ? qc[f] : 0.f;
                 a[D] = active ? 1.f : 0.f;
-                for (int k = 0; k < C::KP; ++k) {
-                    float v = 0.f;
-                    const int blk = k / C::U, f = k - blk * C::U;
-                    if (blk < 3) {
-                        const float hi = tf32_round(a[f]);
-                        v = (blk == 2) ? (a[f] - hi) : hi;
-                    }
-                    *reinterpret_cast<float *>(sA + qtw * C::A_TILE + op_offset(quad * 32 + lane, k, QT)) = v;
-                }
+                for (int k = 0; k < C::KP; ++k) put_split<C::BF16, C::U>(sA + qtw * C::A_TILE, quad * 32 + lane, QT, k, 2, a);
             }
             fence_proxy_async_smem();
             mbar_arrive(a_ready);
@@ -531,13 +588,14 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
             for (uint32_t t = 0; t < ntiles; ++t) {
                 const uint32_t g = G + t;
                 const uint32_t s = g % S, b = g % C::NBUF;
-                if (!mbar_wait_bounded(&t_full[b], (g / C::NBUF) & 1)) aborted = true;
+                if (!mbar_wait_bounded(&t_full[b], (g / C::NBUF) & 1, wait_ns)) aborted = true;
                 if (__any_sync(FULL, aborted)) {
                     aborted = true;
                     break;
                 }
                 tc_fence_after();
                 const float *exs = reinterpret_cast<const float *>(sB + s * C::STAGE_BYTES + C::OP_BYTES);
+                const int32_t *ixs = reinterpret_cast<const int32_t *>(sB + s * C::STAGE_BYTES + C::OP_BYTES + C::EX_BYTES);
                 const int64_t j0 = (pruned ? (int64_t)tl[t] : (int64_t)(tfirst + t)) * RT;  // first ref position of the tile
                 const uint32_t taddr = tmem_base + ((uint32_t)(quad * 32) << 16) + b * C::BUF_COLS + qtw * RT;
                 // screen one 32-column chunk (scores in v): this row's candidate mask, 0 when no row
@@ -629,7 +687,12 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
                             const float tf = sub_rn(rv[f], qo[f]);
                             d2 = add_rn(d2, mul_rn(tf, tf));
                         }
-                        const int64_t jo = pruned ? (int64_t)ref_perm[j0 + col] : j0 + col;  // the ref's index
+                        int64_t jo = j0 + col;  // the ref's point index
+                        if (pruned) {
+                            if constexpr (C::IX_MODE == 1) jo = __float_as_int(rv[C::DP - 1]);
+                            else if constexpr (C::IX_MODE == 2) jo = ixs[col];
+                            else jo = ref_perm[j0 + col];
+                        }
                         keep = d2 <= worst && jo < limit;  // NaN never kept
                         key = (uint64_t)__float_as_uint(d2) << 32 | (uint32_t)jo;
                     }
@@ -676,14 +739,17 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
         __syncthreads();
     }
 
-    // teardown: report a timeout, let copies and MMAs this CTA issued finish (bounded), free TMEM
+    // teardown: report a timeout, let copies and MMAs this CTA issued finish (bounded by the
+    // full kWaitLimitNs whatever wait_ns is), free TMEM
     if ((aborted || *s_abort) && threadIdx.x == 0) flag_or(flags, NNGP_FLAG_TIMEOUT);
     if (producer_warp && lane == 0 && (aborted || *s_abort)) {
         // copies issued but never waited for: let them land before the CTA's shared memory goes
         for (uint32_t g = tma_landed; g < tma_issued; ++g) mbar_wait_bounded(&b_full[g % S], (g / S) & 1);
-        // MMAs in flight: the last t_full phase of each accumulator buffer
-        for (uint32_t i = 1; i <= (uint32_t)C::NBUF && i <= g_tile; ++i) {
-            const uint32_t g = g_tile - i;
+        // MMAs in flight: a commit tracks every earlier tcgen05 operation of this thread, so the
+        // phase of the last committed tile covers them all (a tile whose MMAs were never issued
+        // has no phase to wait for: g_tile counts an aborted item's tiles in full)
+        if (mma_issued > 0) {
+            const uint32_t g = mma_issued - 1;
             mbar_wait_bounded(&t_full[g % C::NBUF], (g / C::NBUF) & 1);
         }
     }
@@ -696,21 +762,28 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
 }
 
 // Self-test of the UMMA operand layout: D = A B^T for A, B given row-major (128 x KP), through
-// the same shared-memory layout, descriptors, tcgen05.mma and tcgen05.ld path as the search.
-template <int KP>
+// the same shared-memory layout, descriptors, tcgen05.mma and tcgen05.ld path as the search
+// (TF32 operands, or BF16 operands converted from A and B when BF16).
+template <int KP, bool BF16 = false>
 __global__ void __launch_bounds__(THREADS) tc_layout_selftest_kernel(const float *__restrict__ a,
                                                                     const float *__restrict__ b,
                                                                     float *__restrict__ d,
                                                                     int32_t *__restrict__ flags) {
-    __shared__ __align__(1024) unsigned char sA[QT * KP * 4];
-    __shared__ __align__(1024) unsigned char sB[RT * KP * 4];
+    constexpr int ESZ = BF16 ? 2 : 4;
+    constexpr int KMMA = BF16 ? 16 : 8;
+    __shared__ __align__(1024) unsigned char sA[QT * KP * ESZ];
+    __shared__ __align__(1024) unsigned char sB[RT * KP * ESZ];
     __shared__ __align__(8) uint64_t bar;
     __shared__ uint32_t tmem_slot;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int e = threadIdx.x; e < QT * KP; e += blockDim.x)
-        *reinterpret_cast<float *>(sA + op_offset(e / KP, e % KP, QT)) = a[e];
-    for (int e = threadIdx.x; e < RT * KP; e += blockDim.x)
-        *reinterpret_cast<float *>(sB + op_offset(e / KP, e % KP, RT)) = b[e];
+    for (int e = threadIdx.x; e < QT * KP; e += blockDim.x) {
+        if constexpr (BF16) *reinterpret_cast<uint16_t *>(sA + op_offset<2>(e / KP, e % KP, QT)) = bf16_bits(a[e]);
+        else *reinterpret_cast<float *>(sA + op_offset<4>(e / KP, e % KP, QT)) = a[e];
+    }
+    for (int e = threadIdx.x; e < RT * KP; e += blockDim.x) {
+        if constexpr (BF16) *reinterpret_cast<uint16_t *>(sB + op_offset<2>(e / KP, e % KP, RT)) = bf16_bits(b[e]);
+        else *reinterpret_cast<float *>(sB + op_offset<4>(e / KP, e % KP, RT)) = b[e];
+    }
     fence_proxy_async_smem();
     if (threadIdx.x == 0) {
         mbar_init(&bar, 1);
@@ -728,9 +801,9 @@ __global__ void __launch_bounds__(THREADS) tc_layout_selftest_kernel(const float
     if (warp == 4 && lane == 0) {
         constexpr uint32_t A_LBO = (QT / 8) * 128, B_LBO = (RT / 8) * 128;
 #pragma unroll
-        for (int i = 0; i < KP / 8; ++i)
-            mma_tf32(tmem_base, smem_desc(smem_addr(sA) + i * 2 * A_LBO, A_LBO, 128),
-                     smem_desc(smem_addr(sB) + i * 2 * B_LBO, B_LBO, 128), i > 0 ? 1u : 0u);
+        for (int i = 0; i < KP / KMMA; ++i)
+            mma_op<BF16>(tmem_base, smem_desc(smem_addr(sA) + i * 2 * A_LBO, A_LBO, 128),
+                         smem_desc(smem_addr(sB) + i * 2 * B_LBO, B_LBO, 128), i > 0 ? 1u : 0u);
         mma_commit(&bar);
     }
     const bool ok = mbar_wait_bounded(&bar, 0);
@@ -802,6 +875,22 @@ extern "C" nngp_status nngp_tc_layout_selftest(const float *a, const float *b, i
         case 16: tc::tc_layout_selftest_kernel<16><<<1, tc::THREADS, 0, st>>>(a, b, d, flags); break;
         case 32: tc::tc_layout_selftest_kernel<32><<<1, tc::THREADS, 0, st>>>(a, b, d, flags); break;
         default: return fail(NNGP_ERR_UNSUPPORTED, "tc_layout_selftest: kp must be 8, 16 or 32");
+    }
+    NNGP_CUDA_TRY(cudaGetLastError());
+    return NNGP_OK;
+}
+
+extern "C" nngp_status nngp_tc_layout_selftest_bf16(const float *a, const float *b, int32_t kp, float *d,
+                                                    int32_t *flags, void *stream) {
+    using namespace nngp;
+    set_error("");
+    if (!a || !b || !d) return fail(NNGP_ERR_INVALID_ARGUMENT, "tc_layout_selftest_bf16: null pointer");
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    switch (kp) {
+        case 16: tc::tc_layout_selftest_kernel<16, true><<<1, tc::THREADS, 0, st>>>(a, b, d, flags); break;
+        case 32: tc::tc_layout_selftest_kernel<32, true><<<1, tc::THREADS, 0, st>>>(a, b, d, flags); break;
+        case 64: tc::tc_layout_selftest_kernel<64, true><<<1, tc::THREADS, 0, st>>>(a, b, d, flags); break;
+        default: return fail(NNGP_ERR_UNSUPPORTED, "tc_layout_selftest_bf16: kp must be 16, 32 or 64");
     }
     NNGP_CUDA_TRY(cudaGetLastError());
     return NNGP_OK;

@@ -22,7 +22,7 @@ struct TcItems {
 
 using TcFn = void (*)(const unsigned char *, const float *, const double *, const unsigned int *, const float *,
                       const int32_t *, const int32_t *, const int64_t *, TcItems, const int32_t *, const int32_t *,
-                      const int32_t *, int *, int64_t, int64_t, int, int64_t, int, int64_t, int32_t *, int32_t *);
+                      const int32_t *, int *, int64_t, int64_t, int, int64_t, int, int64_t, int32_t *, int32_t *, uint64_t);
 // build(xs, n, n_pad, acc, perm, tiles, r2max): tile position i holds point perm[i] (i when perm is null)
 using TcBuildFn = void (*)(const float *, int64_t, int64_t, const double *, const int32_t *, unsigned char *,
                            unsigned int *);

@@ -54,6 +54,7 @@ struct LocalArgs {
     int64_t alpha_below;  // alpha goes on the diagonal slots of neighbours with index < alpha_below
     int weights_out;      // predict: write w = K_nn^-1 k (a.m per point) to `mean` instead of the mean
     int idx_rbf, idx_const, idx_noise, idx_ls, n_theta;
+    unsigned long long *fp64_count;  // systems re-solved in FP64 are added here (may be null)
     double inv_ls[kMaxDimLocal];
 };
 
@@ -404,6 +405,7 @@ __global__ void __launch_bounds__(kLocWarps * 32, 3) local_warp_kernel(
     __syncwarp();
     double ll_acc = 0.0;
     bool used_fp64 = false;
+    unsigned long long n_fp64 = 0;
     const int64_t nwarps = (int64_t)gridDim.x * kLocWarps;
     for (int64_t p = (int64_t)blockIdx.x * kLocWarps + warp; p < a.n_points; p += nwarps) {
         bool done = false;
@@ -412,12 +414,18 @@ __global__ void __launch_bounds__(kLocWarps * 32, 3) local_warp_kernel(
                                                        var, flags);
         }
         if (!done) {
-            if constexpr (std::is_same<TIn, float>::value) used_fp64 = true;
+            if constexpr (std::is_same<TIn, float>::value) {
+                used_fp64 = true;
+                ++n_fp64;
+            }
             warp_system<double, TIn, GRAD, PRED, MATERN>(a, p, lane, x_ref, y_ref, x_pt, y_pt, nbr, wsm, ll_acc, mean, var,
                                                  flags);
         }
     }
-    if (used_fp64 && lane == 0) flag_or(flags, NNGP_FLAG_FP64_FALLBACK);
+    if (used_fp64 && lane == 0) {
+        flag_or(flags, NNGP_FLAG_FP64_FALLBACK);
+        if (a.fp64_count) atomicAdd(a.fp64_count, n_fp64);
+    }
     if (PRED) return;
     // CTA reduction in fixed order: warp w's totals -> slot w, then warp 0 sums
     __shared__ double red[kLocWarps];
@@ -740,6 +748,8 @@ int num_sms() {
 
 size_t block_smem_limit() { return 227 * 1024; }
 
+constexpr size_t kCountBytes = 256;  // head of the log-likelihood workspace: the FP64 re-solve count
+
 struct LocalPlan {
     bool warp = true;
     int grid = 0;
@@ -761,7 +771,8 @@ LocalPlan plan_local(int64_t n_points, int d, int m, int n_theta, bool grad) {
         p.smem = BlockSmem::make(m, d).total;
         p.grid = (int)std::max<int64_t>(1, std::min<int64_t>(n_points, (int64_t)sms * 2));
     }
-    p.ws_bytes = align_up((size_t)p.grid * p.nt * sizeof(double), 256) + 256;
+    // [256 bytes: the count of FP64 re-solves | per-CTA partials], plus 256 of alignment slack
+    p.ws_bytes = kCountBytes + align_up((size_t)p.grid * p.nt * sizeof(double), 256) + 256;
     return p;
 }
 
@@ -793,6 +804,7 @@ nngp_status fill_args(LocalArgs &a, const nngp_kernel *k, int d, int ydim, int m
     a.ard = k->n_ls == d && d > 1;
     a.alpha_below = n_rows;
     a.weights_out = 0;
+    a.fp64_count = nullptr;
     if (k->family < NNGP_FAMILY_RBF || k->family > NNGP_FAMILY_MATERN52)
         return fail(NNGP_ERR_INVALID_ARGUMENT, "kernel family must be one of NNGP_FAMILY_*");
     a.family = k->family;
@@ -847,12 +859,18 @@ nngp_status loglik_impl(const TIn *x, const TIn *y, int64_t n, int d, int ydim, 
     const int nt = 1 + (grad ? a.n_theta : 0);
     if (rows == 0) {
         NNGP_CUDA_TRY(cudaMemsetAsync(out, 0, nt * sizeof(double), stream));
+        if (ws && ws_bytes >= kCountBytes + 256)
+            NNGP_CUDA_TRY(cudaMemsetAsync(reinterpret_cast<void *>(align_up(reinterpret_cast<uintptr_t>(ws), 256)), 0,
+                                          sizeof(unsigned long long), stream));
         return NNGP_OK;
     }
     if (!x || !y || (m > 0 && !nbr)) return fail(NNGP_ERR_INVALID_ARGUMENT, "loglik: null input pointer");
     const LocalPlan pl = plan_local(rows, d, m, a.n_theta, grad);
     if (!ws || ws_bytes < pl.ws_bytes) return fail(NNGP_ERR_WORKSPACE, "loglik: workspace missing or too small");
-    double *block_out = reinterpret_cast<double *>(align_up(reinterpret_cast<uintptr_t>(ws), 256));
+    unsigned char *head = reinterpret_cast<unsigned char *>(align_up(reinterpret_cast<uintptr_t>(ws), 256));
+    a.fp64_count = reinterpret_cast<unsigned long long *>(head);
+    NNGP_CUDA_TRY(cudaMemsetAsync(a.fp64_count, 0, sizeof(unsigned long long), stream));
+    double *block_out = reinterpret_cast<double *>(head + kCountBytes);
     const TIn *x_pt = x + row_begin * d;
     const TIn *y_pt = y + row_begin * ydim;
     if (grad)

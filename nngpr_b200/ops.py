@@ -243,14 +243,16 @@ def _kernel_struct(p: RbfParams, alpha: float, d: int, keep: list) -> _lib.NngpK
 
 
 def loglik(x: torch.Tensor, y: torch.Tensor, nbr: torch.Tensor, p: RbfParams, alpha: float,
-           eval_gradient: bool, pivot_tol: float = DEFAULT_PIVOT_TOL,
+           eval_gradient: bool, pivot_tol: float | None = DEFAULT_PIVOT_TOL,
            flags: torch.Tensor | None = None, out: torch.Tensor | None = None,
-           row_begin: int = 0) -> torch.Tensor:
+           row_begin: int = 0, stats: dict | None = None) -> torch.Tensor:
     """Fit-step log-likelihood (and gradient) on the device: float64 tensor ``[lml, grad...]``.
 
     ``x (n, d)``, ``y (n, ydim)`` of one dtype (float32: FP32 systems with FP64 fallback;
     float64: FP64), ``nbr (rows, m)`` int32 without the self column, for the points
-    ``[row_begin, row_begin + rows)`` (default: all points).
+    ``[row_begin, row_begin + rows)`` (default: all points).  With a ``stats`` dict,
+    ``stats['fp64_systems']`` receives a device int64 0-d tensor: the systems this call re-solved
+    in FP64 (``nngp_loglik_fp64_count``).
     """
     _check_tensor(x, 'x')
     _check_tensor(y, 'y')
@@ -274,13 +276,17 @@ def loglik(x: torch.Tensor, y: torch.Tensor, nbr: torch.Tensor, p: RbfParams, al
     ws = torch.empty(ws_bytes, dtype=torch.uint8, device=x.device)
     fn = L.nngp_loglik_rows_f64 if x.dtype == torch.float64 else L.nngp_loglik_rows_f32
     st = fn(_ptr(x), _ptr(y2), n, d, ydim, int(row_begin), rows, _ptr(nbr), m, ctypes.byref(k),
-            int(bool(eval_gradient)), float(pivot_tol), _ptr(out), _ptr(flags), _ptr(ws), ws_bytes, _stream())
+            int(bool(eval_gradient)), float(DEFAULT_PIVOT_TOL if pivot_tol is None else pivot_tol), _ptr(out),
+            _ptr(flags), _ptr(ws), ws_bytes, _stream())
     _lib.check(st, 'nngp_loglik')
+    if stats is not None:
+        off = int(L.nngp_loglik_fp64_count(_ptr(ws))) - ws.data_ptr()
+        stats['fp64_systems'] = ws[off:off + 8].view(torch.int64)[0]
     return out
 
 
 def predict(x_train: torch.Tensor, y_train: torch.Tensor, x_query: torch.Tensor, nbr: torch.Tensor,
-            p: RbfParams, alpha: float, pivot_tol: float = DEFAULT_PIVOT_TOL,
+            p: RbfParams, alpha: float, pivot_tol: float | None = DEFAULT_PIVOT_TOL,
             flags: torch.Tensor | None = None):
     """Predictive mean ``(nq, ydim)`` and variance ``(nq,)`` conditioned on the training set."""
     for t, nm in ((x_train, 'x_train'), (y_train, 'y_train'), (x_query, 'x_query')):
@@ -302,6 +308,7 @@ def predict(x_train: torch.Tensor, y_train: torch.Tensor, x_query: torch.Tensor,
     L = _lib.lib()
     fn = L.nngp_predict_f64 if x_query.dtype == torch.float64 else L.nngp_predict_f32
     st = fn(_ptr(x_train), _ptr(y2), nt, _ptr(x_query), nq, d, ydim, _ptr(nbr), m, ctypes.byref(k),
-            float(pivot_tol), _ptr(mean), _ptr(var), _ptr(flags), _stream())
+            float(DEFAULT_PIVOT_TOL if pivot_tol is None else pivot_tol), _ptr(mean), _ptr(var), _ptr(flags),
+            _stream())
     _lib.check(st, 'nngp_predict')
     return mean, var

@@ -15,8 +15,12 @@ resident and serves a stream of predict requests of uneven sizes:
   slot's stream, between an H2D copy of the batch and a D2H copy of its results (pinned host
   buffers of the slot);
 * several slots are in flight at once on their own streams, so requests that arrive while
-  others run are admitted as soon as a slot is free and their work overlaps on the device; the
-  number of slots is bounded by the free device memory at start-up;
+  others run are admitted as soon as a slot is free and their work overlaps on the device.
+  Slots are admitted by free device memory: the server starts with ``min_slots``; while requests
+  wait and every slot is busy it adds a slot (its graphs captured on its own stream, all of its
+  buckets sharing one memory pool, since a slot runs one batch at a time) whenever the free
+  device memory, less ``reserve_bytes``, still holds one slot's footprint and the total stays
+  within ``memory_budget``, up to ``max_slots``;
 * a completion thread polls the batches' events, in any order, scatters the rows of each
   finished batch to their requests and completes a request's future when all its rows are back.
 
@@ -77,13 +81,16 @@ class PredictServer:
     """Serve ``predict(X, return_std=True)`` of a fitted :class:`nngpr_b200.B200Nngpr`.
 
     ``buckets``: batch sizes (query points) with a captured CUDA graph each; the largest is the
-    most points one batch takes.  ``slots``: batches in flight at most (lowered when the free
-    device memory does not hold that many).  ``use_graphs=False`` launches the kernels directly
-    (same results; for comparison).
+    most points one batch takes.  ``slots``: batches in flight at most (``max_slots``);
+    ``min_slots`` are created at start-up, the others when requests wait and the free device
+    memory holds them (``memory_budget`` bytes at most for all slots; default ``memory_fraction``
+    of the free memory at start-up; ``reserve_bytes`` always left free).  ``use_graphs=False``
+    launches the kernels directly (same results; for comparison).
     """
 
     def __init__(self, gpr, buckets=DEFAULT_BUCKETS, slots: int = 4, use_graphs: bool = True,
-                 memory_fraction: float = 0.5, small_points: int = 4096):
+                 memory_fraction: float = 0.5, small_points: int = 4096, min_slots: int | None = None,
+                 memory_budget: int | None = None, reserve_bytes: int = 256 << 20):
         if not hasattr(gpr, 'X_train_'):
             raise ValueError('PredictServer needs a fitted model')
         self.gpr = gpr
@@ -107,13 +114,20 @@ class PredictServer:
         self.y_std = np.asarray(gpr._y_train_std, dtype=np.float64).reshape(1, -1)
         self.y_mean = np.asarray(gpr._y_train_mean, dtype=np.float64).reshape(1, -1)
 
-        # slots bounded by free memory: inputs, outputs and the graphs' workspaces of one slot
-        per_slot = self._slot_bytes()
+        # slots are admitted by free device memory: one slot's footprint (inputs, outputs and the
+        # shared pool of its graphs' workspaces) against the budget and the memory free right now
+        self.slot_bytes = self._slot_bytes()
         free, _ = torch.cuda.mem_get_info(self.device)
-        self.n_slots = max(1, min(int(slots), int(free * memory_fraction // max(per_slot, 1))))
+        self.memory_budget = int(free * memory_fraction) if memory_budget is None else int(memory_budget)
+        self.reserve_bytes = int(reserve_bytes)
+        self.max_slots = max(1, int(slots))
+        start = self.max_slots if min_slots is None else max(1, min(int(min_slots), self.max_slots))
+        start = max(1, min(start, self.memory_budget // max(self.slot_bytes, 1)))
         # slot 0 (the small requests' lane when there are several slots) runs on a high-priority
         # stream: its blocks are scheduled ahead of queued blocks of the large batches
-        self.slots = [self._make_slot(high_priority=(i == 0 and self.n_slots > 1)) for i in range(self.n_slots)]
+        self.slots = [self._make_slot(high_priority=(i == 0 and self.max_slots > 1)) for i in range(start)]
+        self.slots_added = 0   # slots added after start-up (memory admission)
+        self.slots_refused = 0  # times a slot was wanted but the free memory or the budget did not hold it
 
         self._queue = collections.deque()        # large requests: [request, next row offset]
         self._small = collections.deque()        # requests of at most small_points rows
@@ -129,11 +143,29 @@ class PredictServer:
         self._done.start()
 
     # ---- set-up ---------------------------------------------------------------------------
+    @property
+    def n_slots(self) -> int:
+        return len(self.slots)
+
     def _slot_bytes(self) -> int:
+        """Device bytes of one slot: its input and outputs for the largest bucket, plus the largest
+        bucket's graph workspace (search workspace, lists, casts, predict outputs); the buckets'
+        graphs share one pool."""
         b = self.max_batch
         io = b * self.d * 8 + b * (self.ydim + 1) * 8
         ws = int(_lib.lib().nngp_knn_workspace_size_f32(self.xt.shape[0], b, self.d, self.m)) + b * self.m * 4
-        return 2 * io + ws * len(self.buckets)
+        return 2 * io + ws + b * self.d * 8
+
+    def _may_add_slot(self) -> bool:
+        """Whether the free device memory (less the reserve) and the budget hold one more slot."""
+        if len(self.slots) >= self.max_slots:
+            return False
+        free, _ = torch.cuda.mem_get_info(self.device)
+        ok = (free - self.reserve_bytes >= self.slot_bytes and
+              (len(self.slots) + 1) * self.slot_bytes <= self.memory_budget)
+        if not ok:
+            self.slots_refused += 1
+        return ok
 
     def _run(self, slot: _Slot, b: int, flags: torch.Tensor):
         """Kernels of one batch of ``b`` points from ``slot.x_in`` (captured into the graphs)."""
@@ -152,6 +184,7 @@ class PredictServer:
                      mean_pin=torch.empty((b, self.ydim), dtype=torch.float64).pin_memory(),
                      var_pin=torch.empty((b,), dtype=torch.float64).pin_memory(),
                      flags_pin=torch.zeros(1, dtype=torch.int32).pin_memory())
+        pool = torch.cuda.graph_pool_handle() if self.use_graphs else None  # one pool for the slot's graphs
         for bucket in self.buckets:
             flags = ops.new_flags(dev)
             mean_out = torch.zeros((bucket, self.ydim), dtype=torch.float64, device=dev)
@@ -162,7 +195,8 @@ class PredictServer:
                     self._run(slot, bucket, flags)  # warm-up outside the capture
                 slot.stream.synchronize()
                 graph = torch.cuda.CUDAGraph()
-                with torch.cuda.graph(graph, stream=slot.stream):
+                # thread-local capture: the completion thread keeps polling other slots' events
+                with torch.cuda.graph(graph, pool=pool, stream=slot.stream, capture_error_mode='thread_local'):
                     flags.zero_()
                     mean, var = self._run(slot, bucket, flags)
                     mean_out.copy_(mean)
@@ -244,11 +278,23 @@ class PredictServer:
         torch.cuda.set_device(self.device)
         try:
             while True:
+                grow = False
                 with self._cv:
                     pick = self._pick()
                     while not self._stop and pick is None:
+                        if self._pending() and self._may_add_slot():
+                            grow = True
+                            break
                         self._cv.wait()
                         pick = self._pick()
+                if grow:  # every slot busy, requests waiting, memory for one more slot
+                    slot = self._make_slot()
+                    with self._cv:
+                        self.slots.append(slot)
+                        self.slots_added += 1
+                    continue
+                with self._cv:
+                    pick = self._pick() if pick is None else pick
                     if pick is None:  # stopping and nothing left to launch
                         if not self._pending():
                             return

@@ -20,6 +20,7 @@ KERNELS = {
     'matern12_n500_d3_m16': lambda: skk.ConstantKernel(0.9) * skk.Matern(0.4, nu=0.5) + skk.WhiteKernel(0.01),
     'matern32_n450_d4_m12': lambda: skk.ConstantKernel(1.2) * skk.Matern(0.7, nu=1.5) + skk.WhiteKernel(0.02),
     'matern52_n400_d2_m10': lambda: skk.ConstantKernel(1.0) * skk.Matern(0.6, nu=2.5) + skk.WhiteKernel(0.005),
+    'wide_n300_d3_m16_y100': lambda: skk.ConstantKernel(1.0) * skk.RBF(0.4) + skk.WhiteKernel(0.02),
 }
 CASES = sorted(KERNELS)
 

@@ -2,7 +2,9 @@
 
 Run in a container that has the reference source (stavoltafunzia/nngpr 0.1.1)::
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py --ref <path of the reference checkout>
+
+(or with the path in the environment variable NNGPR_REFERENCE).
 
 Every value stored here comes from the reference's own ``NumpyNngpr`` (FP64,
 ``allow_downcast_f32='no'``, ``distribute_method='sequential'``) or from
@@ -71,13 +73,18 @@ def case(name, NumpyNngpr, NumpyWorker, kernel_fn, x, y, xq, m, theta_eval=None,
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument('--ref', default='/root/reference')
+    ap.add_argument('--ref', default=os.environ.get('NNGPR_REFERENCE'),
+                    help='directory holding the reference package nngpr (default: $NNGPR_REFERENCE)')
     ap.add_argument('--only', default='', help='comma-separated case groups to (re)generate: rbf,matern')
     args = ap.parse_args()
+    if not args.ref:
+        ap.error('give the reference checkout with --ref or NNGPR_REFERENCE')
     NumpyNngpr, NumpyWorker, bk = _import_reference(args.ref)
     only = set(filter(None, args.only.split(',')))
     if 'full' in only:
         return full_cases(NumpyNngpr, NumpyWorker, bk)
+    if 'wide' in only:
+        return wide_case(NumpyNngpr, NumpyWorker, bk)
     if only and 'rbf' not in only:
         return matern_cases(NumpyNngpr, NumpyWorker, bk)
 
@@ -199,6 +206,21 @@ def full_cases(NumpyNngpr, NumpyWorker, bk):
                             dn_nbr=np.asarray(dn_nn)[:, 1:], dn_cov80=np.asarray(dn_cov),
                             dn_samples60=np.asarray(dn_samples), **extra)
         print('full', name, np.asarray(mean).ravel()[:3], np.asarray(std).ravel()[:3])
+
+
+def wide_case(NumpyNngpr, NumpyWorker, bk):
+    """8. One hundred outputs (normalize_y): every output column is its own right-hand side of
+    each local system and the log-likelihood sums over the columns (base_nngpr.py:578-584).
+    The reference's own known-answer test asks for y_dim = 100 (nngpr_base_tester.py:179) but
+    slices a 150 x 3 array with [:, :100], i.e. runs 3 columns (the reftest_n150_y3 case); this
+    case has 100 genuine columns."""
+    rng = np.random.default_rng(8)
+    x = rng.uniform(0, 1, (300, 3))
+    w = rng.normal(size=(3, 100))
+    y = np.sin(2 * x @ w) + 0.3 * np.arange(100)[None, :] + rng.normal(0, 0.05, (300, 100))
+    xq = rng.uniform(0, 1, (60, 3))
+    case('wide_n300_d3_m16_y100', NumpyNngpr, NumpyWorker,
+         lambda: bk.ConstantKernel(1.0) * bk.RBF(0.4) + bk.WhiteKernel(0.02), x, y, xq, 16, normalize_y=True)
 
 
 def matern_cases(NumpyNngpr, NumpyWorker, bk):

@@ -95,3 +95,44 @@ def test_fit_lbfgs_respects_bounds():
     assert np.all(theta >= bounds[:, 0] - 1e-12) and np.all(theta <= bounds[:, 1] + 1e-12)
     assert 1 <= evals <= 60
     assert np.isfinite(lml)
+
+
+def test_fp32_gradient_on_the_differentiation_subset():
+    """The FP32 path (FP32 search, FP32 local systems with the FP64 re-solve of small pivots) on
+    20,000 points of the d = 8 ARD workload: lml within 1e-5 of |lml| and the gradient w.r.t. the
+    10 log hyperparameters within 1e-5 (max-norm relative) of the FP64 oracle's (the reference's
+    formulas, base_nngpr.py:586-614) on the same lists, and within 1e-4 of central differences
+    (h = 1e-3) of the FP64 log-likelihood on those lists."""
+    from nngpr_b200 import ops
+    from nngpr_b200.kernel_params import params_from_theta
+    from oracle import nngp_oracle as O
+
+    from _common import oracle_params
+    x, y, kernel = _rff_problem()
+    p = extract(kernel)
+    dev = torch.device('cuda')
+    x64 = torch.from_numpy(x).to(dev)
+    y64 = torch.from_numpy(y).to(dev)[:, None]
+    x32, y32 = x64.to(torch.float32), y64.to(torch.float32)
+    nbr = ops.knn(x32, x32, 32, 0, p.length_scale)
+    flags = ops.new_flags(dev)
+    got = ops.loglik(x32, y32, nbr, p, 1e-10, True, flags=flags).cpu().numpy()
+    assert int(flags.item()) & ~8 == 0  # only the informational FP64-re-solve bit may be set
+    want_l, want_g = O.log_marginal_likelihood(x, y[:, None], nbr.cpu().numpy(), oracle_params(p), 1e-10, True)
+    assert abs(got[0] / want_l - 1) < 1e-5, (got[0], want_l)
+    assert rel(got[1:], want_g) < 1e-5, (got[1:], want_g)
+
+    theta0 = kernel.theta.copy()
+    prob_template = extract(kernel)
+
+    def f(th):
+        return float(ops.loglik(x64, y64, nbr, params_from_theta(prob_template, th), 1e-10, False)[0])
+
+    h = 1e-3
+    fd = np.empty(theta0.size)
+    for t in range(theta0.size):
+        tp, tm = theta0.copy(), theta0.copy()
+        tp[t] += h
+        tm[t] -= h
+        fd[t] = (f(tp) - f(tm)) / (2 * h)
+    assert np.max(np.abs(fd - got[1:])) / np.max(np.abs(fd)) < 1e-4

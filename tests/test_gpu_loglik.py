@@ -1,9 +1,7 @@
 """Fit-step log-likelihood and gradient through the C ABI vs the oracle / golden vectors.
 
 Tolerances: FP64 entry point 1e-10 relative (lml) and 1e-9 (gradient, max-norm relative);
-FP32 entry point 1e-5 for the lml relative to the sum of the per-point terms' magnitudes (the
-total can be a cancelled sum; on the golden cases that scale is 1-12x |lml|) and 1e-5 for the
-gradient (max-norm relative).
+FP32 entry point 1e-5 relative to |lml| and 1e-5 for the gradient (max-norm relative).
 """
 import numpy as np
 import pytest
@@ -46,7 +44,7 @@ def test_loglik_golden(name, dtype):
         assert abs(out[0] / g['lml'] - 1) < F64_LML, (out[0], g['lml'])
     else:
         tol_g = F32_GRAD
-        assert abs(out[0] - g['lml']) < F32_LML * lml_scale(name), (out[0], g['lml'])
+        assert abs(out[0] - g['lml']) < F32_LML * abs(g['lml']), (out[0], g['lml'], lml_scale(name))
     assert rel(out[1:], g['grad']) < tol_g, (out[1:], g['grad'])
 
 
@@ -151,3 +149,59 @@ def test_matern_ard_loglik_matches_oracle(nu, m):
     assert flags32 & ~_lib.NNGP_FLAG_FP64_FALLBACK == 0
     assert abs(out32[0] / want_l - 1) < F32_LML
     assert rel(out32[1:], want_g) < F32_GRAD
+
+
+def test_row_shards_sum_to_the_whole_step():
+    """The multi-GPU fit step's per-rank call: ops.loglik(..., row_begin=r0) on each row range of
+    a partition (nngp_loglik_rows_*, one task of the reference's row-batched worker loop,
+    base_nngpr.py:503-538) sums to the single launch and to the FP64 oracle, FP64 and FP32."""
+    rng = np.random.default_rng(11)
+    n = 20000
+    x = rng.uniform(-1, 1, (n, 3)) * np.array([1.0, 0.7, 0.4])
+    y = np.sin(3 * x).sum(1) + rng.normal(0, 0.05, n)
+    p = extract(skk.ConstantKernel(1.0) * skk.RBF(0.2) + skk.WhiteKernel(1e-3))
+    nbr = O.fit_neighbours(x, 32, 0.2, np.float32)
+    want_l, want_g = O.log_marginal_likelihood(x, y, nbr, oracle_params(p), 1e-10, True)
+    bounds = [0, 1, 4999, 12000, 19999, n]  # a one-row shard and the last row alone included
+    for dtype, tdt, tl, tg in ((np.float64, torch.float64, F64_LML, F64_GRAD),
+                               (np.float32, torch.float32, F32_LML, F32_GRAD)):
+        xt = torch.from_numpy(x).to('cuda', tdt)
+        yt = torch.from_numpy(y[:, None]).to('cuda', tdt)
+        nt = torch.from_numpy(nbr).cuda()
+        whole = ops.loglik(xt, yt, nt, p, 1e-10, True).cpu().numpy()
+        parts = np.zeros_like(whole)
+        for r0, r1 in zip(bounds[:-1], bounds[1:]):
+            flags = ops.new_flags(xt.device)
+            part = ops.loglik(xt, yt, nt[r0:r1].contiguous(), p, 1e-10, True, flags=flags, row_begin=r0)
+            assert int(flags.item()) & ~_lib.NNGP_FLAG_FP64_FALLBACK == 0
+            parts += part.cpu().numpy()
+        assert abs(parts[0] / whole[0] - 1) < 1e-12
+        assert rel(parts[1:], whole[1:]) < 1e-11
+        assert abs(parts[0] / want_l - 1) < tl
+        assert rel(parts[1:], want_g) < tg
+
+
+def test_fit_step_rows_shards_equal_the_whole_step():
+    """sharding.fit_step_rows, what one rank of the multi-GPU step runs (its rows' seeded and
+    pruned search against the prefix, then their local systems), over three shards run one after
+    the other on this GPU: the partial sums add up to the single-GPU fit step."""
+    from nngpr_b200.sharding import fit_step_rows, row_partition
+    rng = np.random.default_rng(12)
+    n = 100_000
+    x = rng.uniform(-1, 1, (n, 3)) * np.array([1.0, 0.7, 0.4])
+    y = np.sin(3 * x).sum(1) + rng.normal(0, 0.05, n)
+    p = extract(skk.ConstantKernel(1.0) * skk.RBF(0.2) + skk.WhiteKernel(1e-3))
+    x64 = torch.from_numpy(x).cuda()
+    y64 = torch.from_numpy(y[:, None]).cuda()
+    x32 = x64.to(torch.float32)
+    nbr = ops.knn(x32, x32, 32, 0, 0.2)
+    whole = ops.loglik(x64, y64, nbr, p, 1e-10, True).cpu().numpy()
+    for equal_rows in (True, False):
+        b = row_partition(n, 3, equal_rows=equal_rows)
+        parts = np.zeros_like(whole)
+        for r0, r1 in zip(b[:-1], b[1:]):
+            flags = ops.new_flags(x64.device)
+            parts += fit_step_rows(x32, x64, y64, p, 1e-10, 32, r0, r1, 0.2, flags=flags).cpu().numpy()
+            assert int(flags.item()) == 0
+        assert abs(parts[0] / whole[0] - 1) < 1e-12
+        assert rel(parts[1:], whole[1:]) < 1e-11

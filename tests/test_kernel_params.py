@@ -57,8 +57,8 @@ def test_unsupported_kernels_raise(kernel):
 
 
 def _reference_kernels():
-    for path in (os.path.join(ROOT, 'baseline', '_ref'), '/root/reference'):
-        if os.path.isdir(os.path.join(path, 'nngpr')):
+    for path in (os.path.join(ROOT, 'baseline', '_ref'), os.environ.get('NNGPR_REFERENCE', '')):
+        if path and os.path.isdir(os.path.join(path, 'nngpr')):
             sys.path.insert(0, path)
             try:
                 from nngpr import batched_kernels
