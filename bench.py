@@ -547,17 +547,21 @@ def our_launches_per_step(n, d, m):
 def run_plain(args, torch, x32, y64, xq32, p, flags, flush, lml_ours):
     """Time the plain FP32 GPU form of the same fit step and predict (the comparator of the
     metric): returns the 'plain_gpu' object of the bench line."""
-    from nngpr_b200 import ops
+    from nngpr_b200 import ops, plain_ref
     from nngpr_b200.plain import plain_knn, plain_loglik, plain_predict
 
     y32 = y64.to(torch.float32)
     nbr_ours = ops.knn(x32, x32, M, 0, LS, flags=flags)
+    # the reference's own calc_nn and fill_nn_kernel, compiled from the installed reference's
+    # source, when it is there (else this library's restatement of calc_nn and a torch fill)
+    ref_root = os.path.join(ROOT, 'baseline', '_ref')
+    ref_root = ref_root if plain_ref.available(ref_root) else None
 
     def step(ev=None):
-        nb = plain_knn(x32, x32, M, 0, LS)
+        nb = plain_knn(x32, x32, M, 0, LS, ref_root=ref_root)
         if ev is not None:
             ev.record()
-        return nb, plain_loglik(x32, y32, nb, p, ALPHA, True)
+        return nb, plain_loglik(x32, y32, nb, p, ALPHA, True, ref_root=ref_root)
 
     step()  # warm-up
     ms, knn_ms = [], []
@@ -571,26 +575,31 @@ def run_plain(args, torch, x32, y64, xq32, p, flags, flush, lml_ours):
         ms.append(a.elapsed_time(c))
         knn_ms.append(a.elapsed_time(b))
     same = bool(torch.equal(nb, nbr_ours))
+    rows_differ = int((nb != nbr_ours).any(dim=1).sum().item())
     lml = float(lml.item())
     # predict at the benchmark's query count
-    nq = plain_knn(x32, xq32, M, None, LS)
-    plain_predict(x32, y32, xq32, nq, p, ALPHA)
+    nq = plain_knn(x32, xq32, M, None, LS, ref_root=ref_root)
+    plain_predict(x32, y32, xq32, nq, p, ALPHA, ref_root=ref_root)
     a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     flush.zero_()
     a.record()
-    nq = plain_knn(x32, xq32, M, None, LS)
-    plain_predict(x32, y32, xq32, nq, p, ALPHA)
+    nq = plain_knn(x32, xq32, M, None, LS, ref_root=ref_root)
+    plain_predict(x32, y32, xq32, nq, p, ALPHA, ref_root=ref_root)
     c.record()
     torch.cuda.synchronize()
     pred_ms = a.elapsed_time(c)
     step_ms = float(np.min(ms))  # the comparator's best step (its torch batched solvers vary run to run)
     return {'value': 1e3 / step_ms, 'unit': UNIT, 'ms_per_step': step_ms, 'knn_ms': float(np.min(knn_ms)),
             'ms_all_steps': [float(v) for v in ms],
-            'steps': args.plain_steps, 'lists_identical': same, 'lml': lml,
-            'lml_rel_diff_vs_ours': abs(lml - lml_ours) / abs(lml_ours),
+            'steps': args.plain_steps, 'lists_identical': same, 'rows_with_different_lists': rows_differ,
+            'lml': lml, 'lml_rel_diff_vs_ours': abs(lml - lml_ours) / abs(lml_ours),
             'predict': {'value': N_PRED / (pred_ms * 1e-3), 'unit': 'points/s', 'ms': pred_ms},
-            'form': 'one thread per query FP32 search (calc_nn structure) + torch FP32 batched fill, '
-                    'Cholesky and cholesky_solve with materialised dK (the reference worker), one launch per stage'}
+            'form': ('the reference\'s own calc_nn and fill_nn_kernel (cuda_kernel_accelerators.py:663-863), compiled '
+                     'with NVRTC for sm_100a from the installed reference, + torch FP32 batched Cholesky and '
+                     'cholesky_solve with the materialised dK (the reference worker), one launch per stage'
+                     if ref_root else
+                     'one thread per query FP32 search (calc_nn structure) + torch FP32 batched fill, '
+                     'Cholesky and cholesky_solve with materialised dK (the reference worker), one launch per stage')}
 
 
 def _pct(v, q):
@@ -787,6 +796,28 @@ def run_ours(args):
     torch.cuda.synchronize()
     if int(flags.item()) & ~_lib.NNGP_FLAG_FP64_FALLBACK:
         raise RuntimeError(f'kernel status flags {int(flags.item())}')
+    partition = {'initial': list(bounds)}
+    if world > 1:
+        # one measured step per rank, then the rows are re-cut for equal predicted device time
+        # (sharding.rebalance): what the static rule cannot see, e.g. shards whose tile lists fell
+        # back to index order on the device
+        from nngpr_b200.sharding import rebalance
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        step()
+        e1.record()
+        torch.cuda.synchronize()
+        t_me = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
+        t_all = [torch.zeros_like(t_me) for _ in range(world)]
+        dist.all_gather(t_all, t_me)
+        partition['measured_ms'] = [float(v.item()) for v in t_all]
+        bounds = rebalance(bounds, partition['measured_ms'])
+        r0, r1 = bounds[rank], bounds[rank + 1]
+        q_rows = x32[r0:r1]
+        for _ in range(2):
+            step()
+        torch.cuda.synchronize()
+    partition['final'] = list(bounds)
 
     # ---- timed steps (device-resident inputs, L2 flushed before every step) -------------
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
@@ -981,7 +1012,8 @@ def run_ours(args):
             'scaling': 'strong' if world > 1 else 'weak', 'vs_baseline': None, 'dtype': DTYPE,
             'data': DATA,
             'config': {'workload': WORKLOAD, 'n': n, 'd': D, 'm': M, 'l2': L2_NOTE},
-            'parallelism': f'rows{world}', 'lml': lml_val, 'lml_rel_err_vs_fp64_local': lml_err,
+            'parallelism': f'rows{world}', 'partition': partition if world > 1 else None, 'lml': lml_val,
+            'lml_rel_err_vs_fp64_local': lml_err,
             'e2e': e2e,
             'roofline': dict(roof, traffic=read_profile_traffic()) if ROOF == 'local' else dict(
                 roof, traffic=read_profile_traffic(),

@@ -75,7 +75,7 @@ constexpr uint64_t kEmptyKey = (uint64_t)0x7F800000u << 32 | 0xFFFFFFFFu;
 // tensor pipe's doubled BF16 rate, 4 instead of 7 MMA steps per tile at D = 16.
 template <int D, int QTILES>
 struct Cfg {
-    static constexpr bool BF16 = false && D >= 12;
+    static constexpr bool BF16 = D >= 12;
     static constexpr int ESZ = BF16 ? 2 : 4;        // operand element bytes
     static constexpr int EPC = 16 / ESZ;            // elements per 16-byte core-matrix row
     static constexpr int KMMA = BF16 ? 16 : 8;      // UMMA K of one instruction

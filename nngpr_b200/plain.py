@@ -32,10 +32,14 @@ def _torch():
     return torch
 
 
-def plain_knn(ref, query, num_nn: int, ref_cut_index, length_scale) -> 'torch.Tensor':
+def plain_knn(ref, query, num_nn: int, ref_cut_index, length_scale, ref_root: str | None = None) -> 'torch.Tensor':
     """Neighbour lists ``(n_query, num_nn)`` int32 by the plain FP32 search (same lists as
-    :func:`nngpr_b200.ops.knn`)."""
+    :func:`nngpr_b200.ops.knn`).  With ``ref_root`` (the installed reference), the reference's own
+    ``calc_nn`` compiled from its source (:mod:`nngpr_b200.plain_ref`)."""
     torch = _torch()
+    if ref_root is not None:
+        from . import plain_ref
+        return plain_ref.calc_nn(ref_root, ref, query, num_nn, ref_cut_index, length_scale)
     ref = ref.to(torch.float32)
     query = query.to(torch.float32)
     if length_scale is not None:
@@ -106,9 +110,11 @@ def _fill(xn, valid, p: RbfParams, ls, eval_gradient: bool):
     return K, G
 
 
-def plain_loglik(x, y, nbr, p: RbfParams, alpha: float, eval_gradient: bool = True, batch: int = 65536):
+def plain_loglik(x, y, nbr, p: RbfParams, alpha: float, eval_gradient: bool = True, batch: int = 65536,
+                 ref_root: str | None = None):
     """Log-likelihood (and gradient w.r.t. log theta) of all points in FP32 (per-point terms
-    summed in FP64), ``x (n, d)``, ``y (n,)`` or ``(n, ydim)``, ``nbr (n, m)`` on the GPU."""
+    summed in FP64), ``x (n, d)``, ``y (n,)`` or ``(n, ydim)``, ``nbr (n, m)`` on the GPU.  With
+    ``ref_root`` the fill is the reference's own ``fill_nn_kernel`` (:mod:`nngpr_b200.plain_ref`)."""
     torch = _torch()
     x = x.to(torch.float32)
     y = y.to(torch.float32)
@@ -124,7 +130,11 @@ def plain_loglik(x, y, nbr, p: RbfParams, alpha: float, eval_gradient: bool = Tr
         idx = torch.cat([rows[:, None], nbr[rows]], dim=1)
         valid = idx >= 0
         cl = idx.clamp(min=0)
-        K, G = _fill(x[cl], valid, p, ls, eval_gradient)
+        if ref_root is not None:
+            from . import plain_ref
+            K, G = plain_ref.fill_nn_kernel(ref_root, x, idx, p, eval_gradient)
+        else:
+            K, G = _fill(x[cl], valid, p, ls, eval_gradient)
         ii = torch.arange(idx.shape[1], device=x.device)
         K[:, ii, ii] += torch.where(valid, alpha, 0.0)
         L = torch.linalg.cholesky(K[:, 1:, 1:])
@@ -152,9 +162,11 @@ def plain_loglik(x, y, nbr, p: RbfParams, alpha: float, eval_gradient: bool = Tr
     return (total, grad) if eval_gradient else total
 
 
-def plain_predict(x_train, y_train, x_query, nbr, p: RbfParams, alpha: float, batch: int = 65536):
+def plain_predict(x_train, y_train, x_query, nbr, p: RbfParams, alpha: float, batch: int = 65536,
+                  ref_root: str | None = None):
     """Predictive mean ``(nq, ydim)`` and standard deviation ``(nq,)`` in FP32, conditioning on the
-    training set only (the reference's ``only-train`` worker)."""
+    training set only (the reference's ``only-train`` worker); with ``ref_root`` the fill is the
+    reference's own ``fill_nn_kernel``."""
     torch = _torch()
     x_train = x_train.to(torch.float32)
     x_query = x_query.to(torch.float32)
@@ -171,7 +183,11 @@ def plain_predict(x_train, y_train, x_query, nbr, p: RbfParams, alpha: float, ba
         rows = torch.arange(q0, min(nq, q0 + batch), device=x_train.device)
         idx = torch.cat([(nt + rows)[:, None], nbr[rows]], dim=1)
         valid = idx >= 0
-        K, _ = _fill(x_full[idx.clamp(min=0)], valid, p, ls, False)
+        if ref_root is not None:
+            from . import plain_ref
+            K, _ = plain_ref.fill_nn_kernel(ref_root, x_full, idx, p, False)
+        else:
+            K, _ = _fill(x_full[idx.clamp(min=0)], valid, p, ls, False)
         train = valid & (idx < nt)
         ii = torch.arange(idx.shape[1], device=x_train.device)
         K[:, ii, ii] += torch.where(train, alpha, 0.0)

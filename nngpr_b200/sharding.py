@@ -39,6 +39,40 @@ def row_partition(n: int, world: int, equal_rows: bool = False) -> list[int]:
     return b
 
 
+def rebalance(bounds: list[int], seconds: list[float]) -> list[int]:
+    """A partition of the same rows with equal predicted time per rank, from the time each rank
+    took on its current range (``seconds[r]`` for ``[bounds[r], bounds[r + 1])``, e.g. the device
+    time of one fit step, gathered from every rank).
+
+    The cost of a row is taken as uniform inside each current range (that range's time over its
+    rows), so the cumulative cost is piecewise linear in the row index; the new boundaries cut it
+    into equal parts.  This balances what the static rules cannot see: a shard whose tile lists
+    fell back to index order on the device, or one whose rows are costlier for the data at hand.
+    """
+    world = len(bounds) - 1
+    if world < 1 or len(seconds) != world:
+        raise ValueError('one time per range')
+    n = bounds[-1]
+    t = [max(float(s), 0.0) for s in seconds]
+    total = sum(t)
+    if total <= 0.0 or n == 0:
+        return list(bounds)
+    cum = [0.0]
+    for v in t:
+        cum.append(cum[-1] + v)
+    out = [0]
+    r = 0
+    for k in range(1, world):
+        target = total * k / world
+        while r < world - 1 and cum[r + 1] < target:
+            r += 1
+        lo, hi = bounds[r], bounds[r + 1]
+        frac = (target - cum[r]) / t[r] if t[r] > 0 else 0.0
+        out.append(max(out[-1], min(n, int(round(lo + frac * (hi - lo))))))
+    out.append(n)
+    return out
+
+
 def prefix_pairs(r0: int, r1: int) -> int:
     """Prefix-search pairs of rows [r0, r1): sum of i for i in [r0, r1)."""
     return (r1 * (r1 - 1) - r0 * (r0 - 1)) // 2

@@ -81,3 +81,26 @@ def test_sharded_fit_step_equals_single_process(tmp_path):
     g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), 'golden', 'cpu_n2000_d3_m16.npz'))
     assert abs(got[0] / g['lml'] - 1) < 1e-10
     assert np.max(np.abs(got[1:] - g['grad'])) / np.max(np.abs(g['grad'])) < 1e-9
+
+
+def test_rebalance_equalises_measured_times():
+    from nngpr_b200.sharding import rebalance, row_partition
+    # rows whose cost density is 1 on [0, 600) and 4 on [600, 1000): a rank's time is its cost
+    dens = np.where(np.arange(1000) < 600, 1.0, 4.0)
+
+    def times(b):
+        return [float(dens[b[r]:b[r + 1]].sum()) for r in range(len(b) - 1)]
+
+    b = row_partition(1000, 4, equal_rows=True)
+    t = times(b)
+    assert max(t) / min(t) == 4.0
+    for _ in range(3):  # each round narrows the spread, also where a range straddles the change
+        b = rebalance(b, times(b))
+        assert b[0] == 0 and b[-1] == 1000 and all(b[i] <= b[i + 1] for i in range(4))
+        t2 = times(b)
+        assert max(t2) / min(t2) <= max(t) / min(t)
+        t = t2
+    assert max(t) / min(t) < 1.06
+    # equal times leave the partition as it is; zero times too
+    assert rebalance([0, 5, 10], [1.0, 1.0]) == [0, 5, 10]
+    assert rebalance([0, 5, 10], [0.0, 0.0]) == [0, 5, 10]
