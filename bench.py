@@ -80,7 +80,7 @@ DTYPE = 'f32 search (tf32-split tensor screen) + f64 local'
 WORKLOADS = {
     'fit3d': {},
     'precision': dict(
-        N_TRAIN=1_000_000, D=16, M=32, LS=0.8, NOISE=1e-4, ALPHA=1e-10, LOCAL='f32', ROOF='tensor',
+        N_TRAIN=1_000_000, D=16, M=32, LS=0.8, NOISE=1e-4, ALPHA=1e-10, LOCAL='f32', ROOF='tensor', PIVOT=1e-6,
         WORKLOAD=('nngp fit step, n=1000000 d=16 m=32, 64-component Gaussian mixture, isotropic RBF l=0.8, '
                   'noise 1e-4; tensor-core fp32 exact neighbour search, fp32 local systems with fp64 re-solve of '
                   'small pivots, fp64 reductions'),
@@ -942,7 +942,8 @@ def run_ours(args):
     e2e = None
     if world == 1 and not args.no_e2e:
         gpr = B200Nngpr(kernel=kernel, num_nn=M, alpha=ALPHA, optimizer=None, keep_resident=False,
-                        allow_downcast_f32='yes' if LOCAL == 'f32' else None, device=dev).fit(x, y)
+                        allow_downcast_f32='yes' if LOCAL == 'f32' else None, device=dev,
+                        **({} if PIVOT is None else {'pivot_tol': PIVOT})).fit(x, y)
         theta = gpr.kernel_.theta.copy()
         for _ in range(max(1, args.warmup)):
             gpr.log_marginal_likelihood(theta, eval_gradient=True)

@@ -99,10 +99,12 @@ template <bool MATERN, typename T> __device__ __forceinline__ T kern_g(int famil
 // diagonal kWarpM doubles | gradient accumulator n_theta doubles | the fill's kernel values
 // kWarpM x (kWarpM + 1) doubles (kept for the gradient, which would otherwise recompute them).
 struct WarpSmem {
-    int ds;  // row stride of xs (d + 1)
-    size_t c_bytes, xs_bytes, l_bytes, idg_bytes, g_bytes, e_bytes, total;
-    size_t xs_off, l_off, idg_off, g_off, e_off;
-    __host__ __device__ static WarpSmem make(int d, int n_theta) {
+    int ds;  // row stride of xs (d + 1; FP32 systems use whole float4s, see warp_system)
+    size_t c_bytes, xs_bytes, l_bytes, idg_bytes, g_bytes, e_bytes, r_bytes, total;
+    size_t xs_off, l_off, idg_off, g_off, e_off, r_off;
+    // f32: FP32 inputs, whose systems also keep the fill's squared distances (kWarpM x (kWarpM + 1)
+    // floats) for the gradient instead of recomputing them
+    __host__ __device__ static WarpSmem make(int d, int n_theta, bool f32 = false) {
         WarpSmem s;
         s.ds = d + 1;
         s.c_bytes = (size_t)2 * kWarpM * 8;
@@ -116,7 +118,9 @@ struct WarpSmem {
         s.idg_off = s.l_off + s.l_bytes;
         s.g_off = s.idg_off + s.idg_bytes;
         s.e_off = s.g_off + s.g_bytes;
-        s.total = (s.e_off + s.e_bytes + 15) / 16 * 16;
+        s.r_bytes = f32 ? (size_t)kWarpM * (kWarpM + 1) * 4 : 0;
+        s.r_off = s.e_off + s.e_bytes;
+        s.total = (s.r_off + s.r_bytes + 15) / 16 * 16;
         return s;
     }
 };
@@ -144,7 +148,7 @@ __device__ __forceinline__ bool warp_system(const LocalArgs &a, int64_t p, int l
                                             TIn *__restrict__ var, int32_t *__restrict__ flags) {
     constexpr int M = kWarpM;
     const unsigned FULL = 0xffffffffu;
-    const WarpSmem lay = WarpSmem::make(a.d, a.n_theta);
+    const WarpSmem lay = WarpSmem::make(a.d, a.n_theta, std::is_same<TIn, float>::value);
     TC *colbuf = reinterpret_cast<TC *>(wsm);  // two column slots of kWarpM, 16-byte aligned
     TC *xs = reinterpret_cast<TC *>(wsm + lay.xs_off);
     TC *Ls = reinterpret_cast<TC *>(wsm + lay.l_off);
@@ -152,7 +156,15 @@ __device__ __forceinline__ bool warp_system(const LocalArgs &a, int64_t p, int l
     double *gacc = reinterpret_cast<double *>(wsm + lay.g_off);
     TC *Es = reinterpret_cast<TC *>(wsm + lay.e_off);
     constexpr bool STASH = GRAD && !MATERN;  // RBF gradient: reuse the fill's exponentials
-    const int d = a.d, ds = lay.ds;
+    // FP32 RBF systems also keep the squared distances (the gradient's only other use of the fill)
+    constexpr bool STASH_R = STASH && std::is_same<TC, float>::value && std::is_same<TIn, float>::value;
+    float *Rs = reinterpret_cast<float *>(wsm + lay.r_off);
+    // FP32 rows of xs are whole float4s, an odd number of them (one 16-byte load per 4 features,
+    // rows of different lanes in distinct bank groups), zero padded: the padding adds (0 - 0)^2
+    // terms, so every sum is the same as over the d features alone
+    constexpr bool VEC4 = std::is_same<TC, float>::value;
+    const int d = a.d;
+    const int ds = VEC4 ? 4 * (((d + 3) / 4) | 1) : lay.ds;
 
     // ---- neighbour of this lane --------------------------------------------------------
     int32_t j = -1;
@@ -173,6 +185,10 @@ __device__ __forceinline__ bool warp_system(const LocalArgs &a, int64_t p, int l
         xs[lane * ds + f] = valid ? (TC)x_ref[(int64_t)j * d + f] * s : TC(0);
     }
     for (int f = lane; f < d; f += 32) xs[M * ds + f] = (TC)x_pt[p * d + f] * (TC)a.inv_ls[a.ard ? f : 0];
+    if (VEC4) {
+        for (int f = d; f < ds; ++f) xs[lane * ds + f] = TC(0);
+        for (int f = d + lane; f < ds; f += 32) xs[M * ds + f] = TC(0);
+    }
     __syncwarp();
 
     // ---- fill: squared scaled distances, then kernel values ------------------------------
@@ -180,15 +196,44 @@ __device__ __forceinline__ bool warp_system(const LocalArgs &a, int64_t p, int l
     TC rp = TC(0);
 #pragma unroll
     for (int k = 0; k < M; ++k) r[k] = TC(0);
-    for (int f = 0; f < d; ++f) {
-        const TC xi = xs[lane * ds + f];
+    if constexpr (VEC4) {
+        const float4 *xs4 = reinterpret_cast<const float4 *>(xs);
+        const int ds4 = ds / 4, nf4 = (d + 3) / 4;
+        for (int f4 = 0; f4 < nf4; ++f4) {
+            const float4 xi = xs4[lane * ds4 + f4];
 #pragma unroll
-        for (int k = 0; k < M; ++k) {
-            const TC t = xi - xs[k * ds + f];
-            r[k] = fma(t, t, r[k]);
+            for (int k = 0; k < M; ++k) {
+                const float4 xk = xs4[k * ds4 + f4];
+                float t = xi.x - xk.x;
+                r[k] = fmaf(t, t, r[k]);
+                t = xi.y - xk.y;
+                r[k] = fmaf(t, t, r[k]);
+                t = xi.z - xk.z;
+                r[k] = fmaf(t, t, r[k]);
+                t = xi.w - xk.w;
+                r[k] = fmaf(t, t, r[k]);
+            }
+            const float4 xp = xs4[M * ds4 + f4];
+            float t = xi.x - xp.x;
+            rp = fmaf(t, t, rp);
+            t = xi.y - xp.y;
+            rp = fmaf(t, t, rp);
+            t = xi.z - xp.z;
+            rp = fmaf(t, t, rp);
+            t = xi.w - xp.w;
+            rp = fmaf(t, t, rp);
         }
-        const TC t = xi - xs[M * ds + f];
-        rp = fma(t, t, rp);
+    } else {
+        for (int f = 0; f < d; ++f) {
+            const TC xi = xs[lane * ds + f];
+#pragma unroll
+            for (int k = 0; k < M; ++k) {
+                const TC t = xi - xs[k * ds + f];
+                r[k] = fma(t, t, r[k]);
+            }
+            const TC t = xi - xs[M * ds + f];
+            rp = fma(t, t, rp);
+        }
     }
     const TC rbf = (TC)a.rbf, cst = (TC)a.cst;
     const TC diag_add = (TC)a.noise + ((int64_t)j < a.alpha_below ? (TC)a.alpha : TC(0));
@@ -197,6 +242,7 @@ __device__ __forceinline__ bool warp_system(const LocalArgs &a, int64_t p, int l
         const bool vk = (vmask >> k) & 1u;
         const TC e = rbf * kern_s<MATERN>(a.family, r[k]);
         if (STASH) Es[lane * (M + 1) + k] = e;
+        if (STASH_R) Rs[lane * (M + 1) + k] = (float)r[k];
         TC kv = (valid && vk) ? e + cst : TC(0);
         if (k == lane) kv = valid ? kv + diag_add : TC(1);
         r[k] = kv;
@@ -321,19 +367,25 @@ __device__ __forceinline__ bool warp_system(const LocalArgs &a, int64_t p, int l
         }
     }
 
-    // recompute squared distances (xs is intact)
+    // the fill's squared distances: kept (FP32 RBF), else recomputed (xs is intact); rp still
+    // holds the fill's distance to the point itself
+    if constexpr (STASH_R) {
 #pragma unroll
-    for (int k = 0; k < M; ++k) r[k] = TC(0);
-    rp = TC(0);
-    for (int f = 0; f < d; ++f) {
-        const TC xi = xs[lane * ds + f];
+        for (int k = 0; k < M; ++k) r[k] = (TC)Rs[lane * (M + 1) + k];
+    } else {
 #pragma unroll
-        for (int k = 0; k < M; ++k) {
-            const TC t = xi - xs[k * ds + f];
-            r[k] = fma(t, t, r[k]);
+        for (int k = 0; k < M; ++k) r[k] = TC(0);
+        rp = TC(0);
+        for (int f = 0; f < d; ++f) {
+            const TC xi = xs[lane * ds + f];
+#pragma unroll
+            for (int k = 0; k < M; ++k) {
+                const TC t = xi - xs[k * ds + f];
+                r[k] = fma(t, t, r[k]);
+            }
+            const TC t = xi - xs[M * ds + f];
+            rp = fma(t, t, rp);
         }
-        const TC t = xi - xs[M * ds + f];
-        rp = fma(t, t, rp);
     }
     TC g_amp = TC(0), g_cst = TC(0), g_noise = TC(0), g_iso = TC(0);
 #pragma unroll
@@ -397,7 +449,7 @@ __global__ void __launch_bounds__(kLocWarps * 32, 3) local_warp_kernel(
     const TIn *__restrict__ x_pt, const TIn *__restrict__ y_pt, const int32_t *__restrict__ nbr,
     double *__restrict__ block_out, TIn *__restrict__ mean, TIn *__restrict__ var, int32_t *__restrict__ flags) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const WarpSmem lay = WarpSmem::make(a.d, a.n_theta);
+    const WarpSmem lay = WarpSmem::make(a.d, a.n_theta, std::is_same<TIn, float>::value);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned char *wsm = smem_raw + warp * lay.total;
     double *gacc = reinterpret_cast<double *>(wsm + lay.g_off);
@@ -758,13 +810,14 @@ struct LocalPlan {
     size_t ws_bytes = 0;
 };
 
-LocalPlan plan_local(int64_t n_points, int d, int m, int n_theta, bool grad) {
+// f32: the launch runs the FP32-input kernels (their warp layout keeps the squared distances)
+LocalPlan plan_local(int64_t n_points, int d, int m, int n_theta, bool grad, bool f32 = false) {
     LocalPlan p;
     p.warp = m <= kWarpM;
     p.nt = 1 + (grad ? n_theta : 0);
     const int sms = num_sms();
     if (p.warp) {
-        p.smem = WarpSmem::make(d, n_theta).total * kLocWarps;
+        p.smem = WarpSmem::make(d, n_theta, f32).total * kLocWarps;
         const int64_t need = (n_points + kLocWarps - 1) / kLocWarps;
         p.grid = (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)sms * 8));
     } else {
@@ -865,7 +918,7 @@ nngp_status loglik_impl(const TIn *x, const TIn *y, int64_t n, int d, int ydim, 
         return NNGP_OK;
     }
     if (!x || !y || (m > 0 && !nbr)) return fail(NNGP_ERR_INVALID_ARGUMENT, "loglik: null input pointer");
-    const LocalPlan pl = plan_local(rows, d, m, a.n_theta, grad);
+    const LocalPlan pl = plan_local(rows, d, m, a.n_theta, grad, std::is_same<TIn, float>::value);
     if (!ws || ws_bytes < pl.ws_bytes) return fail(NNGP_ERR_WORKSPACE, "loglik: workspace missing or too small");
     unsigned char *head = reinterpret_cast<unsigned char *>(align_up(reinterpret_cast<uintptr_t>(ws), 256));
     a.fp64_count = reinterpret_cast<unsigned long long *>(head);
@@ -893,7 +946,7 @@ nngp_status predict_impl(const TIn *xt, const TIn *yt, int64_t nt, const TIn *xq
     if (st != NNGP_OK) return st;
     if (nq == 0) return NNGP_OK;
     if (!xq || !mean || !var || (m > 0 && (!nbr || !xt || !yt))) return fail(NNGP_ERR_INVALID_ARGUMENT, "predict: null pointer");
-    const LocalPlan pl = plan_local(nq, d, m, 0, false);
+    const LocalPlan pl = plan_local(nq, d, m, 0, false, std::is_same<TIn, float>::value);
     return launch_local<TIn, false, true>(pl, a, xt, yt, xq, nullptr, nbr, nullptr, mean, var, flags, stream);
 }
 

@@ -62,10 +62,9 @@ def test_reference_calc_nn_compiled_from_its_source(d, m, cut):
     b = ops.knn(x, q, m, cut, ls).cpu().numpy()
     same_rows = np.all(a == b, axis=1).mean()
     assert same_rows >= 0.99, same_rows
-    # the sets agree wherever the lists differ only in a near tie: every row's set overlaps in all
-    # but at most two slots
-    overlap = np.array([len(set(r) & set(s)) for r, s in zip(a, b)])
-    assert overlap.min() >= m - 2
+    # where the lists differ it is a near tie at the edge or a swap: at most two refs differ per row
+    differ = np.array([len(set(r.tolist()) ^ set(s.tolist())) for r, s in zip(a, b)])
+    assert differ.max() <= 4
 
 
 def test_reference_fill_kernel_compiled_from_its_source():
