@@ -85,7 +85,7 @@ WORKLOADS = {
                   'noise 1e-4; tensor-core fp32 exact neighbour search, fp32 local systems with fp64 re-solve of '
                   'small pivots, fp64 reductions'),
         DATA='synthetic (64-component GMM in 16-d, 256 random Fourier features; shape 1000000 x 16)',
-        DTYPE='f32 search (tf32-split tensor screen) + f32 local (f64 re-solve) + f64 sums'),
+        DTYPE='f32 search (bf16x3-split tensor screen) + f32 local (f64 re-solve) + f64 sums'),
 }
 WORKLOADS['differentiation'] = dict(
     N_TRAIN=434_874, D=8, M=32, NOISE=4e-4, ALPHA=1e-10, LOCAL='f32', ROOF='fp32',
@@ -99,7 +99,7 @@ WORKLOADS['serving'] = dict(
     WORKLOAD=('served predict, fitted model n=16599 d=18 m=32 held in HBM, ARD RBF, noise 1e-2; Poisson stream '
               'of requests with log-uniform sizes in [1, 65536]; continuous batching, CUDA graphs per size bucket'),
     DATA='synthetic (N(0,1)^18, ARD length scales log-uniform in [0.5, 5], 256 random Fourier features)',
-    DTYPE='f32 search (tf32-split tensor screen) + f32 local (f64 re-solve)')
+    DTYPE='f32 search (bf16x3-split tensor screen) + f32 local (f64 re-solve)')
 _WL = 'fit3d'
 
 
@@ -466,15 +466,19 @@ def read_profile_traffic():
     return None
 
 
-def tf32_peak_tflops():
-    """Dense TF32 tensor rate: half the BF16 dense rate measured on this pool's B200s
-    (MEASURED_PEAKS.json, burst), the ratio of NVIDIA's dense figures (1.1 vs 2.25 PFLOP/s)."""
+def tensor_peak_tflops(bf16_operands):
+    """Dense tensor rate of the search's operand type: the BF16 dense rate measured on this
+    pool's B200s (MEASURED_PEAKS.json, burst) for BF16 operands, half of it for TF32 (the ratio
+    of NVIDIA's dense figures, 1.1 vs 2.25 PFLOP/s)."""
     try:
         with open(os.path.join(ROOT, 'MEASURED_PEAKS.json')) as f:
             bf16 = float(json.load(f)['bf16_tflops'])
-        return bf16 / 2.0, 'MEASURED_PEAKS.json bf16_tflops (burst) / 2: the TF32 dense rate'
+        src = 'MEASURED_PEAKS.json bf16_tflops (burst)'
     except Exception:
-        return 1590.0 / 2.0, 'fallback 1.59 PFLOP/s BF16 dense / 2: the TF32 dense rate'
+        bf16, src = 1590.0, 'fallback 1.59 PFLOP/s BF16 dense'
+    if bf16_operands:
+        return bf16, src + ': the BF16 dense rate'
+    return bf16 / 2.0, src + ' / 2: the TF32 dense rate'
 
 
 def fp32_peak_tflops(torch, L, stream_ptr):
@@ -979,10 +983,13 @@ def run_ours(args):
         ms_per_step = tot_ms / args.steps
         # the pipe that bounds the search: the FP32/ALU issue of the screen at small d (the distance
         # work is cheap), the tensor pipe at d = 16 (the survey's roofline for that configuration)
-        kp = (3 * (D + 1) + 7) // 8 * 8  # TF32 split width of the tensor-core operands
+        bf16_ops = D >= 12  # the search's operand type: BF16 x3 split from d = 12, TF32 split below
+        kmma = 16 if bf16_ops else 8
+        kp = (3 * (D + 1) + kmma - 1) // kmma * kmma  # split width of the tensor-core operands
         issued = 2.0 * kp * pairs / (knn_avg_ms * 1e-3) / 1e12
         local_avg_ms = float(np.mean([a - b for a, b in zip(step_ms, knn_ms)]))
-        search = {'kernel': f'knn_tc_kernel<{D}> (prefix search: tcgen05 TF32-split screen, exact FP32 rescoring; '
+        screen = 'BF16x3-split (kind::f16)' if bf16_ops else 'TF32-split (kind::tf32)'
+        search = {'kernel': f'knn_tc_kernel<{D}> (prefix search: tcgen05 {screen} screen, exact FP32 rescoring; '
                             f'seeded rows, pruned tile lists)',
                   'ms': knn_avg_ms,
                   'brute_force_equivalent_tflops': achieved,
@@ -998,7 +1005,7 @@ def run_ours(args):
                     'work': 'per point: 2k^3/3 + k(k+1)/2 (3d + 4 + 4 n_theta) + 4k^2 FP64 flops, k = m + 1',
                     'local_ms': local_avg_ms, 'search': search}
         elif ROOF == 'tensor':
-            tpk, tsrc = tf32_peak_tflops()
+            tpk, tsrc = tensor_peak_tflops(bf16_ops)
             roof = {'bound': 'tensor', 'achieved': achieved, 'peak': tpk, 'unit': 'TFLOP/s', 'frac': achieved / tpk,
                     'peak_source': tsrc, 'issued_mma_tflops': issued, 'issued_frac': issued / tpk,
                     'fp32_fma_equivalent': {'peak': peak, 'frac': achieved / peak,
@@ -1018,7 +1025,7 @@ def run_ours(args):
             'e2e': e2e,
             'roofline': dict(roof, traffic=read_profile_traffic()) if ROOF == 'local' else dict(
                 roof, traffic=read_profile_traffic(),
-                kernel=f'knn_tc_kernel<{D}> (prefix search: tcgen05 TF32-split screen, exact FP32 rescoring)',
+                kernel=f'knn_tc_kernel<{D}> (prefix search: tcgen05 {screen} screen, exact FP32 rescoring)',
                 work='2*d flops per (query, ref) pair, n(n-1)/2 pairs, whichever pipe computes them; '
                      'issued_mma = 2*K\' per pair with the split width K\'',
                 pruned=search_is_pruned(n, D),

@@ -585,9 +585,14 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
             };
 
             const uint32_t G = g_tile;
+            // the next tile's list entry is loaded one tile ahead (a global load per tile that
+            // would otherwise sit on the path from the accumulator to the screen)
+            int64_t tl_next = (pruned && ntiles > 0) ? (int64_t)tl[0] : 0;
             for (uint32_t t = 0; t < ntiles; ++t) {
                 const uint32_t g = G + t;
                 const uint32_t s = g % S, b = g % C::NBUF;
+                const int64_t tl_cur = tl_next;
+                if (pruned && t + 1 < ntiles) tl_next = (int64_t)tl[t + 1];
                 if (!mbar_wait_bounded(&t_full[b], (g / C::NBUF) & 1, wait_ns)) aborted = true;
                 if (__any_sync(FULL, aborted)) {
                     aborted = true;
@@ -596,7 +601,7 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
                 tc_fence_after();
                 const float *exs = reinterpret_cast<const float *>(sB + s * C::STAGE_BYTES + C::OP_BYTES);
                 const int32_t *ixs = reinterpret_cast<const int32_t *>(sB + s * C::STAGE_BYTES + C::OP_BYTES + C::EX_BYTES);
-                const int64_t j0 = (pruned ? (int64_t)tl[t] : (int64_t)(tfirst + t)) * RT;  // first ref position of the tile
+                const int64_t j0 = (pruned ? tl_cur : (int64_t)(tfirst + t)) * RT;  // first ref position of the tile
                 const uint32_t taddr = tmem_base + ((uint32_t)(quad * 32) << 16) + b * C::BUF_COLS + qtw * RT;
                 // screen one 32-column chunk (scores in v): this row's candidate mask, 0 when no row
                 // of the warp has one (the common case, a handful of instructions)
