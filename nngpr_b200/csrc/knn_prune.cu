@@ -352,62 +352,113 @@ struct Boxes {
     double gamma;
 };
 
-// May ref tile t hold a neighbour of a row of group g?
-__device__ __forceinline__ bool tile_needed(const Boxes &b, int64_t g, int64_t t) {
-    if (b.tmin[t] >= b.glim[g]) return false;  // every ref of the tile comes after every row
-    const double tau = (double)b.gtau[g];
-    if (isinf(tau)) return true;
-    double lb = 0.0;
-    for (int f = 0; f < b.d; ++f) {
-        const double gap = fmax(0.0, fmax((double)b.tlo[t * b.d + f] - (double)b.ghi[g * b.d + f],
-                                          (double)b.glo[g * b.d + f] - (double)b.thi[t * b.d + f]));  // NaN -> 0
-        lb += gap * gap;
+// 32-bit words of one group's tile masks
+__host__ __device__ __forceinline__ int64_t mask_words(int64_t n_tiles) { return (n_tiles + 31) / 32; }
+
+// The box of group g and its bound, held in registers by every lane of the warp that tests the
+// group against all tiles.
+struct GroupBox {
+    float lo[kMaxDim], hi[kMaxDim];
+    double tau;
+    int32_t lim;
+};
+
+__device__ __forceinline__ GroupBox load_group(const Boxes &b, int64_t g) {
+    GroupBox q;
+#pragma unroll
+    for (int f = 0; f < kMaxDim; ++f) {
+        q.lo[f] = f < b.d ? b.glo[g * b.d + f] : 0.f;
+        q.hi[f] = f < b.d ? b.ghi[g * b.d + f] : 0.f;
     }
-    return !(lb * (1.0 - b.gamma) - 1e-37 > tau);
+    q.tau = (double)b.gtau[g];
+    q.lim = b.glim[g];
+    return q;
 }
 
-// Do the boxes of ref tile t and group g intersect?
-__device__ __forceinline__ bool box_overlap(const Boxes &b, int64_t g, int64_t t) {
-    for (int f = 0; f < b.d; ++f)
-        if (b.tlo[t * b.d + f] > b.ghi[g * b.d + f] || b.glo[g * b.d + f] > b.thi[t * b.d + f]) return false;
-    return true;
+// May ref tile t hold a neighbour of a row of the group (need), and does its box meet the
+// group's (overlap)?
+__device__ __forceinline__ void tile_test(const Boxes &b, const GroupBox &q, int64_t t, bool &need, bool &overlap) {
+    need = false;
+    overlap = false;
+    if (b.tmin[t] >= q.lim) return;  // every ref of the tile comes after every row
+    double lb = 0.0;
+    bool meet = true;
+#pragma unroll
+    for (int f = 0; f < kMaxDim; ++f) {
+        if (f < b.d) {
+            const float tl = b.tlo[t * b.d + f], th = b.thi[t * b.d + f];
+            meet = meet && !(tl > q.hi[f] || q.lo[f] > th);
+            const double gap = fmax(0.0, fmax((double)tl - (double)q.hi[f], (double)q.lo[f] - (double)th));  // NaN -> 0
+            lb += gap * gap;
+        }
+    }
+    need = isinf(q.tau) || !(lb * (1.0 - b.gamma) - 1e-37 > q.tau);
+    overlap = need && meet;
 }
 
-// One warp per group: counts[g] = tiles needed (0 for the slots past the groups).
+// One warp per group: counts[g] = tiles needed (0 for the slots past the groups), and the
+// group's masks of needed tiles and of needed tiles whose box meets the group's (32 tiles per
+// word: masks[(g * words + w) * 2 + {0, 1}]).
 __global__ void __launch_bounds__(kThreads) count_kernel(Boxes b, const DevSizes *__restrict__ pruned,
                                                          int64_t max_groups, int64_t n_tiles,
-                                                         int32_t *__restrict__ counts) {
+                                                         int32_t *__restrict__ counts, uint32_t *__restrict__ masks) {
     const int lane = threadIdx.x & 31;
     const int64_t n_groups = pruned->n_groups;
+    const int64_t words = mask_words(n_tiles);
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t g = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; g < max_groups; g += nw) {
         int c = 0;
-        if (g < n_groups)
-            for (int64_t t = lane; t < n_tiles; t += 32) c += tile_needed(b, g, t) ? 1 : 0;
-        c = (int)__reduce_add_sync(0xFFFFFFFFu, (unsigned)c);
+        if (g < n_groups) {
+            const GroupBox q = load_group(b, g);
+            for (int64_t base = 0; base < n_tiles; base += 32) {
+                const int64_t t = base + lane;
+                bool need = false, ov = false;
+                if (t < n_tiles) tile_test(b, q, t, need, ov);
+                const unsigned nm = __ballot_sync(0xFFFFFFFFu, need), om = __ballot_sync(0xFFFFFFFFu, ov);
+                if (lane == 0) {
+                    masks[(g * words + base / 32) * 2] = nm;
+                    masks[(g * words + base / 32) * 2 + 1] = om;
+                }
+                c += __popc(nm);
+            }
+        }
         if (lane == 0) counts[g] = c;
     }
 }
 
 // One warp per group: the needed tiles at list[offsets[g] ..), first those whose box meets the
 // group's box (they hold most of the rows' nearest refs, so the rows' bounds tighten early),
-// then the others, each part in ascending order.
-__global__ void __launch_bounds__(kThreads) fill_kernel(Boxes b, const DevSizes *__restrict__ pruned, int64_t n_tiles,
+// then the others, each part in ascending order (from the masks of count_kernel).
+__global__ void __launch_bounds__(kThreads) fill_kernel(const DevSizes *__restrict__ pruned, int64_t n_tiles,
                                                         const int32_t *__restrict__ offsets,
+                                                        const uint32_t *__restrict__ masks,
                                                         int32_t *__restrict__ list) {
     const int lane = threadIdx.x & 31;
     const int64_t n_groups = pruned->n_groups;
+    const int64_t words = mask_words(n_tiles);
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t g = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; g < n_groups; g += nw) {
         int64_t o = offsets[g];
+        const uint32_t *mg = masks + g * words * 2;
         for (int pass = 0; pass < 2; ++pass) {
-            for (int64_t base = 0; base < n_tiles; base += 32) {
-                const int64_t t = base + lane;
-                bool need = t < n_tiles && tile_needed(b, g, t);
-                if (need) need = box_overlap(b, g, t) == (pass == 0);
-                const unsigned mask = __ballot_sync(0xFFFFFFFFu, need);
-                if (need) list[o + __popc(mask & ((1u << lane) - 1u))] = (int32_t)t;
-                o += __popc(mask);
+            for (int64_t wb = 0; wb < words; wb += 32) {
+                const int64_t w = wb + lane;
+                uint32_t bits = 0;
+                if (w < words) bits = pass == 0 ? (mg[w * 2] & mg[w * 2 + 1]) : (mg[w * 2] & ~mg[w * 2 + 1]);
+                const int cnt = __popc(bits);
+                int pre = cnt;  // inclusive prefix over the lanes
+#pragma unroll
+                for (int k = 1; k < 32; k <<= 1) {
+                    const int v = __shfl_up_sync(0xFFFFFFFFu, pre, k);
+                    if (lane >= k) pre += v;
+                }
+                int64_t at = o + pre - cnt;
+                while (bits) {
+                    const int bpos = __ffs(bits) - 1;
+                    bits &= bits - 1;
+                    list[at++] = (int32_t)(w * 32 + bpos);
+                }
+                o += __shfl_sync(0xFFFFFFFFu, pre, 31);
             }
         }
     }
@@ -542,7 +593,7 @@ __global__ void uniform_groups_kernel(int64_t n_rows, int G, int64_t n_groups, i
 struct Layout {
     int64_t n_tiles, max_groups;
     size_t tlo, thi, tmin, stats, keys_a, keys_b, vals_a, vals_b, rvals_a, rvals_b, headpos, seg_start, gh, gid, row_off, sizes, glo,
-        ghi, gtau, glim, counts, offsets, list, cub, cub_bytes, total;
+        ghi, gtau, glim, counts, offsets, masks, list, cub, cub_bytes, total;
     int64_t maxg[2], max_items[2];
     size_t cnt[2], cbase[2], K[2], kbase[2], S[2], sbase[2], igroup[2], it0[2], it1[2], islot[2], okey_a[2], okey_b[2],
         oval_a[2], oval_b[2], partial[2];
@@ -582,6 +633,7 @@ Layout layout(int64_t n, int d, int G) {
     L.glim = take((size_t)L.max_groups * 4);
     L.counts = take((size_t)(L.max_groups + 1) * 4);
     L.offsets = take((size_t)(L.max_groups + 1) * 4);
+    L.masks = take((size_t)L.max_groups * mask_words(L.n_tiles) * 2 * 4);
     L.maxg[0] = L.max_groups;
     L.maxg[1] = (n + G - 1) / G;
     for (int p = 0; p < 2; ++p) {
@@ -685,6 +737,7 @@ Layout layout_query(int64_t n_ref, int64_t n_query, int d, int G) {
     L.glim = take((size_t)L.max_groups * 4);
     L.counts = take((size_t)(L.max_groups + 1) * 4);
     L.offsets = take((size_t)(L.max_groups + 1) * 4);
+    L.masks = take((size_t)L.max_groups * mask_words(L.n_tiles) * 2 * 4);
     L.maxg[0] = L.max_groups;
     L.maxg[1] = 0;
     const int64_t g1 = L.maxg[0] + 1;
@@ -814,7 +867,9 @@ nngp_status build(const float *xs, int64_t n, int64_t row_lo, int64_t row_hi, in
     NNGP_CUDA_TRY(cudaGetLastError());
     Boxes b{tlo, thi, glo, ghi, gtau, tmin, glim, d, (double)(d + 3) * 1.1920928955078125e-07};
     NNGP_CUDA_TRY(cudaMemsetAsync(counts + L.max_groups, 0, sizeof(int32_t), stream));
-    count_kernel<<<grid_of(L.max_groups * 32), kThreads, 0, stream>>>(b, sizes, L.max_groups, L.n_tiles, counts);
+    uint32_t *masks = static_cast<uint32_t *>(at(L.masks));
+    count_kernel<<<grid_of(L.max_groups * 32), kThreads, 0, stream>>>(b, sizes, L.max_groups, L.n_tiles, counts,
+                                                                       masks);
     NNGP_CUDA_TRY(cudaGetLastError());
     need = 0;
     NNGP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, need, counts, offsets, (int)(L.max_groups + 1), stream));
@@ -825,7 +880,7 @@ nngp_status build(const float *xs, int64_t n, int64_t row_lo, int64_t row_hi, in
     NNGP_CUDA_TRY(cudaGetLastError());
     fallback_rows_kernel<<<grid_of(row_hi - row_lo), kThreads, 0, stream>>>(row_lo, row_hi, fallback, rows);
     NNGP_CUDA_TRY(cudaGetLastError());
-    fill_kernel<<<grid_of(L.max_groups * 32), kThreads, 0, stream>>>(b, sizes, L.n_tiles, offsets, list);
+    fill_kernel<<<grid_of(L.max_groups * 32), kThreads, 0, stream>>>(sizes, L.n_tiles, offsets, masks, list);
     NNGP_CUDA_TRY(cudaGetLastError());
 
     // work items of both launches: long tile ranges split, most tiles first
@@ -880,14 +935,16 @@ nngp_status build_query(const float *xs_ref, int64_t n_ref, const float *xq, int
     NNGP_CUDA_TRY(cudaGetLastError());
     Boxes b{tlo, thi, glo, ghi, gtau, tmin, glim, d, (double)(d + 3) * 1.1920928955078125e-07};
     NNGP_CUDA_TRY(cudaMemsetAsync(counts + L.max_groups, 0, sizeof(int32_t), stream));
-    count_kernel<<<grid_of(L.max_groups * 32), kThreads, 0, stream>>>(b, sizes, L.max_groups, L.n_tiles, counts);
+    uint32_t *masks = static_cast<uint32_t *>(at(L.masks));
+    count_kernel<<<grid_of(L.max_groups * 32), kThreads, 0, stream>>>(b, sizes, L.max_groups, L.n_tiles, counts,
+                                                                       masks);
     NNGP_CUDA_TRY(cudaGetLastError());
     size_t need = 0;
     NNGP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, need, counts, offsets, (int)(L.max_groups + 1), stream));
     if (need > L.cub_bytes) return fail(NNGP_ERR_WORKSPACE, "knn pruning: scan scratch exceeds the budget");
     size_t have = L.cub_bytes;
     NNGP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(at(L.cub), have, counts, offsets, (int)(L.max_groups + 1), stream));
-    fill_kernel<<<grid_of(L.max_groups * 32), kThreads, 0, stream>>>(b, sizes, L.n_tiles, offsets, list);
+    fill_kernel<<<grid_of(L.max_groups * 32), kThreads, 0, stream>>>(sizes, L.n_tiles, offsets, masks, list);
     NNGP_CUDA_TRY(cudaGetLastError());
     if ((st = plan_items(L, base, 0, sizes, offsets, qorder, G, n_ref, out, stream)) != NNGP_OK) return st;
     out->rows = qorder;

@@ -58,8 +58,10 @@ constexpr int THREADS = 5 * 32;   // layout self-test: 4 epilogue warps + the MM
 constexpr int LIST = 32;       // largest num_nn
 constexpr int HS = 33;         // heap row stride in 64-bit keys (odd: rows of a warp hit distinct banks)
 constexpr int DRAIN_AT = 32;   // queued entries that trigger a drain at the end of a tile (8: +2%, 128: +7% at d = 3)
-constexpr int QCAP = 64;       // candidate queue entries per epilogue warp (a drain runs before an
-                               // iteration that could overflow it; 64 leaves room for a third stage)
+constexpr int QCAP = 64;       // key queue entries per epilogue warp (a drain runs before a batch
+                               // that could overflow it)
+constexpr int CQCAP = 96;      // screened candidates queued per epilogue warp for rescoring
+constexpr int MAX_STAGES = 8;  // ring stages (mbarrier slots)
 constexpr uint32_t kSelftestCols = 2 * RT;  // TMEM columns of the layout self-test
 constexpr float kEpsTc = 1.52587890625e-05f;       // 2^-16: TF32 x3 split
 constexpr float kEpsBf = 6.103515625e-05f;         // 2^-14: BF16 x3 split
@@ -81,7 +83,6 @@ struct Cfg {
     static constexpr int KMMA = BF16 ? 16 : 8;      // UMMA K of one instruction
     static constexpr float EPS = BF16 ? kEpsBf : kEpsTc;
     static constexpr int EPI_WARPS = 4 * QTILES;
-    static constexpr int THREADS = (EPI_WARPS + 1) * 32;
     static constexpr int ROWS = QT * QTILES;        // queries per work item
     static constexpr int U = D + 1;                 // coordinates + the norm column
     static constexpr int KP = (3 * U + KMMA - 1) / KMMA * KMMA;  // split operand width
@@ -89,18 +90,24 @@ struct Cfg {
     static constexpr int DP = (D + 3) / 4 * 4;      // exact-coordinate row length
     static constexpr int OP_BYTES = RT * KP * ESZ;  // B operand block of a ref tile
     static constexpr int EX_BYTES = RT * DP * 4;    // exact coordinates of a ref tile
-    // where a staged tile keeps its refs' point indices: the spare last slot of each exact-coordinate
+    // where a tile record keeps its refs' point indices: the spare last slot of each exact-coordinate
     // row when DP > D (1), a block after the coordinates for the BF16 shapes (2); D = 4 and 8 read
-    // them from global memory (0: a block would cost those shapes a pipeline stage)
+    // them from ref_perm (0)
     static constexpr int IX_MODE = DP > D ? 1 : (BF16 ? 2 : 0);
     static constexpr int IX_BYTES = IX_MODE == 2 ? RT * 4 : 0;
-    static constexpr int STAGE_BYTES = OP_BYTES + EX_BYTES + IX_BYTES;
+    // a ref tile in global memory: [B operand | exact coordinates | indices]; only the B operand
+    // is staged in shared memory (the MMAs' input), so a stage is free again as soon as its MMAs
+    // complete.  The screen passes about one pair in 3,000 at d = 16: the epilogue reads those
+    // pairs' exact coordinates and indices from the record in global memory, 32 at a time.
+    static constexpr int TILE_BYTES = OP_BYTES + EX_BYTES + IX_BYTES;
+    static constexpr int STAGE_BYTES = OP_BYTES;
     static constexpr int A_TILE = QT * KP * ESZ;    // query operand of one query tile
     static constexpr int A_BYTES = A_TILE * QTILES;
     static constexpr int LIST_BYTES = ROWS * HS * 8;  // one heap of keys per query
     static constexpr int QUEUE_BYTES = EPI_WARPS * QCAP * (8 + 1);  // key + row
+    static constexpr int CQ_BYTES = EPI_WARPS * CQCAP * 8;          // ref position << 5 | row
     static constexpr int BAR_BYTES = 256;
-    static constexpr int FIXED = 128 + A_BYTES + LIST_BYTES + QUEUE_BYTES + BAR_BYTES;  // 128: base alignment slack
+    static constexpr int FIXED = 128 + A_BYTES + LIST_BYTES + QUEUE_BYTES + CQ_BYTES + BAR_BYTES;  // 128: alignment slack
     // as many CTAs per SM (up to 3) as hold at least 2 stages each: more epilogue warps per
     // scheduler.  Three CTAs share TMEM with one accumulator buffer each (the epilogue frees it
     // as soon as a tile's scores are in registers); one or two CTAs double-buffer it.
@@ -109,7 +116,14 @@ struct Cfg {
     static constexpr int ST1 = (220 * 1024 - FIXED) / STAGE_BYTES;
     static constexpr int CTAS_PER_SM = ST3 >= 2 ? 3 : (ST2 >= 2 ? 2 : 1);
     static constexpr int STN = CTAS_PER_SM == 3 ? ST3 : (CTAS_PER_SM == 2 ? ST2 : ST1);
-    static constexpr int STAGES = STN > 4 ? 4 : STN;
+    static constexpr int STAGES = STN > MAX_STAGES ? MAX_STAGES : STN;
+    // A CTA alone on its SM streams its tiles from a warp of its own: the MMA warp then waits
+    // only for a staged tile and a free accumulator buffer, never for a stage to be refilled,
+    // and each copy starts as soon as the MMAs of the stage's previous tile complete.  With 2 or
+    // 3 CTAs per SM the other CTAs fill those gaps, and the register budget has no room for
+    // another warp: the MMA warp issues the copies itself.
+    static constexpr bool TMA_WARP = CTAS_PER_SM == 1;
+    static constexpr int THREADS = (EPI_WARPS + 1 + (TMA_WARP ? 1 : 0)) * 32;
     static constexpr int SMEM = FIXED + STAGES * STAGE_BYTES;
     static constexpr int NBUF = CTAS_PER_SM == 3 ? 1 : 2;  // accumulator buffers in TMEM
     static constexpr uint32_t BUF_COLS = RT * QTILES;       // one buffer: a tile per query tile
@@ -291,7 +305,7 @@ __global__ void build_tc_tiles_kernel(const float *__restrict__ xs, int64_t n, i
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n_pad; i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t t = i / RT;
         const int row = (int)(i - t * RT);
-        unsigned char *base = tiles + t * C::STAGE_BYTES;
+        unsigned char *base = tiles + t * C::TILE_BYTES;
         float b[C::U];
         float ex[C::DP];
 #pragma unroll
@@ -359,18 +373,21 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
     unsigned char *sB = sA + C::A_BYTES;
     uint64_t *H = reinterpret_cast<uint64_t *>(sB + S * C::STAGE_BYTES);  // [ROWS][HS] heaps
     unsigned char *qbase = reinterpret_cast<unsigned char *>(H + C::ROWS * HS);
-    uint64_t *bars = reinterpret_cast<uint64_t *>(qbase + C::QUEUE_BYTES);
-    uint64_t *b_full = bars;        // [S <= 4]
-    uint64_t *b_empty = bars + 4;   // [S <= 4]
-    uint64_t *t_full = bars + 8;    // [2]
-    uint64_t *t_empty = bars + 10;  // [2]
-    uint64_t *a_ready = bars + 12;  // [1]
-    volatile uint32_t *tmem_slot = reinterpret_cast<volatile uint32_t *>(bars + 14);
-    volatile int *s_item = reinterpret_cast<volatile int *>(bars + 15);
-    volatile int *s_abort = reinterpret_cast<volatile int *>(bars + 16);
+    uint64_t *cqbase = reinterpret_cast<uint64_t *>(qbase + C::QUEUE_BYTES);  // [EPI_WARPS][CQCAP] candidates
+    uint64_t *bars = cqbase + EPI_WARPS * CQCAP;
+    uint64_t *b_full = bars;                    // [S <= MAX_STAGES]
+    uint64_t *b_empty = bars + MAX_STAGES;      // [S <= MAX_STAGES]
+    uint64_t *t_full = bars + 2 * MAX_STAGES;   // [2]
+    uint64_t *t_empty = t_full + 2;             // [2]
+    uint64_t *a_ready = t_full + 4;             // [1]
+    volatile uint32_t *tmem_slot = reinterpret_cast<volatile uint32_t *>(t_full + 5);
+    volatile int *s_item = reinterpret_cast<volatile int *>(t_full + 6);
+    volatile int *s_abort = reinterpret_cast<volatile int *>(t_full + 7);
+    static_assert((2 * MAX_STAGES + 8) * 8 <= C::BAR_BYTES, "barrier block");
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const bool producer_warp = warp == EPI_WARPS;
+    const bool producer_warp = warp == EPI_WARPS;                 // MMA issue (and the copies without TMA_WARP)
+    const bool copy_warp = C::TMA_WARP && warp == EPI_WARPS + 1;  // the copies with TMA_WARP
     // Rows: positions [first_row, first_row + n_rows) of rows_perm (point indices; the positions
     // themselves when rows_perm is null), from dev_sizes = {first_row, n_rows, n_items} on the
     // device or {0, n_query, ceil(n_query / ROWS)}; work item g is positions
@@ -388,7 +405,7 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
     if (threadIdx.x == 0) {
         for (int s = 0; s < S; ++s) {
             mbar_init(&b_full[s], 1);
-            mbar_init(&b_empty[s], 1 + EPI_WARPS);  // the MMA commit + the epilogue warps (exact coordinates)
+            mbar_init(&b_empty[s], 1);  // the MMA commit: the epilogue never reads a stage
         }
         for (int b = 0; b < C::NBUF; ++b) {
             mbar_init(&t_full[b], 1);
@@ -452,29 +469,54 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
             ntiles = (uint32_t)((block_limit + RT - 1) / RT);
         }
         const int32_t *tl = pruned ? tile_list + tile_off[qtile] + tfirst : nullptr;  // this item's ref tiles
+        const uint32_t G = g_tile;
+        // stage g % S is free once the MMAs and the epilogue of tile g - S are done with it
+        auto wait_empty = [&](uint32_t g) -> bool {
+            const uint32_t k = g / S;
+            return mbar_wait_bounded(&b_empty[g % S], (k & 1) ^ 1, wait_ns);
+        };
+        // the tile record the item's t-th tile comes from
+        auto tile_at = [&](uint32_t t) -> int64_t { return pruned ? (int64_t)tl[t] : (int64_t)(tfirst + t); };
+        auto issue_tma = [&](uint32_t g, int64_t t) {
+            const uint32_t s = g % S;
+            mbar_arrive_expect_tx(&b_full[s], C::STAGE_BYTES);
+            tma_bulk_g2s(sB + s * C::STAGE_BYTES, tiles_g + t * C::TILE_BYTES, C::STAGE_BYTES, &b_full[s]);
+            tma_issued = g + 1;
+        };
 
-        if (producer_warp) {
+        if (copy_warp) {
+            // the item's tiles in order, each as soon as its stage is free (no query operand
+            // needed); the warp reads the tile list 32 entries at a time, so no dependent global
+            // load sits between two copies
+            int64_t ent = 0;
+            for (uint32_t t = 0; t < ntiles; ++t) {
+                if ((t & 31u) == 0) ent = t + lane < ntiles ? tile_at(t + lane) : 0;
+                const int64_t cur = __shfl_sync(FULL, ent, (int)(t & 31u));
+                bool ok = true;
+                if (lane == 0) {
+                    ok = wait_empty(G + t);
+                    if (ok) issue_tma(G + t, cur);
+                }
+                if (!__shfl_sync(FULL, ok, 0)) {
+                    aborted = true;
+                    break;
+                }
+            }
+            __syncwarp();
+        } else if (producer_warp) {
             if (lane == 0) {
                 if (!mbar_wait_bounded(a_ready, it & 1, wait_ns)) aborted = true;  // query operand of this item
-                const uint32_t G = g_tile;
-                auto wait_empty = [&](uint32_t g) -> bool {
-                    const uint32_t k = g / S;
-                    return mbar_wait_bounded(&b_empty[g % S], (k & 1) ^ 1, wait_ns);
-                };
-                auto issue_tma = [&](uint32_t g) {
-                    const uint32_t s = g % S;
-                    const int64_t t = pruned ? (int64_t)tl[g - G] : (int64_t)(tfirst + (g - G));
-                    mbar_arrive_expect_tx(&b_full[s], C::STAGE_BYTES);
-                    tma_bulk_g2s(sB + s * C::STAGE_BYTES, tiles_g + t * C::STAGE_BYTES, C::STAGE_BYTES, &b_full[s]);
-                    tma_issued = g + 1;
-                };
-                for (uint32_t k = 0; k < (uint32_t)S && k < ntiles && !aborted; ++k) {
-                    if (!wait_empty(G + k)) {
-                        aborted = true;
-                        break;
+                if constexpr (!C::TMA_WARP) {
+                    for (uint32_t k = 0; k < (uint32_t)S && k < ntiles && !aborted; ++k) {
+                        if (!wait_empty(G + k)) {
+                            aborted = true;
+                            break;
+                        }
+                        issue_tma(G + k, tile_at(k));
                     }
-                    issue_tma(G + k);
                 }
+                // list entry of the next refill, read one refill ahead
+                int64_t next_fill = (!C::TMA_WARP && (uint32_t)S < ntiles) ? tile_at(S) : 0;
                 const uint32_t a_addr = smem_addr(sA);
                 for (uint32_t t = 0; t < ntiles && !aborted; ++t) {
                     const uint32_t g = G + t;
@@ -504,13 +546,17 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
                     mma_commit(&t_full[b]);
                     mma_commit(&b_empty[s]);
                     mma_issued = g + 1;
-                    const uint32_t gr = g - 1 + S;  // refill the stage that MMA g-1 used
-                    if (t > 0 && gr < G + ntiles) {
-                        if (!wait_empty(gr)) {
-                            aborted = true;
-                            break;
+                    if constexpr (!C::TMA_WARP) {
+                        const uint32_t gr = g - 1 + S;  // refill the stage that MMA g-1 used
+                        if (t > 0 && gr < G + ntiles) {
+                            const int64_t cur = next_fill;
+                            if (gr + 1 < G + ntiles) next_fill = tile_at(gr + 1 - G);
+                            if (!wait_empty(gr)) {
+                                aborted = true;
+                                break;
+                            }
+                            issue_tma(gr, cur);
                         }
-                        issue_tma(gr);
                     }
                 }
             }
@@ -584,13 +630,85 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
                 tq = fminf((worst - nq) + eps, tq_off);
             };
 
-            const uint32_t G = g_tile;
+            // screened candidates waiting for their exact distance: ref position << 5 | row
+            uint64_t *cq = cqbase + warp * CQCAP;
+            int ccount = 0;
+            // rescore queued candidates, one per lane (batches of 32; all of them when `all`, else
+            // the whole batches, the rest moving to the front): the ref's exact coordinates and point
+            // index from its tile record in global memory, the row's query coordinates, bound and
+            // limit by shuffles from the lane that owns the row; survivors of the row's current bound
+            // are queued as keys
+            auto rescore = [&](bool all) {
+                __syncwarp();
+                const int n_do = all ? ccount : (ccount & ~31);
+                for (int base = 0; base < n_do; base += 32) {
+                    if (qcount > QCAP - 32) drain();
+                    const int e = base + lane;
+                    const bool has = e < n_do;
+                    const uint64_t c = has ? cq[e] : 0;
+                    const int r = (int)(c & 31u);
+                    const int64_t jp = (int64_t)(c >> 5);  // the ref's position among the tiles
+                    float qv[D];
+#pragma unroll
+                    for (int f = 0; f < D; ++f) qv[f] = __shfl_sync(FULL, qo[f], r);
+                    const float worst_r = __shfl_sync(FULL, worst, r);
+                    const long long limit_r = __shfl_sync(FULL, (long long)limit, r);
+                    bool keep = false;
+                    uint64_t key = 0;
+                    if (has) {
+                        const int col = (int)(jp & (RT - 1));
+                        const unsigned char *rec = tiles_g + (jp / RT) * C::TILE_BYTES;
+                        // the oracle's arithmetic: ((x0 - q0)^2 + (x1 - q1)^2) + ..., each step rounded
+                        const float4 *rp4 = reinterpret_cast<const float4 *>(rec + C::OP_BYTES) + col * (C::DP / 4);
+                        float rv[C::DP];
+#pragma unroll
+                        for (int f4 = 0; f4 < C::DP / 4; ++f4) {
+                            const float4 t = __ldg(rp4 + f4);
+                            rv[4 * f4] = t.x;
+                            rv[4 * f4 + 1] = t.y;
+                            rv[4 * f4 + 2] = t.z;
+                            rv[4 * f4 + 3] = t.w;
+                        }
+                        int64_t jo = jp;  // index-order tiles: the position is the point index
+                        if (pruned) {
+                            if constexpr (C::IX_MODE == 1) jo = __float_as_int(rv[C::DP - 1]);
+                            else if constexpr (C::IX_MODE == 2)
+                                jo = __ldg(reinterpret_cast<const int32_t *>(rec + C::OP_BYTES + C::EX_BYTES) + col);
+                            else jo = __ldg(ref_perm + jp);
+                        }
+                        const float t0 = sub_rn(rv[0], qv[0]);
+                        float d2 = mul_rn(t0, t0);
+#pragma unroll
+                        for (int f = 1; f < D; ++f) {
+                            const float tf = sub_rn(rv[f], qv[f]);
+                            d2 = add_rn(d2, mul_rn(tf, tf));
+                        }
+                        keep = d2 <= worst_r && jo < (int64_t)limit_r;  // NaN never kept
+                        key = (uint64_t)__float_as_uint(d2) << 32 | (uint32_t)jo;
+                    }
+                    const unsigned mk = __ballot_sync(FULL, keep);
+                    if (keep) {
+                        const int pos = qcount + __popc(mk & ((1u << lane) - 1u));
+                        qk[pos] = key;
+                        qr[pos] = (uint8_t)r;
+                    }
+                    qcount += __popc(mk);
+                }
+                const int rest = ccount - n_do;  // < 32
+                __syncwarp();
+                const uint64_t mv = lane < rest ? cq[n_do + lane] : 0;
+                __syncwarp();
+                if (lane < rest) cq[lane] = mv;
+                __syncwarp();
+                ccount = rest;
+            };
+
             // the next tile's list entry is loaded one tile ahead (a global load per tile that
             // would otherwise sit on the path from the accumulator to the screen)
             int64_t tl_next = (pruned && ntiles > 0) ? (int64_t)tl[0] : 0;
             for (uint32_t t = 0; t < ntiles; ++t) {
                 const uint32_t g = G + t;
-                const uint32_t s = g % S, b = g % C::NBUF;
+                const uint32_t b = g % C::NBUF;
                 const int64_t tl_cur = tl_next;
                 if (pruned && t + 1 < ntiles) tl_next = (int64_t)tl[t + 1];
                 if (!mbar_wait_bounded(&t_full[b], (g / C::NBUF) & 1, wait_ns)) aborted = true;
@@ -599,123 +717,102 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
                     break;
                 }
                 tc_fence_after();
-                const float *exs = reinterpret_cast<const float *>(sB + s * C::STAGE_BYTES + C::OP_BYTES);
-                const int32_t *ixs = reinterpret_cast<const int32_t *>(sB + s * C::STAGE_BYTES + C::OP_BYTES + C::EX_BYTES);
                 const int64_t j0 = (pruned ? tl_cur : (int64_t)(tfirst + t)) * RT;  // first ref position of the tile
                 const uint32_t taddr = tmem_base + ((uint32_t)(quad * 32) << 16) + b * C::BUF_COLS + qtw * RT;
-                // screen one 32-column chunk (scores in v): this row's candidate mask, 0 when no row
-                // of the warp has one (the common case, a handful of instructions)
-                auto screen = [&](const uint32_t (&v)[32]) -> uint32_t {
-                    float gmin[4];  // minimum of each group of 8 columns
+                // 1) screen: the minimum of each group of 8 columns (16 per row), the accumulator read
+                //    in four 32-column chunks, each loading while the previous one is reduced; one
+                //    vote per tile, since most tiles give no row of the warp a candidate.  A tile that
+                //    does reads its passing chunks again (the accumulator is held until the vote) for
+                //    the candidate masks.
+                float gm[16];
+                auto group_mins = [&](const uint32_t (&v)[32], int c) {
 #pragma unroll
                     for (int gi = 0; gi < 4; ++gi) {
 #define NNGP_V(k) __uint_as_float(v[gi * 8 + (k)])
-                        gmin[gi] = fminf(min3f(NNGP_V(0), NNGP_V(1), NNGP_V(2)),
-                                         min3f(NNGP_V(3), NNGP_V(4), fminf(NNGP_V(5), fminf(NNGP_V(6), NNGP_V(7)))));
+                        gm[c * 4 + gi] = fminf(min3f(NNGP_V(0), NNGP_V(1), NNGP_V(2)),
+                                               min3f(NNGP_V(3), NNGP_V(4), fminf(NNGP_V(5), fminf(NNGP_V(6), NNGP_V(7)))));
 #undef NNGP_V
                     }
-                    const float mn = fminf(min3f(gmin[0], gmin[1], gmin[2]), gmin[3]);
-                    uint32_t cm = 0;
-                    if (!__any_sync(FULL, mn < tq)) return cm;
-#pragma unroll
-                    for (int gi = 0; gi < 4; ++gi) {
-                        if (gmin[gi] < tq) {  // only groups whose minimum passes
-#pragma unroll
-                            for (int k = 0; k < 8; ++k)
-                                cm |= (__uint_as_float(v[gi * 8 + k]) < tq ? 1u : 0u) << (gi * 8 + k);
-                        }
-                    }
-                    return cm;
                 };
-                // 1) screen the tile's four chunks (loads one chunk ahead, two register sets) into
-                //    per-chunk candidate masks; the accumulator buffer is freed once all four are read
                 uint32_t va[32], vb[32];
                 tmem_ld32_nowait(taddr, va);
                 tmem_wait_ld(va);
                 tmem_ld32_nowait(taddr + 32, vb);
-                uint32_t cm0 = screen(va);
+                group_mins(va, 0);
                 tmem_wait_ld(vb);
                 tmem_ld32_nowait(taddr + 64, va);
-                uint32_t cm1 = screen(vb);
+                group_mins(vb, 1);
                 tmem_wait_ld(va);
                 tmem_ld32_nowait(taddr + 96, vb);
-                uint32_t cm2 = screen(va);
+                group_mins(va, 2);
                 tmem_wait_ld(vb);
+                group_mins(vb, 3);
+                float cmin[4];  // minimum of each chunk
+#pragma unroll
+                for (int c = 0; c < 4; ++c) cmin[c] = fminf(fminf(gm[4 * c], gm[4 * c + 1]), fminf(gm[4 * c + 2], gm[4 * c + 3]));
+                const bool tile_has = __any_sync(FULL, fminf(fminf(cmin[0], cmin[1]), fminf(cmin[2], cmin[3])) < tq);
+                uint32_t cmk[4] = {0u, 0u, 0u, 0u};
+                if (tile_has) {
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        if (__any_sync(FULL, cmin[c] < tq)) {  // warp-uniform: the load is collective
+                            tmem_ld32_nowait(taddr + 32 * c, va);
+                            tmem_wait_ld(va);
+                            uint32_t cm = 0;
+#pragma unroll
+                            for (int gi = 0; gi < 4; ++gi) {
+                                if (gm[4 * c + gi] < tq) {  // only groups whose minimum passes
+#pragma unroll
+                                    for (int k = 0; k < 8; ++k)
+                                        cm |= (__uint_as_float(va[gi * 8 + k]) < tq ? 1u : 0u) << (gi * 8 + k);
+                                }
+                            }
+                            cmk[c] = cm;
+                        }
+                    }
+                }
                 tc_fence_before();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&t_empty[b]);
-                uint32_t cm3 = screen(vb);
-                {  // columns with j < limit only (pruned: positions < n_ref; the index test is per candidate)
-                    const int64_t room = (pruned ? n_ref : limit) - j0;
-                    if (room < RT) {
-                        auto cut = [&](uint32_t &cm, int c) {
-                            const int64_t r = room - c * 32;
-                            if (r < 32) cm &= r <= 0 ? 0u : ((1u << (uint32_t)r) - 1u);
-                        };
-                        cut(cm0, 0);
-                        cut(cm1, 1);
-                        cut(cm2, 2);
-                        cut(cm3, 3);
+                if (tile_has) {
+                    {  // columns with j < limit only (pruned: positions < n_ref; the index test is per candidate)
+                        const int64_t room = (pruned ? n_ref : limit) - j0;
+                        if (room < RT) {
+#pragma unroll
+                            for (int c = 0; c < 4; ++c) {
+                                const int64_t r = room - c * 32;
+                                if (r < 32) cmk[c] &= r <= 0 ? 0u : ((1u << (uint32_t)r) - 1u);
+                            }
+                        }
+                    }
+                    // 2) queue the tile's candidates (ref position, row): each lane walks its own
+                    //    (column by column, chunks in order), one per warp iteration; whole batches of
+                    //    32 are rescored as soon as they are queued
+                    uint64_t lo = (uint64_t)cmk[0] | (uint64_t)cmk[1] << 32, hi = (uint64_t)cmk[2] | (uint64_t)cmk[3] << 32;
+                    while (__any_sync(FULL, (lo | hi) != 0)) {
+                        if (ccount > CQCAP - 32) rescore(false);
+                        const bool has = (lo | hi) != 0;
+                        int col = 0;
+                        if (has) {
+                            const bool use_lo = lo != 0;  // branch-free pick of the lowest remaining column
+                            const uint64_t w = use_lo ? lo : hi;
+                            col = __ffsll((long long)w) - 1 + (use_lo ? 0 : 64);
+                            const uint64_t w2 = w & (w - 1);
+                            lo = use_lo ? w2 : lo;
+                            hi = use_lo ? hi : w2;
+                        }
+                        const unsigned mk = __ballot_sync(FULL, has);
+                        if (has) cq[ccount + __popc(mk & ((1u << lane) - 1u))] = (uint64_t)(j0 + col) << 5 | (uint32_t)lane;
+                        ccount += __popc(mk);
                     }
                 }
-                // 2) candidates of the whole tile: each lane walks its own (column by column, chunks in
-                //    order), one per warp iteration, so a warp iteration serves every row that has one;
-                //    each is rescored exactly from the stage's coordinates and survivors of the row's
-                //    current bound are queued as keys, then drained into the heaps in batches
-                uint64_t lo = (uint64_t)cm0 | (uint64_t)cm1 << 32, hi = (uint64_t)cm2 | (uint64_t)cm3 << 32;
-                while (__any_sync(FULL, (lo | hi) != 0)) {
-                    if (qcount > QCAP - 32) drain();
-                    bool keep = false;
-                    uint64_t key = 0;
-                    if ((lo | hi) != 0) {
-                        const bool use_lo = lo != 0;  // branch-free pick of the lowest remaining column
-                        const uint64_t w = use_lo ? lo : hi;
-                        const int col = __ffsll((long long)w) - 1 + (use_lo ? 0 : 64);
-                        const uint64_t w2 = w & (w - 1);
-                        lo = use_lo ? w2 : lo;
-                        hi = use_lo ? hi : w2;
-                        // the oracle's arithmetic: ((x0 - q0)^2 + (x1 - q1)^2) + ..., each step rounded
-                        const float4 *rp4 = reinterpret_cast<const float4 *>(exs + col * C::DP);
-                        float rv[C::DP];
-#pragma unroll
-                        for (int f4 = 0; f4 < C::DP / 4; ++f4) {
-                            const float4 t = rp4[f4];
-                            rv[4 * f4] = t.x;
-                            rv[4 * f4 + 1] = t.y;
-                            rv[4 * f4 + 2] = t.z;
-                            rv[4 * f4 + 3] = t.w;
-                        }
-                        const float t0 = sub_rn(rv[0], qo[0]);
-                        float d2 = mul_rn(t0, t0);
-#pragma unroll
-                        for (int f = 1; f < D; ++f) {
-                            const float tf = sub_rn(rv[f], qo[f]);
-                            d2 = add_rn(d2, mul_rn(tf, tf));
-                        }
-                        int64_t jo = j0 + col;  // the ref's point index
-                        if (pruned) {
-                            if constexpr (C::IX_MODE == 1) jo = __float_as_int(rv[C::DP - 1]);
-                            else if constexpr (C::IX_MODE == 2) jo = ixs[col];
-                            else jo = ref_perm[j0 + col];
-                        }
-                        keep = d2 <= worst && jo < limit;  // NaN never kept
-                        key = (uint64_t)__float_as_uint(d2) << 32 | (uint32_t)jo;
-                    }
-                    const unsigned mk = __ballot_sync(FULL, keep);
-                    if (keep) {
-                        const int pos = qcount + __popc(mk & ((1u << lane) - 1u));
-                        qk[pos] = key;
-                        qr[pos] = (uint8_t)lane;
-                    }
-                    qcount += __popc(mk);
-                }
+                if (ccount >= 32) rescore(false);
                 if (qcount >= DRAIN_AT) drain();
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&b_empty[s]);
             }
             // write this warp's rows: each heap sorted ascending across the warp (bitonic, keys unique
             // except empty slots), index -1 for empty slots
             if (!aborted) {
+                if (ccount > 0) rescore(true);
                 if (qcount > 0) drain();
                 __syncwarp();
                 for (int rr = 0; rr < 32; ++rr) {
@@ -747,9 +844,15 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
     // teardown: report a timeout, let copies and MMAs this CTA issued finish (bounded by the
     // full kWaitLimitNs whatever wait_ns is), free TMEM
     if ((aborted || *s_abort) && threadIdx.x == 0) flag_or(flags, NNGP_FLAG_TIMEOUT);
+    if ((C::TMA_WARP ? copy_warp : producer_warp) && lane == 0 && (aborted || *s_abort)) {
+        // copies issued but never waited for: let them land before the CTA's shared memory goes.
+        // With TMA_WARP the copying thread does not know which ones the MMA thread waited for; the
+        // last S it issued are the latest uses of their stages (earlier ones were waited for before
+        // their stage was refilled), and a wait on a phase that has completed returns at once.
+        const uint32_t g_from = C::TMA_WARP ? (tma_issued > (uint32_t)S ? tma_issued - S : 0u) : tma_landed;
+        for (uint32_t g = g_from; g < tma_issued; ++g) mbar_wait_bounded(&b_full[g % S], (g / S) & 1);
+    }
     if (producer_warp && lane == 0 && (aborted || *s_abort)) {
-        // copies issued but never waited for: let them land before the CTA's shared memory goes
-        for (uint32_t g = tma_landed; g < tma_issued; ++g) mbar_wait_bounded(&b_full[g % S], (g / S) & 1);
         // MMAs in flight: a commit tracks every earlier tcgen05 operation of this thread, so the
         // phase of the last committed tile covers them all (a tile whose MMAs were never issued
         // has no phase to wait for: g_tile counts an aborted item's tiles in full)
@@ -838,7 +941,7 @@ template <int D, int QTILES = (D == 12 || D == 16) ? 2 : 1> TcVariant tc_make() 
     v.fn = knn_tc_kernel<D, QTILES>;
     v.build = build_tc_tiles_kernel<D>;
     v.smem = C::SMEM;
-    v.stage_bytes = C::STAGE_BYTES;
+    v.stage_bytes = C::TILE_BYTES;  // bytes of a tile record in global memory
     v.dp = C::DP;
     v.ctas_per_sm = C::CTAS_PER_SM;
     v.threads = C::THREADS;
