@@ -95,13 +95,16 @@ template <bool MATERN, typename T> __device__ __forceinline__ T kern_g(int famil
 // Warp kernel
 // ---------------------------------------------------------------------------------------
 // Shared memory per warp (bytes): two Cholesky column slots 2 x kWarpM doubles (16-byte
-// aligned, first) | xs (kWarpM + 1) x ds doubles | L kWarpM x (kWarpM + 1) doubles | inverse
-// diagonal kWarpM doubles | gradient accumulator n_theta doubles | the fill's kernel values
-// kWarpM x (kWarpM + 1) doubles (kept for the gradient, which would otherwise recompute them).
+// aligned, first) | xs (kWarpM + 1) x ds doubles | P kWarpM x (kWarpM + 1) doubles | inverse
+// diagonal kWarpM doubles | gradient accumulator n_theta doubles.  P holds two triangles: the
+// strictly lower part of the factor, L[i][k] at P[i][k] (k < i), and the fill's kernel values
+// of the lower triangle, E[i][k] at P[k][i + 1] (k <= i, so column i + 1 > row k), which the
+// gradient reuses instead of recomputing them.  One array for both halves the footprint of a
+// warp (more resident warps per SM).
 struct WarpSmem {
     int ds;  // row stride of xs (d + 1; FP32 systems use whole float4s, see warp_system)
-    size_t c_bytes, xs_bytes, l_bytes, idg_bytes, g_bytes, e_bytes, r_bytes, total;
-    size_t xs_off, l_off, idg_off, g_off, e_off, r_off;
+    size_t c_bytes, xs_bytes, l_bytes, idg_bytes, g_bytes, r_bytes, total;
+    size_t xs_off, l_off, idg_off, g_off, r_off;
     // f32: FP32 inputs, whose systems also keep the fill's squared distances (kWarpM x (kWarpM + 1)
     // floats) for the gradient instead of recomputing them
     __host__ __device__ static WarpSmem make(int d, int n_theta, bool f32 = false) {
@@ -112,14 +115,12 @@ struct WarpSmem {
         s.l_bytes = (size_t)kWarpM * (kWarpM + 1) * 8;
         s.idg_bytes = (size_t)kWarpM * 8;
         s.g_bytes = (size_t)(n_theta > 0 ? n_theta : 1) * 8;
-        s.e_bytes = (size_t)kWarpM * (kWarpM + 1) * 8;
         s.xs_off = s.c_bytes;
         s.l_off = s.xs_off + s.xs_bytes;
         s.idg_off = s.l_off + s.l_bytes;
         s.g_off = s.idg_off + s.idg_bytes;
-        s.e_off = s.g_off + s.g_bytes;
         s.r_bytes = f32 ? (size_t)kWarpM * (kWarpM + 1) * 4 : 0;
-        s.r_off = s.e_off + s.e_bytes;
+        s.r_off = s.g_off + s.g_bytes;
         s.total = (s.r_off + s.r_bytes + 15) / 16 * 16;
         return s;
     }
@@ -154,7 +155,6 @@ __device__ __forceinline__ bool warp_system(const LocalArgs &a, int64_t p, int l
     TC *Ls = reinterpret_cast<TC *>(wsm + lay.l_off);
     TC *idg = reinterpret_cast<TC *>(wsm + lay.idg_off);
     double *gacc = reinterpret_cast<double *>(wsm + lay.g_off);
-    TC *Es = reinterpret_cast<TC *>(wsm + lay.e_off);
     constexpr bool STASH = GRAD && !MATERN;  // RBF gradient: reuse the fill's exponentials
     // FP32 RBF systems also keep the squared distances (the gradient's only other use of the fill)
     constexpr bool STASH_R = STASH && std::is_same<TC, float>::value && std::is_same<TIn, float>::value;
@@ -241,7 +241,7 @@ __device__ __forceinline__ bool warp_system(const LocalArgs &a, int64_t p, int l
     for (int k = 0; k < M; ++k) {
         const bool vk = (vmask >> k) & 1u;
         const TC e = rbf * kern_s<MATERN>(a.family, r[k]);
-        if (STASH) Es[lane * (M + 1) + k] = e;
+        if (STASH && k <= lane) Ls[k * (M + 1) + lane + 1] = e;  // E[lane][k], upper triangle of P
         if (STASH_R) Rs[lane * (M + 1) + k] = (float)r[k];
         TC kv = (valid && vk) ? e + cst : TC(0);
         if (k == lane) kv = valid ? kv + diag_add : TC(1);
@@ -294,9 +294,11 @@ __device__ __forceinline__ bool warp_system(const LocalArgs &a, int64_t p, int l
     }
     if (!(minpiv > TC(0)) || !(s2 > TC(0))) flag_or(flags, NNGP_FLAG_NOT_PD);
 
-    // L (strictly lower part) and inverse diagonal to shared memory for the backward solves
+    // L (strictly lower part, the upper part of P keeps E) and inverse diagonal to shared
+    // memory for the backward solves
 #pragma unroll
-    for (int k = 0; k < M; ++k) Ls[lane * (M + 1) + k] = r[k];
+    for (int k = 0; k < M; ++k)
+        if (k < lane) Ls[lane * (M + 1) + k] = r[k];
     idg[lane] = TC(1) / dg_own;
     __syncwarp();
 
@@ -397,7 +399,8 @@ __device__ __forceinline__ bool warp_system(const LocalArgs &a, int64_t p, int l
         const TC wgt = (valid && vk_ok) ? (k < lane ? TC(2) : (k == lane ? TC(1) : TC(0))) : TC(0);
         const TC s = STASH ? TC(0) : kern_s<MATERN>(a.family, r[k]);
         const TC gw = wgt * G;
-        const TC ge = gw * (STASH ? Es[lane * (M + 1) + k] : rbf * s);
+        // E[lane][k] for k <= lane (wgt is 0 above the diagonal, where P holds L)
+        const TC ge = gw * (STASH ? (k <= lane ? Ls[k * (M + 1) + lane + 1] : TC(0)) : rbf * s);
         const TC gl = MATERN ? gw * (rbf * kern_g<MATERN>(a.family, r[k], s)) : ge;
         g_amp += ge;
         g_cst += gw;
