@@ -55,6 +55,10 @@ struct LocalArgs {
     int weights_out;      // predict: write w = K_nn^-1 k (a.m per point) to `mean` instead of the mean
     int idx_rbf, idx_const, idx_noise, idx_ls, n_theta;
     unsigned long long *fp64_count;  // systems re-solved in FP64 are added here (may be null)
+    // fit step with FP32 inputs: bit p marks point p (counted from the launch's first row), whose
+    // FP32 system needs the FP64 re-solve that local_redo_kernel then runs (predict re-solves in
+    // place and leaves this null)
+    uint32_t *redo_bits;
     double inv_ls[kMaxDimLocal];
 };
 
@@ -473,8 +477,14 @@ __global__ void __launch_bounds__(kLocWarps * 32, 3) local_warp_kernel(
                 used_fp64 = true;
                 ++n_fp64;
             }
-            warp_system<double, TIn, GRAD, PRED, MATERN>(a, p, lane, x_ref, y_ref, x_pt, y_pt, nbr, wsm, ll_acc, mean, var,
-                                                 flags);
+            if constexpr (std::is_same<TIn, float>::value && !PRED) {
+                // the fit step's FP32 kernel carries no FP64 system (registers): the point is
+                // marked for local_redo_kernel
+                if (lane == 0) atomicOr(a.redo_bits + (p >> 5), 1u << (p & 31));
+            } else {
+                warp_system<double, TIn, GRAD, PRED, MATERN>(a, p, lane, x_ref, y_ref, x_pt, y_pt, nbr, wsm, ll_acc, mean,
+                                                             var, flags);
+            }
         }
     }
     if (used_fp64 && lane == 0) {
@@ -483,6 +493,53 @@ __global__ void __launch_bounds__(kLocWarps * 32, 3) local_warp_kernel(
     }
     if (PRED) return;
     // CTA reduction in fixed order: warp w's totals -> slot w, then warp 0 sums
+    __shared__ double red[kLocWarps];
+    if (lane == 0) red[warp] = ll_acc;
+    __syncthreads();
+    const int nt = 1 + (GRAD ? a.n_theta : 0);
+    double *o = block_out + (int64_t)blockIdx.x * nt;
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < kLocWarps; ++w) s += red[w];
+        o[0] = s;
+    }
+    if (GRAD) {
+        for (int t = threadIdx.x; t < a.n_theta; t += blockDim.x) {
+            double s = 0.0;
+            for (int w = 0; w < kLocWarps; ++w)
+                s += reinterpret_cast<const double *>(smem_raw + w * lay.total + lay.g_off)[t];
+            o[1 + t] = s;
+        }
+    }
+}
+
+// FP64 re-solve of the fit-step systems the FP32 kernel marked (warp per point, the same warp
+// layout); the points of a 32-point word go to one warp, words to warps in a fixed order, so the
+// per-CTA partials are deterministic for a given launch shape.
+template <bool GRAD, bool MATERN>
+__global__ void __launch_bounds__(kLocWarps * 32, 3) local_redo_kernel(
+    const __grid_constant__ LocalArgs a, const float *__restrict__ x_ref, const float *__restrict__ y_ref,
+    const float *__restrict__ x_pt, const float *__restrict__ y_pt, const int32_t *__restrict__ nbr,
+    double *__restrict__ block_out, int32_t *__restrict__ flags) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const WarpSmem lay = WarpSmem::make(a.d, a.n_theta, true);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned char *wsm = smem_raw + warp * lay.total;
+    double *gacc = reinterpret_cast<double *>(wsm + lay.g_off);
+    for (int t = lane; t < a.n_theta; t += 32) gacc[t] = 0.0;
+    __syncwarp();
+    double ll_acc = 0.0;
+    const int64_t words = (a.n_points + 31) / 32;
+    const int64_t nwarps = (int64_t)gridDim.x * kLocWarps;
+    for (int64_t w = (int64_t)blockIdx.x * kLocWarps + warp; w < words; w += nwarps) {
+        uint32_t bits = a.redo_bits[w];
+        while (bits) {
+            const int64_t p = w * 32 + (__ffs(bits) - 1);
+            bits &= bits - 1;
+            warp_system<double, float, GRAD, false, MATERN>(a, p, lane, x_ref, y_ref, x_pt, y_pt, nbr, wsm, ll_acc,
+                                                            nullptr, nullptr, flags);
+        }
+    }
     __shared__ double red[kLocWarps];
     if (lane == 0) red[warp] = ll_acc;
     __syncthreads();
@@ -808,8 +865,10 @@ constexpr size_t kCountBytes = 256;  // head of the log-likelihood workspace: th
 struct LocalPlan {
     bool warp = true;
     int grid = 0;
+    int redo_grid = 0;  // CTAs of local_redo_kernel (their partials follow the main kernel's)
     size_t smem = 0;
     int nt = 1;
+    size_t bits_off = 0;  // byte offset of the FP64 re-solve bitmask from the workspace head
     size_t ws_bytes = 0;
 };
 
@@ -827,8 +886,13 @@ LocalPlan plan_local(int64_t n_points, int d, int m, int n_theta, bool grad, boo
         p.smem = BlockSmem::make(m, d).total;
         p.grid = (int)std::max<int64_t>(1, std::min<int64_t>(n_points, (int64_t)sms * 2));
     }
-    // [256 bytes: the count of FP64 re-solves | per-CTA partials], plus 256 of alignment slack
-    p.ws_bytes = kCountBytes + align_up((size_t)p.grid * p.nt * sizeof(double), 256) + 256;
+    // [256 bytes: the count of FP64 re-solves | per-CTA partials of the main kernel, then of the
+    // re-solve kernel | the re-solve bitmask, one bit per point], plus 256 of alignment slack
+    // (laid out for FP32 inputs whatever the dtype: the workspace size does not depend on it)
+    const int64_t words = (n_points + 31) / 32;
+    p.redo_grid = (int)std::max<int64_t>(1, std::min<int64_t>((words + kLocWarps - 1) / kLocWarps, (int64_t)sms * 2));
+    p.bits_off = kCountBytes + align_up((size_t)(p.grid + p.redo_grid) * p.nt * sizeof(double), 256);
+    p.ws_bytes = p.bits_off + align_up((size_t)words * sizeof(uint32_t), 256) + 256;
     return p;
 }
 
@@ -861,6 +925,7 @@ nngp_status fill_args(LocalArgs &a, const nngp_kernel *k, int d, int ydim, int m
     a.alpha_below = n_rows;
     a.weights_out = 0;
     a.fp64_count = nullptr;
+    a.redo_bits = nullptr;
     if (k->family < NNGP_FAMILY_RBF || k->family > NNGP_FAMILY_MATERN52)
         return fail(NNGP_ERR_INVALID_ARGUMENT, "kernel family must be one of NNGP_FAMILY_*");
     a.family = k->family;
@@ -929,12 +994,31 @@ nngp_status loglik_impl(const TIn *x, const TIn *y, int64_t n, int d, int ydim, 
     double *block_out = reinterpret_cast<double *>(head + kCountBytes);
     const TIn *x_pt = x + row_begin * d;
     const TIn *y_pt = y + row_begin * ydim;
+    // FP32 warp systems: the points that need the FP64 re-solve are marked, then re-solved by a
+    // second kernel (its partials follow the main kernel's; finalize sums both in a fixed order)
+    const bool redo = std::is_same<TIn, float>::value && pl.warp;
+    if (redo) {
+        a.redo_bits = reinterpret_cast<uint32_t *>(head + pl.bits_off);
+        NNGP_CUDA_TRY(cudaMemsetAsync(a.redo_bits, 0, (size_t)((rows + 31) / 32) * sizeof(uint32_t), stream));
+    }
     if (grad)
         st = launch_local<TIn, true, false>(pl, a, x, y, x_pt, y_pt, nbr, block_out, nullptr, nullptr, flags, stream);
     else
         st = launch_local<TIn, false, false>(pl, a, x, y, x_pt, y_pt, nbr, block_out, nullptr, nullptr, flags, stream);
     if (st != NNGP_OK) return st;
-    finalize_kernel<<<1, 256, 0, stream>>>(block_out, pl.grid, pl.nt, out);
+    int parts = pl.grid;
+    if constexpr (std::is_same<TIn, float>::value) {
+        if (redo) {
+            double *redo_out = block_out + (size_t)pl.grid * pl.nt;
+            auto fn = a.family == NNGP_FAMILY_RBF ? (grad ? local_redo_kernel<true, false> : local_redo_kernel<false, false>)
+                                                  : (grad ? local_redo_kernel<true, true> : local_redo_kernel<false, true>);
+            NNGP_CUDA_TRY(ensure_smem_limit(reinterpret_cast<const void *>(fn), (int)pl.smem));
+            fn<<<pl.redo_grid, kLocWarps * 32, pl.smem, stream>>>(a, x, y, x_pt, y_pt, nbr, redo_out, flags);
+            NNGP_CUDA_TRY(cudaGetLastError());
+            parts += pl.redo_grid;
+        }
+    }
+    finalize_kernel<<<1, 256, 0, stream>>>(block_out, parts, pl.nt, out);
     NNGP_CUDA_TRY(cudaGetLastError());
     return NNGP_OK;
 }

@@ -117,6 +117,40 @@ def test_fp64_fallback_on_near_singular_systems():
     assert rel(out[1:], want_g) < F32_GRAD
 
 
+@pytest.mark.parametrize('row_begin', [0, 3000])
+@pytest.mark.parametrize('kind', ['rbf', 'matern'])
+def test_every_fp32_system_resolved_in_fp64(row_begin, kind):
+    """pivot_tol = 1e30 marks every FP32 system for the FP64 re-solve kernel (the fit step's FP32
+    kernel carries no FP64 path; a bitmask over the launch's points hands them over).  The result
+    equals the FP64 kernel on the same FP32-rounded inputs up to the order of the partial sums
+    (1e-12), whole set and a row range, and the re-solve count is every system."""
+    rng = np.random.default_rng(11)
+    n = 8000
+    x = (rng.uniform(-1, 1, (n, 3)) * np.array([1.0, 0.7, 0.4])).astype(np.float32)
+    y = (np.sin(3 * x).sum(1) + rng.normal(0, 0.05, n)).astype(np.float32)
+    stat = skk.RBF(0.2) if kind == 'rbf' else skk.Matern(0.3, nu=1.5)
+    p = extract(skk.ConstantKernel(1.0) * stat + skk.WhiteKernel(1e-3))
+    nbr_all = O.fit_neighbours(x.astype(np.float64), 32, 0.2, np.float32)
+    rows = n - row_begin
+    nbr = torch.from_numpy(np.ascontiguousarray(nbr_all[row_begin:], dtype=np.int32)).cuda()
+    outs = {}
+    for dt in (torch.float32, torch.float64):
+        xt = torch.from_numpy(x).to('cuda', dt)
+        yt = torch.from_numpy(y.reshape(n, 1)).to('cuda', dt)
+        flags = ops.new_flags(xt.device)
+        st = {}
+        outs[dt] = ops.loglik(xt, yt, nbr, p, 1e-10, True, 1e30, flags=flags, row_begin=row_begin,
+                              stats=st).cpu().numpy()
+        f = int(flags.item())
+        if dt == torch.float32:
+            assert f & _lib.NNGP_FLAG_FP64_FALLBACK
+            assert int(st['fp64_systems'].item()) == rows
+        assert f & ~_lib.NNGP_FLAG_FP64_FALLBACK == 0
+    a, b = outs[torch.float32], outs[torch.float64]
+    assert abs(a[0] / b[0] - 1) < 1e-12
+    assert rel(a[1:], b[1:]) < 1e-12
+
+
 def test_bad_neighbour_index_is_flagged_not_read():
     g = load('const_n300_d2_m10')
     p = extract(KERNELS['const_n300_d2_m10']().clone_with_theta(g['theta']))
