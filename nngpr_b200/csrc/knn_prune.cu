@@ -15,7 +15,9 @@
 // distance of the same FP32 coordinates (all terms are non-negative), minus at most
 // (D + 2) 2^-150 from subnormal rounding; the box distance is at most the exact distance.  A tile
 // is dropped only if box_distance^2 (1 - gamma) - 1e-37 > seed, gamma = (D + 3) 2^-23, so every
-// ref in it has an FP32 distance above every row's bound and could never enter a list.
+// ref in it has an FP32 distance above every row's bound and could never enter a list.  The
+// left side is evaluated in FP32 with every operation rounded toward -inf (gaps, squares, sums,
+// the shrink and the 1e-37), so it never exceeds its exact value and the rule stays safe.
 //
 // Rows: band = floor(log2(n / i)) groups rows whose prefixes differ by less than a factor of
 // two, hence seeds of similar size.  A row whose seed exceeds 16 times its band's geometric mean
@@ -349,7 +351,7 @@ struct Boxes {
     const float *tlo, *thi, *glo, *ghi, *gtau;
     const int32_t *tmin, *glim;
     int d;
-    double gamma;
+    float shrink;  // 1 - gamma, gamma = (d + 3) 2^-23 (exact in FP32)
 };
 
 // 32-bit words of one group's tile masks
@@ -375,54 +377,79 @@ __device__ __forceinline__ GroupBox load_group(const Boxes &b, int64_t g) {
     return q;
 }
 
-// May ref tile t hold a neighbour of a row of the group (need), and does its box meet the
-// group's (overlap)?
-__device__ __forceinline__ void tile_test(const Boxes &b, const GroupBox &q, int64_t t, bool &need, bool &overlap) {
+constexpr int kBoxChunk = 128;  // tiles whose boxes a CTA stages in shared memory at a time
+
+// May ref tile tt of the staged chunk hold a neighbour of a row of the group (need), and does
+// its box meet the group's (overlap)?  slo / shi: the chunk's boxes, feature-major.
+__device__ __forceinline__ void tile_test(const Boxes &b, const GroupBox &q, const float (*slo)[kBoxChunk],
+                                          const float (*shi)[kBoxChunk], int32_t tmin, int tt, bool &need,
+                                          bool &overlap) {
     need = false;
     overlap = false;
-    if (b.tmin[t] >= q.lim) return;  // every ref of the tile comes after every row
-    double lb = 0.0;
+    if (tmin >= q.lim) return;  // every ref of the tile comes after every row
+    // lb <= the exact squared box distance: every FP32 operation rounded toward -inf
+    float lb = 0.f;
     bool meet = true;
 #pragma unroll
     for (int f = 0; f < kMaxDim; ++f) {
         if (f < b.d) {
-            const float tl = b.tlo[t * b.d + f], th = b.thi[t * b.d + f];
+            const float tl = slo[f][tt], th = shi[f][tt];
             meet = meet && !(tl > q.hi[f] || q.lo[f] > th);
-            const double gap = fmax(0.0, fmax((double)tl - (double)q.hi[f], (double)q.lo[f] - (double)th));  // NaN -> 0
-            lb += gap * gap;
+            const float gap = fmaxf(0.f, fmaxf(__fsub_rd(tl, q.hi[f]), __fsub_rd(q.lo[f], th)));  // NaN -> 0
+            lb = __fadd_rd(lb, __fmul_rd(gap, gap));
         }
     }
-    need = isinf(q.tau) || !(lb * (1.0 - b.gamma) - 1e-37 > q.tau);
+    need = isinf(q.tau) || !(__fsub_rd(__fmul_rd(lb, b.shrink), 1e-37f) > (float)q.tau);
     overlap = need && meet;
 }
 
-// One warp per group: counts[g] = tiles needed (0 for the slots past the groups), and the
-// group's masks of needed tiles and of needed tiles whose box meets the group's (32 tiles per
-// word: masks[(g * words + w) * 2 + {0, 1}]).
+// One warp per group, the CTA's groups tested against chunks of kBoxChunk tiles whose boxes the
+// CTA stages in shared memory (each box read once per CTA instead of once per group):
+// counts[g] = tiles needed (0 for the slots past the groups), and the group's masks of needed
+// tiles and of needed tiles whose box meets the group's (32 tiles per word:
+// masks[(g * words + w) * 2 + {0, 1}]).
 __global__ void __launch_bounds__(kThreads) count_kernel(Boxes b, const DevSizes *__restrict__ pruned,
                                                          int64_t max_groups, int64_t n_tiles,
                                                          int32_t *__restrict__ counts, uint32_t *__restrict__ masks) {
-    const int lane = threadIdx.x & 31;
+    __shared__ float slo[kMaxDim][kBoxChunk], shi[kMaxDim][kBoxChunk];
+    __shared__ int32_t smin[kBoxChunk];
+    constexpr int kWarps = kThreads / 32;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t n_groups = pruned->n_groups;
     const int64_t words = mask_words(n_tiles);
-    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t g = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; g < max_groups; g += nw) {
+    // the loop bounds are the same for every warp of the CTA (it synchronises inside)
+    for (int64_t gb = (int64_t)blockIdx.x * kWarps; gb < max_groups; gb += (int64_t)gridDim.x * kWarps) {
+        const int64_t g = gb + warp;
+        const bool act = g < n_groups;
+        GroupBox q{};
+        if (act) q = load_group(b, g);
         int c = 0;
-        if (g < n_groups) {
-            const GroupBox q = load_group(b, g);
-            for (int64_t base = 0; base < n_tiles; base += 32) {
-                const int64_t t = base + lane;
-                bool need = false, ov = false;
-                if (t < n_tiles) tile_test(b, q, t, need, ov);
-                const unsigned nm = __ballot_sync(0xFFFFFFFFu, need), om = __ballot_sync(0xFFFFFFFFu, ov);
-                if (lane == 0) {
-                    masks[(g * words + base / 32) * 2] = nm;
-                    masks[(g * words + base / 32) * 2 + 1] = om;
+        for (int64_t t0 = 0; t0 < n_tiles; t0 += kBoxChunk) {
+            const int nt = (int)min((int64_t)kBoxChunk, n_tiles - t0);
+            __syncthreads();
+            for (int i = threadIdx.x; i < nt * b.d; i += kThreads) {
+                const int tt = i / b.d, f = i - tt * b.d;
+                slo[f][tt] = b.tlo[(t0 + tt) * b.d + f];
+                shi[f][tt] = b.thi[(t0 + tt) * b.d + f];
+            }
+            for (int i = threadIdx.x; i < nt; i += kThreads) smin[i] = b.tmin[t0 + i];
+            __syncthreads();
+            if (act) {
+                for (int base = 0; base < nt; base += 32) {
+                    const int tt = base + lane;
+                    bool need = false, ov = false;
+                    if (tt < nt) tile_test(b, q, slo, shi, smin[tt], tt, need, ov);
+                    const unsigned nm = __ballot_sync(0xFFFFFFFFu, need), om = __ballot_sync(0xFFFFFFFFu, ov);
+                    if (lane == 0) {
+                        const int64_t w = (t0 + base) / 32;
+                        masks[(g * words + w) * 2] = nm;
+                        masks[(g * words + w) * 2 + 1] = om;
+                    }
+                    c += __popc(nm);
                 }
-                c += __popc(nm);
             }
         }
-        if (lane == 0) counts[g] = c;
+        if (lane == 0 && g < max_groups) counts[g] = c;
     }
 }
 
@@ -865,7 +892,7 @@ nngp_status build(const float *xs, int64_t n, int64_t row_lo, int64_t row_hi, in
     group_box_kernel<<<grid_of(L.max_groups * 32), kThreads, 0, stream>>>(xs, d, dp, rows, row_off, sizes, seeds, 0,
                                                                           glo, ghi, gtau, glim);
     NNGP_CUDA_TRY(cudaGetLastError());
-    Boxes b{tlo, thi, glo, ghi, gtau, tmin, glim, d, (double)(d + 3) * 1.1920928955078125e-07};
+    Boxes b{tlo, thi, glo, ghi, gtau, tmin, glim, d, 1.0f - (float)(d + 3) * 1.1920928955078125e-07f};
     NNGP_CUDA_TRY(cudaMemsetAsync(counts + L.max_groups, 0, sizeof(int32_t), stream));
     uint32_t *masks = static_cast<uint32_t *>(at(L.masks));
     count_kernel<<<grid_of(L.max_groups * 32), kThreads, 0, stream>>>(b, sizes, L.max_groups, L.n_tiles, counts,
@@ -933,7 +960,7 @@ nngp_status build_query(const float *xs_ref, int64_t n_ref, const float *xq, int
     group_box_kernel<<<grid_of(L.max_groups * 32), kThreads, 0, stream>>>(xq, d, dp, qorder, row_off, sizes, seeds, 1,
                                                                           glo, ghi, gtau, glim);
     NNGP_CUDA_TRY(cudaGetLastError());
-    Boxes b{tlo, thi, glo, ghi, gtau, tmin, glim, d, (double)(d + 3) * 1.1920928955078125e-07};
+    Boxes b{tlo, thi, glo, ghi, gtau, tmin, glim, d, 1.0f - (float)(d + 3) * 1.1920928955078125e-07f};
     NNGP_CUDA_TRY(cudaMemsetAsync(counts + L.max_groups, 0, sizeof(int32_t), stream));
     uint32_t *masks = static_cast<uint32_t *>(at(L.masks));
     count_kernel<<<grid_of(L.max_groups * 32), kThreads, 0, stream>>>(b, sizes, L.max_groups, L.n_tiles, counts,

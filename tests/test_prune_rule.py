@@ -110,3 +110,40 @@ def test_dropped_tiles_hold_no_neighbour_of_any_row():
             else:
                 kept += 1
     assert dropped > 0.25 * (dropped + kept)  # the rule does prune (slab tiles of a sort order here)
+
+
+def _rd(x):
+    """x (float64 array, the exact result of one FP32 operation) rounded to FP32 toward -inf."""
+    f = x.astype(np.float32)
+    lower = f.astype(np.float64) > x
+    f[lower] = np.nextafter(f[lower], np.float32(-np.inf))
+    return f
+
+
+def test_round_down_box_bound_never_exceeds_the_exact_bound():
+    """The search planning evaluates the rule's left side in FP32 rounded toward -inf (every
+    operation: gap, square, sum, shrink, minus 1e-37).  Emulated here operation by operation
+    (each FP32 operation's exact value is a float64 sum / product of floats, rounded down), the
+    result never exceeds the exact left side, so whatever the FP32 form drops the exact rule
+    drops too."""
+    rng = np.random.default_rng(5)
+    for d in (1, 3, 8, 16, 24):
+        shrink = np.float32(1.0 - (d + 3) * 2.0 ** -23)
+        for scale in (1e-20, 1.0, 1e6, 1e18):
+            n = 5000
+            glo = (rng.normal(size=(n, d)) * scale).astype(np.float32)
+            ghi = (glo + np.abs(rng.normal(size=(n, d))) * scale).astype(np.float32)
+            tlo = (rng.normal(size=(n, d)) * scale * 3).astype(np.float32)
+            thi = (tlo + np.abs(rng.normal(size=(n, d))) * scale).astype(np.float32)
+            lb = np.zeros(n, dtype=np.float32)
+            for f in range(d):
+                a = _rd(tlo[:, f].astype(np.float64) - ghi[:, f].astype(np.float64))
+                b = _rd(glo[:, f].astype(np.float64) - thi[:, f].astype(np.float64))
+                gap = np.maximum(np.float32(0), np.maximum(a, b))
+                sq = _rd(gap.astype(np.float64) * gap.astype(np.float64))
+                lb = _rd(lb.astype(np.float64) + sq.astype(np.float64))
+            lhs = _rd(_rd(lb.astype(np.float64) * np.float64(shrink)).astype(np.float64) - 1e-37)
+            exact = box_bound(glo, ghi, tlo, thi) * (1.0 - (d + 3) * 2.0 ** -23) - 1e-37
+            ok = np.isfinite(exact)
+            assert np.all(lhs.astype(np.float64)[ok] <= exact[ok]), (d, scale)
+
