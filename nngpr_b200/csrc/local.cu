@@ -111,13 +111,16 @@ struct WarpSmem {
     size_t xs_off, l_off, idg_off, g_off, r_off;
     // f32: FP32 inputs, whose systems also keep the fill's squared distances (kWarpM x (kWarpM + 1)
     // floats) for the gradient instead of recomputing them
-    __host__ __device__ static WarpSmem make(int d, int n_theta, bool f32 = false) {
+    // sys4: the warp only ever solves FP32 systems (the fit step's FP32 kernel), so the column
+    // slots, xs, P and the inverse diagonal take 4-byte elements
+    __host__ __device__ static WarpSmem make(int d, int n_theta, bool f32 = false, bool sys4 = false) {
         WarpSmem s;
+        const size_t e = sys4 ? 4 : 8;
         s.ds = d + 1;
-        s.c_bytes = (size_t)2 * kWarpM * 8;
-        s.xs_bytes = (size_t)(kWarpM + 1) * s.ds * 8;
-        s.l_bytes = (size_t)kWarpM * (kWarpM + 1) * 8;
-        s.idg_bytes = (size_t)kWarpM * 8;
+        s.c_bytes = (size_t)2 * kWarpM * e;
+        s.xs_bytes = sys4 ? (size_t)(kWarpM + 1) * 4 * (((d + 3) / 4) | 1) * 4 : (size_t)(kWarpM + 1) * s.ds * 8;
+        s.l_bytes = (size_t)kWarpM * (kWarpM + 1) * e;
+        s.idg_bytes = (size_t)kWarpM * e;
         s.g_bytes = (size_t)(n_theta > 0 ? n_theta : 1) * 8;
         s.xs_off = s.c_bytes;
         s.l_off = s.xs_off + s.xs_bytes;
@@ -153,7 +156,8 @@ __device__ __forceinline__ bool warp_system(const LocalArgs &a, int64_t p, int l
                                             TIn *__restrict__ var, int32_t *__restrict__ flags) {
     constexpr int M = kWarpM;
     const unsigned FULL = 0xffffffffu;
-    const WarpSmem lay = WarpSmem::make(a.d, a.n_theta, std::is_same<TIn, float>::value);
+    const WarpSmem lay = WarpSmem::make(a.d, a.n_theta, std::is_same<TIn, float>::value,
+                                        std::is_same<TIn, float>::value && !PRED && std::is_same<TC, float>::value);
     TC *colbuf = reinterpret_cast<TC *>(wsm);  // two column slots of kWarpM, 16-byte aligned
     TC *xs = reinterpret_cast<TC *>(wsm + lay.xs_off);
     TC *Ls = reinterpret_cast<TC *>(wsm + lay.l_off);
@@ -450,13 +454,18 @@ __device__ __forceinline__ bool warp_system(const LocalArgs &a, int64_t p, int l
     return true;
 }
 
+// Resident CTAs per SM the register budget is set for: the fit step's FP32 kernel (FP32 systems
+// only, 4-byte warp layout) 4, the others 3.
+template <typename TIn, bool PRED> constexpr int kLocMinBlocks = (std::is_same<TIn, float>::value && !PRED) ? 4 : 3;
+
 template <typename TIn, bool GRAD, bool PRED, bool MATERN>
-__global__ void __launch_bounds__(kLocWarps * 32, 3) local_warp_kernel(
+__global__ void __launch_bounds__(kLocWarps * 32, (kLocMinBlocks<TIn, PRED>)) local_warp_kernel(
     const __grid_constant__ LocalArgs a, const TIn *__restrict__ x_ref, const TIn *__restrict__ y_ref,
     const TIn *__restrict__ x_pt, const TIn *__restrict__ y_pt, const int32_t *__restrict__ nbr,
     double *__restrict__ block_out, TIn *__restrict__ mean, TIn *__restrict__ var, int32_t *__restrict__ flags) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const WarpSmem lay = WarpSmem::make(a.d, a.n_theta, std::is_same<TIn, float>::value);
+    const WarpSmem lay = WarpSmem::make(a.d, a.n_theta, std::is_same<TIn, float>::value,
+                                        std::is_same<TIn, float>::value && !PRED);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned char *wsm = smem_raw + warp * lay.total;
     double *gacc = reinterpret_cast<double *>(wsm + lay.g_off);
@@ -872,14 +881,15 @@ struct LocalPlan {
     size_t ws_bytes = 0;
 };
 
-// f32: the launch runs the FP32-input kernels (their warp layout keeps the squared distances)
-LocalPlan plan_local(int64_t n_points, int d, int m, int n_theta, bool grad, bool f32 = false) {
+// f32: the launch runs the FP32-input kernels (their warp layout keeps the squared distances);
+// sys4: and only FP32 systems (the fit step: 4-byte warp layout)
+LocalPlan plan_local(int64_t n_points, int d, int m, int n_theta, bool grad, bool f32 = false, bool sys4 = false) {
     LocalPlan p;
     p.warp = m <= kWarpM;
     p.nt = 1 + (grad ? n_theta : 0);
     const int sms = num_sms();
     if (p.warp) {
-        p.smem = WarpSmem::make(d, n_theta, f32).total * kLocWarps;
+        p.smem = WarpSmem::make(d, n_theta, f32, sys4).total * kLocWarps;
         const int64_t need = (n_points + kLocWarps - 1) / kLocWarps;
         p.grid = (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)sms * 8));
     } else {
@@ -986,7 +996,8 @@ nngp_status loglik_impl(const TIn *x, const TIn *y, int64_t n, int d, int ydim, 
         return NNGP_OK;
     }
     if (!x || !y || (m > 0 && !nbr)) return fail(NNGP_ERR_INVALID_ARGUMENT, "loglik: null input pointer");
-    const LocalPlan pl = plan_local(rows, d, m, a.n_theta, grad, std::is_same<TIn, float>::value);
+    const LocalPlan pl = plan_local(rows, d, m, a.n_theta, grad, std::is_same<TIn, float>::value,
+                                    std::is_same<TIn, float>::value);
     if (!ws || ws_bytes < pl.ws_bytes) return fail(NNGP_ERR_WORKSPACE, "loglik: workspace missing or too small");
     unsigned char *head = reinterpret_cast<unsigned char *>(align_up(reinterpret_cast<uintptr_t>(ws), 256));
     a.fp64_count = reinterpret_cast<unsigned long long *>(head);
@@ -1012,8 +1023,9 @@ nngp_status loglik_impl(const TIn *x, const TIn *y, int64_t n, int d, int ydim, 
             double *redo_out = block_out + (size_t)pl.grid * pl.nt;
             auto fn = a.family == NNGP_FAMILY_RBF ? (grad ? local_redo_kernel<true, false> : local_redo_kernel<false, false>)
                                                   : (grad ? local_redo_kernel<true, true> : local_redo_kernel<false, true>);
-            NNGP_CUDA_TRY(ensure_smem_limit(reinterpret_cast<const void *>(fn), (int)pl.smem));
-            fn<<<pl.redo_grid, kLocWarps * 32, pl.smem, stream>>>(a, x, y, x_pt, y_pt, nbr, redo_out, flags);
+            const int redo_smem = (int)(WarpSmem::make(d, a.n_theta, true).total * kLocWarps);  // FP64 systems
+            NNGP_CUDA_TRY(ensure_smem_limit(reinterpret_cast<const void *>(fn), redo_smem));
+            fn<<<pl.redo_grid, kLocWarps * 32, redo_smem, stream>>>(a, x, y, x_pt, y_pt, nbr, redo_out, flags);
             NNGP_CUDA_TRY(cudaGetLastError());
             parts += pl.redo_grid;
         }
