@@ -900,7 +900,7 @@ LocalPlan plan_local(int64_t n_points, int d, int m, int n_theta, bool grad, boo
     // re-solve kernel | the re-solve bitmask, one bit per point], plus 256 of alignment slack
     // (laid out for FP32 inputs whatever the dtype: the workspace size does not depend on it)
     const int64_t words = (n_points + 31) / 32;
-    p.redo_grid = (int)std::max<int64_t>(1, std::min<int64_t>((words + kLocWarps - 1) / kLocWarps, (int64_t)sms * 2));
+    p.redo_grid = (int)std::max<int64_t>(1, std::min<int64_t>((words + kLocWarps - 1) / kLocWarps, (int64_t)sms * 8));
     p.bits_off = kCountBytes + align_up((size_t)(p.grid + p.redo_grid) * p.nt * sizeof(double), 256);
     p.ws_bytes = p.bits_off + align_up((size_t)words * sizeof(uint32_t), 256) + 256;
     return p;
