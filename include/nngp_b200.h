@@ -43,7 +43,7 @@
 extern "C" {
 #endif
 
-#define NNGP_ABI_VERSION 2
+#define NNGP_ABI_VERSION 3
 
 typedef enum nngp_status {
     NNGP_OK = 0,
@@ -74,6 +74,11 @@ typedef enum nngp_status {
  * kernel.theta (get_kernel_theta_mapping, :583-649), -1 when fixed or absent; the
  * n_ls length-scale positions are idx_ls, idx_ls+1, ...  Gradients are with respect
  * to these log-hyperparameters.
+ *
+ * dev_params (may be NULL): a DEVICE block that nngp_theta_params filled from a device theta;
+ * the log-likelihood calls then take the hyperparameter values from it instead of the fields
+ * above (the structure -- idx_*, n_ls, family, alpha -- still comes from this struct), so a fit
+ * loop can keep theta on the device.
  */
 typedef struct nngp_kernel {
     double rbf_level;
@@ -88,6 +93,7 @@ typedef struct nngp_kernel {
     int32_t idx_ls;
     int32_t n_theta;
     int32_t family;             /* NNGP_FAMILY_* (0 = RBF) */
+    const double *dev_params;   /* DEVICE pointer or NULL: see nngp_theta_params */
 } nngp_kernel;
 
 #define NNGP_FAMILY_RBF 0
@@ -142,6 +148,18 @@ nngp_status nngp_knn_f32(const float *ref, int64_t n_ref, const float *query, in
                          int32_t has_ref_cut, int64_t ref_cut_index, int32_t *out_idx,
                          int32_t *status_flags, void *workspace, size_t workspace_bytes,
                          void *stream);
+/* nngp_knn_f32 / _f64 with the length scale (n_ls values, 1 or d) in DEVICE memory, e.g. the block
+ * of nngp_theta_params (a fit loop that keeps theta on the device). */
+nngp_status nngp_knn_f32_ls_device(const float *ref, int64_t n_ref, const float *query, int64_t n_query,
+                                   int32_t d, const double *length_scale_dev, int32_t n_ls, int32_t num_nn,
+                                   int32_t has_ref_cut, int64_t ref_cut_index, int32_t *out_idx,
+                                   int32_t *status_flags, void *workspace, size_t workspace_bytes,
+                                   void *stream);
+nngp_status nngp_knn_f64_ls_device(const double *ref, int64_t n_ref, const double *query, int64_t n_query,
+                                   int32_t d, const double *length_scale_dev, int32_t n_ls, int32_t num_nn,
+                                   int32_t has_ref_cut, int64_t ref_cut_index, int32_t *out_idx,
+                                   int32_t *status_flags, void *workspace, size_t workspace_bytes,
+                                   void *stream);
 size_t nngp_knn_workspace_size_f64(int64_t n_ref, int64_t n_query, int32_t d, int32_t num_nn);
 nngp_status nngp_knn_f64(const double *ref, int64_t n_ref, const double *query, int64_t n_query,
                          int32_t d, const double *length_scale, int32_t n_ls, int32_t num_nn,
@@ -205,6 +223,20 @@ nngp_status nngp_loglik_f64(const double *x, const double *y, int64_t n, int32_t
  * (its FP32 mode has no FP64 re-solve); a host-only function, no GPU work.
  */
 const uint64_t *nngp_loglik_fp64_count(const void *workspace);
+
+/*
+ * Hyperparameter values from a DEVICE theta (log-hyperparameters, the layout of kernel.theta)
+ * without a host round trip: writes NNGP_THETA_PARAMS_LEN(d) doubles at params_dev (device),
+ * [rbf_level, const_value, noise_level, pivot_abs, 1/l_0 .. 1/l_{d-1}, l_0 .. l_{d-1}], each free
+ * hyperparameter exp of its theta entry (Kernel.theta's map, get_kernel_theta_mapping,
+ * nngpr/base_nngpr.py:583-649; sklearn's clone_with_theta), fixed ones and the structure from
+ * *k; pivot_abs = pivot_tol * |rbf_level + const_value + noise_level + alpha| (the FP32 re-solve
+ * threshold).  Set k->dev_params = params_dev for nngp_loglik_* and pass params_dev + 4 + d as
+ * the DEVICE length scale of nngp_knn_f32_ls_device.  Stream-ordered, one small kernel.
+ */
+#define NNGP_THETA_PARAMS_LEN(d) (4 + 2 * (d))
+nngp_status nngp_theta_params(const nngp_kernel *k, const double *theta_dev, int32_t d, double pivot_tol,
+                              double *params_dev, void *stream);
 
 /*
  * Same as nngp_loglik_f32/_f64 restricted to the points [row_begin, row_begin + row_count)

@@ -29,7 +29,7 @@ EXPORTED = (
     'nngp_tc_layout_selftest_bf16',
     'nngp_plain_knn_f32', 'nngp_knn_reuse_prepare_f32', 'nngp_knn_reuse_rank_f32',
     'nngp_predict_full_workspace_size', 'nngp_predict_full_f64', 'nngp_sample_full_f64',
-    'nngp_predict_cov_full_f64',
+    'nngp_predict_cov_full_f64', 'nngp_theta_params', 'nngp_knn_f32_ls_device', 'nngp_knn_f64_ls_device',
 )
 
 
@@ -48,6 +48,7 @@ class NngpKernel(ctypes.Structure):
         ('idx_ls', ctypes.c_int32),
         ('n_theta', ctypes.c_int32),
         ('family', ctypes.c_int32),
+        ('dev_params', ctypes.c_void_p),  # device block of nngp_theta_params, or None
     ]
 
 
@@ -71,6 +72,11 @@ _SIGS = {
     'nngp_knn_workspace_size_f64': ([_i64, _i64, _i32, _i32], _sz),
     'nngp_knn_f32': ([_vp, _i64, _vp, _i64, _i32, _dp, _i32, _i32, _i32, _i64, _vp, _vp, _vp, _sz, _vp], ctypes.c_int),
     'nngp_knn_f64': ([_vp, _i64, _vp, _i64, _i32, _dp, _i32, _i32, _i32, _i64, _vp, _vp, _vp, _sz, _vp], ctypes.c_int),
+    'nngp_knn_f32_ls_device': ([_vp, _i64, _vp, _i64, _i32, _vp, _i32, _i32, _i32, _i64, _vp, _vp, _vp, _sz, _vp],
+                               ctypes.c_int),
+    'nngp_knn_f64_ls_device': ([_vp, _i64, _vp, _i64, _i32, _vp, _i32, _i32, _i32, _i64, _vp, _vp, _vp, _sz, _vp],
+                               ctypes.c_int),
+    'nngp_theta_params': ([_kp, _vp, _i32, _f64, _vp, _vp], ctypes.c_int),
     'nngp_loglik_workspace_size': ([_i64, _i32, _i32, _i32, _i32], _sz),
     'nngp_loglik_fp64_count': ([_vp], _vp),
     'nngp_set_wait_limit_ns': ([ctypes.c_uint64], ctypes.c_uint64),

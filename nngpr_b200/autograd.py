@@ -7,8 +7,11 @@ computes the gradient (the adjoint identity, no ``dK`` tensor), so ``backward`` 
 saved gradient.  What the reference does in ``Nngpr.log_marginal_likelihood``
 (``nngpr/base_nngpr.py:385-451``), one neighbour search and one local-systems pass per call.
 
-``theta`` crosses to the host once per evaluation (``n_theta`` doubles): the kernels take the
-hyperparameters by value.  Everything of size n stays on the device.
+A CUDA ``theta`` never leaves the device: ``nngp_theta_params`` turns it into the
+hyperparameter values on the device, the search reads its length scale there and the
+local-systems kernels read their values there, so an evaluation makes no host round trip
+(``torch.cuda.set_sync_debug_mode('error')`` passes over forward and backward).  A host
+``theta`` takes the by-value path.  Everything of size n stays on the device.
 """
 from __future__ import annotations
 
@@ -64,6 +67,24 @@ class LogLikProblem:
         self.evaluations += 1
         return out
 
+    def evaluate_device(self, theta: torch.Tensor) -> torch.Tensor:
+        """``[lml, d lml / d theta...]`` at a float64 CUDA ``theta`` without copying it to the
+        host: the values come from ``ops.theta_params`` on the device."""
+        p = self.template
+        n, d = self.x.shape
+        m = min(self.num_nn, max(n - 1, 0))
+        params = ops.theta_params(p, theta.to(self.x.device, torch.float64), self.alpha, d, self.pivot_tol)
+        ls = None
+        if self.nn_type == 'kernel-space' and p.length_scale is not None:
+            n_ls = d if p.n_ls == d else 1
+            ls = params[4 + d:4 + d + n_ls]
+        self.flags.zero_()
+        nbr = ops.knn(self.x_search, self.x_search, m, 0, ls, flags=self.flags)
+        out = ops.loglik(self.x, self.y, nbr, p, self.alpha, True, pivot_tol=self.pivot_tol, flags=self.flags,
+                         params_dev=params)
+        self.evaluations += 1
+        return out
+
     def check(self) -> None:
         """Raise on a status raised by the kernels of the last evaluation (reads one int)."""
         ops.raise_on_flags(int(self.flags.item()) & ~_lib.NNGP_FLAG_FP64_FALLBACK, 'log-likelihood')
@@ -74,8 +95,10 @@ class NngpLogLik(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, theta: torch.Tensor, problem: LogLikProblem):
-        th = theta.detach().to('cpu', torch.float64).numpy()
-        out = problem.evaluate(th)
+        if theta.is_cuda:
+            out = problem.evaluate_device(theta.detach())
+        else:
+            out = problem.evaluate(theta.detach().to(torch.float64).numpy())
         ctx.save_for_backward(out[1:].to(theta.device, theta.dtype))
         return out[0].to(theta.device, theta.dtype)
 

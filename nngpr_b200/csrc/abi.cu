@@ -21,6 +21,11 @@ nngp_status knn_f32(const float *, int64_t, const float *, int64_t, int, const d
                     int32_t *, int32_t *, void *, size_t, cudaStream_t);
 nngp_status knn_f64(const double *, int64_t, const double *, int64_t, int, const double *, int, int, int, int64_t,
                     int32_t *, int32_t *, void *, size_t, cudaStream_t);
+nngp_status knn_f32_ls_device(const float *, int64_t, const float *, int64_t, int, const double *, int, int, int,
+                              int64_t, int32_t *, int32_t *, void *, size_t, cudaStream_t);
+nngp_status knn_f64_ls_device(const double *, int64_t, const double *, int64_t, int, const double *, int, int, int,
+                              int64_t, int32_t *, int32_t *, void *, size_t, cudaStream_t);
+nngp_status theta_params(const nngp_kernel *, const double *, int, double, double *, cudaStream_t);
 size_t loglik_workspace(int64_t n, int d, int ydim, int m, int n_theta);
 nngp_status loglik_f32(const float *, const float *, int64_t, int, int, const int32_t *, int, const nngp_kernel *, int,
                        double, double *, int32_t *, void *, size_t, cudaStream_t);
@@ -167,6 +172,31 @@ nngp_status nngp_knn_f32(const float *ref, int64_t n_ref, const float *query, in
         return knn_f32(ref, n_ref, query, n_query, d, length_scale, n_ls, num_nn, has_ref_cut != 0, ref_cut_index,
                        out_idx, status_flags, workspace, workspace_bytes, as_stream(stream));
     });
+}
+
+nngp_status nngp_knn_f32_ls_device(const float *ref, int64_t n_ref, const float *query, int64_t n_query, int32_t d,
+                                   const double *length_scale_dev, int32_t n_ls, int32_t num_nn, int32_t has_ref_cut,
+                                   int64_t ref_cut_index, int32_t *out_idx, int32_t *status_flags, void *workspace,
+                                   size_t workspace_bytes, void *stream) {
+    return guarded([&] {
+        return knn_f32_ls_device(ref, n_ref, query, n_query, d, length_scale_dev, n_ls, num_nn, has_ref_cut != 0,
+                                 ref_cut_index, out_idx, status_flags, workspace, workspace_bytes, as_stream(stream));
+    });
+}
+
+nngp_status nngp_knn_f64_ls_device(const double *ref, int64_t n_ref, const double *query, int64_t n_query, int32_t d,
+                                   const double *length_scale_dev, int32_t n_ls, int32_t num_nn, int32_t has_ref_cut,
+                                   int64_t ref_cut_index, int32_t *out_idx, int32_t *status_flags, void *workspace,
+                                   size_t workspace_bytes, void *stream) {
+    return guarded([&] {
+        return knn_f64_ls_device(ref, n_ref, query, n_query, d, length_scale_dev, n_ls, num_nn, has_ref_cut != 0,
+                                 ref_cut_index, out_idx, status_flags, workspace, workspace_bytes, as_stream(stream));
+    });
+}
+
+nngp_status nngp_theta_params(const nngp_kernel *k, const double *theta_dev, int32_t d, double pivot_tol,
+                              double *params_dev, void *stream) {
+    return guarded([&] { return theta_params(k, theta_dev, d, pivot_tol, params_dev, as_stream(stream)); });
 }
 
 nngp_status nngp_knn_f64(const double *ref, int64_t n_ref, const double *query, int64_t n_query, int32_t d,

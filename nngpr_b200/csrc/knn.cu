@@ -52,10 +52,13 @@ template <typename T> struct LsParam {
     T v[kMaxDim];
 };
 
-// dst (n_pad x dp) = src (n x d) / ls, zero padded (columns d..dp-1 and rows n..n_pad-1).
+// dst (n_pad x dp) = src (n x d) / ls, zero padded (columns d..dp-1 and rows n..n_pad-1).  The
+// length scale comes from ls (by value) or, when ls_dev is set, from device memory (n_ls values,
+// each rounded to T as the host does for ls).
 template <typename T>
 __global__ void scale_pad_kernel(const T *__restrict__ src, int64_t n, int d, int dp, int64_t n_pad,
-                                 LsParam<T> ls, int use_ls, T *__restrict__ dst) {
+                                 LsParam<T> ls, int use_ls, const double *__restrict__ ls_dev, int n_ls,
+                                 T *__restrict__ dst) {
     const int64_t total = n_pad * dp;
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = e / dp;
@@ -63,7 +66,7 @@ __global__ void scale_pad_kernel(const T *__restrict__ src, int64_t n, int d, in
         T v = T(0);
         if (i < n && f < d) {
             v = src[i * d + f];
-            if (use_ls) v = div_rn(v, ls.v[f]);
+            if (use_ls) v = div_rn(v, ls_dev ? (T)ls_dev[n_ls == 1 ? 0 : f] : ls.v[f]);
         }
         dst[e] = v;
     }
@@ -601,10 +604,11 @@ int grid_for(int64_t work, int per_block = 256) {
     return (int)std::max<int64_t>(1, std::min<int64_t>((work + per_block - 1) / per_block, (int64_t)kNumSMsB200 * 16));
 }
 
+// ls_device: ls points to device memory (read by the scaling kernel), else to host memory
 template <typename T>
 nngp_status knn_impl(const T *ref, int64_t n_ref, const T *query, int64_t n_query, int d, const double *ls,
                      int n_ls, int m, int has_cut, int64_t cut, int32_t *out, int32_t *flags, void *ws,
-                     size_t ws_bytes, cudaStream_t stream) {
+                     size_t ws_bytes, cudaStream_t stream, bool ls_device = false) {
     if (n_ref < 0 || n_query < 0 || d <= 0 || m < 0) return fail(NNGP_ERR_INVALID_ARGUMENT, "knn: negative size or d <= 0");
     if (d > kMaxDim) return fail(NNGP_ERR_UNSUPPORTED, "knn: d > 256 is not supported");
     if (n_ref > INT32_MAX - 1 || n_query > INT32_MAX - 1) return fail(NNGP_ERR_UNSUPPORTED, "knn: more than 2^31-2 points");
@@ -623,14 +627,15 @@ nngp_status knn_impl(const T *ref, int64_t n_ref, const T *query, int64_t n_quer
     T *qsc = reinterpret_cast<T *>(base + p.off_q);
 
     LsParam<T> lp;
-    for (int f = 0; f < d; ++f) lp.v[f] = ls ? (T)(n_ls == 1 ? ls[0] : ls[f]) : T(1);
+    for (int f = 0; f < d; ++f) lp.v[f] = (ls && !ls_device) ? (T)(n_ls == 1 ? ls[0] : ls[f]) : T(1);
     const int use_ls = ls != nullptr;
+    const double *ls_dev = ls_device ? ls : nullptr;
     scale_pad_kernel<T><<<grid_for(p.n_ref_pad * p.dp), 256, 0, stream>>>(ref, n_ref, d, p.dp, p.n_ref_pad, lp, use_ls,
-                                                                          refs);
+                                                                          ls_dev, n_ls, refs);
     NNGP_CUDA_TRY(cudaGetLastError());
     if (!same) {
         scale_pad_kernel<T><<<grid_for(n_query * p.dp), 256, 0, stream>>>(query, n_query, d, p.dp, n_query, lp,
-                                                                          use_ls, qsc);
+                                                                          use_ls, ls_dev, n_ls, qsc);
         NNGP_CUDA_TRY(cudaGetLastError());
     }
     if (p.path == KnnPath::Tc) {
@@ -833,6 +838,20 @@ nngp_status knn_f32(const float *ref, int64_t n_ref, const float *query, int64_t
                     int n_ls, int m, int has_cut, int64_t cut, int32_t *out, int32_t *flags, void *ws, size_t ws_bytes,
                     cudaStream_t stream) {
     return knn_impl<float>(ref, n_ref, query, n_query, d, ls, n_ls, m, has_cut, cut, out, flags, ws, ws_bytes, stream);
+}
+nngp_status knn_f32_ls_device(const float *ref, int64_t n_ref, const float *query, int64_t n_query, int d,
+                              const double *ls_dev, int n_ls, int m, int has_cut, int64_t cut, int32_t *out,
+                              int32_t *flags, void *ws, size_t ws_bytes, cudaStream_t stream) {
+    if (!ls_dev) return fail(NNGP_ERR_INVALID_ARGUMENT, "knn: the device length scale is null");
+    return knn_impl<float>(ref, n_ref, query, n_query, d, ls_dev, n_ls, m, has_cut, cut, out, flags, ws, ws_bytes,
+                           stream, true);
+}
+nngp_status knn_f64_ls_device(const double *ref, int64_t n_ref, const double *query, int64_t n_query, int d,
+                              const double *ls_dev, int n_ls, int m, int has_cut, int64_t cut, int32_t *out,
+                              int32_t *flags, void *ws, size_t ws_bytes, cudaStream_t stream) {
+    if (!ls_dev) return fail(NNGP_ERR_INVALID_ARGUMENT, "knn: the device length scale is null");
+    return knn_impl<double>(ref, n_ref, query, n_query, d, ls_dev, n_ls, m, has_cut, cut, out, flags, ws, ws_bytes,
+                            stream, true);
 }
 nngp_status knn_f64(const double *ref, int64_t n_ref, const double *query, int64_t n_query, int d, const double *ls,
                     int n_ls, int m, int has_cut, int64_t cut, int32_t *out, int32_t *flags, void *ws, size_t ws_bytes,

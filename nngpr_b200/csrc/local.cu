@@ -59,8 +59,25 @@ struct LocalArgs {
     // FP32 system needs the FP64 re-solve that local_redo_kernel then runs (predict re-solves in
     // place and leaves this null)
     uint32_t *redo_bits;
+    // device block of nngp_theta_params (may be null): [rbf, cst, noise, pivot_abs, 1/l_f ...];
+    // when set, the kernels take these values instead of the fields above
+    const double *dev_params;
     double inv_ls[kMaxDimLocal];
 };
+
+// The hyperparameter values a kernel works with: from the arguments, or from the device block
+// of a theta that never left the device.
+struct Hyp {
+    double rbf, cst, noise, pivot_abs;
+    const double *inv_ls;
+};
+__device__ __forceinline__ Hyp hyp_of(const LocalArgs &a) {
+    if (a.dev_params) {
+        const double *q = a.dev_params;
+        return Hyp{q[0], q[1], q[2], q[3], q + 4};
+    }
+    return Hyp{a.rbf, a.cst, a.noise, a.pivot_abs, a.inv_ls};
+}
 
 template <typename T> __device__ __forceinline__ T dsqrt(T v) { return sqrt(v); }
 template <typename T> __device__ __forceinline__ T drsqrt(T v) { return rsqrt(v); }
@@ -155,6 +172,7 @@ __device__ __forceinline__ bool warp_system(const LocalArgs &a, int64_t p, int l
                                             unsigned char *wsm, double &ll_acc, TIn *__restrict__ mean,
                                             TIn *__restrict__ var, int32_t *__restrict__ flags) {
     constexpr int M = kWarpM;
+    const Hyp h = hyp_of(a);
     const unsigned FULL = 0xffffffffu;
     const WarpSmem lay = WarpSmem::make(a.d, a.n_theta, std::is_same<TIn, float>::value,
                                         std::is_same<TIn, float>::value && !PRED && std::is_same<TC, float>::value);
@@ -189,10 +207,10 @@ __device__ __forceinline__ bool warp_system(const LocalArgs &a, int64_t p, int l
     // ---- gather scaled coordinates: rows 0..M-1 neighbours, row M the point ------------
     __syncwarp();
     for (int f = 0; f < d; ++f) {
-        const TC s = (TC)a.inv_ls[a.ard ? f : 0];
+        const TC s = (TC)h.inv_ls[a.ard ? f : 0];
         xs[lane * ds + f] = valid ? (TC)x_ref[(int64_t)j * d + f] * s : TC(0);
     }
-    for (int f = lane; f < d; f += 32) xs[M * ds + f] = (TC)x_pt[p * d + f] * (TC)a.inv_ls[a.ard ? f : 0];
+    for (int f = lane; f < d; f += 32) xs[M * ds + f] = (TC)x_pt[p * d + f] * (TC)h.inv_ls[a.ard ? f : 0];
     if (VEC4) {
         for (int f = d; f < ds; ++f) xs[lane * ds + f] = TC(0);
         for (int f = d + lane; f < ds; f += 32) xs[M * ds + f] = TC(0);
@@ -243,8 +261,8 @@ __device__ __forceinline__ bool warp_system(const LocalArgs &a, int64_t p, int l
             rp = fma(t, t, rp);
         }
     }
-    const TC rbf = (TC)a.rbf, cst = (TC)a.cst;
-    const TC diag_add = (TC)a.noise + ((int64_t)j < a.alpha_below ? (TC)a.alpha : TC(0));
+    const TC rbf = (TC)h.rbf, cst = (TC)h.cst;
+    const TC diag_add = (TC)h.noise + ((int64_t)j < a.alpha_below ? (TC)a.alpha : TC(0));
 #pragma unroll
     for (int k = 0; k < M; ++k) {
         const bool vk = (vmask >> k) & 1u;
@@ -257,7 +275,7 @@ __device__ __forceinline__ bool warp_system(const LocalArgs &a, int64_t p, int l
     }
     const TC ep0 = rbf * kern_s<MATERN>(a.family, rp);  // kept for the gradient
     TC kvec = valid ? ep0 + cst : TC(0);                 // K[p][lane]
-    const TC kpp = rbf + cst + (TC)a.noise + (PRED ? TC(0) : (TC)a.alpha);
+    const TC kpp = rbf + cst + (TC)h.noise + (PRED ? TC(0) : (TC)a.alpha);
 
     // ---- Cholesky of the neighbour block fused with l = L^-1 k ----------------------------
     TC minpiv = TC(3.0e38);
@@ -298,7 +316,7 @@ __device__ __forceinline__ bool warp_system(const LocalArgs &a, int64_t p, int l
     }
     const TC s2 = kpp - ss;
     if constexpr (std::is_same<TC, float>::value) {
-        if (!(minpiv >= (TC)a.pivot_abs) || !(s2 >= (TC)a.pivot_abs)) return false;  // NaN-safe
+        if (!(minpiv >= (TC)h.pivot_abs) || !(s2 >= (TC)h.pivot_abs)) return false;  // NaN-safe
     }
     if (!(minpiv > TC(0)) || !(s2 > TC(0))) flag_or(flags, NNGP_FLAG_NOT_PD);
 
@@ -424,15 +442,15 @@ __device__ __forceinline__ bool warp_system(const LocalArgs &a, int64_t p, int l
     g_amp += gpe;
     g_cst += TC(2) * Gp;
     g_iso = fma(gpl, rp, g_iso);
-    const double amp_t = (double)warp_sum(g_amp) + (double)wsum * a.rbf;
+    const double amp_t = (double)warp_sum(g_amp) + (double)wsum * h.rbf;
     const double cst_t = (double)warp_sum(g_cst) + (double)wsum;
     const double noi_t = (double)warp_sum(g_noise) + (double)wsum;
     const double iso_t = (double)warp_sum(g_iso);
     if (lane == 0) {
         ll_acc += ll;
         if (a.idx_rbf >= 0) gacc[a.idx_rbf] += amp_t;
-        if (a.idx_const >= 0) gacc[a.idx_const] += a.cst * cst_t;
-        if (a.idx_noise >= 0) gacc[a.idx_noise] += a.noise * noi_t;
+        if (a.idx_const >= 0) gacc[a.idx_const] += h.cst * cst_t;
+        if (a.idx_noise >= 0) gacc[a.idx_noise] += h.noise * noi_t;
         if (a.idx_ls >= 0 && !a.ard) gacc[a.idx_ls] += iso_t;
     }
     if (a.idx_ls >= 0 && a.ard) {
@@ -613,6 +631,7 @@ __global__ void __launch_bounds__(kBlkThreads) local_block_kernel(
     const TIn *__restrict__ x_pt, const TIn *__restrict__ y_pt, const int32_t *__restrict__ nbr,
     double *__restrict__ block_out, TIn *__restrict__ mean, TIn *__restrict__ var, int32_t *__restrict__ flags) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    const Hyp h = hyp_of(a);
     const BlockSmem L = BlockSmem::make(a.m, a.d);
     double *A = reinterpret_cast<double *>(smem_raw + L.a_off);
     double *xs = reinterpret_cast<double *>(smem_raw + L.xs_off);
@@ -646,7 +665,7 @@ __global__ void __launch_bounds__(kBlkThreads) local_block_kernel(
         for (int e = tid; e < n1 * d; e += blockDim.x) {
             const int i = e / d, f = e - i * d;
             const int32_t jj = ids[i];
-            const double s = a.inv_ls[a.ard ? f : 0];
+            const double s = h.inv_ls[a.ard ? f : 0];
             double v = 0.0;
             if (jj >= 0) v = (double)x_ref[(int64_t)jj * d + f] * s;
             else if (jj == -2) v = (double)x_pt[p * d + f] * s;
@@ -665,9 +684,9 @@ __global__ void __launch_bounds__(kBlkThreads) local_block_kernel(
                     const double t = xs[i * d + f] - xs[jx * d + f];
                     r = fma(t, t, r);
                 }
-                kv = a.rbf * kern_s<true>(a.family, r) + a.cst;
+                kv = h.rbf * kern_s<true>(a.family, r) + h.cst;
                 if (i == jx)
-                    kv += a.noise + (((i == m && PRED) || (i < m && (int64_t)ids[i] >= a.alpha_below)) ? 0.0 : a.alpha);
+                    kv += h.noise + (((i == m && PRED) || (i < m && (int64_t)ids[i] >= a.alpha_below)) ? 0.0 : a.alpha);
             } else {
                 kv = (i == jx) ? 1.0 : 0.0;
             }
@@ -789,10 +808,10 @@ __global__ void __launch_bounds__(kBlkThreads) local_block_kernel(
                 r = fma(t, t, r);
             }
             const double s0 = kern_s<true>(a.family, r);
-            t_amp += wgt * G * a.rbf * s0;
+            t_amp += wgt * G * h.rbf * s0;
             t_cst += wgt * G;
             if (i == jx) t_noise += G;
-            t_iso += wgt * G * a.rbf * kern_g<true>(a.family, r, s0) * r;
+            t_iso += wgt * G * h.rbf * kern_g<true>(a.family, r, s0) * r;
         }
         g_loc[0] += t_amp;
         g_loc[1] += t_cst;
@@ -814,7 +833,7 @@ __global__ void __launch_bounds__(kBlkThreads) local_block_kernel(
                         r = fma(t, t, r);
                     }
                     const double t = xs[i * d + f] - xs[jx * d + f];
-                    acc += 2.0 * G * a.rbf * kern_g<true>(a.family, r, kern_s<true>(a.family, r)) * t * t;
+                    acc += 2.0 * G * h.rbf * kern_g<true>(a.family, r, kern_s<true>(a.family, r)) * t * t;
                 }
                 const double s = block_sum(acc, scratch);
                 if (tid == 0) o[1 + a.idx_ls + f] += s;
@@ -832,8 +851,8 @@ __global__ void __launch_bounds__(kBlkThreads) local_block_kernel(
         const double s3 = block_sum(g_loc[3], scratch);
         if (tid == 0) {
             if (a.idx_rbf >= 0) o[1 + a.idx_rbf] += s0;
-            if (a.idx_const >= 0) o[1 + a.idx_const] += a.cst * s1;
-            if (a.idx_noise >= 0) o[1 + a.idx_noise] += a.noise * s2v;
+            if (a.idx_const >= 0) o[1 + a.idx_const] += h.cst * s1;
+            if (a.idx_noise >= 0) o[1 + a.idx_noise] += h.noise * s2v;
             if (a.idx_ls >= 0 && !a.ard) o[1 + a.idx_ls] += s3;
         }
     }
@@ -936,6 +955,7 @@ nngp_status fill_args(LocalArgs &a, const nngp_kernel *k, int d, int ydim, int m
     a.weights_out = 0;
     a.fp64_count = nullptr;
     a.redo_bits = nullptr;
+    a.dev_params = k->dev_params;
     if (k->family < NNGP_FAMILY_RBF || k->family > NNGP_FAMILY_MATERN52)
         return fail(NNGP_ERR_INVALID_ARGUMENT, "kernel family must be one of NNGP_FAMILY_*");
     a.family = k->family;
@@ -1417,6 +1437,69 @@ nngp_status predict_f64(const double *xt, const double *yt, int64_t nt, const do
                         const int32_t *nbr, int m, const nngp_kernel *k, double pivot_tol, double *mean, double *var,
                         int32_t *flags, cudaStream_t stream) {
     return predict_impl<double>(xt, yt, nt, xq, nq, d, ydim, nbr, m, k, pivot_tol, mean, var, flags, stream);
+}
+
+// ---------------------------------------------------------------------------------------
+// Hyperparameter values from a device theta (nngp_theta_params)
+// ---------------------------------------------------------------------------------------
+struct ThetaMap {
+    int idx_rbf, idx_const, idx_noise, idx_ls, n_ls, d;
+    double rbf, cst, noise, alpha, pivot_tol;  // the fixed values (used where the index is -1)
+    double ls[kMaxDimLocal];                   // fixed length scales (idx_ls = -1)
+};
+
+// One CTA: out = [rbf, cst, noise, pivot_abs, 1/l_0 .. 1/l_{d-1}, l_0 .. l_{d-1}], the values
+// fill_args computes on the host from kernel.clone_with_theta(theta).
+__global__ void __launch_bounds__(256) theta_params_kernel(const __grid_constant__ ThetaMap t,
+                                                           const double *__restrict__ theta,
+                                                           double *__restrict__ out) {
+    const double rbf = t.idx_rbf >= 0 ? exp(theta[t.idx_rbf]) : t.rbf;
+    const double cst = t.idx_const >= 0 ? exp(theta[t.idx_const]) : t.cst;
+    const double noise = t.idx_noise >= 0 ? exp(theta[t.idx_noise]) : t.noise;
+    if (threadIdx.x == 0) {
+        out[0] = rbf;
+        out[1] = cst;
+        out[2] = noise;
+        out[3] = t.pivot_tol * fabs(rbf + cst + noise + t.alpha);
+    }
+    for (int f = threadIdx.x; f < t.d; f += blockDim.x) {
+        const int q = t.n_ls > 1 ? f : 0;
+        const double l = t.n_ls == 0 ? 1.0 : (t.idx_ls >= 0 ? exp(theta[t.idx_ls + q]) : t.ls[q]);
+        out[4 + f] = 1.0 / l;
+        out[4 + t.d + f] = l;
+    }
+}
+
+nngp_status theta_params(const nngp_kernel *k, const double *theta_dev, int d, double pivot_tol, double *out,
+                         cudaStream_t stream) {
+    if (!k || !theta_dev || !out) return fail(NNGP_ERR_INVALID_ARGUMENT, "theta_params: null pointer");
+    if (d <= 0 || d > kMaxDimLocal) return fail(NNGP_ERR_UNSUPPORTED, "theta_params: d must be in [1, 256]");
+    if (k->n_ls != 0 && k->n_ls != 1 && k->n_ls != d)
+        return fail(NNGP_ERR_INVALID_ARGUMENT, "theta_params: n_ls must be 0, 1 or d");
+    ThetaMap t{};
+    t.idx_rbf = k->idx_rbf_level;
+    t.idx_const = k->idx_const;
+    t.idx_noise = k->idx_noise;
+    t.idx_ls = k->n_ls > 0 ? k->idx_ls : -1;
+    t.n_ls = k->n_ls;
+    t.d = d;
+    t.rbf = k->rbf_level;
+    t.cst = k->const_value;
+    t.noise = k->noise_level;
+    t.alpha = k->alpha;
+    t.pivot_tol = pivot_tol;
+    const int spans[4] = {1, 1, 1, t.n_ls > 1 ? t.n_ls : 1};
+    const int idx[4] = {t.idx_rbf, t.idx_const, t.idx_noise, t.idx_ls};
+    for (int i = 0; i < 4; ++i)
+        if (idx[i] >= 0 && idx[i] + spans[i] > k->n_theta)
+            return fail(NNGP_ERR_INVALID_ARGUMENT, "theta_params: a theta index is outside [0, n_theta)");
+    if (k->n_ls > 0 && t.idx_ls < 0) {
+        if (!k->length_scale) return fail(NNGP_ERR_INVALID_ARGUMENT, "theta_params: length_scale is null");
+        for (int f = 0; f < k->n_ls; ++f) t.ls[f] = k->length_scale[f];
+    }
+    theta_params_kernel<<<1, 256, 0, stream>>>(t, theta_dev, out);
+    NNGP_CUDA_TRY(cudaGetLastError());
+    return NNGP_OK;
 }
 
 }  // namespace nngp

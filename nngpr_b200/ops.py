@@ -191,7 +191,8 @@ def knn(ref: torch.Tensor, query: torch.Tensor, num_nn: int, ref_cut_index=None,
     Same contract as ``NngprWorker.find_nearest_neighbors`` (``base_nngpr.py:1613-1686``):
     kernel-space search divides by ``length_scale`` (``None`` = input space), ``ref_cut_index``
     restricts query ``j`` to refs ``[0, j + ref_cut_index)``.  Computes in the dtype of the
-    inputs (both must match).
+    inputs (both must match).  ``length_scale`` may be a float64 CUDA tensor (1 or d values): it
+    is then read on the device (``nngp_knn_f32_ls_device`` / ``_f64_ls_device``).
     """
     _check_tensor(ref, 'ref')
     _check_tensor(query, 'query')
@@ -204,13 +205,24 @@ def knn(ref: torch.Tensor, query: torch.Tensor, num_nn: int, ref_cut_index=None,
     out = torch.empty((n_q, num_nn), dtype=torch.int32, device=query.device)
     if n_q == 0 or num_nn == 0:
         return out
-    ls, n_ls = _ls_array(length_scale, d)
     L = _lib.lib()
     f64 = ref.dtype == torch.float64
     size_fn = L.nngp_knn_workspace_size_f64 if f64 else L.nngp_knn_workspace_size_f32
-    fn = L.nngp_knn_f64 if f64 else L.nngp_knn_f32
     ws_bytes = int(size_fn(n_ref, n_q, d, num_nn))
     ws = torch.empty(ws_bytes, dtype=torch.uint8, device=query.device)
+    if isinstance(length_scale, torch.Tensor) and length_scale.is_cuda:
+        _check_tensor(length_scale, 'length_scale', (torch.float64,))
+        n_ls = length_scale.numel()
+        if n_ls not in (1, d):
+            raise ValueError('length_scale must hold 1 or d values')
+        has_cut = ref_cut_index is not None
+        fn = L.nngp_knn_f64_ls_device if f64 else L.nngp_knn_f32_ls_device
+        st = fn(_ptr(ref), n_ref, _ptr(query), n_q, d, _ptr(length_scale), n_ls, num_nn, int(has_cut),
+                int(ref_cut_index) if has_cut else 0, _ptr(out), _ptr(flags), _ptr(ws), ws_bytes, _stream())
+        _lib.check(st, 'nngp_knn')
+        return out
+    ls, n_ls = _ls_array(length_scale, d)
+    fn = L.nngp_knn_f64 if f64 else L.nngp_knn_f32
     ls_p = ls.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if ls is not None else None
     has_cut = ref_cut_index is not None
     st = fn(_ptr(ref), n_ref, _ptr(query), n_q, d, ls_p, n_ls, num_nn, int(has_cut),
@@ -239,18 +251,43 @@ def _kernel_struct(p: RbfParams, alpha: float, d: int, keep: list) -> _lib.NngpK
     k.idx_ls = p.idx_ls
     k.n_theta = p.n_theta
     k.family = int(p.family)
+    k.dev_params = None
     return k
+
+
+def theta_params(p: RbfParams, theta: torch.Tensor, alpha: float, d: int,
+                 pivot_tol: float | None = DEFAULT_PIVOT_TOL) -> torch.Tensor:
+    """The hyperparameter values at a DEVICE ``theta`` (float64 CUDA tensor, the layout of
+    ``kernel.theta``), computed on the device (``nngp_theta_params``): a float64 tensor
+    ``[rbf, const, noise, pivot_abs, 1/l_0..1/l_{d-1}, l_0..l_{d-1}]`` for ``loglik(...,
+    params_dev=...)`` and, from index ``4 + d``, the device length scale of :func:`knn`.  ``p``
+    gives the structure (which hyperparameters are free, the fixed values)."""
+    _check_tensor(theta, 'theta', (torch.float64,))
+    if theta.numel() != p.n_theta:
+        raise ValueError(f'theta has {theta.numel()} entries, the kernel {p.n_theta}')
+    keep = []
+    k = _kernel_struct(p, alpha, d, keep)
+    out = torch.empty(4 + 2 * d, dtype=torch.float64, device=theta.device)
+    th = theta.contiguous()
+    st = _lib.lib().nngp_theta_params(ctypes.byref(k), _ptr(th), d,
+                                      float(DEFAULT_PIVOT_TOL if pivot_tol is None else pivot_tol), _ptr(out),
+                                      _stream())
+    _lib.check(st, 'nngp_theta_params')
+    return out
 
 
 def loglik(x: torch.Tensor, y: torch.Tensor, nbr: torch.Tensor, p: RbfParams, alpha: float,
            eval_gradient: bool, pivot_tol: float | None = DEFAULT_PIVOT_TOL,
            flags: torch.Tensor | None = None, out: torch.Tensor | None = None,
-           row_begin: int = 0, stats: dict | None = None) -> torch.Tensor:
+           row_begin: int = 0, stats: dict | None = None,
+           params_dev: torch.Tensor | None = None) -> torch.Tensor:
     """Fit-step log-likelihood (and gradient) on the device: float64 tensor ``[lml, grad...]``.
 
     ``x (n, d)``, ``y (n, ydim)`` of one dtype (float32: FP32 systems with FP64 fallback;
     float64: FP64), ``nbr (rows, m)`` int32 without the self column, for the points
-    ``[row_begin, row_begin + rows)`` (default: all points).  With a ``stats`` dict,
+    ``[row_begin, row_begin + rows)`` (default: all points).  ``params_dev`` (from
+    :func:`theta_params`) makes the kernels read the hyperparameter values from the device
+    instead of ``p``'s (``p`` still gives the structure).  With a ``stats`` dict,
     ``stats['fp64_systems']`` receives a device int64 0-d tensor: the systems this call re-solved
     in FP64 (``nngp_loglik_fp64_count``).
     """
@@ -271,6 +308,11 @@ def loglik(x: torch.Tensor, y: torch.Tensor, nbr: torch.Tensor, p: RbfParams, al
         out = torch.empty(nt, dtype=torch.float64, device=x.device)
     keep = []
     k = _kernel_struct(p, alpha, d, keep)
+    if params_dev is not None:  # the values of a device theta (theta_params), read by the kernels
+        _check_tensor(params_dev, 'params_dev', (torch.float64,))
+        if params_dev.numel() < 4 + 2 * d:
+            raise ValueError('params_dev is shorter than theta_params writes')
+        k.dev_params = params_dev.data_ptr()
     L = _lib.lib()
     ws_bytes = int(L.nngp_loglik_workspace_size(max(rows, 1), d, ydim, m, p.n_theta))
     ws = torch.empty(ws_bytes, dtype=torch.uint8, device=x.device)

@@ -30,7 +30,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_version_and_status_strings():
     L = _lib.lib()
-    assert L.nngp_abi_version() == 2
+    assert L.nngp_abi_version() == 3
     assert L.nngp_status_string(0) == b'NNGP_OK'
     assert L.nngp_status_string(3) == b'NNGP_ERR_WORKSPACE'
 

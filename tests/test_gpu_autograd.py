@@ -36,6 +36,50 @@ def test_backward_gives_reference_gradient(name):
     assert rel(theta.grad.cpu().numpy(), 3.0 * g['grad']) < 1e-9
 
 
+@pytest.mark.parametrize('mode', ['no', 'yes'])
+@pytest.mark.parametrize('name', ['cpu_n2000_d3_m16', 'ard_n400_d5_m12_y2', 'const_n300_d2_m10'])
+def test_device_theta_equals_host_theta(name, mode):
+    """A CUDA theta stays on the device (nngp_theta_params, the search's device length scale,
+    the kernels' device parameter block); the result equals the by-value path up to the last
+    bits of exp (FP64 systems 1e-12, FP32 systems 1e-6), and both search paths give the same
+    lists."""
+    from nngpr_b200 import ops
+    g, gpr, prob = _problem(name, mode)
+    th = np.asarray(g['theta'], dtype=np.float64)
+    host = prob.evaluate(th).cpu().numpy()
+    dev = prob.evaluate_device(torch.tensor(th, device='cuda')).cpu().numpy()
+    tol = 1e-12 if mode == 'no' else 1e-6
+    assert abs(dev[0] / host[0] - 1) < tol
+    assert rel(dev[1:], host[1:]) < 10 * tol
+    p = prob.params(th)
+    if p.length_scale is not None:
+        d = prob.x.shape[1]
+        params = ops.theta_params(prob.template, torch.tensor(th, device='cuda'), prob.alpha, d, prob.pivot_tol)
+        n_ls = d if p.n_ls == d else 1
+        m = min(prob.num_nn, prob.x.shape[0] - 1)
+        a = ops.knn(prob.x_search, prob.x_search, m, 0, p.length_scale).cpu().numpy()
+        b = ops.knn(prob.x_search, prob.x_search, m, 0, params[4 + d:4 + d + n_ls]).cpu().numpy()
+        np.testing.assert_array_equal(a, b)
+        np.testing.assert_allclose(params[4 + d:4 + 2 * d].cpu().numpy(), p.ls_vector(d), rtol=1e-15)
+
+
+def test_device_theta_evaluation_makes_no_host_sync():
+    """Forward and backward at a CUDA theta make no synchronising CUDA call (torch's sync debug
+    mode raises on one): theta is never read on the host."""
+    g, gpr, prob = _problem('ard_n400_d5_m12_y2', 'yes')
+    theta = torch.tensor(g['theta'], dtype=torch.float64, device='cuda', requires_grad=True)
+    torch.cuda.synchronize()
+    torch.cuda.set_sync_debug_mode('error')
+    try:
+        lml = NngpLogLik.apply(theta, prob)
+        lml.backward()
+    finally:
+        torch.cuda.set_sync_debug_mode('default')
+    # FP32 systems against the FP64 golden values: a sanity bound, the point here is the sync
+    assert abs(float(lml.detach()) / float(g['lml']) - 1) < 1e-4
+    assert rel(theta.grad.cpu().numpy(), g['grad']) < 1e-3
+
+
 def _rff_problem(n=20000, d=8, seed=4):
     """The differentiation workload's shape on a 20,000-point subset: x ~ U[0, 1]^8, y a
     512-feature random Fourier draw with log-uniform ARD length scales in [0.1, 1]."""
