@@ -87,6 +87,10 @@ struct Cfg {
     static constexpr int U = D + 1;                 // coordinates + the norm column
     static constexpr int KP = (3 * U + KMMA - 1) / KMMA * KMMA;  // split operand width
     static constexpr int NMMA = KP / KMMA;
+    // operand rows of exactly 128 bytes (d = 16, 20 BF16, d = 8 TF32) use the 128-byte swizzle:
+    // operands 1024-byte aligned, one MMA's K slice = 32 bytes further along the row
+    static constexpr bool SW128 = KP * ESZ == 128;
+    static constexpr int ALIGN = SW128 ? 1024 : 128;
     static constexpr int DP = (D + 3) / 4 * 4;      // exact-coordinate row length
     static constexpr int OP_BYTES = RT * KP * ESZ;  // B operand block of a ref tile
     static constexpr int EX_BYTES = RT * DP * 4;    // exact coordinates of a ref tile
@@ -107,7 +111,7 @@ struct Cfg {
     static constexpr int QUEUE_BYTES = EPI_WARPS * QCAP * (8 + 1);  // key + row
     static constexpr int CQ_BYTES = EPI_WARPS * CQCAP * 8;          // ref position << 5 | row
     static constexpr int BAR_BYTES = 256;
-    static constexpr int FIXED = 128 + A_BYTES + LIST_BYTES + QUEUE_BYTES + CQ_BYTES + BAR_BYTES;  // 128: alignment slack
+    static constexpr int FIXED = ALIGN + A_BYTES + LIST_BYTES + QUEUE_BYTES + CQ_BYTES + BAR_BYTES;  // ALIGN: base slack
     // as many CTAs per SM (up to 3) as hold at least 2 stages each: more epilogue warps per
     // scheduler.  Three CTAs share TMEM with one accumulator buffer each (the epilogue frees it
     // as soon as a tile's scores are in registers); one or two CTAs double-buffer it.
@@ -131,18 +135,24 @@ struct Cfg {
     static_assert(TMEM_COLS <= 512 && (TMEM_COLS & (TMEM_COLS - 1)) == 0, "TMEM columns");
     static_assert(CTAS_PER_SM * TMEM_COLS <= 512, "TMEM of the CTAs sharing an SM");
     static_assert(STAGES >= 2, "ref tile too large for two stages");
-    // K-major no-swizzle canonical layout: 8-row x 16-byte core matrices, SBO = 128 B between
-    // 8-row groups, LBO between 16-byte K chunks
-    static constexpr uint32_t A_LBO = (QT / 8) * 128;
-    static constexpr uint32_t B_LBO = (RT / 8) * 128;
 };
 
-// byte offset of element (row, k) of a K-major, no-swizzle UMMA operand with `rows` rows and
-// ESZ-byte elements (core matrices of 8 rows x 16 bytes)
-template <int ESZ = 4>
+// byte offset of element (row, k) of a K-major UMMA operand with `rows` rows and ESZ-byte
+// elements.  SW = false: no swizzle, core matrices of 8 rows x 16 bytes.  SW = true: the 128-byte
+// swizzle for rows of exactly 128 bytes (K * ESZ = 128): 8-row atoms of 1 KB, row r of an atom at
+// byte 128 (r % 8), its 16-byte chunk c at chunk c ^ (r % 8) -- the order in which the tensor core
+// reads a 1024-byte-aligned atom with SWIZZLE_128B (bank-conflict free, unlike the no-swizzle
+// layout whose 8 rows of one core matrix share 128 bytes)
+template <int ESZ = 4, bool SW = false>
 __host__ __device__ __forceinline__ uint32_t op_offset(int row, int k, int rows) {
-    constexpr int EPC = 16 / ESZ;
-    return (uint32_t)((k / EPC) * (rows / 8) * 128 + (row >> 3) * 128 + (row & 7) * 16 + (k % EPC) * ESZ);
+    if constexpr (SW) {
+        const uint32_t byte = (uint32_t)k * ESZ;
+        return (uint32_t)(row >> 3) * 1024u + (uint32_t)(row & 7) * 128u +
+               ((((byte >> 4) ^ (uint32_t)(row & 7)) & 7u) << 4) + (byte & 15u);
+    } else {
+        constexpr int EPC = 16 / ESZ;
+        return (uint32_t)((k / EPC) * (rows / 8) * 128 + (row >> 3) * 128 + (row & 7) * 16 + (k % EPC) * ESZ);
+    }
 }
 
 __device__ __forceinline__ float tf32_round(float x) {
@@ -162,7 +172,7 @@ __device__ __forceinline__ float bf16_value(uint16_t b) { return __uint_as_float
 // Element k of one row of a split operand: blocks [hi | hi | lo] (query side, lo_block = 2) or
 // [hi | lo | hi] (ref side, lo_block = 1) of the U values v, then zeros; the products
 // A' B'^T = a_hi b_hi + a_hi b_lo + a_lo b_hi.  Stored at `dst` as TF32 (float) or BF16.
-template <bool BF16, int U>
+template <bool BF16, int U, bool SW = false>
 __device__ __forceinline__ void put_split(unsigned char *dst_row_base, int row, int rows, int k, int lo_block,
                                           const float (&v)[U]) {
     float val = 0.f;
@@ -173,23 +183,34 @@ __device__ __forceinline__ void put_split(unsigned char *dst_row_base, int row, 
             const uint16_t hi = bf16_bits(v[f]);
             bits = (blk == lo_block) ? bf16_bits(v[f] - bf16_value(hi)) : hi;
         }
-        *reinterpret_cast<uint16_t *>(dst_row_base + op_offset<2>(row, k, rows)) = bits;
+        *reinterpret_cast<uint16_t *>(dst_row_base + op_offset<2, SW>(row, k, rows)) = bits;
     } else {
         if (blk < 3) {
             const float hi = tf32_round(v[f]);
             val = (blk == lo_block) ? (v[f] - hi) : hi;
         }
-        *reinterpret_cast<float *>(dst_row_base + op_offset<4>(row, k, rows)) = val;
+        *reinterpret_cast<float *>(dst_row_base + op_offset<4, SW>(row, k, rows)) = val;
     }
 }
 
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo, bool sw128 = false) {
     uint64_t d = 0;
     d |= (uint64_t)((addr >> 4) & 0x3FFFu);
     d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
     d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
     d |= (uint64_t)1 << 46;  // descriptor version for sm_100
-    return d;                // base offset 0, lbo mode 0, layout SWIZZLE_NONE
+    if (sw128) d |= (uint64_t)2 << 61;  // layout SWIZZLE_128B (else 0, SWIZZLE_NONE); base offset 0, lbo mode 0
+    return d;
+}
+
+// Descriptor of K slice i (K = KMMA elements) of a K-major operand at smem address base with
+// `rows` rows: no swizzle (LBO between 16-byte K chunks = rows / 8 core matrices, SBO 128 between
+// 8-row groups; one slice spans two chunks) or the 128-byte swizzle (rows of 128 bytes, 8-row atoms
+// of 1 KB = SBO, LBO unused (16), the slice starting 32 bytes further along the row)
+template <bool SW, int ESZ, int KMMA>
+__device__ __forceinline__ uint64_t op_desc(uint32_t base, int rows, int i) {
+    if constexpr (SW) return smem_desc(base + (uint32_t)(i * KMMA * ESZ), 16, 1024, true);
+    else return smem_desc(base + (uint32_t)(i * 2 * (rows / 8) * 128), (uint32_t)((rows / 8) * 128), 128);
 }
 
 // instruction descriptors: F32 accumulate, both operands K-major, N = RT, M = QT; A and B TF32
@@ -327,7 +348,7 @@ __global__ void build_tc_tiles_kernel(const float *__restrict__ xs, int64_t n, i
             for (int f = 0; f < D; ++f) b[f] = 0.f;
             b[D] = kPadNorm;
         }
-        for (int k = 0; k < C::KP; ++k) put_split<C::BF16, C::U>(base, row, RT, k, 1, b);  // [b_hi | b_lo | b_hi]
+        for (int k = 0; k < C::KP; ++k) put_split<C::BF16, C::U, C::SW128>(base, row, RT, k, 1, b);  // [b_hi | b_lo | b_hi]
         const int32_t pidx = i < n ? (int32_t)(perm ? (int64_t)perm[i] : i) : -1;
         if (C::IX_MODE == 1) ex[C::DP - 1] = __int_as_float(pidx);
         float *exo = reinterpret_cast<float *>(base + C::OP_BYTES) + row * C::DP;
@@ -365,10 +386,11 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
     constexpr int S = C::STAGES;
     constexpr int EPI_WARPS = C::EPI_WARPS;
     constexpr unsigned FULL = 0xffffffffu;
-    // 128-byte base: the no-swizzle UMMA operands and the bulk copies need 16-byte alignment
+    // base aligned to C::ALIGN: 1024 for the swizzled operands (their atoms), else 128 (the
+    // no-swizzle operands and the bulk copies need 16)
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    unsigned char *sm =
-        reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    unsigned char *sm = reinterpret_cast<unsigned char *>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + (C::ALIGN - 1)) & ~uintptr_t(C::ALIGN - 1));
     unsigned char *sA = sm;
     unsigned char *sB = sA + C::A_BYTES;
     uint64_t *H = reinterpret_cast<uint64_t *>(sB + S * C::STAGE_BYTES);  // [ROWS][HS] heaps
@@ -538,8 +560,8 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
                         const uint32_t aq = a_addr + qt * C::A_TILE;
 #pragma unroll
                         for (int i = 0; i < C::NMMA; ++i) {  // one MMA spans two 16-byte K chunks
-                            const uint64_t ad = smem_desc(aq + i * 2 * C::A_LBO, C::A_LBO, 128);
-                            const uint64_t bd = smem_desc(b_addr + i * 2 * C::B_LBO, C::B_LBO, 128);
+                            const uint64_t ad = op_desc<C::SW128, C::ESZ, C::KMMA>(aq, QT, i);
+                            const uint64_t bd = op_desc<C::SW128, C::ESZ, C::KMMA>(b_addr, RT, i);
                             mma_op<C::BF16>(d_tmem, ad, bd, i > 0 ? 1u : 0u);
                         }
                     }
@@ -586,7 +608,8 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
 #pragma unroll
                 for (int f = 0; f < D; ++f) a[f] = active ? qc[f] : 0.f;
                 a[D] = active ? 1.f : 0.f;
-                for (int k = 0; k < C::KP; ++k) put_split<C::BF16, C::U>(sA + qtw * C::A_TILE, quad * 32 + lane, QT, k, 2, a);
+                for (int k = 0; k < C::KP; ++k)
+                    put_split<C::BF16, C::U, C::SW128>(sA + qtw * C::A_TILE, quad * 32 + lane, QT, k, 2, a);
             }
             fence_proxy_async_smem();
             mbar_arrive(a_ready);
@@ -879,18 +902,19 @@ __global__ void __launch_bounds__(THREADS) tc_layout_selftest_kernel(const float
                                                                     int32_t *__restrict__ flags) {
     constexpr int ESZ = BF16 ? 2 : 4;
     constexpr int KMMA = BF16 ? 16 : 8;
+    constexpr bool SW = KP * ESZ == 128;  // the search's choice for the same shape
     __shared__ __align__(1024) unsigned char sA[QT * KP * ESZ];
     __shared__ __align__(1024) unsigned char sB[RT * KP * ESZ];
     __shared__ __align__(8) uint64_t bar;
     __shared__ uint32_t tmem_slot;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int e = threadIdx.x; e < QT * KP; e += blockDim.x) {
-        if constexpr (BF16) *reinterpret_cast<uint16_t *>(sA + op_offset<2>(e / KP, e % KP, QT)) = bf16_bits(a[e]);
-        else *reinterpret_cast<float *>(sA + op_offset<4>(e / KP, e % KP, QT)) = a[e];
+        if constexpr (BF16) *reinterpret_cast<uint16_t *>(sA + op_offset<2, SW>(e / KP, e % KP, QT)) = bf16_bits(a[e]);
+        else *reinterpret_cast<float *>(sA + op_offset<4, SW>(e / KP, e % KP, QT)) = a[e];
     }
     for (int e = threadIdx.x; e < RT * KP; e += blockDim.x) {
-        if constexpr (BF16) *reinterpret_cast<uint16_t *>(sB + op_offset<2>(e / KP, e % KP, RT)) = bf16_bits(b[e]);
-        else *reinterpret_cast<float *>(sB + op_offset<4>(e / KP, e % KP, RT)) = b[e];
+        if constexpr (BF16) *reinterpret_cast<uint16_t *>(sB + op_offset<2, SW>(e / KP, e % KP, RT)) = bf16_bits(b[e]);
+        else *reinterpret_cast<float *>(sB + op_offset<4, SW>(e / KP, e % KP, RT)) = b[e];
     }
     fence_proxy_async_smem();
     if (threadIdx.x == 0) {
@@ -907,11 +931,10 @@ __global__ void __launch_bounds__(THREADS) tc_layout_selftest_kernel(const float
     tc_fence_after();
     const uint32_t tmem_base = tmem_slot;
     if (warp == 4 && lane == 0) {
-        constexpr uint32_t A_LBO = (QT / 8) * 128, B_LBO = (RT / 8) * 128;
 #pragma unroll
         for (int i = 0; i < KP / KMMA; ++i)
-            mma_op<BF16>(tmem_base, smem_desc(smem_addr(sA) + i * 2 * A_LBO, A_LBO, 128),
-                         smem_desc(smem_addr(sB) + i * 2 * B_LBO, B_LBO, 128), i > 0 ? 1u : 0u);
+            mma_op<BF16>(tmem_base, op_desc<SW, ESZ, KMMA>(smem_addr(sA), QT, i),
+                         op_desc<SW, ESZ, KMMA>(smem_addr(sB), RT, i), i > 0 ? 1u : 0u);
         mma_commit(&bar);
     }
     const bool ok = mbar_wait_bounded(&bar, 0);
