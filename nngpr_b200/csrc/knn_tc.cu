@@ -104,7 +104,13 @@ struct Cfg {
     // complete.  The screen passes about one pair in 3,000 at d = 16: the epilogue reads those
     // pairs' exact coordinates and indices from the record in global memory, 32 at a time.
     static constexpr int TILE_BYTES = OP_BYTES + EX_BYTES + IX_BYTES;
-    static constexpr int STAGE_BYTES = OP_BYTES;
+    // d = 16: a stage holds two ref tiles, multiplied by one MMA of N = 256 per query tile and K
+    // slice (half the MMA instructions and 12 KB of operand reads per 256 x 128 x 16 instead of
+    // 16 KB); its accumulators fill the 512 TMEM columns, single-buffered
+    static constexpr bool PAIR = D == 16 && QTILES == 2;
+    static constexpr int TPS = PAIR ? 2 : 1;        // ref tiles per stage
+    static constexpr int RS = RT * TPS;             // refs per stage (MMA N)
+    static constexpr int STAGE_BYTES = OP_BYTES * TPS;
     static constexpr int A_TILE = QT * KP * ESZ;    // query operand of one query tile
     static constexpr int A_BYTES = A_TILE * QTILES;
     static constexpr int LIST_BYTES = ROWS * HS * 8;  // one heap of keys per query
@@ -129,8 +135,8 @@ struct Cfg {
     static constexpr bool TMA_WARP = CTAS_PER_SM == 1;
     static constexpr int THREADS = (EPI_WARPS + 1 + (TMA_WARP ? 1 : 0)) * 32;
     static constexpr int SMEM = FIXED + STAGES * STAGE_BYTES;
-    static constexpr int NBUF = CTAS_PER_SM == 3 ? 1 : 2;  // accumulator buffers in TMEM
-    static constexpr uint32_t BUF_COLS = RT * QTILES;       // one buffer: a tile per query tile
+    static constexpr int NBUF = (CTAS_PER_SM == 3 || PAIR) ? 1 : 2;  // accumulator buffers in TMEM
+    static constexpr uint32_t BUF_COLS = RS * QTILES;                 // one buffer: a stage per query tile
     static constexpr uint32_t TMEM_COLS = NBUF * BUF_COLS;  // a power of two >= 32, <= 512
     static_assert(TMEM_COLS <= 512 && (TMEM_COLS & (TMEM_COLS - 1)) == 0, "TMEM columns");
     static_assert(CTAS_PER_SM * TMEM_COLS <= 512, "TMEM of the CTAs sharing an SM");
@@ -220,28 +226,36 @@ constexpr uint32_t kIdesc =
 constexpr uint32_t kIdescBf16 =
     (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(RT >> 3) << 17) | ((uint32_t)(QT >> 4) << 24);
 
-__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate,
+                                         uint32_t idesc = kIdesc) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
-        "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0)
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0)
         : "memory");
 }
 
-__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate,
+                                         uint32_t idesc = kIdescBf16) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
-        "l"(adesc), "l"(bdesc), "r"(kIdescBf16), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0)
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0)
         : "memory");
 }
 
-template <bool BF16>
+// instruction descriptor of an M = QT, N = n product (F32 accumulate, K-major A and B)
+constexpr uint32_t idesc_of(bool bf16, int n) {
+    return (1u << 4) | ((bf16 ? 1u : 2u) << 7) | ((bf16 ? 1u : 2u) << 10) | ((uint32_t)(n >> 3) << 17) |
+           ((uint32_t)(QT >> 4) << 24);
+}
+
+template <bool BF16, int N = RT>
 __device__ __forceinline__ void mma_op(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
-    if constexpr (BF16) mma_bf16(tmem_d, adesc, bdesc, accumulate);
-    else mma_tf32(tmem_d, adesc, bdesc, accumulate);
+    if constexpr (BF16) mma_bf16(tmem_d, adesc, bdesc, accumulate, idesc_of(true, N));
+    else mma_tf32(tmem_d, adesc, bdesc, accumulate, idesc_of(false, N));
 }
 
 __device__ __forceinline__ void mma_commit(uint64_t *bar) {
@@ -429,9 +443,12 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
             mbar_init(&b_full[s], 1);
             mbar_init(&b_empty[s], 1);  // the MMA commit: the epilogue never reads a stage
         }
-        for (int b = 0; b < C::NBUF; ++b) {
+        // accumulator barriers: one pair per TMEM buffer, or with PAIR one pair per query tile (its
+        // 256 columns are released by its own four warps, so the MMAs of one query tile's next
+        // stage overlap the other tile's epilogue)
+        for (int b = 0; b < (C::PAIR ? QTILES : C::NBUF); ++b) {
             mbar_init(&t_full[b], 1);
-            mbar_init(&t_empty[b], EPI_WARPS);
+            mbar_init(&t_empty[b], C::PAIR ? 4 : EPI_WARPS);
         }
         mbar_init(a_ready, EPI_WARPS * 32);
         *s_abort = 0;
@@ -449,11 +466,12 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
     const uint32_t tmem_base = *tmem_slot;
     const float rmax = sqrtf(__uint_as_float(*r2max_bits)) * 1.0001f;
 
-    uint32_t g_tile = 0;  // tiles this CTA has streamed (phases of the ring and TMEM buffers)
+    uint32_t g_tile = 0;  // stages this CTA has streamed (phases of the ring and TMEM buffers)
     uint32_t it = 0;      // work items this CTA has processed (phase of a_ready)
     bool aborted = false;
     uint32_t tma_issued = 0, tma_landed = 0;  // producer lane: copies issued / waited for (drain on abort)
-    uint32_t mma_issued = 0;                  // producer lane: tiles whose MMAs were issued and committed
+    int last_tf = -1;                         // producer lane: accumulator barrier of the last commit
+    uint32_t last_tf_par = 0;                 // and the parity of that phase
 
     auto limit_of = [&](int64_t qq) -> int64_t {
         if (!has_cut) return n_ref;
@@ -491,33 +509,43 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
             ntiles = (uint32_t)((block_limit + RT - 1) / RT);
         }
         const int32_t *tl = pruned ? tile_list + tile_off[qtile] + tfirst : nullptr;  // this item's ref tiles
-        const uint32_t G = g_tile;
-        // stage g % S is free once the MMAs and the epilogue of tile g - S are done with it
+        // the item's stages: its tiles one per stage, or two (PAIR: tiles 2u and 2u + 1 in stage u,
+        // the second half of the last stage empty when ntiles is odd)
+        const uint32_t nstg = (ntiles + C::TPS - 1) / C::TPS;
+        const uint32_t G = g_tile;  // stages this CTA streamed before the item
+        // stage buffer g % S is free once the MMAs of stage g - S are done with it
         auto wait_empty = [&](uint32_t g) -> bool {
             const uint32_t k = g / S;
             return mbar_wait_bounded(&b_empty[g % S], (k & 1) ^ 1, wait_ns);
         };
         // the tile record the item's t-th tile comes from
         auto tile_at = [&](uint32_t t) -> int64_t { return pruned ? (int64_t)tl[t] : (int64_t)(tfirst + t); };
-        auto issue_tma = [&](uint32_t g, int64_t t) {
+        // stage g: the B operand of tile record ta, and of tb after it when tb >= 0
+        auto issue_stage = [&](uint32_t g, int64_t ta, int64_t tb) {
             const uint32_t s = g % S;
-            mbar_arrive_expect_tx(&b_full[s], C::STAGE_BYTES);
-            tma_bulk_g2s(sB + s * C::STAGE_BYTES, tiles_g + t * C::TILE_BYTES, C::STAGE_BYTES, &b_full[s]);
+            mbar_arrive_expect_tx(&b_full[s], (uint32_t)C::OP_BYTES * (tb >= 0 ? 2u : 1u));
+            tma_bulk_g2s(sB + s * C::STAGE_BYTES, tiles_g + ta * C::TILE_BYTES, C::OP_BYTES, &b_full[s]);
+            if (tb >= 0)
+                tma_bulk_g2s(sB + s * C::STAGE_BYTES + C::OP_BYTES, tiles_g + tb * C::TILE_BYTES, C::OP_BYTES,
+                             &b_full[s]);
             tma_issued = g + 1;
         };
+        auto issue_tma = [&](uint32_t g, int64_t t) { issue_stage(g, t, -1); };
 
         if (copy_warp) {
             // the item's tiles in order, each as soon as its stage is free (no query operand
             // needed); the warp reads the tile list 32 entries at a time, so no dependent global
             // load sits between two copies
             int64_t ent = 0;
-            for (uint32_t t = 0; t < ntiles; ++t) {
+            for (uint32_t u = 0; u < nstg; ++u) {
+                const uint32_t t = u * C::TPS;  // the stage's first tile (t + 1 is in the same batch of 32)
                 if ((t & 31u) == 0) ent = t + lane < ntiles ? tile_at(t + lane) : 0;
                 const int64_t cur = __shfl_sync(FULL, ent, (int)(t & 31u));
+                const int64_t cur2 = C::PAIR ? __shfl_sync(FULL, ent, (int)((t + 1) & 31u)) : 0;
                 bool ok = true;
                 if (lane == 0) {
-                    ok = wait_empty(G + t);
-                    if (ok) issue_tma(G + t, cur);
+                    ok = wait_empty(G + u);
+                    if (ok) issue_stage(G + u, cur, (C::PAIR && t + 1 < ntiles) ? cur2 : (int64_t)-1);
                 }
                 if (!__shfl_sync(FULL, ok, 0)) {
                     aborted = true;
@@ -540,7 +568,7 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
                 // list entry of the next refill, read one refill ahead
                 int64_t next_fill = (!C::TMA_WARP && (uint32_t)S < ntiles) ? tile_at(S) : 0;
                 const uint32_t a_addr = smem_addr(sA);
-                for (uint32_t t = 0; t < ntiles && !aborted; ++t) {
+                for (uint32_t t = 0; t < nstg && !aborted; ++t) {  // t: the item's stage
                     const uint32_t g = G + t;
                     const uint32_t s = g % S, b = g % C::NBUF, use = g / C::NBUF;
                     if (!mbar_wait_bounded(&b_full[s], (g / S) & 1, wait_ns)) {
@@ -548,31 +576,47 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
                         break;
                     }
                     tma_landed = g + 1;
-                    if (!mbar_wait_bounded(&t_empty[b], (use & 1) ^ 1, wait_ns)) {
+                    const uint32_t b_addr = smem_addr(sB + s * C::STAGE_BYTES);
+                    bool stop_mma = false;
+#pragma unroll
+                    for (int qt = 0; qt < QTILES; ++qt) {  // every query tile against the same staged refs
+                        if (C::PAIR || qt == 0) {  // the accumulator(s) this query tile writes are free
+                            const uint32_t tb = C::PAIR ? (uint32_t)qt : b;
+                            if (!mbar_wait_bounded(&t_empty[tb], ((C::PAIR ? g : use) & 1) ^ 1, wait_ns)) {
+                                stop_mma = true;
+                                break;
+                            }
+                            tc_fence_after();
+                        }
+                        const uint32_t d_tmem = tmem_base + b * C::BUF_COLS + qt * C::RS;
+                        const uint32_t aq = a_addr + qt * C::A_TILE;
+#pragma unroll
+                        for (int i = 0; i < C::NMMA; ++i) {  // one K slice per MMA
+                            const uint64_t ad = op_desc<C::SW128, C::ESZ, C::KMMA>(aq, QT, i);
+                            const uint64_t bd = op_desc<C::SW128, C::ESZ, C::KMMA>(b_addr, C::RS, i);
+                            mma_op<C::BF16, C::RS>(d_tmem, ad, bd, i > 0 ? 1u : 0u);
+                        }
+                        if (C::PAIR) {
+                            mma_commit(&t_full[qt]);
+                            last_tf = qt;
+                            last_tf_par = g & 1;
+                        }
+                    }
+                    if (stop_mma) {
                         aborted = true;
                         break;
                     }
-                    tc_fence_after();
-                    const uint32_t b_addr = smem_addr(sB + s * C::STAGE_BYTES);
-#pragma unroll
-                    for (int qt = 0; qt < QTILES; ++qt) {  // every query tile against the same ref tile
-                        const uint32_t d_tmem = tmem_base + b * C::BUF_COLS + qt * RT;
-                        const uint32_t aq = a_addr + qt * C::A_TILE;
-#pragma unroll
-                        for (int i = 0; i < C::NMMA; ++i) {  // one MMA spans two 16-byte K chunks
-                            const uint64_t ad = op_desc<C::SW128, C::ESZ, C::KMMA>(aq, QT, i);
-                            const uint64_t bd = op_desc<C::SW128, C::ESZ, C::KMMA>(b_addr, RT, i);
-                            mma_op<C::BF16>(d_tmem, ad, bd, i > 0 ? 1u : 0u);
-                        }
+                    if (!C::PAIR) {
+                        mma_commit(&t_full[b]);
+                        last_tf = (int)b;
+                        last_tf_par = use & 1;
                     }
-                    mma_commit(&t_full[b]);
                     mma_commit(&b_empty[s]);
-                    mma_issued = g + 1;
                     if constexpr (!C::TMA_WARP) {
                         const uint32_t gr = g - 1 + S;  // refill the stage that MMA g-1 used
-                        if (t > 0 && gr < G + ntiles) {
+                        if (t > 0 && gr < G + nstg) {
                             const int64_t cur = next_fill;
-                            if (gr + 1 < G + ntiles) next_fill = tile_at(gr + 1 - G);
+                            if (gr + 1 < G + nstg) next_fill = tile_at(gr + 1 - G);
                             if (!wait_empty(gr)) {
                                 aborted = true;
                                 break;
@@ -726,92 +770,113 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
                 ccount = rest;
             };
 
-            // the next tile's list entry is loaded one tile ahead (a global load per tile that
-            // would otherwise sit on the path from the accumulator to the screen)
-            int64_t tl_next = (pruned && ntiles > 0) ? (int64_t)tl[0] : 0;
-            for (uint32_t t = 0; t < ntiles; ++t) {
-                const uint32_t g = G + t;
+            // the next stage's list entries are loaded one stage ahead (global loads that would
+            // otherwise sit on the path from the accumulator to the screen)
+            int64_t nx[C::TPS];
+#pragma unroll
+            for (int h = 0; h < C::TPS; ++h) nx[h] = (pruned && (uint32_t)h < ntiles) ? (int64_t)tl[h] : 0;
+            for (uint32_t u = 0; u < nstg; ++u) {
+                const uint32_t g = G + u;
                 const uint32_t b = g % C::NBUF;
-                const int64_t tl_cur = tl_next;
-                if (pruned && t + 1 < ntiles) tl_next = (int64_t)tl[t + 1];
-                if (!mbar_wait_bounded(&t_full[b], (g / C::NBUF) & 1, wait_ns)) aborted = true;
+                const uint32_t t0 = u * C::TPS;                                  // the stage's first tile
+                const int nh = (int)min((uint32_t)C::TPS, ntiles - t0);           // tiles in the stage
+                int64_t j0[C::TPS];                                               // first ref position of each
+#pragma unroll
+                for (int h = 0; h < C::TPS; ++h) {
+                    j0[h] = (pruned ? nx[h] : (int64_t)(tfirst + t0 + h)) * RT;
+                    const uint32_t tn = t0 + C::TPS + h;
+                    if (pruned && tn < ntiles) nx[h] = (int64_t)tl[tn];
+                }
+                const uint32_t tb = C::PAIR ? (uint32_t)qtw : b;  // this warp's accumulator barriers
+                if (!mbar_wait_bounded(&t_full[tb], (g / C::NBUF) & 1, wait_ns)) aborted = true;
                 if (__any_sync(FULL, aborted)) {
                     aborted = true;
                     break;
                 }
                 tc_fence_after();
-                const int64_t j0 = (pruned ? tl_cur : (int64_t)(tfirst + t)) * RT;  // first ref position of the tile
-                const uint32_t taddr = tmem_base + ((uint32_t)(quad * 32) << 16) + b * C::BUF_COLS + qtw * RT;
-                // 1) screen: the minimum of each group of 8 columns (16 per row), the accumulator read
-                //    in four 32-column chunks, each loading while the previous one is reduced; one
-                //    vote per tile, since most tiles give no row of the warp a candidate.  A tile that
-                //    does reads its passing chunks again (the accumulator is held until the vote) for
-                //    the candidate masks.
-                float gm[16];
-                auto group_mins = [&](const uint32_t (&v)[32], int c) {
+                // 1) screen each tile of the stage: the minimum of each group of 8 columns (16 per row),
+                //    the accumulator read in four 32-column chunks, each loading while the previous one
+                //    is reduced; one vote per tile, since most tiles give no row of the warp a
+                //    candidate.  A tile that does reads its passing chunks again (the accumulator is
+                //    held until every tile of the stage is screened) for the candidate masks.
+                uint32_t cmk[C::TPS][4];
+                bool has_t[C::TPS];
 #pragma unroll
-                    for (int gi = 0; gi < 4; ++gi) {
+                for (int h = 0; h < C::TPS; ++h) {
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) cmk[h][c] = 0u;
+                    has_t[h] = false;
+                    if (h >= nh) continue;  // warp-uniform
+                    const uint32_t taddr =
+                        tmem_base + ((uint32_t)(quad * 32) << 16) + b * C::BUF_COLS + qtw * C::RS + h * RT;
+                    float gm[16];
+                    auto group_mins = [&](const uint32_t (&v)[32], int c) {
+#pragma unroll
+                        for (int gi = 0; gi < 4; ++gi) {
 #define NNGP_V(k) __uint_as_float(v[gi * 8 + (k)])
-                        gm[c * 4 + gi] = fminf(min3f(NNGP_V(0), NNGP_V(1), NNGP_V(2)),
-                                               min3f(NNGP_V(3), NNGP_V(4), fminf(NNGP_V(5), fminf(NNGP_V(6), NNGP_V(7)))));
+                            gm[c * 4 + gi] = fminf(min3f(NNGP_V(0), NNGP_V(1), NNGP_V(2)),
+                                                   min3f(NNGP_V(3), NNGP_V(4), fminf(NNGP_V(5), fminf(NNGP_V(6), NNGP_V(7)))));
 #undef NNGP_V
-                    }
-                };
-                uint32_t va[32], vb[32];
-                tmem_ld32_nowait(taddr, va);
-                tmem_wait_ld(va);
-                tmem_ld32_nowait(taddr + 32, vb);
-                group_mins(va, 0);
-                tmem_wait_ld(vb);
-                tmem_ld32_nowait(taddr + 64, va);
-                group_mins(vb, 1);
-                tmem_wait_ld(va);
-                tmem_ld32_nowait(taddr + 96, vb);
-                group_mins(va, 2);
-                tmem_wait_ld(vb);
-                group_mins(vb, 3);
-                float cmin[4];  // minimum of each chunk
+                        }
+                    };
+                    uint32_t va[32], vb[32];
+                    tmem_ld32_nowait(taddr, va);
+                    tmem_wait_ld(va);
+                    tmem_ld32_nowait(taddr + 32, vb);
+                    group_mins(va, 0);
+                    tmem_wait_ld(vb);
+                    tmem_ld32_nowait(taddr + 64, va);
+                    group_mins(vb, 1);
+                    tmem_wait_ld(va);
+                    tmem_ld32_nowait(taddr + 96, vb);
+                    group_mins(va, 2);
+                    tmem_wait_ld(vb);
+                    group_mins(vb, 3);
+                    float cmin[4];  // minimum of each chunk
 #pragma unroll
-                for (int c = 0; c < 4; ++c) cmin[c] = fminf(fminf(gm[4 * c], gm[4 * c + 1]), fminf(gm[4 * c + 2], gm[4 * c + 3]));
-                const bool tile_has = __any_sync(FULL, fminf(fminf(cmin[0], cmin[1]), fminf(cmin[2], cmin[3])) < tq);
-                uint32_t cmk[4] = {0u, 0u, 0u, 0u};
-                if (tile_has) {
+                    for (int c = 0; c < 4; ++c) cmin[c] = fminf(fminf(gm[4 * c], gm[4 * c + 1]), fminf(gm[4 * c + 2], gm[4 * c + 3]));
+                    has_t[h] = __any_sync(FULL, fminf(fminf(cmin[0], cmin[1]), fminf(cmin[2], cmin[3])) < tq);
+                    if (has_t[h]) {
 #pragma unroll
-                    for (int c = 0; c < 4; ++c) {
-                        if (__any_sync(FULL, cmin[c] < tq)) {  // warp-uniform: the load is collective
-                            tmem_ld32_nowait(taddr + 32 * c, va);
-                            tmem_wait_ld(va);
-                            uint32_t cm = 0;
+                        for (int c = 0; c < 4; ++c) {
+                            if (__any_sync(FULL, cmin[c] < tq)) {  // warp-uniform: the load is collective
+                                tmem_ld32_nowait(taddr + 32 * c, va);
+                                tmem_wait_ld(va);
+                                uint32_t cm = 0;
 #pragma unroll
-                            for (int gi = 0; gi < 4; ++gi) {
-                                if (gm[4 * c + gi] < tq) {  // only groups whose minimum passes
+                                for (int gi = 0; gi < 4; ++gi) {
+                                    if (gm[4 * c + gi] < tq) {  // only groups whose minimum passes
 #pragma unroll
-                                    for (int k = 0; k < 8; ++k)
-                                        cm |= (__uint_as_float(va[gi * 8 + k]) < tq ? 1u : 0u) << (gi * 8 + k);
+                                        for (int k = 0; k < 8; ++k)
+                                            cm |= (__uint_as_float(va[gi * 8 + k]) < tq ? 1u : 0u) << (gi * 8 + k);
+                                    }
                                 }
+                                cmk[h][c] = cm;
                             }
-                            cmk[c] = cm;
                         }
                     }
                 }
                 tc_fence_before();
                 __syncwarp();
-                if (lane == 0) mbar_arrive(&t_empty[b]);
-                if (tile_has) {
+                if (lane == 0) mbar_arrive(&t_empty[tb]);
+#pragma unroll
+                for (int h = 0; h < C::TPS; ++h) {
+                    if (!has_t[h]) continue;
                     {  // columns with j < limit only (pruned: positions < n_ref; the index test is per candidate)
-                        const int64_t room = (pruned ? n_ref : limit) - j0;
+                        const int64_t room = (pruned ? n_ref : limit) - j0[h];
                         if (room < RT) {
 #pragma unroll
                             for (int c = 0; c < 4; ++c) {
                                 const int64_t r = room - c * 32;
-                                if (r < 32) cmk[c] &= r <= 0 ? 0u : ((1u << (uint32_t)r) - 1u);
+                                if (r < 32) cmk[h][c] &= r <= 0 ? 0u : ((1u << (uint32_t)r) - 1u);
                             }
                         }
                     }
                     // 2) queue the tile's candidates (ref position, row): each lane walks its own
                     //    (column by column, chunks in order), one per warp iteration; whole batches of
                     //    32 are rescored as soon as they are queued
-                    uint64_t lo = (uint64_t)cmk[0] | (uint64_t)cmk[1] << 32, hi = (uint64_t)cmk[2] | (uint64_t)cmk[3] << 32;
+                    uint64_t lo = (uint64_t)cmk[h][0] | (uint64_t)cmk[h][1] << 32;
+                    uint64_t hi = (uint64_t)cmk[h][2] | (uint64_t)cmk[h][3] << 32;
                     while (__any_sync(FULL, (lo | hi) != 0)) {
                         if (ccount > CQCAP - 32) rescore(false);
                         const bool has = (lo | hi) != 0;
@@ -825,7 +890,7 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
                             hi = use_lo ? hi : w2;
                         }
                         const unsigned mk = __ballot_sync(FULL, has);
-                        if (has) cq[ccount + __popc(mk & ((1u << lane) - 1u))] = (uint64_t)(j0 + col) << 5 | (uint32_t)lane;
+                        if (has) cq[ccount + __popc(mk & ((1u << lane) - 1u))] = (uint64_t)(j0[h] + col) << 5 | (uint32_t)lane;
                         ccount += __popc(mk);
                     }
                 }
@@ -858,7 +923,7 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
                 }
             }
         }
-        g_tile += ntiles;
+        g_tile += nstg;
         ++it;
         if (aborted) *s_abort = 1;
         __syncthreads();
@@ -878,11 +943,8 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
     if (producer_warp && lane == 0 && (aborted || *s_abort)) {
         // MMAs in flight: a commit tracks every earlier tcgen05 operation of this thread, so the
         // phase of the last committed tile covers them all (a tile whose MMAs were never issued
-        // has no phase to wait for: g_tile counts an aborted item's tiles in full)
-        if (mma_issued > 0) {
-            const uint32_t g = mma_issued - 1;
-            mbar_wait_bounded(&t_full[g % C::NBUF], (g / C::NBUF) & 1);
-        }
+        // has no phase to wait for: g_tile counts an aborted item's stages in full)
+        if (last_tf >= 0) mbar_wait_bounded(&t_full[last_tf], last_tf_par);
     }
     tc_fence_before();
     __syncthreads();
