@@ -632,7 +632,11 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
             // warp w serves query tile w / 4 through TMEM lane quadrant w % 4 (a warp reaches the
             // lanes of its own quadrant only)
             const int qtw = warp >> 2, quad = warp & 3;
-            const int row = warp * 32 + lane;  // query row in the work item
+            // query row in the work item.  PAIR: the rows are dealt out to the warps in turn (row r
+            // to warp r mod EPI_WARPS), so that the candidates of a spatially clustered run of rows
+            // spread over the warps that must release an accumulator together (-1 % at d = 16; the
+            // other shapes keep runs of 32)
+            const int row = C::PAIR ? lane * EPI_WARPS + warp : warp * 32 + lane;
             const bool active = row < n_item_rows;
             const int64_t q = active ? point_of(q0 + row) : 0;  // the point's index
             const int64_t limit = active ? limit_of(q) : 0;
@@ -914,7 +918,7 @@ __global__ void __launch_bounds__(Cfg<D, QTILES>::THREADS, Cfg<D, QTILES>::CTAS_
                             x = take_min ? (o < x ? o : x) : (o > x ? o : x);
                         }
                     }
-                    const int64_t rq = warp * 32 + rr;
+                    const int64_t rq = C::PAIR ? rr * EPI_WARPS + warp : warp * 32 + rr;  // item row of row rr
                     if (out_slot >= 0) {
                         items.partial[((int64_t)out_slot * C::ROWS + rq) * 32 + lane] = x;
                     } else if (rq < n_item_rows && lane < m) {
