@@ -1006,10 +1006,18 @@ def run_ours(args):
                     'local_ms': local_avg_ms, 'search': search}
         elif ROOF == 'tensor':
             tpk, tsrc = tensor_peak_tflops(bf16_ops)
+            # the step's other kernel: the FP32 local systems (and the FP64 re-solve of marked points)
+            lach = local_flops_per_point(M, D, p.n_theta) * (r1 - r0) / (local_avg_ms * 1e-3) / 1e12
             roof = {'bound': 'tensor', 'achieved': achieved, 'peak': tpk, 'unit': 'TFLOP/s', 'frac': achieved / tpk,
                     'peak_source': tsrc, 'issued_mma_tflops': issued, 'issued_frac': issued / tpk,
                     'fp32_fma_equivalent': {'peak': peak, 'frac': achieved / peak,
-                                            'peak_source': 'FP32 FMA probe measured in this run'}}
+                                            'peak_source': 'FP32 FMA probe measured in this run'},
+                    'local_systems': {'kernel': 'local_warp_kernel<float, grad> + local_redo_kernel',
+                                      'ms': local_avg_ms, 'achieved': lach, 'peak': peak, 'unit': 'TFLOP/s',
+                                      'frac': lach / peak,
+                                      'peak_source': 'FP32 FMA probe measured in this run',
+                                      'work': 'per point: 2k^3/3 + k(k+1)/2 (3d + 4 + 4 n_theta) + 4k^2 flops, '
+                                              'k = m + 1'}}
         else:
             roof = {'bound': 'fp32', 'achieved': achieved, 'peak': peak, 'unit': 'TFLOP/s', 'frac': achieved / peak,
                     'peak_source': 'FP32 FMA probe measured in this run (MEASURED_PEAKS.json has no FP32 figure)',
