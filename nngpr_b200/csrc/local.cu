@@ -278,20 +278,19 @@ __device__ __forceinline__ bool warp_system(const LocalArgs &a, int64_t p, int l
     const TC kpp = rbf + cst + (TC)h.noise + (PRED ? TC(0) : (TC)a.alpha);
 
     // ---- Cholesky of the neighbour block fused with l = L^-1 k ----------------------------
+    // A lane's own results (its pivot's reciprocal, l_lane, z_lane, b_lane, v_lane) are not picked
+    // out of the step that produces them: the running value a lane holds stops changing once
+    // its own step is reached, so each is formed once after the loop, from the same operands.
     TC minpiv = TC(3.0e38);
     TC ss = TC(0);
-    TC l_own = TC(0);
-    TC dg_own = TC(1);
 #pragma unroll
     for (int k = 0; k < M; ++k) {
         const TC piv = __shfl_sync(FULL, r[k], k);
-        minpiv = piv < minpiv ? piv : minpiv;
+        minpiv = fmin(minpiv, piv);
         const TC inv = drsqrt<TC>(piv);  // 1 / L_kk
-        const TC sq = piv * inv;         // L_kk
-        r[k] = (lane == k) ? sq : r[k] * inv;
-        if (lane == k) dg_own = sq;
+        r[k] = r[k] * inv;               // L_jk, and L_kk = piv * inv on lane k itself
+        if (lane == k) idg[k] = inv;
         const TC lk = __shfl_sync(FULL, kvec, k) * inv;
-        if (lane == k) l_own = lk;
         if (lane > k) kvec = fma(-r[k], lk, kvec);
         ss = fma(lk, lk, ss);
         if (k + 1 < M) {
@@ -325,20 +324,20 @@ __device__ __forceinline__ bool warp_system(const LocalArgs &a, int64_t p, int l
 #pragma unroll
     for (int k = 0; k < M; ++k)
         if (k < lane) Ls[lane * (M + 1) + k] = r[k];
-    idg[lane] = TC(1) / dg_own;
+    const TC l_own = kvec * idg[lane];  // l_lane (this lane's own write of idg)
     __syncwarp();
 
     if (PRED && a.weights_out) {
         // conditioning weights w = L^-T l = K_nn^-1 k and the variance term s2 (no outputs yet:
         // the full-conditioning recursion combines them with earlier predictions)
-        TC bv = l_own, b_own = TC(0);
+        TC bv = l_own;
 #pragma unroll
         for (int k = M - 1; k >= 0; --k) {
             const TC bk = __shfl_sync(FULL, bv, k) * idg[k];
-            if (lane == k) b_own = bk;
             const TC lkj = Ls[k * (M + 1) + lane];
             if (lane < k) bv = fma(-lkj, bk, bv);
         }
+        const TC b_own = bv * idg[lane];
         if (lane < a.m) mean[p * a.m + lane] = (TIn)b_own;
         if (lane == 0) var[p] = (TIn)s2;
         return true;
@@ -350,13 +349,12 @@ __device__ __forceinline__ bool warp_system(const LocalArgs &a, int64_t p, int l
     double ll = 0.0;
     for (int c = 0; c < a.ydim; ++c) {
         TC yv = valid ? (TC)y_ref[(int64_t)j * a.ydim + c] : TC(0);
-        TC z_own = TC(0);
 #pragma unroll
         for (int k = 0; k < M; ++k) {
             const TC zk = __shfl_sync(FULL, yv, k) * idg[k];
-            if (lane == k) z_own = zk;
             if (lane > k) yv = fma(-r[k], zk, yv);
         }
+        const TC z_own = yv * idg[lane];
         const TC mu = warp_sum(l_own * z_own);
         if (PRED) {
             if (lane == 0) mean[p * a.ydim + c] = (TIn)mu;
@@ -381,19 +379,19 @@ __device__ __forceinline__ bool warp_system(const LocalArgs &a, int64_t p, int l
     }
 
     // ---- adjoint: b = L^-T l, v = L^-T zw ------------------------------------------------
-    TC bv = l_own, vv = zw, b_own = TC(0), v_own = TC(0);
+    TC bv = l_own, vv = zw;
 #pragma unroll
     for (int k = M - 1; k >= 0; --k) {
         const TC ik = idg[k];
         const TC bk = __shfl_sync(FULL, bv, k) * ik;
         const TC vk = __shfl_sync(FULL, vv, k) * ik;
-        if (lane == k) { b_own = bk; v_own = vk; }
         const TC lkj = Ls[k * (M + 1) + lane];
         if (lane < k) {
             bv = fma(-lkj, bk, bv);
             vv = fma(-lkj, vk, vv);
         }
     }
+    const TC b_own = bv * idg[lane], v_own = vv * idg[lane];
 
     // the fill's squared distances: kept (FP32 RBF), else recomputed (xs is intact); rp still
     // holds the fill's distance to the point itself
